@@ -1,0 +1,58 @@
+// internal.h -- host-side helpers shared by the entry points of libcudapic.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/cudapic.h"
+
+namespace cudapic {
+
+// Records a message for cudapic_last_error() and returns `status`.
+int fail(int status, const std::string &msg);
+// Maps a CUDA error to CUDAPIC_ERR_CUDA with a message (OK stays OK).
+int check_cuda(cudaError_t e, const char *what);
+// Launch-error check after a <<<>>> launch.
+int check_launch(const char *kernel);
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+// Dynamic shared memory ceiling per block of the current device.
+int max_smem_optin();
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Validation shared by the entry points.
+int validate_grid(const cudapic_grid *g);
+
+// Launchers used by both the drop-in entry points and the driver.
+int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
+                   const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream);
+int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
+                            const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
+                            const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
+                            cudaStream_t stream);
+int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
+                        float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
+                        float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
+                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream);
+int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
+                        float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
+                        const cudapic_grid &g, cudaStream_t stream);
+int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
+                const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream);
+
+}  // namespace cudapic
+
+#define CUDAPIC_CHECK(expr)                                   \
+    do {                                                      \
+        int _rc = (expr);                                     \
+        if (_rc != CUDAPIC_OK) return _rc;                    \
+    } while (0)
+
+#define CUDAPIC_REQUIRE(cond, msg)                                   \
+    do {                                                             \
+        if (!(cond)) return ::cudapic::fail(CUDAPIC_ERR_ARG, (msg)); \
+    } while (0)

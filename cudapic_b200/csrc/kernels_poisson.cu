@@ -1,0 +1,318 @@
+// kernels_poisson.cu -- single-CTA scan-based Poisson solve and field.
+//
+// Reference: solve_poisson_scan_f32, Rust-CUDA/src/main.rs:408-494 (one
+// thread per node, N_G <= 416, f32 block scans) and solve_poisson_dps_flexible,
+// :496-564.  The Dirichlet problem pot[i-1] - 2 pot[i] + pot[i+1] = f_i has
+// unit tridiagonal coefficients, so the Thomas recurrences collapse to
+//     G_i = sum_{j<=i} j f_j,   r_i = -G_i / ((i+1) i),   pot_i = i sum_{j=i}^{N-2} r_j,
+// i.e. two inclusive prefix sums (C/eduPIC.cc:461-494 is the sequential
+// Thomas form of the same system).
+//
+// B200 design: one CTA of up to 1024 threads, each thread owning
+// ceil(N_G / blockDim) consecutive nodes (N_G up to 16384), warp-shuffle
+// scans plus one shared-memory pass over the warp totals.  The sums run in
+// FP64 by default: in f32 the cancellation in R_total - R_i grows with N_G
+// (relative L2 error ~4e-3 at N_G = 4096 against the FP64 Thomas solve),
+// in FP64 it is at the f32 output rounding.  CUDAPIC_FLAG_POISSON_F32_SCAN
+// selects the reference's f32 arithmetic.  Latency-bound: a few us.
+//
+// The driver variant reads pot0 from a device table indexed by a device
+// step counter (so that one captured CUDA graph serves every RF phase) and
+// advances the counter.
+#include "common.cuh"
+#include "internal.h"
+
+namespace cudapic {
+
+constexpr int POIS_MAX_THREADS = 1024;
+constexpr int POIS_MAX_PER_THREAD = 16;  // N_G <= 16384
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+// Exclusive block scan of one value per thread; also returns the block total.
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T *wsum, T &total) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    T incl = warp_incl_scan(v, lane);
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nwarps ? wsum[lane] : T(0);
+        w = warp_incl_scan(w, lane);
+        if (lane < nwarps) wsum[lane] = w;
+    }
+    __syncthreads();
+    T excl = incl - v + (warp > 0 ? wsum[warp - 1] : T(0));
+    total = wsum[nwarps - 1];
+    __syncthreads();
+    return excl;
+}
+
+// T: arithmetic type of the scans (double or float); PT: nodes per thread.
+template <typename T, int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    poisson_kernel(const float *__restrict__ e_density, const float *__restrict__ i_density,
+                   float *__restrict__ pot_out, float *__restrict__ efield_out, float pot0_arg,
+                   const float *__restrict__ pot0_table, uint32_t *__restrict__ step_counter,
+                   const cudapic_grid g) {
+    constexpr int per_thread = PT;
+    extern __shared__ unsigned char smem_raw[];
+    T *pot_s = reinterpret_cast<T *>(smem_raw);        // n_g
+    __shared__ T wsum[32];
+    __shared__ T r_total_s;
+    __shared__ float pot0_s;
+
+    const int n = (int)g.n_g;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        float p0 = pot0_arg;
+        if (pot0_table) {
+            uint32_t t = *step_counter;
+            p0 = pot0_table[t % g.n_t];
+            *step_counter = t + 1;
+        }
+        pot0_s = p0;
+    }
+    __syncthreads();
+    const T pot0 = (T)pot0_s;
+
+    // node-dependent constants in the arithmetic type of the solve
+    const T e_charge = sizeof(T) == 8 ? (T)1.60217662e-19 : (T)g.e_charge;
+    const T alpha = sizeof(T) == 8 ? (T)(-g.dx * g.dx / 8.85418781e-12) : (T)g.alpha;
+
+    const int first = tid * per_thread;
+    T rho[PT];
+    T G[PT];
+    T local = 0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            T rh = 0, gi = 0;
+            if (i < n) {
+                if (sizeof(T) == 8)
+                    rh = e_charge * ((T)i_density[i] - (T)e_density[i]);
+                else
+                    rh = e_charge * (T)(i_density[i] - e_density[i]);
+                if (i != 0) {
+                    T fi = alpha * rh - (i == 1 ? pot0 : T(0));
+                    gi = (T)i * fi;
+                }
+            }
+            rho[j] = rh;
+            local += gi;
+            G[j] = local;
+        }
+    }
+    T tot;
+    T off = block_excl_scan<T>(local, wsum, tot);
+
+    T r[PT];
+    T R[PT];
+    local = 0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            T ri = 0;
+            if (i != 0 && i < n - 1) {
+                T hi = -(G[j] + off) / ((T)i + T(1));
+                ri = hi / (T)i;
+            }
+            r[j] = ri;
+            local += ri;
+            R[j] = local;
+        }
+    }
+    off = block_excl_scan<T>(local, wsum, tot);
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread && first + j == n - 2) r_total_s = R[j] + off;
+    }
+    __syncthreads();
+    const T r_total = r_total_s;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            if (i < n) {
+                T p;
+                if (i == 0) p = pot0;
+                else if (i < n - 1) p = (T)i * (r_total - (R[j] + off) + r[j]);
+                else p = T(0);
+                pot_s[i] = p;
+            }
+        }
+    }
+    __syncthreads();
+    const T inv_dx = sizeof(T) == 8 ? (T)(1.0 / g.dx) : (T)g.inv_dx;
+    const T half_inv_dx = sizeof(T) == 8 ? (T)(0.5 / g.dx) : (T)g.half_inv_dx;
+    const T half_dx_over_eps = sizeof(T) == 8 ? (T)(g.dx / (2.0 * 8.85418781e-12)) : (T)g.half_dx_over_eps;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            if (i < n) {
+                T pk = pot_s[i];
+                T e;
+                if (i == 0) e = (pk - pot_s[1]) * inv_dx - rho[j] * half_dx_over_eps;
+                else if (i == n - 1) e = (pot_s[n - 2] - pk) * inv_dx + rho[j] * half_dx_over_eps;
+                else e = (pot_s[i - 1] - pot_s[i + 1]) * half_inv_dx;
+                pot_out[i] = (float)pk;
+                efield_out[i] = (float)e;
+            }
+        }
+    }
+}
+
+// solve_poisson_dps_flexible: the same closed form with runtime n, dx and
+// both Dirichlet values (used by the reference's Hakim convergence test,
+// Rust-CUDA/src/main.rs:1895-1981).  FP64 sums.
+template <int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    poisson_flexible_kernel(const float *__restrict__ source, float *__restrict__ pot_out, int n,
+                            double psi_left, double psi_right, double dx) {
+    constexpr int per_thread = PT;
+    __shared__ double wsum[32];
+    __shared__ double r_total_s;
+    const int tid = threadIdx.x;
+    const int first = tid * per_thread;
+    double G[PT];
+    double local = 0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            double gi = 0;
+            if (i != 0 && i < n) {
+                double fi = dx * dx * (double)source[i];
+                if (i == 1) fi -= psi_left;
+                if (i == n - 2) fi -= psi_right;
+                gi = (double)i * fi;
+            }
+            local += gi;
+            G[j] = local;
+        }
+    }
+    double tot;
+    double off = block_excl_scan<double>(local, wsum, tot);
+    double r[PT], R[PT];
+    local = 0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            double ri = 0;
+            if (i != 0 && i < n - 1) ri = (-(G[j] + off) / ((double)i + 1.0)) / (double)i;
+            r[j] = ri;
+            local += ri;
+            R[j] = local;
+        }
+    }
+    off = block_excl_scan<double>(local, wsum, tot);
+#pragma unroll
+    for (int j = 0; j < PT; ++j)
+        if (j < per_thread && first + j == n - 2) r_total_s = R[j] + off;
+    __syncthreads();
+    const double r_total = r_total_s;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        if (j < per_thread) {
+            const int i = first + j;
+            if (i < n) {
+                double p;
+                if (i == 0) p = psi_left;
+                else if (i < n - 1) p = (double)i * (r_total - (R[j] + off) + r[j]);
+                else p = psi_right;
+                pot_out[i] = (float)p;
+            }
+        }
+    }
+}
+
+// Threads and nodes per thread (a power of two) for n nodes.
+void poisson_shape(uint32_t n_g, int &threads, int &per_thread) {
+    per_thread = 1;
+    while ((uint32_t)per_thread * POIS_MAX_THREADS < n_g) per_thread *= 2;
+    threads = (int)((((n_g + per_thread - 1) / per_thread) + 31) / 32 * 32);
+}
+
+template <typename T, int PT>
+int launch_poisson_t(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
+                     const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, int threads,
+                     cudaStream_t stream) {
+    size_t smem = (size_t)g.n_g * sizeof(T);
+    auto kern = poisson_kernel<T, PT>;
+    if (smem > 48 * 1024)
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                 "cudaFuncSetAttribute(poisson)"));
+    kern<<<1, threads, smem, stream>>>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g);
+    return check_launch("solve_poisson_scan");
+}
+
+template <typename T>
+int launch_poisson_pt(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
+                      const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
+                      cudaStream_t stream) {
+    int threads, pt;
+    poisson_shape(g.n_g, threads, pt);
+    switch (pt) {
+    case 1: return launch_poisson_t<T, 1>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    case 2: return launch_poisson_t<T, 2>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    case 4: return launch_poisson_t<T, 4>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    case 8: return launch_poisson_t<T, 8>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    default: return launch_poisson_t<T, 16>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    }
+}
+
+int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
+                   const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
+                   cudaStream_t stream) {
+    if (g.n_g > (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD))
+        return fail(CUDAPIC_ERR_ARG, "solve_poisson: n_g > 16384");
+    if (g.flags & CUDAPIC_FLAG_POISSON_F32_SCAN)
+        return launch_poisson_pt<float>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream);
+    return launch_poisson_pt<double>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream);
+}
+
+}  // namespace cudapic
+
+using namespace cudapic;
+
+extern "C" int cudapic_solve_poisson_scan_f32(const float *e_density, const float *i_density, float *pot,
+                                              float *efield, float pot0, const cudapic_grid *grid,
+                                              cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(e_density && i_density && pot && efield, "solve_poisson_scan_f32: null pointer");
+    return launch_poisson(e_density, i_density, pot, efield, pot0, nullptr, nullptr, *grid,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int cudapic_solve_poisson_dps_flexible(const float *source, float *pot, uint32_t n, float psi_left,
+                                                  float psi_right, float dx, cudapic_stream_t stream) {
+    CUDAPIC_REQUIRE(source && pot, "solve_poisson_dps_flexible: null pointer");
+    CUDAPIC_REQUIRE(n >= 3 && n <= (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD),
+                    "solve_poisson_dps_flexible: n must be in [3, 16384]");
+    int threads, pt;
+    poisson_shape(n, threads, pt);
+    cudaStream_t st = (cudaStream_t)stream;
+    const double l = psi_left, r = psi_right, h = dx;
+    switch (pt) {
+    case 1: poisson_flexible_kernel<1><<<1, threads, 0, st>>>(source, pot, (int)n, l, r, h); break;
+    case 2: poisson_flexible_kernel<2><<<1, threads, 0, st>>>(source, pot, (int)n, l, r, h); break;
+    case 4: poisson_flexible_kernel<4><<<1, threads, 0, st>>>(source, pot, (int)n, l, r, h); break;
+    case 8: poisson_flexible_kernel<8><<<1, threads, 0, st>>>(source, pot, (int)n, l, r, h); break;
+    default: poisson_flexible_kernel<16><<<1, threads, 0, st>>>(source, pot, (int)n, l, r, h); break;
+    }
+    return check_launch("solve_poisson_dps_flexible");
+}

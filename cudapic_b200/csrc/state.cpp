@@ -1,0 +1,482 @@
+// state.cpp -- the simulation state and the per-step driver of libcudapic.
+//
+// Reference: GpuSimState (Rust-CUDA/src/main.rs:131-350) owns SoA particle
+// buffers preallocated to MAX_PARTICLES, ping-pong tmp_* buffers, 4 RNG
+// planes per species, the device counters n_electrons / n_ions /
+// alive_counter, the grid arrays, the cross-section tables and the
+// measurement accumulators; main() (:1725-1808) enqueues, for every time
+// step t, the launches and memsets below in this order.  Here:
+//  * capacity, N_G, ... are runtime values (cudapic_params);
+//  * each species owns its own ping-pong pair (the reference rotates one
+//    shared tmp set between the species), so pointer swaps are per species;
+//  * the RF phase pot0 = V cos(2 pi t / N_T) is a device table indexed by a
+//    device step counter advanced by the Poisson kernel, so one captured CUDA
+//    graph of 2 * N_SUB steps (electron and ion buffers back on the side
+//    they started) is replayed for every RF phase;
+//  * a device particle-step counter (electrons every step, ions every N_SUB
+//    steps) measures the work actually done.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "internal.h"
+
+using namespace cudapic;
+
+struct cudapic_state {
+    int device = 0;
+    cudapic_params params{};
+    cudapic_grid grid{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // [species][side]
+    float *x[2][2] = {}, *vx[2][2] = {}, *vy[2][2] = {}, *vz[2][2] = {};
+    int side[2] = {0, 0};
+    uint32_t *rng[2][4] = {};
+    // counters block: n_e, n_i, alive, step, dev_err, pad..., work (u64 at +32)
+    uint32_t *counters = nullptr;
+    float *efield = nullptr, *pot = nullptr, *e_density = nullptr, *i_density = nullptr, *pot0_table = nullptr;
+    float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
+    double *cumul_e = nullptr, *cumul_i = nullptr;
+    uint32_t *eepf = nullptr;
+
+    bool measure = false;
+    uint64_t steps_done = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
+    bool graphs_enabled = true;
+    std::vector<void *> allocations;
+
+    uint32_t *n_e() const { return counters + 0; }
+    uint32_t *n_i() const { return counters + 1; }
+    uint32_t *alive() const { return counters + 2; }
+    uint32_t *step_counter() const { return counters + 3; }
+    uint32_t *dev_err() const { return counters + 4; }
+    unsigned long long *work() const { return reinterpret_cast<unsigned long long *>(counters + 8); }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = 0;
+    bool ok = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(dev) == cudaSuccess) ok = true;
+    }
+    ~DeviceGuard() {
+        if (ok) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+int dalloc(cudapic_state *s, T **p, size_t count) {
+    void *ptr = nullptr;
+    size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaMalloc");
+    s->allocations.push_back(ptr);
+    *p = static_cast<T *>(ptr);
+    return CUDAPIC_OK;
+}
+
+void destroy_graphs(cudapic_state *s) {
+    for (auto &g : s->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+// One reference time step (Rust-CUDA/src/main.rs:1728-1807).
+int enqueue_step(cudapic_state *s, bool ion_step) {
+    const cudapic_grid &g = s->grid;
+    cudaStream_t st = s->stream;
+    const int E = 0, I = 1;
+    const uint32_t n_g = g.n_g;
+    int se = s->side[E], si = s->side[I];
+
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density, 0, n_g * sizeof(float), st), "memset e_density"));
+    CUDAPIC_CHECK(cudapic_get_density(s->x[E][se], s->e_density, s->n_e(), &g, (cudapic_stream_t)st));
+    if (ion_step) {
+        CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_density, 0, n_g * sizeof(float), st), "memset i_density"));
+        CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_density, s->n_i(), &g, (cudapic_stream_t)st));
+    }
+    CUDAPIC_CHECK(launch_poisson(s->e_density, s->i_density, s->pot, s->efield, 0.0f, s->pot0_table,
+                                 s->step_counter(), g, st));
+    if (s->measure) {
+        CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density, s->cumul_e, &g, (cudapic_stream_t)st));
+        if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density, s->cumul_i, &g, (cudapic_stream_t)st));
+    }
+    // electrons: push + compact into the other side
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
+    CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
+                                          s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
+                                          s->alive(), s->n_e(), g.factor_e, g.dt_e, g, st));
+    se ^= 1;
+    s->side[E] = se;
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
+                             "copy alive -> n_e"));
+    if (ion_step) {
+        CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
+        CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
+                                              s->x[I][si ^ 1], s->vx[I][si ^ 1], s->vy[I][si ^ 1],
+                                              s->vz[I][si ^ 1], s->alive(), s->n_i(), g.factor_i, g.dt_i, g, st));
+        si ^= 1;
+        s->side[I] = si;
+        CUDAPIC_CHECK(check_cuda(
+            cudaMemcpyAsync(s->n_i(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "copy alive -> n_i"));
+        CUDAPIC_CHECK(check_cuda(
+            cudaMemcpyAsync(s->alive(), s->n_e(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st), "copy n_e -> alive"));
+    }
+    CUDAPIC_CHECK(launch_collisions_e(s->sigma_tot_e, s->cs, s->n_e(), s->x[E][se], s->vx[E][se], s->vy[E][se],
+                                      s->vz[E][se], s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3],
+                                      s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si], s->alive(), s->n_i(),
+                                      nullptr, g, st));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
+                             "copy alive -> n_e"));
+    if (ion_step) {
+        CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
+                                          s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
+                                          nullptr, g, st));
+    }
+    if (s->measure) {
+        CUDAPIC_CHECK(launch_eepf(s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->efield, s->n_e(),
+                                  s->eepf, g, st));
+    }
+    return CUDAPIC_OK;
+}
+
+bool is_ion_step(const cudapic_state *s, uint64_t step) {
+    return ((step % s->params.n_t) % s->params.n_sub) == 0;
+}
+
+// Graph period: 2 * N_SUB steps returns both species to their starting
+// side; requires N_T % N_SUB == 0 so that the ion-step pattern repeats.
+uint64_t graph_period(const cudapic_state *s) { return 2ull * s->params.n_sub; }
+
+int build_graph(cudapic_state *s) {
+    const int m = s->measure ? 1 : 0;
+    if (s->graph[m]) return CUDAPIC_OK;
+    cudaGraph_t graph = nullptr;
+    const uint64_t period = graph_period(s);
+    const int side0[2] = {s->side[0], s->side[1]};
+    CUDAPIC_CHECK(check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
+    int rc = CUDAPIC_OK;
+    for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k) rc = enqueue_step(s, is_ion_step(s, s->steps_done + k));
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    s->side[0] = side0[0];
+    s->side[1] = side0[1];
+    if (rc != CUDAPIC_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    CUDAPIC_CHECK(check_cuda(e, "end capture"));
+    e = cudaGraphInstantiate(&s->graph[m], graph, 0);
+    cudaGraphDestroy(graph);
+    return check_cuda(e, "cudaGraphInstantiate");
+}
+
+}  // namespace
+
+extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic_state **out) {
+    if (!p || !out) return fail(CUDAPIC_ERR_ARG, "state_create: null pointer");
+    *out = nullptr;
+    cudapic_grid grid;
+    CUDAPIC_CHECK(cudapic_grid_from_params(p, &grid));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(CUDAPIC_ERR_NOT_SUPPORTED, "state_create: no CUDA device");
+    if (device < 0 || device >= ndev) return fail(CUDAPIC_ERR_ARG, "state_create: bad device index");
+    DeviceGuard dg(device);
+    cudaDeviceProp prop;
+    CUDAPIC_CHECK(check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties"));
+    if (prop.major < 10)
+        return fail(CUDAPIC_ERR_NOT_SUPPORTED, "state_create: libcudapic is built for sm_100a (B200)");
+
+    cudapic_state *s = new (std::nothrow) cudapic_state();
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_create: out of host memory");
+    s->device = device;
+    s->params = *p;
+    // capacity rounded up to a multiple of 4 for the bulk-copy push path
+    s->params.capacity = (p->capacity + 3u) & ~3u;
+    s->grid = grid;
+    s->grid.capacity = s->params.capacity;
+    s->graphs_enabled = (p->n_t % p->n_sub) == 0;
+
+    auto cleanup = [&](int rc) {
+        cudapic_state_destroy(s);
+        return rc;
+    };
+    int rc;
+    if ((rc = check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate")) !=
+        CUDAPIC_OK)
+        return cleanup(rc);
+    s->own_stream = true;
+    const size_t cap = s->params.capacity;
+    for (int sp = 0; sp < 2; ++sp) {
+        for (int side = 0; side < 2; ++side) {
+            if ((rc = dalloc(s, &s->x[sp][side], cap)) || (rc = dalloc(s, &s->vx[sp][side], cap)) ||
+                (rc = dalloc(s, &s->vy[sp][side], cap)) || (rc = dalloc(s, &s->vz[sp][side], cap)))
+                return cleanup(rc);
+        }
+        for (int k = 0; k < 4; ++k)
+            if ((rc = dalloc(s, &s->rng[sp][k], cap))) return cleanup(rc);
+    }
+    const size_t n_g = p->n_g;
+    if ((rc = dalloc(s, &s->counters, 64)) || (rc = dalloc(s, &s->efield, n_g)) || (rc = dalloc(s, &s->pot, n_g)) ||
+        (rc = dalloc(s, &s->e_density, n_g)) || (rc = dalloc(s, &s->i_density, n_g)) ||
+        (rc = dalloc(s, &s->pot0_table, p->n_t)) || (rc = dalloc(s, &s->cs, 5ull * CUDAPIC_CS_RANGES)) ||
+        (rc = dalloc(s, &s->sigma_tot_e, CUDAPIC_CS_RANGES)) || (rc = dalloc(s, &s->sigma_tot_i, CUDAPIC_CS_RANGES)) ||
+        (rc = dalloc(s, &s->cumul_e, n_g)) || (rc = dalloc(s, &s->cumul_i, n_g)) || (rc = dalloc(s, &s->eepf, 2000)))
+        return cleanup(rc);
+    s->grid.dev_err = s->dev_err();
+    s->grid.work = s->work();
+
+    // zero everything that is read before written
+    for (int sp = 0; sp < 2; ++sp)
+        for (int side = 0; side < 2; ++side)
+            for (float *b : {s->x[sp][side], s->vx[sp][side], s->vy[sp][side], s->vz[sp][side]})
+                if ((rc = check_cuda(cudaMemsetAsync(b, 0, cap * sizeof(float), s->stream), "memset")))
+                    return cleanup(rc);
+    if ((rc = check_cuda(cudaMemsetAsync(s->counters, 0, 64 * sizeof(uint32_t), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->efield, 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->pot, 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->e_density, 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->i_density, 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "memset")))
+        return cleanup(rc);
+
+    // RF boundary table: (V cos(2 pi t / N_T)) as f32, Rust-CUDA/src/main.rs:1741
+    std::vector<float> table(p->n_t);
+    for (uint32_t t = 0; t < p->n_t; ++t)
+        table[t] = (float)(p->voltage * std::cos(((double)t / (double)p->n_t) * (2.0 * 3.141592653589793)));
+    // cross sections (host, all threads), Rust-CUDA/src/main.rs:1649, 1378-1444
+    std::vector<float> cs(5ull * CUDAPIC_CS_RANGES), se(CUDAPIC_CS_RANGES), si(CUDAPIC_CS_RANGES);
+    if ((rc = cudapic_cross_sections(grid.gas_density, cs.data(), se.data(), si.data()))) return cleanup(rc);
+    if ((rc = check_cuda(cudaMemcpyAsync(s->pot0_table, table.data(), table.size() * sizeof(float),
+                                         cudaMemcpyHostToDevice, s->stream), "upload pot0 table")) ||
+        (rc = check_cuda(cudaMemcpyAsync(s->cs, cs.data(), cs.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream),
+                         "upload cs")) ||
+        (rc = check_cuda(cudaMemcpyAsync(s->sigma_tot_e, se.data(), se.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                         s->stream), "upload sigma_tot_e")) ||
+        (rc = check_cuda(cudaMemcpyAsync(s->sigma_tot_i, si.data(), si.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                         s->stream), "upload sigma_tot_i")) ||
+        (rc = check_cuda(cudaStreamSynchronize(s->stream), "state_create sync")))
+        return cleanup(rc);
+    *out = s;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_destroy(cudapic_state *s) {
+    if (!s) return CUDAPIC_OK;
+    DeviceGuard dg(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graphs(s);
+    for (void *p : s->allocations) cudaFree(p);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_set_stream(cudapic_state *s, cudapic_stream_t stream) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_stream: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_stream sync"));
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->own_stream = false;
+    s->stream = (cudaStream_t)stream;
+    destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
+extern "C" cudapic_stream_t cudapic_state_stream(const cudapic_state *s) {
+    return s ? (cudapic_stream_t)s->stream : nullptr;
+}
+
+extern "C" int cudapic_state_grid(const cudapic_state *s, cudapic_grid *out) {
+    if (!s || !out) return fail(CUDAPIC_ERR_ARG, "state_grid: null pointer");
+    *out = s->grid;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_buffers(const cudapic_state *s, cudapic_buffers *o) {
+    if (!s || !o) return fail(CUDAPIC_ERR_ARG, "state_buffers: null pointer");
+    std::memset(o, 0, sizeof(*o));
+    for (int sp = 0; sp < 2; ++sp) {
+        const int a = s->side[sp], b = a ^ 1;
+        o->x[sp] = s->x[sp][a];
+        o->vx[sp] = s->vx[sp][a];
+        o->vy[sp] = s->vy[sp][a];
+        o->vz[sp] = s->vz[sp][a];
+        o->tmp_x[sp] = s->x[sp][b];
+        o->tmp_vx[sp] = s->vx[sp][b];
+        o->tmp_vy[sp] = s->vy[sp][b];
+        o->tmp_vz[sp] = s->vz[sp][b];
+        for (int k = 0; k < 4; ++k) o->rng[sp][k] = s->rng[sp][k];
+    }
+    o->n_electrons = s->n_e();
+    o->n_ions = s->n_i();
+    o->alive_counter = s->alive();
+    o->efield = s->efield;
+    o->pot = s->pot;
+    o->e_density = s->e_density;
+    o->i_density = s->i_density;
+    o->cs = s->cs;
+    o->sigma_tot_e = s->sigma_tot_e;
+    o->sigma_tot_i = s->sigma_tot_i;
+    o->cumul_e_density = s->cumul_e;
+    o->cumul_i_density = s->cumul_i;
+    o->eepf = s->eepf;
+    o->dev_err = s->dev_err();
+    o->work = s->work();
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_upload(cudapic_state *s, int species, const float *x, const float *vx, const float *vy,
+                                    const float *vz, uint32_t n) {
+    if (!s || (species != 0 && species != 1)) return fail(CUDAPIC_ERR_ARG, "state_upload: bad state/species");
+    if (n > s->params.capacity) return fail(CUDAPIC_ERR_CAPACITY, "state_upload: n exceeds capacity");
+    if (n && (!x || !vx || !vy || !vz)) return fail(CUDAPIC_ERR_ARG, "state_upload: null pointer");
+    DeviceGuard dg(s->device);
+    const int a = s->side[species];
+    const size_t bytes = (size_t)n * sizeof(float);
+    if (n) {
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->x[species][a], x, bytes, cudaMemcpyHostToDevice, s->stream), "upload x"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->vx[species][a], vx, bytes, cudaMemcpyHostToDevice, s->stream), "upload vx"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->vy[species][a], vy, bytes, cudaMemcpyHostToDevice, s->stream), "upload vy"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->vz[species][a], vz, bytes, cudaMemcpyHostToDevice, s->stream), "upload vz"));
+    }
+    uint32_t *cnt = species == 0 ? s->n_e() : s->n_i();
+    const uint32_t count = n;
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(cnt, &count, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream),
+                             "upload count"));
+    return check_cuda(cudaStreamSynchronize(s->stream), "upload sync");
+}
+
+extern "C" int cudapic_state_download(cudapic_state *s, int species, float *x, float *vx, float *vy, float *vz,
+                                      uint32_t max_n, uint32_t *n_out) {
+    if (!s || (species != 0 && species != 1)) return fail(CUDAPIC_ERR_ARG, "state_download: bad state/species");
+    DeviceGuard dg(s->device);
+    uint32_t n = 0;
+    uint32_t *cnt = species == 0 ? s->n_e() : s->n_i();
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(&n, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream), "read count"));
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "download sync"));
+    n = std::min(n, s->params.capacity);
+    if (n_out) *n_out = n;
+    const uint32_t m = std::min(n, max_n);
+    const int a = s->side[species];
+    const size_t bytes = (size_t)m * sizeof(float);
+    if (m) {
+        if (!x || !vx || !vy || !vz) return fail(CUDAPIC_ERR_ARG, "state_download: null pointer");
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(x, s->x[species][a], bytes, cudaMemcpyDeviceToHost, s->stream), "download x"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(vx, s->vx[species][a], bytes, cudaMemcpyDeviceToHost, s->stream), "download vx"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(vy, s->vy[species][a], bytes, cudaMemcpyDeviceToHost, s->stream), "download vy"));
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(vz, s->vz[species][a], bytes, cudaMemcpyDeviceToHost, s->stream), "download vz"));
+    }
+    return check_cuda(cudaStreamSynchronize(s->stream), "download sync");
+}
+
+extern "C" int cudapic_state_seed(cudapic_state *s, const uint32_t e_master[4], const uint32_t i_master[4]) {
+    if (!s || !e_master || !i_master) return fail(CUDAPIC_ERR_ARG, "state_seed: null pointer");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(cudapic_xoshiro128_seed_streams(e_master, s->params.capacity, s->rng[0][0], s->rng[0][1],
+                                                  s->rng[0][2], s->rng[0][3], (cudapic_stream_t)s->stream));
+    CUDAPIC_CHECK(cudapic_xoshiro128_seed_streams(i_master, s->params.capacity, s->rng[1][0], s->rng[1][1],
+                                                  s->rng[1][2], s->rng[1][3], (cudapic_stream_t)s->stream));
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_set_measure(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_measure: null state");
+    DeviceGuard dg(s->device);
+    const size_t n_g = s->params.n_g;
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "zero cumul_e"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "zero cumul_i"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "zero eepf"));
+    s->measure = on != 0;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_run_steps: null state");
+    DeviceGuard dg(s->device);
+    const uint64_t period = graph_period(s);
+    while (n_steps > 0) {
+        if (s->graphs_enabled && (s->steps_done % period) == 0 && n_steps >= period) {
+            int rc = build_graph(s);
+            if (rc != CUDAPIC_OK) {
+                s->graphs_enabled = false;  // fall back to direct launches
+                continue;
+            }
+            CUDAPIC_CHECK(check_cuda(cudaGraphLaunch(s->graph[s->measure ? 1 : 0], s->stream), "cudaGraphLaunch"));
+            s->steps_done += period;
+            n_steps -= period;
+            continue;
+        }
+        CUDAPIC_CHECK(enqueue_step(s, is_ion_step(s, s->steps_done)));
+        s->steps_done += 1;
+        n_steps -= 1;
+    }
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_counts: null state");
+    DeviceGuard dg(s->device);
+    uint32_t c[2];
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost, s->stream), "read counts"));
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "counts sync"));
+    if (n_e) *n_e = std::min(c[0], s->params.capacity);
+    if (n_i) *n_i = std::min(c[1], s->params.capacity);
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_device_error(cudapic_state *s, uint32_t *bits) {
+    if (!s || !bits) return fail(CUDAPIC_ERR_ARG, "state_device_error: null pointer");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(bits, s->dev_err(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream),
+                             "read device error word"));
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "device error sync"));
+    if (*bits & (CUDAPIC_DEVERR_SPAWN_E | CUDAPIC_DEVERR_SPAWN_I | CUDAPIC_DEVERR_ACTIVE))
+        return fail(CUDAPIC_ERR_CAPACITY, "device reported a capacity overflow");
+    if (*bits & CUDAPIC_DEVERR_TIMEOUT) return fail(CUDAPIC_ERR_TIMEOUT, "device reported a wait timeout");
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_work(cudapic_state *s, unsigned long long *particle_steps) {
+    if (!s || !particle_steps) return fail(CUDAPIC_ERR_ARG, "state_work: null pointer");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(particle_steps, s->work(), sizeof(unsigned long long),
+                                             cudaMemcpyDeviceToHost, s->stream), "read work"));
+    return check_cuda(cudaStreamSynchronize(s->stream), "work sync");
+}
+
+extern "C" int cudapic_state_steps_done(const cudapic_state *s, uint64_t *steps) {
+    if (!s || !steps) return fail(CUDAPIC_ERR_ARG, "state_steps_done: null pointer");
+    *steps = s->steps_done;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_synchronize(cudapic_state *s) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_synchronize: null state");
+    DeviceGuard dg(s->device);
+    return check_cuda(cudaStreamSynchronize(s->stream), "state_synchronize");
+}
+
+extern "C" int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, double *cumul_i,
+                                                   uint32_t *eepf) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_download_measurements: null state");
+    DeviceGuard dg(s->device);
+    const size_t n_g = s->params.n_g;
+    if (cumul_e)
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(cumul_e, s->cumul_e, n_g * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "download cumul_e"));
+    if (cumul_i)
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(cumul_i, s->cumul_i, n_g * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "download cumul_i"));
+    if (eepf)
+        CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(eepf, s->eepf, 2000 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream), "download eepf"));
+    return check_cuda(cudaStreamSynchronize(s->stream), "download measurements sync");
+}

@@ -1,0 +1,285 @@
+/*
+ * cudapic.h -- C ABI of libcudapic.so, the B200 (sm_100a) implementation of
+ * cudaPIC's per-timestep PIC/MCC cycle (1d3v argon CCP, eduPIC physics).
+ *
+ * Two layers:
+ *
+ *  1. Drop-in kernel entry points.  One function per reference kernel of the
+ *     cuda-oxide module `kernels` (Rust-CUDA/src/main.rs:352-1358), with the
+ *     reference's argument order.  The reference bakes the discharge
+ *     constants in at compile time (Rust-CUDA/src/main.rs:29-110); here they
+ *     travel in a `cudapic_grid` built once by cudapic_grid_from_params().
+ *     All pointers are device pointers owned by the caller; no entry point
+ *     allocates device memory or synchronises; every launch goes to the
+ *     caller's stream.  Counters (n_active, alive_counter, ...) stay in
+ *     device memory exactly as in the reference, so a sequence of calls
+ *     never needs the host to read a count.
+ *
+ *  2. A simulation state (`cudapic_state`) that owns the SoA buffers, the
+ *     cross-section tables and the RNG planes (the reference's GpuSimState,
+ *     Rust-CUDA/src/main.rs:131-350) and runs the reference's per-step loop
+ *     (Rust-CUDA/src/main.rs:1725-1808) from CUDA graphs.
+ *
+ * Every function returns a cudapic_status.  Kernels never trap: device-side
+ * problems (spawn beyond capacity, a particle outside [0, L]) set bits of a
+ * device error word (cudapic_grid.dev_err) and the offending write is
+ * skipped.  cudapic_last_error() returns a message for the last failure of
+ * the calling thread.
+ */
+#ifndef CUDAPIC_H
+#define CUDAPIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUDAPIC_VERSION 100
+
+/* Same object as cudaStream_t (the CUDA runtime's stream handle). */
+typedef struct CUstream_st *cudapic_stream_t;
+
+typedef enum cudapic_status {
+    CUDAPIC_OK = 0,
+    CUDAPIC_ERR_CUDA = 1,          /* a CUDA runtime call failed                  */
+    CUDAPIC_ERR_CAPACITY = 2,      /* a device error word reports a capacity hit  */
+    CUDAPIC_ERR_ARG = 3,           /* invalid argument (null, size, alignment)    */
+    CUDAPIC_ERR_TIMEOUT = 4,       /* a bounded device wait gave up               */
+    CUDAPIC_ERR_NOT_SUPPORTED = 5, /* device is not sm_100 / feature unavailable  */
+    CUDAPIC_ERR_STATE = 6          /* call out of order on a cudapic_state        */
+} cudapic_status;
+
+/* Bits of the device error word. */
+#define CUDAPIC_DEVERR_SPAWN_E  0x1u  /* electron spawn dropped: capacity reached   */
+#define CUDAPIC_DEVERR_SPAWN_I  0x2u  /* ion spawn dropped: capacity reached        */
+#define CUDAPIC_DEVERR_POSITION 0x4u  /* gather/deposit met x outside [0,L] or NaN  */
+#define CUDAPIC_DEVERR_ACTIVE   0x8u  /* a count exceeded capacity and was clamped  */
+#define CUDAPIC_DEVERR_TIMEOUT  0x10u /* a bounded wait on an async copy gave up    */
+
+/* Discharge and run parameters: the reference's compile-time constants
+ * (Rust-CUDA/src/main.rs:40-50, :79) as runtime values. */
+typedef struct cudapic_params {
+    uint32_t n_g;            /* grid points, 3..16384                        */
+    uint32_t n_t;            /* time steps per RF period                     */
+    uint32_t n_sub;          /* ion subcycling factor                        */
+    uint32_t capacity;       /* preallocated particles per species           */
+    double frequency;        /* RF frequency [Hz]                            */
+    double voltage;          /* RF amplitude [V]                             */
+    double gap;              /* electrode gap L [m]                          */
+    double pressure;         /* gas pressure [Pa]                            */
+    double temperature;      /* gas temperature [K]                          */
+    double weight;           /* superparticle weight                         */
+    double electrode_area;   /* electrode area [m^2]                         */
+    uint32_t flags;          /* CUDAPIC_FLAG_*                               */
+} cudapic_params;
+
+/* Poisson prefix sums in f32 as the reference does (default: FP64 sums,
+ * f32 inputs/outputs). */
+#define CUDAPIC_FLAG_POISSON_F32_SCAN 0x1u
+
+/* Derived per-discharge constants handed to every drop-in kernel (by value
+ * on the kernel side).  Built by cudapic_grid_from_params(); the fields are
+ * the reference's `X as Real` constants (Rust-CUDA/src/main.rs:53-109). */
+typedef struct cudapic_grid {
+    uint32_t n_g;
+    uint32_t capacity;
+    uint32_t n_t;
+    uint32_t n_sub;
+    uint32_t flags;
+    float inv_dx;
+    float weight_factor;
+    float gap;
+    float dt_e, dt_i;
+    float factor_e, factor_i;
+    float e_charge;
+    float alpha;
+    float half_dx_over_eps;
+    float half_inv_dx;
+    float normal_range;
+    float f1, f2;
+    float half_me_over_e;
+    float half_mu_over_e;
+    float min_x, max_x;
+    float eepf_half_kick;
+    double dx;
+    double weight_factor_d;
+    double gas_density;
+    double voltage;
+    uint32_t *dev_err;             /* device error word (may be NULL)          */
+    unsigned long long *work;      /* device particle-step counter (may be NULL) */
+} cudapic_grid;
+
+void cudapic_params_default(cudapic_params *p);
+int cudapic_grid_from_params(const cudapic_params *p, cudapic_grid *out);
+const char *cudapic_status_string(int status);
+const char *cudapic_last_error(void);
+int cudapic_version(void);
+
+/* ------------------------------------------------------------------ */
+/* 1. drop-in kernels                                                  */
+/* ------------------------------------------------------------------ */
+
+/* get_density (Rust-CUDA/src/main.rs:356-406): CIC deposit of x[0..*n_active)
+ * ADDED to density[n_g] (pre-zero it, as the reference's loop does at :1729).
+ * Boundary nodes receive double weight. */
+int cudapic_get_density(const float *x, float *density, const uint32_t *n_active,
+                        const cudapic_grid *grid, cudapic_stream_t stream);
+
+/* solve_poisson_scan_f32 (Rust-CUDA/src/main.rs:408-494): potential with
+ * pot[0] = pot0, pot[n_g-1] = 0 and the field, from the two densities.
+ * One CTA; FP64 prefix sums unless CUDAPIC_FLAG_POISSON_F32_SCAN. */
+int cudapic_solve_poisson_scan_f32(const float *e_density, const float *i_density, float *pot,
+                                   float *efield, float pot0, const cudapic_grid *grid,
+                                   cudapic_stream_t stream);
+
+/* solve_poisson_dps_flexible (Rust-CUDA/src/main.rs:496-564): psi'' = source
+ * on n nodes spaced dx with psi[0] = psi_left, psi[n-1] = psi_right. */
+int cudapic_solve_poisson_dps_flexible(const float *source, float *pot, uint32_t n, float psi_left,
+                                       float psi_right, float dx, cudapic_stream_t stream);
+
+/* move_and_compact (Rust-CUDA/src/main.rs:566-678): leapfrog push of
+ * src[0..*n_active), survivors (0 <= x' <= L) appended to dst at
+ * atomicAdd(alive_counter).  Survivor order is unspecified across blocks, as
+ * in the reference.  src and dst must not overlap; all particle pointers
+ * 16-byte aligned. */
+int cudapic_move_and_compact(const float *efield, const float *src_x, const float *src_vx,
+                             const float *src_vy, const float *src_vz, float *dst_x, float *dst_vx,
+                             float *dst_vy, float *dst_vz, uint32_t *alive_counter,
+                             const uint32_t *n_active, float factor, float dt,
+                             const cudapic_grid *grid, cudapic_stream_t stream);
+
+/* check_collisions_e (Rust-CUDA/src/main.rs:971-1165): MCC of electrons
+ * [0, *active_e) against the gas; ionization appends an electron at
+ * atomicAdd(alive_e) and an ion at atomicAdd(alive_i) (bounded by capacity).
+ * total_cs_e[1e6], cs[5*1e6] are the tables of cudapic_cross_sections(). */
+int cudapic_check_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e,
+                               float *x, float *vx, float *vy, float *vz, uint32_t *rng0,
+                               uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *i_x,
+                               float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e,
+                               uint32_t *alive_i, const cudapic_grid *grid,
+                               cudapic_stream_t stream);
+
+/* check_collisions_i (Rust-CUDA/src/main.rs:1167-1292): MCC of ions
+ * [0, *active_i) against Maxwellian target atoms. */
+int cudapic_check_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i,
+                               float *vx, float *vy, float *vz, uint32_t *rng0, uint32_t *rng1,
+                               uint32_t *rng2, uint32_t *rng3, const cudapic_grid *grid,
+                               cudapic_stream_t stream);
+
+/* Same as the two above, also writing the collision event of every particle
+ * to events[0..*active) (0 none, 1 elastic, 2 excitation, 3 ionization;
+ * 4 isotropic, 5 backscatter for ions).  No reference counterpart: a
+ * diagnostic used by the parity tests. */
+int cudapic_check_collisions_e_events(const float *total_cs_e, const float *cs,
+                                      const uint32_t *active_e, float *x, float *vx, float *vy,
+                                      float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
+                                      uint32_t *rng3, float *i_x, float *i_vx, float *i_vy,
+                                      float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
+                                      uint8_t *events, const cudapic_grid *grid,
+                                      cudapic_stream_t stream);
+int cudapic_check_collisions_i_events(const float *total_cs_i, const float *cs,
+                                      const uint32_t *active_i, float *vx, float *vy, float *vz,
+                                      uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
+                                      uint32_t *rng3, uint8_t *events, const cudapic_grid *grid,
+                                      cudapic_stream_t stream);
+
+/* accumulate_density (Rust-CUDA/src/main.rs:1294-1299): cumul[k] += density[k]. */
+int cudapic_accumulate_density(const float *density, double *cumul, const cudapic_grid *grid,
+                               cudapic_stream_t stream);
+
+/* accumulate_eepf (Rust-CUDA/src/main.rs:1301-1339): EEPF histogram
+ * (2000 bins of 0.05 eV) of electrons in (0.45 L, 0.55 L). */
+int cudapic_accumulate_eepf(const float *x, const float *vx, const float *vy, const float *vz,
+                            const float *efield, const uint32_t *active_e, uint32_t *eepf,
+                            const cudapic_grid *grid, cudapic_stream_t stream);
+
+/* xoshiro128p_test_wrapper (Rust-CUDA/src/main.rs:1341-1357): one step from
+ * (s0..s3); dest[0] = output, dest[1..4] = next state. */
+int cudapic_xoshiro128p_test_wrapper(uint32_t s0, uint32_t s1, uint32_t s2, uint32_t s3,
+                                     uint32_t *dest, cudapic_stream_t stream);
+
+/* xoshiro128_seed_streams (Rust-CUDA/src/main.rs:1446-1496), on the GPU:
+ * stream k = master after k jumps of 2^64, written to the four planes.
+ * n <= 2^28. */
+int cudapic_xoshiro128_seed_streams(const uint32_t master[4], uint32_t n, uint32_t *rng0,
+                                    uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
+                                    cudapic_stream_t stream);
+
+/* init_cross_sections (Rust-CUDA/src/main.rs:1378-1444), on the host:
+ * cs[5*1e6] (elastic, excitation, ionization, ion isotropic, ion backward)
+ * and the total macroscopic tables for the given gas density.  Host
+ * pointers.  Uses all host threads. */
+#define CUDAPIC_CS_RANGES 1000000u
+int cudapic_cross_sections(double gas_density, float *cs, float *sigma_tot_e, float *sigma_tot_i);
+
+/* Evaluates the kernels' f32 transcendental functions on device arrays
+ * (fn: 0 exp, 1 log, 2 sin, 3 cos, 4 tan, 5 atan, 6 acos, 7 atan2(in, in2)).
+ * No reference counterpart: a diagnostic for the bit-exactness tests. */
+int cudapic_math_eval(int fn, const float *in, const float *in2, float *out, uint32_t n,
+                      cudapic_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* 2. simulation state and driver                                      */
+/* ------------------------------------------------------------------ */
+
+typedef struct cudapic_state cudapic_state;
+
+/* Device pointers of a state (current ping-pong side). */
+typedef struct cudapic_buffers {
+    float *x[2], *vx[2], *vy[2], *vz[2];     /* [0] electrons, [1] ions            */
+    float *tmp_x[2], *tmp_vx[2], *tmp_vy[2], *tmp_vz[2];
+    uint32_t *rng[2][4];
+    uint32_t *n_electrons, *n_ions, *alive_counter;
+    float *efield, *pot, *e_density, *i_density;
+    float *cs, *sigma_tot_e, *sigma_tot_i;
+    double *cumul_e_density, *cumul_i_density;
+    uint32_t *eepf;
+    uint32_t *dev_err;
+    unsigned long long *work;
+} cudapic_buffers;
+
+#define CUDAPIC_ELECTRONS 0
+#define CUDAPIC_IONS 1
+
+/* Allocates every buffer on `device`, builds the cross-section tables,
+ * zeroes counters.  The state launches on its own non-blocking stream
+ * unless cudapic_state_set_stream() is called. */
+int cudapic_state_create(const cudapic_params *p, int device, cudapic_state **out);
+int cudapic_state_destroy(cudapic_state *s);
+int cudapic_state_set_stream(cudapic_state *s, cudapic_stream_t stream);
+cudapic_stream_t cudapic_state_stream(const cudapic_state *s);
+int cudapic_state_grid(const cudapic_state *s, cudapic_grid *out);
+int cudapic_state_buffers(const cudapic_state *s, cudapic_buffers *out);
+
+/* Host <-> device particle transfer (host pointers; pinned memory gives
+ * asynchronous copies).  upload sets the species count to n. */
+int cudapic_state_upload(cudapic_state *s, int species, const float *x, const float *vx,
+                         const float *vy, const float *vz, uint32_t n);
+/* Copies min(count, max_n) particles; *n_out = device count (synchronises). */
+int cudapic_state_download(cudapic_state *s, int species, float *x, float *vx, float *vy,
+                           float *vz, uint32_t max_n, uint32_t *n_out);
+/* Seeds both species' RNG planes from master states (all capacity slots). */
+int cudapic_state_seed(cudapic_state *s, const uint32_t e_master[4], const uint32_t i_master[4]);
+/* Zeroes the measurement accumulators and turns per-step measurement on/off
+ * (accumulate_density + accumulate_eepf, Rust-CUDA/src/main.rs:1746-1756, 1802-1807). */
+int cudapic_state_set_measure(cudapic_state *s, int on);
+/* Enqueues n_steps reference-order time steps (Rust-CUDA/src/main.rs:1728-1807)
+ * on the state's stream.  Asynchronous. */
+int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps);
+/* Reads the counters (synchronises the state's stream). */
+int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i);
+/* Reads and returns the device error word (synchronises). */
+int cudapic_state_device_error(cudapic_state *s, uint32_t *bits);
+/* Particle-steps processed so far (electrons each step, ions each N_SUB). */
+int cudapic_state_work(cudapic_state *s, unsigned long long *particle_steps);
+int cudapic_state_steps_done(const cudapic_state *s, uint64_t *steps);
+int cudapic_state_synchronize(cudapic_state *s);
+int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, double *cumul_i,
+                                        uint32_t *eepf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDAPIC_H */

@@ -1,0 +1,251 @@
+"""ctypes bindings of ``libcudapic_oracle.so`` (test infrastructure only).
+
+Each wrapper takes and returns numpy arrays and mirrors one function of
+``cudapic_oracle.h``; see that header for the reference file:line each one
+restates.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcudapic_oracle.so")
+REF_DIR = os.path.join(_HERE, "_ref")
+CS_RANGES = 1_000_000
+N_EEPF = 2000
+
+__all__ = [
+    "lib", "build", "OrcParams", "OrcPhys", "default_params", "phys_from_params",
+    "xoshiro_stream", "u32_to_real", "jump", "seed_streams", "math_apply",
+    "cross_sections", "get_density_f32", "get_density_f64", "poisson_thomas_f64",
+    "poisson_scan_f32", "poisson_dps_flexible_f64", "move_and_compact",
+    "check_collisions_e", "check_collisions_i", "p_coll_e_exact",
+    "accumulate_density", "accumulate_eepf", "REF_DIR", "CS_RANGES", "N_EEPF",
+    "MATH_FN",
+]
+
+MATH_FN = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "tan": 4, "atan": 5, "acos": 6, "atan2": 7}
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("n_g", C.c_uint32), ("n_t", C.c_uint32), ("n_sub", C.c_uint32), ("capacity", C.c_uint32),
+        ("frequency", C.c_double), ("voltage", C.c_double), ("gap", C.c_double),
+        ("pressure", C.c_double), ("temperature", C.c_double), ("weight", C.c_double),
+        ("electrode_area", C.c_double),
+    ]
+
+
+class OrcPhys(C.Structure):
+    _fields_ = [
+        ("n_g", C.c_uint32), ("capacity", C.c_uint32),
+        ("inv_dx", C.c_float), ("weight_factor", C.c_float), ("gap", C.c_float),
+        ("dt_e", C.c_float), ("dt_i", C.c_float), ("factor_e", C.c_float), ("factor_i", C.c_float),
+        ("e_charge", C.c_float), ("alpha", C.c_float), ("half_dx_over_eps", C.c_float),
+        ("half_inv_dx", C.c_float), ("normal_range", C.c_float), ("f1", C.c_float), ("f2", C.c_float),
+        ("half_me_over_e", C.c_float), ("half_mu_over_e", C.c_float), ("min_x", C.c_float),
+        ("max_x", C.c_float), ("eepf_half_kick", C.c_float),
+        ("dx", C.c_double), ("weight_factor_d", C.c_double), ("gas_density", C.c_double),
+        ("dt_e_d", C.c_double), ("dt_i_d", C.c_double), ("voltage", C.c_double), ("omega", C.c_double),
+        ("n_t", C.c_uint32), ("n_sub", C.c_uint32),
+    ]
+
+
+def build():
+    """Compile the oracle library with its Makefile (gcc only)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "libcudapic_oracle.so"], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def _declare(L):
+    P = C.POINTER
+    L.orc_params_default.argtypes = [P(OrcParams)]
+    L.orc_phys_from_params.argtypes = [P(OrcParams), P(OrcPhys)]
+    L.orc_xoshiro128p_next.argtypes = [_u32p]
+    L.orc_xoshiro128p_next.restype = C.c_uint32
+    L.orc_xoshiro128p_stream.argtypes = [_u32p, C.c_uint32, _u32p]
+    L.orc_u32_to_real.argtypes = [C.c_uint32]
+    L.orc_u32_to_real.restype = C.c_float
+    L.orc_jump.argtypes = [_u32p]
+    L.orc_seed_streams.argtypes = [_u32p, C.c_uint32, _u32p, _u32p, _u32p, _u32p]
+    L.orc_seed_streams.restype = C.c_int
+    L.orc_math_apply.argtypes = [C.c_int, _f32p, _f32p, _f32p, C.c_uint32]
+    L.orc_cross_sections.argtypes = [C.c_double, _f32p, _f32p, _f32p]
+    L.orc_get_density_f32.argtypes = [_f32p, C.c_uint32, _f32p, P(OrcPhys)]
+    L.orc_get_density_f64.argtypes = [_f32p, C.c_uint32, _f64p, P(OrcPhys)]
+    L.orc_poisson_thomas_f64.argtypes = [_f32p, _f32p, C.c_double, _f64p, _f64p, P(OrcPhys)]
+    L.orc_poisson_scan_f32.argtypes = [_f32p, _f32p, C.c_float, _f32p, _f32p, P(OrcPhys)]
+    L.orc_poisson_dps_flexible_f64.argtypes = [_f64p, _f64p, C.c_uint32, C.c_double, C.c_double, C.c_double]
+    L.orc_move_and_compact.argtypes = [_f32p] + [_f32p] * 8 + [C.c_uint32, C.c_float, C.c_float,
+                                                              P(OrcPhys), _u32p]
+    L.orc_move_and_compact.restype = C.c_uint32
+    L.orc_check_collisions_e.argtypes = ([_f32p, _f32p, C.c_uint32] + [_f32p] * 4 + [_u32p] * 4 +
+                                         [_f32p] * 4 + [P(C.c_uint32), P(C.c_uint32), P(OrcPhys),
+                                                        _u8p, P(C.c_uint32)])
+    L.orc_check_collisions_i.argtypes = ([_f32p, _f32p, C.c_uint32] + [_f32p] * 3 + [_u32p] * 4 +
+                                         [P(OrcPhys), _u8p])
+    L.orc_p_coll_e_exact.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, P(OrcPhys)]
+    L.orc_p_coll_e_exact.restype = C.c_double
+    L.orc_accumulate_density.argtypes = [_f32p, _f64p, C.c_uint32]
+    L.orc_accumulate_eepf.argtypes = [_f32p] * 5 + [C.c_uint32, _u32p, P(OrcPhys)]
+
+
+def default_params(**overrides):
+    p = OrcParams()
+    lib().orc_params_default(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def phys_from_params(p=None, **overrides):
+    if p is None:
+        p = default_params(**overrides)
+    ph = OrcPhys()
+    lib().orc_phys_from_params(C.byref(p), C.byref(ph))
+    return ph
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def xoshiro_stream(seed, n):
+    out = np.empty(n, np.uint32)
+    lib().orc_xoshiro128p_stream(_u32(seed), n, out)
+    return out
+
+
+def u32_to_real(x):
+    return lib().orc_u32_to_real(int(x))
+
+
+def jump(state):
+    s = _u32(state).copy()
+    lib().orc_jump(s)
+    return s
+
+
+def seed_streams(master, n):
+    planes = [np.empty(n, np.uint32) for _ in range(4)]
+    rc = lib().orc_seed_streams(_u32(master), n, *planes)
+    if rc != 0:
+        raise ValueError("xoshiro128+ master state must not be all zero")
+    return planes
+
+
+def math_apply(fn, x, y=None):
+    x = _f32(x)
+    y = _f32(y if y is not None else np.zeros_like(x))
+    out = np.empty_like(x)
+    lib().orc_math_apply(MATH_FN[fn] if isinstance(fn, str) else fn, x, y, out, x.size)
+    return out
+
+
+def cross_sections(gas_density):
+    cs = np.empty(5 * CS_RANGES, np.float32)
+    se = np.empty(CS_RANGES, np.float32)
+    si = np.empty(CS_RANGES, np.float32)
+    lib().orc_cross_sections(float(gas_density), cs, se, si)
+    return cs, se, si
+
+
+def get_density_f32(x, ph):
+    x = _f32(x)
+    d = np.empty(ph.n_g, np.float32)
+    lib().orc_get_density_f32(x, x.size, d, C.byref(ph))
+    return d
+
+
+def get_density_f64(x, ph):
+    x = _f32(x)
+    d = np.empty(ph.n_g, np.float64)
+    lib().orc_get_density_f64(x, x.size, d, C.byref(ph))
+    return d
+
+
+def poisson_thomas_f64(e_density, i_density, pot0, ph):
+    pot = np.empty(ph.n_g, np.float64)
+    ef = np.empty(ph.n_g, np.float64)
+    lib().orc_poisson_thomas_f64(_f32(e_density), _f32(i_density), float(pot0), pot, ef, C.byref(ph))
+    return pot, ef
+
+
+def poisson_scan_f32(e_density, i_density, pot0, ph):
+    pot = np.empty(ph.n_g, np.float32)
+    ef = np.empty(ph.n_g, np.float32)
+    lib().orc_poisson_scan_f32(_f32(e_density), _f32(i_density), float(pot0), pot, ef, C.byref(ph))
+    return pot, ef
+
+
+def poisson_dps_flexible_f64(source, psi_left, psi_right, dx):
+    source = np.ascontiguousarray(source, np.float64)
+    pot = np.empty_like(source)
+    lib().orc_poisson_dps_flexible_f64(source, pot, source.size, psi_left, psi_right, dx)
+    return pot
+
+
+def move_and_compact(efield, x, vx, vy, vz, factor, dt, ph):
+    """Returns (x, vx, vy, vz, src_index) of the survivors in index order."""
+    n = len(x)
+    out = [np.empty(max(n, 1), np.float32) for _ in range(4)]
+    idx = np.empty(max(n, 1), np.uint32)
+    m = lib().orc_move_and_compact(_f32(efield), _f32(x), _f32(vx), _f32(vy), _f32(vz), *out,
+                                   n, float(factor), float(dt), C.byref(ph), idx)
+    return tuple(a[:m] for a in out) + (idx[:m],)
+
+
+def check_collisions_e(sigma_tot_e, cs, n_active, e, rng, ions, n_e, n_i, ph):
+    """In-place MCC of electrons.  e = [x, vx, vy, vz] (capacity-sized float32
+    arrays), rng = 4 uint32 planes, ions = [x, vx, vy, vz] of the ions.
+    Returns (events, n_e, n_i, dropped)."""
+    ne = C.c_uint32(n_e)
+    ni = C.c_uint32(n_i)
+    dropped = C.c_uint32(0)
+    events = np.zeros(max(n_active, 1), np.uint8)
+    lib().orc_check_collisions_e(sigma_tot_e, cs, n_active, *e, *rng, *ions,
+                                 C.byref(ne), C.byref(ni), C.byref(ph), events, C.byref(dropped))
+    return events[:n_active], ne.value, ni.value, dropped.value
+
+
+def check_collisions_i(sigma_tot_i, cs, n_active, v, rng, ph):
+    events = np.zeros(max(n_active, 1), np.uint8)
+    lib().orc_check_collisions_i(sigma_tot_i, cs, n_active, *v, *rng, C.byref(ph), events)
+    return events[:n_active]
+
+
+def p_coll_e_exact(sigma_tot_e, vx, vy, vz, ph):
+    return lib().orc_p_coll_e_exact(sigma_tot_e, float(vx), float(vy), float(vz), C.byref(ph))
+
+
+def accumulate_density(density, cumul):
+    lib().orc_accumulate_density(_f32(density), cumul, cumul.size)
+
+
+def accumulate_eepf(x, vx, vy, vz, efield, n_active, eepf, ph):
+    lib().orc_accumulate_eepf(_f32(x), _f32(vx), _f32(vy), _f32(vz), _f32(efield), n_active, eepf,
+                              C.byref(ph))

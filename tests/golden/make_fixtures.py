@@ -1,0 +1,62 @@
+"""Regenerates the golden fixtures of tests/golden/ from the reference tree.
+
+Run in a container that has the reference checkout (default /root/reference,
+override with CUDAPIC_REFERENCE):
+
+    python tests/golden/make_fixtures.py
+
+It writes:
+  xoshiro128p_10000.txt  -- 10 000 xoshiro128+ outputs from state {1,1,1,1},
+      produced by the reference's own generator
+      (Rust-CUDA/xorshiro128c/xoshiro128p.c, built by oracle/Makefile into
+      oracle/_ref/) and checked byte-identical to the file the reference
+      ships (Rust-CUDA/xorshiro128c/10000-c.txt).
+  edupic_ref_density.txt -- converged cycle-averaged n_e, n_i of the
+      eduPIC reference case (C/ReferenceCase_RawData/Figure10_density.dat).
+  edupic_ref_eepf.txt    -- its EEPF (Figure12_eepf.dat).
+  edupic_ref_conv_tail.txt -- last 100 cycles of its particle counts
+      (Figure9_conv.dat).
+  edupic_c0_conv.txt     -- cycle, N_e, N_i of the reference CPU program
+      (eduPIC 1.0 built from C/eduPIC.cc by oracle/Makefile, Mersenne
+      Twister seed 5489) for the init cycle plus 10 cycles from 1000 + 1000
+      particles.
+"""
+import filecmp
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+ORACLE = os.path.join(ROOT, "oracle")
+REF = os.environ.get("CUDAPIC_REFERENCE", "/root/reference")
+
+
+def main():
+    subprocess.run(["make", "-s", "-C", ORACLE, "ref", "REF=" + REF], check=True)
+    gen = os.path.join(ORACLE, "_ref", "10000-c.txt")
+    shipped = os.path.join(REF, "Rust-CUDA", "xorshiro128c", "10000-c.txt")
+    if not filecmp.cmp(gen, shipped, shallow=False):
+        sys.exit("xoshiro128p.c output differs from the shipped 10000-c.txt")
+    shutil.copyfile(gen, os.path.join(HERE, "xoshiro128p_10000.txt"))
+
+    raw = os.path.join(REF, "C", "ReferenceCase_RawData")
+    shutil.copyfile(os.path.join(raw, "Figure10_density.dat"), os.path.join(HERE, "edupic_ref_density.txt"))
+    shutil.copyfile(os.path.join(raw, "Figure12_eepf.dat"), os.path.join(HERE, "edupic_ref_eepf.txt"))
+    with open(os.path.join(raw, "Figure9_conv.dat")) as f:
+        lines = [ln for ln in f if ln.strip()]
+    with open(os.path.join(HERE, "edupic_ref_conv_tail.txt"), "w") as f:
+        f.writelines(lines[-100:])
+
+    exe = os.path.join(ORACLE, "_ref", "eduPIC")
+    with tempfile.TemporaryDirectory() as d:
+        subprocess.run([exe, "0"], cwd=d, check=True, capture_output=True)
+        subprocess.run([exe, "10"], cwd=d, check=True, capture_output=True)
+        shutil.copyfile(os.path.join(d, "conv.dat"), os.path.join(HERE, "edupic_c0_conv.txt"))
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

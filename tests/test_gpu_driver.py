@@ -1,0 +1,118 @@
+"""GPU tests of the simulation state and the per-step driver (reference loop
+Rust-CUDA/src/main.rs:1725-1808, replayed from CUDA graphs)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _c0_state(cudapic, seed=0, **kw):
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    from cudapic_b200.workloads import edupic_initial
+    st = GpuSimState(**kw)
+    st.upload_electrons(ParticlesSoA(*edupic_initial(1000, seed=seed)))
+    st.upload_ions(ParticlesSoA(*edupic_initial(1000, seed=seed + 1)))
+    st.seed()
+    return st
+
+
+def test_state_roundtrip_and_buffers(cudapic, cuda_device):
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    st = GpuSimState(capacity=10_000)
+    rng = np.random.default_rng(0)
+    p = ParticlesSoA(*(rng.random(777).astype(np.float32) for _ in range(4)))
+    st.upload_ions(p)
+    q, n = st.download_ions()
+    assert n == 777
+    for a, b in zip((p.x, p.vx, p.vy, p.vz), (q.x, q.vx, q.vy, q.vz)):
+        assert np.array_equal(a, b)
+    assert st.counts() == (0, 777)
+    b = st.buffers()
+    assert b.x[0] and b.tmp_x[0] and b.n_electrons and b.sigma_tot_e
+    st.close()
+
+
+def test_upload_beyond_capacity_is_rejected(cudapic, cuda_device):
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    st = GpuSimState(capacity=100)
+    with pytest.raises(cudapic.CudapicError):
+        st.upload_electrons(ParticlesSoA.with_capacity(101))
+    st.close()
+
+
+def test_c0_growth_matches_edupic(cudapic, cuda_device):
+    """Plain eduPIC case: 1000 + 1000 particles at rest, 11 RF cycles.  The
+    particle counts track the reference CPU program's (same physics, other
+    random numbers) within statistical tolerance."""
+    conv = np.loadtxt(os.path.join(GOLDEN, "edupic_c0_conv.txt"))
+    st = _c0_state(cudapic)
+    counts = []
+    for _ in range(11):
+        st.run_cycles(1)
+        counts.append(st.counts())
+    assert st.device_error() == 0
+    ne, ni = np.array(counts).T
+    # first cycle: ions created by ionization, electrons lost to the walls
+    assert 0.6 * conv[0, 2] < ni[0] < 1.4 * conv[0, 2]
+    assert 0.6 * conv[-1, 1] < ne[-1] < 1.4 * conv[-1, 1]
+    assert 0.6 * conv[-1, 2] < ni[-1] < 1.4 * conv[-1, 2]
+    assert np.all(np.diff(ne[2:]) > 0)  # the discharge is igniting
+    assert st.steps_done() == 11 * 4000
+    st.close()
+
+
+def test_work_counter_counts_particle_steps(cudapic, cuda_device):
+    st = _c0_state(cudapic)
+    st.run_steps(1)   # step 0 is an ion step: 1000 electrons + 1000 ions pushed
+    assert st.work() == 2000
+    n_e, _ = st.counts()
+    st.run_steps(1)   # electrons only
+    assert st.work() == 2000 + n_e
+    st.close()
+
+
+def test_graph_replay_equals_direct_launch_statistics(cudapic, cuda_device):
+    """run_steps(40) (one graph replay) and 40 x run_steps(1) (direct launches)
+    enqueue the same sequence; with the same seeds and inputs the counts agree
+    to within the nondeterminism of the compaction order."""
+    a = _c0_state(cudapic)
+    b = _c0_state(cudapic)
+    a.run_steps(400)
+    for _ in range(400):
+        b.run_steps(1)
+    na, nb = a.counts(), b.counts()
+    assert abs(na[0] - nb[0]) <= 0.2 * na[0] + 20
+    assert abs(na[1] - nb[1]) <= 0.2 * na[1] + 20
+    a.close()
+    b.close()
+
+
+def test_measurement_accumulators(cudapic, cuda_device):
+    st = _c0_state(cudapic)
+    st.run_cycles(2)
+    st.set_measure(True)
+    st.run_cycles(1)
+    ce, ci, eepf = st.download_measurements()
+    assert ce.sum() > 0 and ci.sum() > 0 and eepf.sum() > 0
+    assert np.all(ce >= 0) and np.all(ci >= 0)
+    st.close()
+
+
+def test_c1_population_steps_without_device_errors(cudapic, cuda_device):
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    from cudapic_b200.workloads import steady_state
+    n = 1 << 22
+    st = GpuSimState(capacity=n + n // 8, weight=7.0e4 * 120000 / n)
+    g = st.grid
+    st.upload_electrons(ParticlesSoA(*steady_state(n, 9.10938356e-31, 3.0, dt=g.dt_e, seed=1)))
+    st.upload_ions(ParticlesSoA(*steady_state(n, 6.63352090e-26, 0.03, dt=g.dt_i, seed=2)))
+    st.seed()
+    st.run_steps(40)
+    ne, ni = st.counts()
+    assert 0.9 * n < ne <= n * 1.01 and 0.95 * n < ni <= n * 1.01
+    assert st.device_error() == 0
+    st.close()

@@ -1,0 +1,350 @@
+"""GPU parity tests: every drop-in kernel of libcudapic, called through the C
+ABI on a B200, against the oracle on the same seeded inputs.
+
+Bar per kernel (reference file:line in the kernel sources):
+  RNG, seeding, EEPF, density accumulation .......... bit-exact
+  move_and_compact .... survivor count and survivor set bit-exact
+  check_collisions_e/i  event types, RNG states and velocities bit-exact;
+                        spawned particles bit-exact as a set
+  get_density ......... relative L2 <= 2e-5 vs the FP64 eduPIC deposit
+  solve_poisson ....... relative L2 <= 1e-6 (FP64 sums) vs FP64 Thomas;
+                        <= 1e-3 (N_G = 400) / 5e-2 (4096) in f32 mode
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from gpu_util import counter, dev, host, sorted_rows, zeros
+
+pytestmark = pytest.mark.gpu
+
+E_MASS = 9.10938356e-31
+AR_MASS = 6.63352090e-26
+
+
+@pytest.fixture(scope="module")
+def K(cudapic, cuda_device):
+    return cudapic.kernels
+
+
+@pytest.fixture(scope="module")
+def dev_tables(tables, cuda_device):
+    cs, se, si = tables
+    return dev(cs), dev(se), dev(si)
+
+
+# ---------------------------------------------------------------- RNG
+
+def test_xoshiro_known_answer(K):
+    # Rust-CUDA/src/main.rs:2002-2063 with a real assert
+    gold = np.loadtxt(os.path.join(GOLDEN, "xoshiro128p_10000.txt"), dtype=np.uint64).astype(np.uint32)
+    dest = zeros(5, np.uint32)
+    s = [1, 1, 1, 1]
+    out = np.empty(10000, np.uint32)
+    for i in range(10000):
+        K.xoshiro128p_test_wrapper(*s, dest)
+        h = host(dest)
+        out[i] = h[0]
+        s = [int(v) for v in h[1:5]]
+    assert np.array_equal(out, gold)
+
+
+@pytest.mark.parametrize("n", [1, 17, 100_003, 4_194_304])
+def test_seed_streams_bit_exact(K, oracle, n):
+    master = [0x12345678, 0x11112222, 0x22223333, 0x33334444]
+    planes = [zeros(n, np.uint32) for _ in range(4)]
+    K.xoshiro128_seed_streams(master, n, *planes)
+    ref = oracle.seed_streams(master, n)
+    for p, r in zip(planes, ref):
+        assert np.array_equal(host(p), r)
+
+
+@pytest.mark.parametrize("fn,lo,hi", [("exp", -40.0, 5.0), ("log", 1e-9, 1.0), ("sin", -10.0, 10.0),
+                                      ("cos", -10.0, 10.0), ("tan", -1.5, 1.5), ("atan", -60.0, 60.0),
+                                      ("acos", -1.0, 1.0), ("atan2", -4.0, 4.0)])
+def test_math_bit_exact_with_oracle(K, oracle, fn, lo, hi):
+    rng = np.random.default_rng(21)
+    x = rng.uniform(lo, hi, 1 << 20).astype(np.float32)
+    y = rng.uniform(lo, hi, 1 << 20).astype(np.float32)
+    out = zeros(x.size)
+    K.math_eval(fn, dev(x), out, y=dev(y))
+    ref = oracle.math_apply(fn, x, y)
+    assert np.array_equal(host(out).view(np.uint32), ref.view(np.uint32))
+
+
+# ---------------------------------------------------------------- deposit
+
+@pytest.mark.parametrize("n_g", [400, 4096])
+@pytest.mark.parametrize("n", [0, 1, 1001, 100_003, 4_194_304])
+def test_get_density_vs_fp64(cudapic, K, oracle, n_g, n):
+    g = cudapic.grid_from_params(n_g=n_g, capacity=max(n, 4))
+    ph = oracle.phys_from_params(n_g=n_g, capacity=max(n, 4))
+    rng = np.random.default_rng(n + n_g)
+    x = (rng.random(n) * 0.025).astype(np.float32)
+    if n:
+        x[0] = np.float32(0.025)  # exactly at the grounded electrode
+    dens = zeros(n_g)
+    K.get_density(dev(x) if n else zeros(4), dens, counter(n), g)
+    got = host(dens).astype(np.float64)
+    ref = oracle.get_density_f64(x, ph)
+    if n == 0:
+        assert not got.any()
+        return
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+    big = ref > 1e-3 * ref.max()
+    assert np.max(np.abs(got[big] - ref[big]) / ref[big]) < 1e-4
+
+
+def test_get_density_unaligned_pointer(cudapic, K, oracle):
+    n, n_g = 50_001, 400
+    g = cudapic.grid_from_params(n_g=n_g, capacity=n + 1)
+    ph = oracle.phys_from_params(n_g=n_g)
+    x = (np.random.default_rng(5).random(n) * 0.025).astype(np.float32)
+    buf = dev(np.concatenate([[0.0], x]).astype(np.float32))
+    dens = zeros(n_g)
+    K.get_density(buf.data_ptr() + 4, dens, counter(n), g)
+    ref = oracle.get_density_f64(x, ph)
+    assert np.linalg.norm(host(dens) - ref) / np.linalg.norm(ref) < 2e-5
+
+
+def test_accumulate_density_bit_exact(cudapic, K, oracle):
+    g = cudapic.grid_from_params()
+    d = np.random.default_rng(3).random(400).astype(np.float32) * 1e14
+    c0 = np.random.default_rng(4).random(400) * 1e16
+    cum = dev(c0)
+    K.accumulate_density(dev(d), cum, g)
+    ref = c0.copy()
+    oracle.accumulate_density(d, ref)
+    assert np.array_equal(host(cum), ref)
+
+
+# ---------------------------------------------------------------- Poisson
+
+def _profile(n_g, seed):
+    ref = np.loadtxt(os.path.join(GOLDEN, "edupic_ref_density.txt"))
+    xs = np.linspace(0, 1, n_g)
+    ne = np.interp(xs, np.linspace(0, 1, ref.shape[0]), ref[:, 1])
+    ni = np.interp(xs, np.linspace(0, 1, ref.shape[0]), ref[:, 2])
+    noise = np.random.default_rng(seed).normal(0, 0.02, (2, n_g))
+    return (ne * (1 + noise[0])).astype(np.float32), (ni * (1 + noise[1])).astype(np.float32)
+
+
+@pytest.mark.parametrize("n_g", [3, 33, 400, 1025, 4096, 16384])
+@pytest.mark.parametrize("pot0", [250.0, -117.3])
+def test_poisson_fp64_scan_vs_thomas(cudapic, K, oracle, n_g, pot0):
+    g = cudapic.grid_from_params(n_g=n_g)
+    ph = oracle.phys_from_params(n_g=n_g)
+    ne, ni = _profile(n_g, n_g)
+    pot, ef = zeros(n_g), zeros(n_g)
+    K.solve_poisson_scan_f32(dev(ne), dev(ni), pot, ef, pot0, g)
+    pt, et = oracle.poisson_thomas_f64(ne, ni, np.float32(pot0), ph)
+    gp, ge = host(pot).astype(np.float64), host(ef).astype(np.float64)
+    assert np.linalg.norm(gp - pt) / np.linalg.norm(pt) < 1e-6
+    assert np.linalg.norm(ge - et) / np.linalg.norm(et) < 1e-5
+    assert gp[0] == np.float32(pot0) and gp[-1] == 0.0
+
+
+@pytest.mark.parametrize("n_g,tol", [(400, 1e-3), (4096, 5e-2)])
+def test_poisson_f32_scan_vs_thomas(cudapic, K, oracle, n_g, tol):
+    g = cudapic.grid_from_params(n_g=n_g, flags=cudapic.FLAG_POISSON_F32_SCAN)
+    ph = oracle.phys_from_params(n_g=n_g)
+    ne, ni = _profile(n_g, 1)
+    pot, ef = zeros(n_g), zeros(n_g)
+    K.solve_poisson_scan_f32(dev(ne), dev(ni), pot, ef, 250.0, g)
+    pt, _ = oracle.poisson_thomas_f64(ne, ni, 250.0, ph)
+    assert np.linalg.norm(host(pot) - pt) / np.linalg.norm(pt) < tol
+
+
+def test_poisson_hakim_convergence(K, oracle):
+    # Rust-CUDA/src/main.rs:1895-1981, with the assert the reference omits
+    errs = []
+    for n_elem in (8, 16, 32, 64):
+        n = n_elem + 1
+        dx = 1.0 / n_elem
+        xs = np.arange(n) * dx
+        src = (1.0 - 2.0 * xs * xs).astype(np.float32)
+        pot = zeros(n)
+        K.solve_poisson_dps_flexible(dev(src), pot, n, 0.0, 0.0, dx)
+        p = host(pot).astype(np.float64)
+        exact = xs ** 2 / 2 - xs ** 4 / 6 - xs / 3
+        ref = oracle.poisson_dps_flexible_f64(src.astype(np.float64), 0.0, 0.0, np.float32(dx))
+        assert np.max(np.abs(p - ref)) < 1e-6
+        errs.append(np.mean(np.abs(p[1:-1] - exact[1:-1])))
+    orders = [math.log(errs[i] / errs[i + 1]) / math.log(2.0) for i in range(3)]
+    assert all(1.9 < o < 2.1 for o in orders), orders
+
+
+# ---------------------------------------------------------------- push + compaction
+
+def _population(n, species, seed, dt):
+    from cudapic_b200.workloads import steady_state
+    if species == "e":
+        return steady_state(n, E_MASS, 3.0, dt=dt, seed=seed)
+    return steady_state(n, AR_MASS, 0.03, dt=dt * 20, seed=seed)
+
+
+@pytest.mark.parametrize("species", ["e", "i"])
+@pytest.mark.parametrize("n", [0, 5, 2047, 2048, 2049, 100_003, 4_194_304])
+@pytest.mark.parametrize("n_g", [400, 4096])
+def test_move_and_compact_bit_exact(cudapic, K, oracle, species, n, n_g):
+    from cudapic_b200.workloads import field_profile
+    cap = max(4, (n + 3) // 4 * 4)
+    g = cudapic.grid_from_params(n_g=n_g, capacity=cap)
+    ph = oracle.phys_from_params(n_g=n_g, capacity=cap)
+    factor, dt = (g.factor_e, g.dt_e) if species == "e" else (g.factor_i, g.dt_i)
+    x, vx, vy, vz = _population(n, species, n + 7, g.dt_e)
+    ef = field_profile(n_g)
+    src = [dev(np.concatenate([a, np.zeros(cap - n, np.float32)])) for a in (x, vx, vy, vz)]
+    dst = [zeros(cap) for _ in range(4)]
+    alive = counter(0)
+    K.move_and_compact(dev(ef), *src, *dst, alive, counter(n), factor, dt, g)
+    m = int(host(alive)[0])
+    rx, rvx, rvy, rvz, _ = oracle.move_and_compact(ef, x, vx, vy, vz, factor, dt, ph)
+    assert m == rx.size
+    got = [host(d)[:m] for d in dst]
+    assert np.array_equal(sorted_rows(*got), sorted_rows(rx, rvx, rvy, rvz))
+
+
+def test_move_and_compact_unaligned_uses_reference_layout(cudapic, K, oracle):
+    from cudapic_b200.workloads import field_profile
+    n, n_g = 70_001, 400
+    g = cudapic.grid_from_params(n_g=n_g, capacity=n + 1)
+    ph = oracle.phys_from_params(n_g=n_g)
+    x, vx, vy, vz = _population(n, "e", 9, g.dt_e)
+    ef = field_profile(n_g)
+    srcb = [dev(np.concatenate([[0.0], a]).astype(np.float32)) for a in (x, vx, vy, vz)]
+    dst = [zeros(n + 1) for _ in range(4)]
+    alive = counter(0)
+    K.move_and_compact(dev(ef), *[b.data_ptr() + 4 for b in srcb], *dst, alive, counter(n), g.factor_e, g.dt_e, g)
+    m = int(host(alive)[0])
+    ref = oracle.move_and_compact(ef, x, vx, vy, vz, g.factor_e, g.dt_e, ph)
+    assert m == ref[0].size
+    assert np.array_equal(sorted_rows(*[host(d)[:m] for d in dst]), sorted_rows(*ref[:4]))
+
+
+def test_move_and_compact_appends_to_counter(cudapic, K, oracle):
+    """alive_counter is an append cursor: survivors land after its start value."""
+    from cudapic_b200.workloads import field_profile
+    n = 10_000
+    g = cudapic.grid_from_params(capacity=2 * n)
+    x, vx, vy, vz = _population(n, "e", 3, g.dt_e)
+    src = [dev(np.concatenate([a, np.zeros(n, np.float32)])) for a in (x, vx, vy, vz)]
+    dst = [dev(np.full(2 * n, -1.0, np.float32)) for _ in range(4)]
+    alive = counter(123)
+    K.move_and_compact(dev(field_profile(400)), *src, *dst, alive, counter(n), g.factor_e, g.dt_e, g)
+    m = int(host(alive)[0]) - 123
+    hx = host(dst[0])
+    assert np.all(hx[:123] == -1.0) and np.all(hx[123:123 + m] >= 0) and np.all(hx[123 + m:] == -1.0)
+
+
+# ---------------------------------------------------------------- collisions
+
+def _mcc_case(n, temp_ev, seed, mass):
+    from cudapic_b200.workloads import steady_state
+    return steady_state(n, mass, temp_ev, seed=seed, edge_fraction=0.0)
+
+
+@pytest.mark.parametrize("n,n_t,temp", [(1, 4000, 30.0), (4099, 200, 30.0), (300_001, 4000, 20.0),
+                                        (300_001, 100, 60.0), (4_194_304, 4000, 3.0)])
+def test_check_collisions_e_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp):
+    cs, se, si = tables
+    dcs, dse, _ = dev_tables
+    n_i0 = 1000
+    cap = n + n // 4 + 1024
+    g = cudapic.grid_from_params(n_t=n_t, capacity=cap)
+    ph = oracle.phys_from_params(n_t=n_t, capacity=cap)
+    x, vx, vy, vz = _mcc_case(n, temp, n, E_MASS)
+    rng = [np.asarray(p) for p in oracle.seed_streams([9, 8, 7, 6], n)]
+    pad = lambda a, dt=np.float32: np.concatenate([a, np.zeros(cap - len(a), dt)])
+    e_h = [pad(a) for a in (x, vx, vy, vz)]
+    i_h = [pad(np.full(n_i0, 0.0125, np.float32)) for _ in range(4)]
+    r_h = [pad(p, np.uint32) for p in rng]
+    e_d = [dev(a) for a in e_h]
+    i_d = [dev(a) for a in i_h]
+    r_d = [dev(a) for a in r_h]
+    alive_e, alive_i = counter(n), counter(n_i0)
+    events = zeros(max(n, 1), np.uint8)
+    K.check_collisions_e(dse, dcs, counter(n), *e_d, *r_d, *i_d, alive_e, alive_i, g, events=events)
+    ev_ref, ne_ref, ni_ref, dropped = oracle.check_collisions_e(se, cs, n, e_h, r_h, i_h, n, n_i0, ph)
+    assert dropped == 0
+    ge = host(events)[:n]
+    assert np.array_equal(ge, ev_ref)
+    if n > 4000:
+        assert (ge > 0).sum() > 10
+    ne, ni = int(host(alive_e)[0]), int(host(alive_i)[0])
+    assert ne == ne_ref and ni == ni_ref
+    for d, h in zip(r_d, r_h):
+        assert np.array_equal(host(d)[:n], h[:n])
+    ge_arr = [host(d) for d in e_d]
+    for a, h in zip(ge_arr, e_h):
+        assert np.array_equal(a[:n].view(np.uint32), h[:n].view(np.uint32))
+    # spawned electrons and ions: same set, order unspecified
+    assert np.array_equal(sorted_rows(*[a[n:ne] for a in ge_arr]), sorted_rows(*[h[n:ne] for h in e_h]))
+    gi_arr = [host(d) for d in i_d]
+    assert np.array_equal(sorted_rows(*[a[n_i0:ni] for a in gi_arr]), sorted_rows(*[h[n_i0:ni] for h in i_h]))
+
+
+@pytest.mark.parametrize("n,n_t,temp", [(1, 4000, 1.0), (65_537, 4000, 0.03), (300_001, 200, 2.0),
+                                        (4_194_304, 4000, 0.03)])
+def test_check_collisions_i_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp):
+    cs, se, si = tables
+    dcs, _, dsi = dev_tables
+    g = cudapic.grid_from_params(n_t=n_t, capacity=n)
+    ph = oracle.phys_from_params(n_t=n_t, capacity=n)
+    _, vx, vy, vz = _mcc_case(n, temp, n + 1, AR_MASS)
+    rng = [np.asarray(p) for p in oracle.seed_streams([5, 6, 7, 8], n)]
+    v_h = [a.copy() for a in (vx, vy, vz)]
+    r_h = [p.copy() for p in rng]
+    v_d = [dev(a) for a in v_h]
+    r_d = [dev(a) for a in r_h]
+    events = zeros(n, np.uint8)
+    K.check_collisions_i(dsi, dcs, counter(n), *v_d, *r_d, g, events=events)
+    ev_ref = oracle.check_collisions_i(si, cs, n, v_h, r_h, ph)
+    assert np.array_equal(host(events), ev_ref)
+    for d, h in zip(r_d, r_h):
+        assert np.array_equal(host(d), h)
+    for d, h in zip(v_d, v_h):
+        assert np.array_equal(host(d).view(np.uint32), h.view(np.uint32))
+
+
+def test_spawn_capacity_is_enforced(cudapic, K, oracle, dev_tables, tables):
+    """Ionization spawns beyond capacity are dropped and flagged, never
+    written past the buffers (the reference writes unbounded)."""
+    cs, se, si = tables
+    dcs, dse, _ = dev_tables
+    n, cap, guard = 200_000, 200_032, 4096
+    flag = zeros(1, np.uint32)
+    g = cudapic.grid_from_params(n_t=50, capacity=cap)
+    g.dev_err = flag.data_ptr()
+    x, vx, vy, vz = _mcc_case(n, 60.0, 17, E_MASS)
+    pad = lambda a, dt=np.float32: np.concatenate([a, np.full(cap + guard - len(a), 7.0, dt)])
+    e_d = [dev(pad(a)) for a in (x, vx, vy, vz)]
+    i_d = [dev(pad(np.zeros(cap - 16, np.float32))) for _ in range(4)]
+    r_d = [dev(np.concatenate([p, np.zeros(guard, np.uint32)])) for p in oracle.seed_streams([1, 3, 5, 7], cap)]
+    alive_e, alive_i = counter(n), counter(cap - 16)
+    K.check_collisions_e(dse, dcs, counter(n), *e_d, *r_d, *i_d, alive_e, alive_i, g)
+    assert int(host(alive_e)[0]) <= cap and int(host(alive_i)[0]) <= cap
+    bits = int(host(flag)[0])
+    assert bits & cudapic.DEVERR_SPAWN_E and bits & cudapic.DEVERR_SPAWN_I
+    for d in e_d + i_d:
+        assert np.all(host(d)[cap:] == 7.0)
+
+
+# ---------------------------------------------------------------- diagnostics
+
+def test_accumulate_eepf_bit_exact(cudapic, K, oracle):
+    from cudapic_b200.workloads import field_profile
+    n = 500_000
+    g = cudapic.grid_from_params(capacity=n)
+    ph = oracle.phys_from_params(capacity=n)
+    x, vx, vy, vz = _population(n, "e", 4, g.dt_e)
+    ef = field_profile(400)
+    eepf = zeros(2000, np.uint32)
+    K.accumulate_eepf(dev(x), dev(vx), dev(vy), dev(vz), dev(ef), counter(n), eepf, g)
+    ref = np.zeros(2000, np.uint32)
+    oracle.accumulate_eepf(x, vx, vy, vz, ef, n, ref, ph)
+    assert ref.sum() > 10_000
+    assert np.array_equal(host(eepf), ref)
