@@ -260,6 +260,7 @@ def kernel_breakdown(st, K, reps, flush):
         t = statistics.median(ts)
         d = {"us": t * 1e6, "n": n}
         if bytes_per:
+            d["bytes_per_particle"] = bytes_per
             d["algo_bytes"] = bytes_per * n
             d["gbs"] = bytes_per * n / t / 1e9
         res[name] = d
@@ -394,7 +395,7 @@ def run_ours(args):
         traffic = ncu_traffic(dom, d["n"])
         roofline = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
                     "frac": d["gbs"] / peak, "traffic": traffic, "peak_source": peak_kind,
-                    "algo_bytes_per_particle": ALGO_BYTES[dom.rsplit("_", 1)[0]]}
+                    "algo_bytes_per_particle": d["bytes_per_particle"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(MC_THREADS)
     uint64_t *bar = reinterpret_cast<uint64_t *>(ef + ef_pad);
     __shared__ uint32_t wsum[MC_WARPS];
     __shared__ uint32_t s_base, s_tot0, s_total;
+    __shared__ int s_ready;
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -103,12 +104,19 @@ __global__ void __launch_bounds__(MC_THREADS)
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int s = (int)(it % MC_STAGES);
         const uint32_t parity = (it / MC_STAGES) & 1u;
-        if (!mbar_wait_bounded(&bar[s], parity)) {
-            set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
-            // let the other stage's copy (if any) land before the CTA exits
-            mbar_wait_bounded(&bar[s ^ 1], ((it + 1) / MC_STAGES) & 1u);
-            return;
+        // One thread waits (bounded) on the stage's barrier and publishes the
+        // verdict, so that a timeout makes the whole CTA leave together.
+        if (tid == 0) {
+            int ok = mbar_wait_bounded(&bar[s], parity) ? 1 : 0;
+            if (!ok) {
+                set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
+                // the other stage's copy, if one was issued, must land before exit
+                if (tile + gridDim.x < ntiles) mbar_wait_bounded(&bar[s ^ 1], ((it + 1) / MC_STAGES) & 1u);
+            }
+            s_ready = ok;
         }
+        __syncthreads();
+        if (!s_ready) return;
         const uint32_t t0 = tile * MC_TILE;
         const uint32_t cnt = min((uint32_t)MC_TILE, n - t0);
         const float *bx = in + (s * 4 + 0) * MC_TILE;

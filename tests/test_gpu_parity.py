@@ -93,9 +93,16 @@ def test_get_density_vs_fp64(cudapic, K, oracle, n_g, n):
     if n == 0:
         assert not got.any()
         return
-    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+    # f32 restatement (same arithmetic, sequential summation order)
+    r32 = oracle.get_density_f32(x, ph).astype(np.float64)
+    assert np.linalg.norm(got - r32) / np.linalg.norm(r32) < 2e-5
+    # FP64 eduPIC deposit: the f32 position x*inv_dx carries an absolute
+    # rounding error up to N_G * 2^-24 in the CIC weights (the reference's
+    # f32 arithmetic), which averages out only over many particles per node.
+    tol = max(2e-5, 1.5 * n_g * 2.0 ** -24)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol
     big = ref > 1e-3 * ref.max()
-    assert np.max(np.abs(got[big] - ref[big]) / ref[big]) < 1e-4
+    assert np.max(np.abs(got[big] - ref[big]) / ref[big]) < max(1e-4, 3.0 * n_g * 2.0 ** -24)
 
 
 def test_get_density_unaligned_pointer(cudapic, K, oracle):
