@@ -244,20 +244,10 @@ def kernel_breakdown(st, K, reps, flush):
     n_e, n_i = st.counts()
     res = {}
 
+    from cudapic_b200.timing import time_launch
+
     def timed(name, fn, n, bytes_per, pre=None):
-        ts = []
-        for _ in range(reps):
-            flush.zero_()
-            if pre is not None:
-                pre()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1) * 1e-3)
-        t = statistics.median(ts)
+        t = time_launch(fn, stream, reps, flush=flush, pre=pre)
         d = {"us": t * 1e6, "n": n}
         if bytes_per:
             d["bytes_per_particle"] = bytes_per
@@ -303,7 +293,7 @@ def run_ours(args):
     from cudapic_b200.sim import GpuSimState, ParticlesSoA
 
     n = args.particles
-    params = cp.default_params(n_g=args.n_g, capacity=n + n // 8, weight=7.0e4 * 120000 / n)
+    params = cp.default_params(n_g=args.n_g, capacity=2 * n, weight=7.0e4 * 120000 / n)
     st = GpuSimState(params, device=local)
     stream = torch.cuda.Stream()
     st.set_stream(stream)
@@ -382,8 +372,8 @@ def run_ours(args):
     roofline = None
     peak, peak_kind = measured_peaks()
     if not args.no_breakdown:
-        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-        breakdown = kernel_breakdown(st, cp.kernels, reps=7, flush=flush)
+        from cudapic_b200.timing import L2Flusher
+        breakdown = kernel_breakdown(st, cp.kernels, reps=7, flush=L2Flusher())
         share_w = {"get_density_e": STEP, "solve_poisson": STEP, "move_and_compact_e": STEP,
                    "check_collisions_e": STEP, "get_density_i": ion_steps, "move_and_compact_i": ion_steps,
                    "check_collisions_i": ion_steps}

@@ -20,7 +20,7 @@ import ctypes as _C
 
 from . import _lib
 from ._lib import (CS_RANGES, ELECTRONS, IONS, N_EEPF, Buffers, CudapicError, Grid, Params,  # noqa: F401
-                   FLAG_POISSON_F32_SCAN, DEVERR_SPAWN_E, DEVERR_SPAWN_I, DEVERR_POSITION,
+                   FLAG_POISSON_F32_SCAN, FLAG_DEPOSIT_FIXED_POINT, DEVERR_SPAWN_E, DEVERR_SPAWN_I, DEVERR_POSITION,
                    DEVERR_ACTIVE, DEVERR_TIMEOUT)
 
 lib = _lib.load()
@@ -56,6 +56,25 @@ def grid_from_params(params=None, **overrides):
 
 def version():
     return lib.cudapic_version()
+
+
+def get_tuning():
+    """Current kernel launch shapes (cudapic_tuning) as a dict."""
+    t = _lib.Tuning()
+    check(lib.cudapic_get_tuning(_C.byref(t)))
+    return t.as_dict()
+
+
+def set_tuning(**fields):
+    """Updates kernel launch shapes; unspecified fields keep their values."""
+    cur = get_tuning()
+    for k, v in fields.items():
+        if k not in cur:
+            raise AttributeError("unknown tuning field %r" % k)
+        cur[k] = int(v)
+    t = _lib.Tuning(**cur)
+    check(lib.cudapic_set_tuning(_C.byref(t)))
+    return get_tuning()
 
 
 from . import kernels  # noqa: E402,F401

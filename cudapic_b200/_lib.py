@@ -25,6 +25,7 @@ DEVERR_ACTIVE = 0x8
 DEVERR_TIMEOUT = 0x10
 
 FLAG_POISSON_F32_SCAN = 0x1
+FLAG_DEPOSIT_FIXED_POINT = 0x2
 CS_RANGES = 1_000_000
 N_EEPF = 2000
 ELECTRONS = 0
@@ -60,6 +61,15 @@ class Grid(C.Structure):
         ("voltage", C.c_double),
         ("dev_err", C.c_void_p), ("work", C.c_void_p),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [(name, C.c_int) for name in (
+        "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
+        "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 _P2 = C.c_void_p * 2
@@ -99,6 +109,8 @@ SIGNATURES = {
     "cudapic_cross_sections": [C.c_double, _VP, _VP, _VP],
     "cudapic_math_eval": [C.c_int, _VP, _VP, _VP, _U32, _VP],
     "cudapic_grid_from_params": [C.POINTER(Params), _GP],
+    "cudapic_get_tuning": [C.POINTER(Tuning)],
+    "cudapic_set_tuning": [C.POINTER(Tuning)],
     "cudapic_version": [],
     "cudapic_state_create": [C.POINTER(Params), C.c_int, C.POINTER(_VP)],
     "cudapic_state_destroy": [_VP],

@@ -64,6 +64,26 @@ int check_launch(const char *kernel) {
 int sm_count() { return device_info().sms; }
 int max_smem_optin() { return device_info().smem_optin; }
 
+namespace {
+// Built-in launch shapes (chosen with cudapic_b200.autotune on B200).
+constexpr cudapic_tuning kDefaultTuning = {
+    /*density_threads*/ 512, /*density_ctas_per_sm*/ 2, /*density_copies*/ 16, /*density_cluster*/ 4,
+    /*push_stages*/ 3, /*push_ctas_per_sm*/ 4,
+    /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1};
+std::mutex g_tune_mu;
+cudapic_tuning g_tuning = kDefaultTuning;
+}  // namespace
+
+cudapic_tuning tuning() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return g_tuning;
+}
+
+unsigned persistent_grid(int per_sm, uint64_t units) {
+    const uint64_t cap = (uint64_t)sm_count() * (uint64_t)std::max(per_sm, 1);
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(cap, units));
+}
+
 int validate_grid(const cudapic_grid *g) {
     if (!g) return fail(CUDAPIC_ERR_ARG, "grid is null");
     if (g->n_g < 3 || g->n_g > 16384) return fail(CUDAPIC_ERR_ARG, "grid.n_g must be in [3, 16384]");
@@ -158,6 +178,39 @@ extern "C" const char *cudapic_status_string(int s) {
 }
 
 extern "C" const char *cudapic_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int cudapic_get_tuning(cudapic_tuning *out) {
+    if (!out) return fail(CUDAPIC_ERR_ARG, "get_tuning: null pointer");
+    *out = tuning();
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
+    if (!t) return fail(CUDAPIC_ERR_ARG, "set_tuning: null pointer");
+    cudapic_tuning v = *t;
+    const cudapic_tuning d = kDefaultTuning;
+    if (!v.density_threads) v.density_threads = d.density_threads;
+    if (!v.density_ctas_per_sm) v.density_ctas_per_sm = d.density_ctas_per_sm;
+    if (!v.density_copies) v.density_copies = d.density_copies;
+    if (!v.density_cluster) v.density_cluster = d.density_cluster;
+    if (!v.push_stages) v.push_stages = d.push_stages;
+    if (!v.push_ctas_per_sm) v.push_ctas_per_sm = d.push_ctas_per_sm;
+    if (!v.mcc_stages) v.mcc_stages = d.mcc_stages;
+    if (!v.mcc_ctas_per_sm) v.mcc_ctas_per_sm = d.mcc_ctas_per_sm;
+    if (!v.mcc_variant) v.mcc_variant = d.mcc_variant;
+    const bool ok = (v.density_threads == 256 || v.density_threads == 512 || v.density_threads == 1024) &&
+                    v.density_ctas_per_sm >= 1 && v.density_ctas_per_sm <= 8 && v.density_copies >= 1 &&
+                    v.density_copies <= 32 &&
+                    (v.density_cluster == 1 || v.density_cluster == 2 || v.density_cluster == 4 ||
+                     v.density_cluster == 8) &&
+                    v.push_stages >= 2 && v.push_stages <= 6 && v.push_ctas_per_sm >= 1 && v.push_ctas_per_sm <= 8 &&
+                    v.mcc_stages >= 2 && v.mcc_stages <= 4 && v.mcc_ctas_per_sm >= 1 && v.mcc_ctas_per_sm <= 8 &&
+                    (v.mcc_variant == 1 || v.mcc_variant == 2);
+    if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuning = v;
+    return CUDAPIC_OK;
+}
 
 extern "C" int cudapic_version(void) { return CUDAPIC_VERSION; }
 

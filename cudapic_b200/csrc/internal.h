@@ -27,6 +27,12 @@ inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 
 // Validation shared by the entry points.
 int validate_grid(const cudapic_grid *g);
 
+// Current launch shapes (defaults filled in for zero fields).
+cudapic_tuning tuning();
+
+// Grid of a persistent kernel: min(SMs x per_sm, work units), at least 1.
+unsigned persistent_grid(int per_sm, uint64_t units);
+
 // Launchers used by both the drop-in entry points and the driver.
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream);

@@ -5,17 +5,27 @@
 // with one global atomic per non-zero node and block).
 //
 // B200 design:
-//  * persistent grid (SM count x resident clusters), float4 loads of x;
+//  * persistent grid (SMs x resident CTAs, whole clusters), float4 loads of x;
 //  * warp-privatised shared histograms: warp w adds into copy (w % copies),
 //    so concurrent shared atomics of different warps never contend on the
-//    same word; `copies` is as many N_G-float copies as fit in 64 KB;
-//  * copies are summed inside the CTA, then a thread-block cluster of
-//    DENS_CLUSTER CTAs sums its CTAs' histograms through distributed shared
-//    memory, and only one CTA per cluster touches each global node: the
-//    global flush costs (grid / DENS_CLUSTER) x N_G atomics instead of
-//    grid x N_G.
+//    same word;
+//  * default arithmetic: the reference's f32 weights (1-rem) W, rem W added
+//    with shared f32 atomics (about 1.5 lane-updates per clock per SM on
+//    B200: the bound of this kernel);
+//  * CUDAPIC_FLAG_DEPOSIT_FIXED_POINT: the CIC fraction rem = pos - p (an f32
+//    in [0, 1)) becomes the 32.32 fixed-point integer round(rem * 2^32) --
+//    exact for every pos >= 1 -- and the node weights 2^32 - r and r are
+//    summed with 64-bit integer shared atomics: exact and order-independent
+//    within a cluster, about 25 % slower;
+//  * copies are summed inside the CTA, then the CTAs of a thread-block
+//    cluster sum their histograms through distributed shared memory, and one
+//    CTA per cluster adds each node (boundary nodes doubled) to the f32
+//    density with one global atomic.
+// CTA size, copies, cluster size and CTAs per SM come from cudapic_tuning.
 // HBM traffic: 4 B per particle (x) plus the flush.
 #include <cooperative_groups.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "internal.h"
@@ -24,40 +34,57 @@ namespace cg = cooperative_groups;
 
 namespace cudapic {
 
-constexpr int DENS_BLOCK = 512;
-constexpr int DENS_CLUSTER = 4;
-constexpr int DENS_SMEM_BUDGET = 64 * 1024;
+using u64 = unsigned long long;
 
-__device__ __forceinline__ void deposit_one(float xv, float *h, const cudapic_grid &g) {
-    float pos = xv * g.inv_dx;
+__device__ __forceinline__ float cic_fraction(float xv, const cudapic_grid &g, int &p) {
+    const float pos = xv * g.inv_dx;
     if (!(pos >= 0.0f && pos < (float)g.n_g - 0.5f)) set_dev_err(g.dev_err, CUDAPIC_DEVERR_POSITION);
-    int p = cell_of(pos, g.n_g);
-    float rem = pos - (float)p;
-    float c1 = (1.0f - rem) * g.weight_factor;
-    float c2 = rem * g.weight_factor;
-    atomicAdd(&h[p], c1);
-    atomicAdd(&h[p + 1], c2);
+    p = cell_of(pos, g.n_g);
+    return pos - (float)p;
 }
 
-template <bool VEC>
-__global__ void __launch_bounds__(DENS_BLOCK)
+// reference arithmetic: c1 = (1-rem) W, c2 = rem W in f32 (Rust-CUDA/src/main.rs:377-387)
+__device__ __forceinline__ void deposit_one(float xv, float *h, const cudapic_grid &g) {
+    int p;
+    const float rem = cic_fraction(xv, g, p);
+    atomicAdd(&h[p], (1.0f - rem) * g.weight_factor);
+    atomicAdd(&h[p + 1], rem * g.weight_factor);
+}
+
+// fixed point: weights 2^32 - r and r, r = round(rem 2^32)
+__device__ __forceinline__ void deposit_one(float xv, u64 *h, const cudapic_grid &g) {
+    int p;
+    const float rem = cic_fraction(xv, g, p);
+    const u64 r = __float2ull_rn(rem * 4294967296.0f);
+    atomicAdd(&h[p], (1ull << 32) - r);
+    atomicAdd(&h[p + 1], r);
+}
+
+__device__ __forceinline__ float node_value(float s, const cudapic_grid &) { return s; }
+__device__ __forceinline__ float node_value(u64 s, const cudapic_grid &g) {
+    return (float)((double)s * (g.weight_factor_d * 0x1p-32));
+}
+
+template <int BLOCK, bool VEC, typename Acc>
+__global__ void __launch_bounds__(BLOCK)
     get_density_kernel(const float *__restrict__ x, float *__restrict__ density,
                        const uint32_t *__restrict__ n_active, const cudapic_grid g, int copies) {
-    extern __shared__ float hist[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Acc *hist = reinterpret_cast<Acc *>(smem_raw);
     const uint32_t n_g = g.n_g;
     const int tid = threadIdx.x;
-    for (uint32_t k = tid; k < (uint32_t)copies * n_g; k += DENS_BLOCK) hist[k] = 0.0f;
+    for (uint32_t k = tid; k < (uint32_t)copies * n_g; k += BLOCK) hist[k] = Acc(0);
     __syncthreads();
 
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
-    float *h = hist + (uint32_t)((tid >> 5) % copies) * n_g;
-    const uint32_t stride = gridDim.x * DENS_BLOCK;
-    uint32_t start = blockIdx.x * DENS_BLOCK + tid;
+    Acc *h = hist + (uint32_t)((tid >> 5) % copies) * n_g;
+    const uint32_t stride = gridDim.x * BLOCK;
+    const uint32_t start = blockIdx.x * BLOCK + tid;
     if (VEC) {
         const uint32_t n4 = n >> 2;
         const float4 *x4 = reinterpret_cast<const float4 *>(x);
         for (uint32_t j = start; j < n4; j += stride) {
-            float4 v = x4[j];
+            const float4 v = x4[j];
             deposit_one(v.x, h, g);
             deposit_one(v.y, h, g);
             deposit_one(v.z, h, g);
@@ -71,8 +98,8 @@ __global__ void __launch_bounds__(DENS_BLOCK)
 
     // sum the warp copies into copy 0
     if (copies > 1) {
-        for (uint32_t k = tid; k < n_g; k += DENS_BLOCK) {
-            float s = hist[k];
+        for (uint32_t k = tid; k < n_g; k += BLOCK) {
+            Acc s = hist[k];
             for (int c = 1; c < copies; ++c) s += hist[(uint32_t)c * n_g + k];
             hist[k] = s;
         }
@@ -86,15 +113,16 @@ __global__ void __launch_bounds__(DENS_BLOCK)
     const uint32_t chunk = (n_g + csize - 1) / csize;
     const uint32_t k0 = rank * chunk;
     const uint32_t k1 = min(n_g, k0 + chunk);
-    for (uint32_t k = k0 + tid; k < k1; k += DENS_BLOCK) {
-        float s = 0.0f;
+    for (uint32_t k = k0 + tid; k < k1; k += BLOCK) {
+        Acc s = Acc(0);
         for (unsigned q = 0; q < csize; ++q) {
-            const float *remote = cluster.map_shared_rank(hist, q);
+            const Acc *remote = cluster.map_shared_rank(hist, q);
             s += remote[k];
         }
-        if (s != 0.0f) {
-            if (k == 0 || k == n_g - 1) s *= 2.0f;
-            atomicAdd(&density[k], s);
+        if (s != Acc(0)) {
+            float v = node_value(s, g);
+            if (k == 0 || k == n_g - 1) v *= 2.0f;
+            atomicAdd(&density[k], v);
         }
     }
     cluster.sync();
@@ -109,49 +137,60 @@ __global__ void accumulate_density_kernel(const float *__restrict__ density, dou
 
 namespace {
 
-struct DensityLaunch {
-    int grid = 0;
-    int copies = 1;
-    size_t smem = 0;
-};
-
-template <bool VEC>
-int launch_density(const float *x, float *density, const uint32_t *n_active, const cudapic_grid &g,
-                   cudaStream_t stream) {
-    DensityLaunch L;
-    const size_t per_copy = (size_t)g.n_g * sizeof(float);
-    L.copies = (int)std::min<size_t>(DENS_BLOCK / 32, std::max<size_t>(1, DENS_SMEM_BUDGET / per_copy));
-    L.smem = per_copy * (size_t)L.copies;
-    if (L.smem > (size_t)max_smem_optin())
-        return fail(CUDAPIC_ERR_ARG, "get_density: n_g too large for one shared histogram");
-    auto kern = get_density_kernel<VEC>;
-    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)L.smem),
+template <int BLOCK, bool VEC, typename Acc>
+int launch_density_t(const float *x, float *density, const uint32_t *n_active, const cudapic_grid &g,
+                     const cudapic_tuning &t, cudaStream_t stream) {
+    const size_t per_copy = (size_t)g.n_g * sizeof(Acc);
+    const size_t budget = (size_t)max_smem_optin();
+    if (per_copy > budget) return fail(CUDAPIC_ERR_ARG, "get_density: n_g too large for one shared histogram");
+    int copies = std::min(t.density_copies, BLOCK / 32);
+    copies = (int)std::min<size_t>((size_t)copies, std::max<size_t>(1, budget / per_copy));
+    const size_t smem = per_copy * (size_t)copies;
+    auto kern = get_density_kernel<BLOCK, VEC, Acc>;
+    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                              "cudaFuncSetAttribute(get_density)"));
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = DENS_CLUSTER;
+    attr[0].val.clusterDim.x = (unsigned)t.density_cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(DENS_BLOCK);
-    cfg.dynamicSmemBytes = L.smem;
+    cfg.blockDim = dim3(BLOCK);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    // grid: resident clusters, but no more CTAs than the capacity needs
+    const int cl = t.density_cluster;
     int max_clusters = 0;
-    cfg.gridDim = dim3(DENS_CLUSTER * 64);
+    cfg.gridDim = dim3(cl * 64);
     CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg),
                              "cudaOccupancyMaxActiveClusters(get_density)"));
     if (max_clusters < 1) return fail(CUDAPIC_ERR_NOT_SUPPORTED, "get_density: no resident cluster");
-    uint64_t need = ((uint64_t)g.capacity + 4ull * DENS_BLOCK - 1) / (4ull * DENS_BLOCK);
-    uint64_t clusters = std::min<uint64_t>((uint64_t)max_clusters,
-                                           std::max<uint64_t>(1, (need + DENS_CLUSTER - 1) / DENS_CLUSTER));
-    cfg.gridDim = dim3((unsigned)(clusters * DENS_CLUSTER));
-    CUDAPIC_CHECK(check_cuda(cudaLaunchKernelEx(&cfg, kern, x, density, n_active, g, L.copies),
-                             "launch get_density"));
+    const uint64_t want = (uint64_t)sm_count() * (uint64_t)t.density_ctas_per_sm / (uint64_t)cl;
+    const uint64_t need = ((uint64_t)g.capacity + 4ull * BLOCK - 1) / (4ull * BLOCK);
+    const uint64_t clusters = std::min(std::min((uint64_t)max_clusters, std::max<uint64_t>(1, want)),
+                                       std::max<uint64_t>(1, (need + cl - 1) / cl));
+    cfg.gridDim = dim3((unsigned)(clusters * cl));
+    CUDAPIC_CHECK(check_cuda(cudaLaunchKernelEx(&cfg, kern, x, density, n_active, g, copies), "launch get_density"));
     return CUDAPIC_OK;
+}
+
+template <bool VEC, typename Acc>
+int launch_density_acc(const float *x, float *density, const uint32_t *n_active, const cudapic_grid &g,
+                       cudaStream_t stream) {
+    const cudapic_tuning t = tuning();
+    switch (t.density_threads) {
+    case 256: return launch_density_t<256, VEC, Acc>(x, density, n_active, g, t, stream);
+    case 1024: return launch_density_t<1024, VEC, Acc>(x, density, n_active, g, t, stream);
+    default: return launch_density_t<512, VEC, Acc>(x, density, n_active, g, t, stream);
+    }
+}
+
+template <bool VEC>
+int launch_density(const float *x, float *density, const uint32_t *n_active, const cudapic_grid &g,
+                   cudaStream_t stream) {
+    if (g.flags & CUDAPIC_FLAG_DEPOSIT_FIXED_POINT) return launch_density_acc<VEC, u64>(x, density, n_active, g, stream);
+    return launch_density_acc<VEC, float>(x, density, n_active, g, stream);
 }
 
 }  // namespace

@@ -10,22 +10,33 @@
 // scattering.  The RNG draw order of the reference is kept exactly.
 //
 // B200 design: HBM-bound streaming (28 B read + 16 B RNG written per
-// particle, velocities written only by colliders, ~1-5 % per step):
-//  * persistent grid-stride loop, one particle per thread and iteration,
-//    coalesced SoA loads; the RNG state is held in registers for all draws;
-//  * sigma_tot gathers through the read-only path (__ldg: L1 / 126 MB L2
-//    resident 4 MB table); the per-process tables only for colliders;
+// particle; velocities written only by colliders, ~0.5 % of electrons per
+// step at the reference conditions):
+//  * persistent grid; the seven SoA input tiles of 512 particles (vx, vy,
+//    vz and the four RNG planes, 14 KB) are staged into shared memory by
+//    cp.async.bulk on an mbarrier, four stages deep;
+//  * pass 1 (every particle, uniform work): first draw(s), collision test;
+//    non-colliders store their advanced RNG state (coalesced);
+//  * colliders are appended to a shared-memory queue (index, RNG state,
+//    velocity, energy index); when it holds more than 256 entries, and at the
+//    end, the whole CTA drains it one collider per thread, so the long
+//    scattering path runs on full warps instead of one lane in 32;
+//  * sigma_tot gathers through the read-only path (the 4 MB table stays
+//    L2-resident); the per-process tables are read only by colliders;
 //  * ionization spawns claim slots with one warp-aggregated atomicAdd per
-//    counter (coalesced group of the ionizing lanes), bounded by capacity:
-//    a spawn that does not fit is dropped and flagged, never written
-//    out of bounds (the reference writes unbounded, :1132-1149);
+//    counter, bounded by capacity: a spawn that does not fit is dropped and
+//    flagged, never written out of bounds (the reference writes unbounded,
+//    :1132-1149);
 //  * transcendentals from detmath.cuh (bit-reproducible, see there).
+// One-particle-per-thread kernels without bulk copies serve pointers that
+// are not 16-byte aligned or capacities that are not a multiple of 4.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
 #include "detmath.cuh"
 #include "internal.h"
 #include "rng.cuh"
+#include "tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -81,165 +92,456 @@ __device__ __forceinline__ bool claim_slot(uint32_t *counter, uint32_t capacity,
     return grp.thread_rank() < granted;
 }
 
-template <bool EVENTS>
-__global__ void __launch_bounds__(MCC_THREADS)
-    check_collisions_e_kernel(const float *__restrict__ sigma_tot_e, const float *__restrict__ cs,
-                              const uint32_t *__restrict__ active_e, float *__restrict__ x,
-                              float *__restrict__ vx, float *__restrict__ vy, float *__restrict__ vz,
-                              uint32_t *__restrict__ rng0, uint32_t *__restrict__ rng1,
-                              uint32_t *__restrict__ rng2, uint32_t *__restrict__ rng3,
-                              float *__restrict__ ix, float *__restrict__ ivx, float *__restrict__ ivy,
-                              float *__restrict__ ivz, uint32_t *__restrict__ alive_e,
-                              uint32_t *__restrict__ alive_i, uint8_t *__restrict__ events,
-                              const cudapic_grid g) {
-    const uint32_t n = load_count(active_e, g.capacity, g.dev_err);
-    const uint32_t stride = gridDim.x * MCC_THREADS;
-    const float exc_j = 11.5f * E_CHARGE_F;
-    const float ion_j = 15.8f * E_CHARGE_F;
-    for (uint32_t i = blockIdx.x * MCC_THREADS + threadIdx.x; i < n; i += stride) {
-        Xoshiro128p rs{rng0[i], rng1[i], rng2[i], rng3[i]};
-        const float vxi = vx[i], vyi = vy[i], vzi = vz[i];
-        const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
-        const float energy = g.half_me_over_e * v2;
-        const uint32_t idx = energy_index(energy);
-        const float velocity = sqrtf(v2);
-        const float nu = __ldg(sigma_tot_e + idx) * velocity;
-        const float rand_val = rs.uniform();
-        const float p_coll = 1.0f - dm::expf_det(-nu * g.dt_e);
-        uint8_t ev = 0;
-        if (rand_val < p_coll) {
-            float gx = vxi, gy = vyi, gz = vzi;
-            float gm = sqrtf(gx * gx + gy * gy + gz * gz);
-            const float wx = g.f1 * vxi, wy = g.f1 * vyi, wz = g.f1 * vzi;
-            const float t0 = __ldg(cs + idx);
-            const float t1 = t0 + __ldg(cs + CS_RANGES + idx);
-            const float t2 = t1 + __ldg(cs + 2 * CS_RANGES + idx);
-            const Euler eu = euler_angles(gx, gy, gz);
-            float chi_s, chi_c, eta;
-            const float rnd = rs.uniform();
-            if (rnd < t0 / t2) {
-                ev = 1;  // elastic
-                const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
-                eta = TWO_PI_F * rs.uniform();
-                dm::sincosf_det(chi, &chi_s, &chi_c);
-            } else if (rnd < t1 / t2) {
-                ev = 2;  // excitation
-                float en = 0.5f * E_MASS_F * gm * gm;
-                en = fabsf(en - exc_j);
-                gm = sqrtf(2.0f * en / E_MASS_F);
-                const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
-                eta = TWO_PI_F * rs.uniform();
-                dm::sincosf_det(chi, &chi_s, &chi_c);
-            } else {
-                ev = 3;  // ionization
-                float en = 0.5f * E_MASS_F * gm * gm;
-                en = fabsf(en - ion_j);
-                const float e_new = 10.0f * dm::tanf_det(rs.uniform() * dm::atanf_det(en / E_CHARGE_F / 20.0f)) *
-                                    E_CHARGE_F;
-                const float e_orig = fabsf(en - e_new);
-                gm = sqrtf(2.0f * e_orig / E_MASS_F);
-                const float g_new = sqrtf(2.0f * e_new / E_MASS_F);
-                const float chi = dm::acosf_det(sqrtf(e_orig / en));
-                const float chi_new = dm::acosf_det(sqrtf(e_new / en));
-                eta = TWO_PI_F * rs.uniform();
-                const float eta_new = eta + PI_F;
-                float sc2, cc2, se2, ce2;
-                dm::sincosf_det(chi_new, &sc2, &cc2);
-                dm::sincosf_det(eta_new, &se2, &ce2);
-                float ngx, ngy, ngz;
-                rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
-                const float xi = x[i];
-                uint32_t slot;
-                if (claim_slot(alive_e, g.capacity, slot)) {
-                    x[slot] = xi;
-                    vx[slot] = wx + g.f2 * ngx;
-                    vy[slot] = wy + g.f2 * ngy;
-                    vz[slot] = wz + g.f2 * ngz;
-                } else {
-                    set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
-                }
-                float a, b, c;
-                rs.three_normal(g.normal_range, a, b, c);
-                if (claim_slot(alive_i, g.capacity, slot)) {
-                    ix[slot] = xi;
-                    ivx[slot] = a;
-                    ivy[slot] = b;
-                    ivz[slot] = c;
-                } else {
-                    set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
-                }
-                dm::sincosf_det(chi, &chi_s, &chi_c);
-            }
-            float se, ce;
-            dm::sincosf_det(eta, &se, &ce);
-            float ngx, ngy, ngz;
-            rotate(gm, chi_s, chi_c, se, ce, eu, ngx, ngy, ngz);
-            vx[i] = wx + g.f2 * ngx;
-            vy[i] = wy + g.f2 * ngy;
-            vz[i] = wz + g.f2 * ngz;
-        }
-        rng0[i] = rs.s0;
-        rng1[i] = rs.s1;
-        rng2[i] = rs.s2;
-        rng3[i] = rs.s3;
-        if (EVENTS) events[i] = ev;
-    }
+// Collision decision u < p with p = 1 - exp(-a), a = nu dt (the reference
+// evaluates exp(-nu * dt) with -nu * dt == -(nu * dt) exactly,
+// Rust-CUDA/src/main.rs:1011, 1196).  Since 1 - e^-a <= a, exp_det is
+// within 2 ulp and 1 - y is exact for y >= 1/2, the computed p never
+// exceeds a + 3.1e-7: any u >= fl(a + 5e-7) is a certain "no collision",
+// decided without evaluating exp (about 99 % of draws at the reference
+// conditions).  The decision is bit-identical to the full test.
+__device__ __forceinline__ bool collision_draw(float u, float a) {
+    if (u >= a + 5e-7f) return false;
+    const float p_coll = 1.0f - dm::expf_det(-a);
+    return u < p_coll;
 }
 
-template <bool EVENTS>
-__global__ void __launch_bounds__(MCC_THREADS)
-    check_collisions_i_kernel(const float *__restrict__ sigma_tot_i, const float *__restrict__ cs,
-                              const uint32_t *__restrict__ active_i, float *__restrict__ vx,
-                              float *__restrict__ vy, float *__restrict__ vz, uint32_t *__restrict__ rng0,
-                              uint32_t *__restrict__ rng1, uint32_t *__restrict__ rng2,
-                              uint32_t *__restrict__ rng3, uint8_t *__restrict__ events, const cudapic_grid g) {
-    const uint32_t n = load_count(active_i, g.capacity, g.dev_err);
-    const uint32_t stride = gridDim.x * MCC_THREADS;
-    for (uint32_t i = blockIdx.x * MCC_THREADS + threadIdx.x; i < n; i += stride) {
-        Xoshiro128p rs{rng0[i], rng1[i], rng2[i], rng3[i]};
-        float vxa, vya, vza;
-        rs.three_normal(g.normal_range, vxa, vya, vza);
-        const float vxi = vx[i], vyi = vy[i], vzi = vz[i];
-        const float gx = vxi - vxa, gy = vyi - vya, gz = vzi - vza;
-        const float g2 = gx * gx + gy * gy + gz * gz;
-        const float energy = g.half_mu_over_e * g2;
-        const uint32_t idx = energy_index(energy);
-        const float gmag = sqrtf(g2);
-        const float nu = __ldg(sigma_tot_i + idx) * gmag;
-        const float rand_val = rs.uniform();
-        const float p_coll = 1.0f - dm::expf_det(-nu * g.dt_i);
-        uint8_t ev = 0;
-        if (rand_val < p_coll) {
-            const float t0 = __ldg(cs + 3 * CS_RANGES + idx);
-            const float t1 = t0 + __ldg(cs + 4 * CS_RANGES + idx);
-            const float gg = sqrtf(gx * gx + gy * gy + gz * gz);
-            const float wx = 0.5f * (vxi + vxa), wy = 0.5f * (vyi + vya), wz = 0.5f * (vzi + vza);
-            const Euler eu = euler_angles(gx, gy, gz);
-            const float rnd = rs.uniform();
-            float chi;
-            if (rnd < t0 / t1) {
-                ev = 4;
-                chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
-            } else {
-                ev = 5;
-                chi = PI_F;
-            }
-            const float eta = TWO_PI_F * rs.uniform();
-            float sc, cc, se, ce;
-            dm::sincosf_det(chi, &sc, &cc);
-            dm::sincosf_det(eta, &se, &ce);
-            float ngx, ngy, ngz;
-            rotate(gg, sc, cc, se, ce, eu, ngx, ngy, ngz);
-            vx[i] = wx + 0.5f * ngx;
-            vy[i] = wy + 0.5f * ngy;
-            vz[i] = wz + 0.5f * ngz;
-        }
-        rng0[i] = rs.s0;
-        rng1[i] = rs.s1;
-        rng2[i] = rs.s2;
-        rng3[i] = rs.s3;
-        if (EVENTS) events[i] = ev;
+// Outcome of the collision test of one particle.
+struct Test {
+    uint32_t idx;
+    bool collide;
+};
+
+// sigma_tot lookups: straight from the global table (read-only path), or
+// from a shared-memory copy of its first `resident` entries.
+struct GlobalTable {
+    const float *__restrict__ t;
+    __device__ __forceinline__ float operator()(uint32_t idx) const { return __ldg(t + idx); }
+};
+struct ResidentTable {
+    const float *__restrict__ t;   // global table
+    const float *s;                // shared copy of t[0 .. resident)
+    uint32_t resident;
+    __device__ __forceinline__ float operator()(uint32_t idx) const {
+        return idx < resident ? s[idx] : __ldg(t + idx);
     }
+};
+
+// Electron collision test, Rust-CUDA/src/main.rs:992-1012 (one draw).
+template <typename Table>
+__device__ __forceinline__ Test test_electron(float vxi, float vyi, float vzi, Xoshiro128p &rs,
+                                              const Table &sigma_tot_e, const cudapic_grid &g) {
+    const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
+    const float energy = g.half_me_over_e * v2;
+    Test t;
+    t.idx = energy_index(energy);
+    const float velocity = sqrtf(v2);
+    const float nu = sigma_tot_e(t.idx) * velocity;
+    const float rand_val = rs.uniform();
+    t.collide = collision_draw(rand_val, nu * g.dt_e);
+    return t;
+}
+
+// collision_e, Rust-CUDA/src/main.rs:1035-1165: scatters electron i (state
+// rs already past the test draw), writes its velocity and any spawns;
+// returns the event (1 elastic, 2 excitation, 3 ionization).
+__device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
+                                                  Xoshiro128p &rs, const float *__restrict__ cs, float *x, float *vx,
+                                                  float *vy, float *vz, float *ix, float *ivx, float *ivy,
+                                                  float *ivz, uint32_t *alive_e, uint32_t *alive_i,
+                                                  const cudapic_grid &g) {
+    const float exc_j = 11.5f * E_CHARGE_F;
+    const float ion_j = 15.8f * E_CHARGE_F;
+    float gx = vxi, gy = vyi, gz = vzi;
+    float gm = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float wx = g.f1 * vxi, wy = g.f1 * vyi, wz = g.f1 * vzi;
+    const float t0 = __ldg(cs + idx);
+    const float t1 = t0 + __ldg(cs + CS_RANGES + idx);
+    const float t2 = t1 + __ldg(cs + 2 * CS_RANGES + idx);
+    const Euler eu = euler_angles(gx, gy, gz);
+    float chi_s, chi_c, eta;
+    uint32_t ev;
+    const float rnd = rs.uniform();
+    if (rnd < t0 / t2) {
+        ev = 1;  // elastic
+        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        eta = TWO_PI_F * rs.uniform();
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    } else if (rnd < t1 / t2) {
+        ev = 2;  // excitation
+        float en = 0.5f * E_MASS_F * gm * gm;
+        en = fabsf(en - exc_j);
+        gm = sqrtf(2.0f * en / E_MASS_F);
+        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        eta = TWO_PI_F * rs.uniform();
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    } else {
+        ev = 3;  // ionization
+        float en = 0.5f * E_MASS_F * gm * gm;
+        en = fabsf(en - ion_j);
+        const float e_new =
+            10.0f * dm::tanf_det(rs.uniform() * dm::atanf_det(en / E_CHARGE_F / 20.0f)) * E_CHARGE_F;
+        const float e_orig = fabsf(en - e_new);
+        gm = sqrtf(2.0f * e_orig / E_MASS_F);
+        const float g_new = sqrtf(2.0f * e_new / E_MASS_F);
+        const float chi = dm::acosf_det(sqrtf(e_orig / en));
+        const float chi_new = dm::acosf_det(sqrtf(e_new / en));
+        eta = TWO_PI_F * rs.uniform();
+        const float eta_new = eta + PI_F;
+        float sc2, cc2, se2, ce2;
+        dm::sincosf_det(chi_new, &sc2, &cc2);
+        dm::sincosf_det(eta_new, &se2, &ce2);
+        float ngx, ngy, ngz;
+        rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
+        const float xi = x[i];
+        uint32_t slot;
+        if (claim_slot(alive_e, g.capacity, slot)) {
+            x[slot] = xi;
+            vx[slot] = wx + g.f2 * ngx;
+            vy[slot] = wy + g.f2 * ngy;
+            vz[slot] = wz + g.f2 * ngz;
+        } else {
+            set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
+        }
+        float a, b, c;
+        rs.three_normal(g.normal_range, a, b, c);
+        if (claim_slot(alive_i, g.capacity, slot)) {
+            ix[slot] = xi;
+            ivx[slot] = a;
+            ivy[slot] = b;
+            ivz[slot] = c;
+        } else {
+            set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
+        }
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    }
+    float se, ce;
+    dm::sincosf_det(eta, &se, &ce);
+    float ngx, ngy, ngz;
+    rotate(gm, chi_s, chi_c, se, ce, eu, ngx, ngy, ngz);
+    vx[i] = wx + g.f2 * ngx;
+    vy[i] = wy + g.f2 * ngy;
+    vz[i] = wz + g.f2 * ngz;
+    return ev;
+}
+
+struct IonTest {
+    uint32_t idx;
+    float vxa, vya, vza;
+    bool collide;
+};
+
+// Ion collision test with a Maxwellian target, Rust-CUDA/src/main.rs:1180-1197.
+template <typename Table>
+__device__ __forceinline__ IonTest test_ion(float vxi, float vyi, float vzi, Xoshiro128p &rs,
+                                            const Table &sigma_tot_i, const cudapic_grid &g) {
+    IonTest t;
+    rs.three_normal(g.normal_range, t.vxa, t.vya, t.vza);
+    const float gx = vxi - t.vxa, gy = vyi - t.vya, gz = vzi - t.vza;
+    const float g2 = gx * gx + gy * gy + gz * gz;
+    const float energy = g.half_mu_over_e * g2;
+    t.idx = energy_index(energy);
+    const float gmag = sqrtf(g2);
+    const float nu = sigma_tot_i(t.idx) * gmag;
+    const float rand_val = rs.uniform();
+    t.collide = collision_draw(rand_val, nu * g.dt_i);
+    return t;
+}
+
+// collision_i, Rust-CUDA/src/main.rs:1221-1292; returns 4 isotropic, 5 backscatter.
+__device__ __noinline__ uint32_t collide_ion(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi, float vxa,
+                                             float vya, float vza, Xoshiro128p &rs, const float *__restrict__ cs,
+                                             float *vx, float *vy, float *vz, const cudapic_grid &g) {
+    const float gx = vxi - vxa, gy = vyi - vya, gz = vzi - vza;
+    const float t0 = __ldg(cs + 3 * CS_RANGES + idx);
+    const float t1 = t0 + __ldg(cs + 4 * CS_RANGES + idx);
+    const float gg = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float wx = 0.5f * (vxi + vxa), wy = 0.5f * (vyi + vya), wz = 0.5f * (vzi + vza);
+    const Euler eu = euler_angles(gx, gy, gz);
+    const float rnd = rs.uniform();
+    float chi;
+    uint32_t ev;
+    if (rnd < t0 / t1) {
+        ev = 4;
+        chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+    } else {
+        ev = 5;
+        chi = PI_F;
+    }
+    const float eta = TWO_PI_F * rs.uniform();
+    float sc, cc, se, ce;
+    dm::sincosf_det(chi, &sc, &cc);
+    dm::sincosf_det(eta, &se, &ce);
+    float ngx, ngy, ngz;
+    rotate(gg, sc, cc, se, ce, eu, ngx, ngy, ngz);
+    vx[i] = wx + 0.5f * ngx;
+    vy[i] = wy + 0.5f * ngy;
+    vz[i] = wz + 0.5f * ngz;
+    return ev;
+}
+
+// ------------------------------------------------------------------ bulk-copy kernels
+
+constexpr int MT_U = 2;                       // particles per thread and tile
+constexpr int MT_TILE = MCC_THREADS * MT_U;   // 512
+constexpr int MT_MAX_STAGES = 4;              // pipeline depth: cudapic_tuning.mcc_stages
+constexpr int MT_ARRAYS = 7;                  // vx, vy, vz, rng0..3
+constexpr int MT_QFLUSH = 256;                // drain the queue when it holds more
+constexpr int MT_QCAP = MT_QFLUSH + MT_TILE;  // never overflows: one tile adds <= 512
+constexpr int MT_QWORDS = 5;                  // slot index + the RNG state before the test
+
+size_t mcc_tma_smem_bytes(int stages) {
+    return (size_t)stages * MT_ARRAYS * MT_TILE * 4 + (size_t)MT_QCAP * MT_QWORDS * 4 +
+           (size_t)stages * sizeof(uint64_t);
+}
+
+// ION = false: check_collisions_e; ION = true: check_collisions_i.
+// A queued collider keeps only its slot and its RNG state before the test;
+// the drain re-runs the (deterministic) test from that state, reading the
+// velocity again, and continues into the scattering.
+template <bool ION, bool EVENTS>
+__global__ void __launch_bounds__(MCC_THREADS, 4)
+    check_collisions_tma_kernel(const float *__restrict__ sigma_tot, const float *__restrict__ cs,
+                                const uint32_t *__restrict__ active, float *x, float *vx, float *vy, float *vz,
+                                uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *ix,
+                                float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i,
+                                uint8_t *events, const __grid_constant__ cudapic_grid g, int stages) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint32_t *in = reinterpret_cast<uint32_t *>(smem);             // [stages][7][TILE]
+    uint32_t *queue = in + stages * MT_ARRAYS * MT_TILE;           // [5][QCAP]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(queue + MT_QWORDS * MT_QCAP);
+    __shared__ uint32_t s_q;
+    __shared__ int s_ready;
+
+    const int tid = threadIdx.x;
+    const uint32_t n = load_count(active, g.capacity, g.dev_err);
+    const uint32_t ntiles = (n + MT_TILE - 1) / MT_TILE;
+    const void *src[MT_ARRAYS] = {vx, vy, vz, rng0, rng1, rng2, rng3};
+
+    auto issue = [&](uint32_t tile, int stage) {
+        const uint32_t t0 = tile * MT_TILE;
+        const uint32_t cnt = min((uint32_t)MT_TILE, n - t0);
+        const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;
+        mbar_arrive_expect_tx(&bar[stage], MT_ARRAYS * bytes);
+#pragma unroll
+        for (int a = 0; a < MT_ARRAYS; ++a)
+            bulk_load(in + (stage * MT_ARRAYS + a) * MT_TILE, static_cast<const uint32_t *>(src[a]) + t0, bytes,
+                      &bar[stage]);
+    };
+
+    const GlobalTable table{sigma_tot};
+    // Drains the collider queue: one collider per thread, full warps.
+    auto drain = [&]() {
+        const uint32_t qn = s_q;
+        for (uint32_t q = tid; q < qn; q += MCC_THREADS) {
+            const uint32_t i = queue[0 * MT_QCAP + q];
+            Xoshiro128p rs{queue[1 * MT_QCAP + q], queue[2 * MT_QCAP + q], queue[3 * MT_QCAP + q],
+                           queue[4 * MT_QCAP + q]};
+            const float vxi = vx[i], vyi = vy[i], vzi = vz[i];
+            uint32_t ev;
+            if (ION) {
+                const IonTest t = test_ion(vxi, vyi, vzi, rs, table, g);
+                ev = collide_ion(i, t.idx, vxi, vyi, vzi, t.vxa, t.vya, t.vza, rs, cs, vx, vy, vz, g);
+            } else {
+                const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
+                ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
+                                      alive_i, g);
+            }
+            rng0[i] = rs.s0;
+            rng1[i] = rs.s1;
+            rng2[i] = rs.s2;
+            rng3[i] = rs.s3;
+            if (EVENTS) events[i] = (uint8_t)ev;
+        }
+        __syncthreads();
+        if (tid == 0) s_q = 0;
+        __syncthreads();
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+        s_q = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) {
+            const uint32_t tile = blockIdx.x + (uint32_t)s * gridDim.x;
+            if (tile < ntiles) issue(tile, s);
+        }
+    }
+
+    uint32_t it = 0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int s = (int)(it % (uint32_t)stages);
+        const uint32_t parity = (it / (uint32_t)stages) & 1u;
+        if (tid == 0) {
+            const int ok = mbar_wait_bounded(&bar[s], parity) ? 1 : 0;
+            if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
+            s_ready = ok;
+        }
+        __syncthreads();
+        if (!s_ready) return;
+        const uint32_t t0 = tile * MT_TILE;
+        const uint32_t cnt = min((uint32_t)MT_TILE, n - t0);
+        const uint32_t *b = in + s * MT_ARRAYS * MT_TILE;
+#pragma unroll
+        for (int u = 0; u < MT_U; ++u) {
+            const uint32_t j = (uint32_t)u * MCC_THREADS + tid;
+            if (j < cnt) {
+                const uint32_t i = t0 + j;
+                const uint32_t q0 = b[3 * MT_TILE + j], q1 = b[4 * MT_TILE + j], q2 = b[5 * MT_TILE + j],
+                               q3 = b[6 * MT_TILE + j];
+                Xoshiro128p rs{q0, q1, q2, q3};
+                const float vxi = __uint_as_float(b[0 * MT_TILE + j]);
+                const float vyi = __uint_as_float(b[1 * MT_TILE + j]);
+                const float vzi = __uint_as_float(b[2 * MT_TILE + j]);
+                bool collide;
+                if (ION) collide = test_ion(vxi, vyi, vzi, rs, table, g).collide;
+                else collide = test_electron(vxi, vyi, vzi, rs, table, g).collide;
+                if (collide) {
+                    const uint32_t q = atomicAdd(&s_q, 1u);
+                    queue[0 * MT_QCAP + q] = i;
+                    queue[1 * MT_QCAP + q] = q0;
+                    queue[2 * MT_QCAP + q] = q1;
+                    queue[3 * MT_QCAP + q] = q2;
+                    queue[4 * MT_QCAP + q] = q3;
+                } else {
+                    rng0[i] = rs.s0;
+                    rng1[i] = rs.s1;
+                    rng2[i] = rs.s2;
+                    rng3[i] = rs.s3;
+                    if (EVENTS) events[i] = 0;
+                }
+            }
+        }
+        __syncthreads();  // stage consumed; queue count visible
+        if (tid == 0) {
+            const uint32_t next = tile + (uint32_t)stages * gridDim.x;
+            if (next < ntiles) issue(next, s);
+        }
+        if (s_q > (uint32_t)MT_QFLUSH) drain();
+    }
+    __syncthreads();
+    if (s_q > 0) drain();
+}
+
+// ------------------------------------------------------------------ resident-table kernels
+//
+// One 1024-thread CTA per SM, no bulk copies and no block barrier in the
+// main loop:
+//  * the first MR_RESIDENT entries of sigma_tot (energies below 32.768 eV,
+//    where almost every particle sits) are copied into shared memory once
+//    per launch; the collision-frequency gather becomes a shared load
+//    (higher energies still read the global table);
+//  * each thread issues the 7 loads of MR_U particles before any compute;
+//  * colliders go to a queue private to their warp (slot and RNG state
+//    before the test); whenever it holds 32 the warp drains 32 of them, one
+//    per lane -- only __syncwarp, no block-wide synchronisation.
+// Plain loads: no alignment requirement on any pointer.
+
+constexpr int MR_THREADS = 1024;
+constexpr int MR_WARPS = MR_THREADS / 32;
+constexpr int MR_U = 2;                        // particles per thread and iteration
+constexpr uint32_t MR_RESIDENT = 32768;        // sigma_tot entries kept in shared memory
+constexpr int MR_QCAP = 32 + 32 * MR_U;        // a warp drains at 32; one iteration adds <= 64
+constexpr size_t MR_SMEM = MR_RESIDENT * sizeof(float) + (size_t)MR_WARPS * 5 * MR_QCAP * sizeof(uint32_t);
+
+template <bool ION, bool EVENTS>
+__global__ void __launch_bounds__(MR_THREADS, 1)
+    check_collisions_resident_kernel(const float *__restrict__ sigma_tot, const float *__restrict__ cs,
+                                     const uint32_t *__restrict__ active, float *x, float *vx, float *vy,
+                                     float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
+                                     float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive_e,
+                                     uint32_t *alive_i, uint8_t *events, const __grid_constant__ cudapic_grid g) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *tab = reinterpret_cast<float *>(smem);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    uint32_t *wq = reinterpret_cast<uint32_t *>(tab + MR_RESIDENT) + (size_t)warp * 5 * MR_QCAP;  // [5][QCAP]
+    const unsigned lt = lanemask_lt();
+
+    for (uint32_t k = tid; k < MR_RESIDENT; k += MR_THREADS) tab[k] = __ldg(sigma_tot + k);
+    __syncthreads();
+    const ResidentTable table{sigma_tot, tab, MR_RESIDENT};
+    const uint32_t n = load_count(active, g.capacity, g.dev_err);
+
+    auto drain = [&](uint32_t first, uint32_t count) {  // lanes < count take entries first + lane
+        if ((uint32_t)lane < count) {
+            const uint32_t q = first + lane;
+            const uint32_t i = wq[0 * MR_QCAP + q];
+            Xoshiro128p rs{wq[1 * MR_QCAP + q], wq[2 * MR_QCAP + q], wq[3 * MR_QCAP + q], wq[4 * MR_QCAP + q]};
+            const float vxi = vx[i], vyi = vy[i], vzi = vz[i];
+            uint32_t ev;
+            if (ION) {
+                const IonTest t = test_ion(vxi, vyi, vzi, rs, table, g);
+                ev = collide_ion(i, t.idx, vxi, vyi, vzi, t.vxa, t.vya, t.vza, rs, cs, vx, vy, vz, g);
+            } else {
+                const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
+                ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
+                                      alive_i, g);
+            }
+            rng0[i] = rs.s0;
+            rng1[i] = rs.s1;
+            rng2[i] = rs.s2;
+            rng3[i] = rs.s3;
+            if (EVENTS) events[i] = (uint8_t)ev;
+        }
+        __syncwarp();
+    };
+
+    uint32_t qn = 0;  // entries in this warp's queue (warp-uniform)
+    const uint32_t step = gridDim.x * (uint32_t)(MR_THREADS * MR_U);
+    for (uint32_t base = blockIdx.x * (uint32_t)(MR_THREADS * MR_U); base < n; base += step) {
+        uint32_t s[MR_U][4];
+        float v[MR_U][3];
+#pragma unroll
+        for (int u = 0; u < MR_U; ++u) {
+            const uint32_t i = base + (uint32_t)u * MR_THREADS + tid;
+            if (i < n) {
+                s[u][0] = rng0[i];
+                s[u][1] = rng1[i];
+                s[u][2] = rng2[i];
+                s[u][3] = rng3[i];
+                v[u][0] = vx[i];
+                v[u][1] = vy[i];
+                v[u][2] = vz[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < MR_U; ++u) {
+            const uint32_t i = base + (uint32_t)u * MR_THREADS + tid;
+            bool collide = false;
+            if (i < n) {
+                Xoshiro128p rs{s[u][0], s[u][1], s[u][2], s[u][3]};
+                if (ION) collide = test_ion(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
+                else collide = test_electron(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
+                if (!collide) {
+                    rng0[i] = rs.s0;
+                    rng1[i] = rs.s1;
+                    rng2[i] = rs.s2;
+                    rng3[i] = rs.s3;
+                    if (EVENTS) events[i] = 0;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, collide);
+            if (collide) {
+                const uint32_t q = qn + __popc(m & lt);
+                wq[0 * MR_QCAP + q] = i;
+                wq[1 * MR_QCAP + q] = s[u][0];
+                wq[2 * MR_QCAP + q] = s[u][1];
+                wq[3 * MR_QCAP + q] = s[u][2];
+                wq[4 * MR_QCAP + q] = s[u][3];
+            }
+            qn += __popc(m);
+        }
+        __syncwarp();
+        while (qn >= 32) {  // full-warp drains from the top of the queue
+            qn -= 32;
+            drain(qn, 32);
+        }
+    }
+    if (qn) drain(0, qn);
 }
 
 // accumulate_eepf, Rust-CUDA/src/main.rs:1301-1339: per-block shared
@@ -272,45 +574,90 @@ __global__ void __launch_bounds__(256)
         if (h[k]) atomicAdd(&eepf[k], h[k]);
 }
 
-int mcc_grid(uint32_t capacity, const void *kernel) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, MCC_THREADS, 0) != cudaSuccess) per_sm = 4;
-    per_sm = std::max(per_sm, 1);
-    const uint64_t need = ((uint64_t)capacity + MCC_THREADS - 1) / MCC_THREADS;
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, need));
+namespace {
+
+bool tma_ready(uint32_t capacity, std::initializer_list<const void *> ptrs) {
+    if (capacity % 4u) return false;
+    for (const void *p : ptrs)
+        if (!aligned16(p)) return false;
+    return true;
 }
+
+template <bool ION, bool EVENTS>
+int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
+               float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx, float *ivy,
+               float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events, const cudapic_grid &g,
+               cudaStream_t stream) {
+    auto kern = check_collisions_tma_kernel<ION, EVENTS>;
+    const cudapic_tuning t = tuning();
+    const int stages = std::min(std::max(t.mcc_stages, 2), MT_MAX_STAGES);
+    const size_t smem = mcc_tma_smem_bytes(stages);
+    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                             "cudaFuncSetAttribute(check_collisions)"));
+    int per_sm = 0;
+    CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MCC_THREADS, smem),
+                             "occupancy(check_collisions)"));
+    per_sm = std::min(std::max(per_sm, 1), t.mcc_ctas_per_sm);
+    const uint64_t tiles_max = ((uint64_t)g.capacity + MT_TILE - 1) / MT_TILE;
+    const unsigned grid = persistent_grid(per_sm, tiles_max);
+    kern<<<grid, MCC_THREADS, smem, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
+                                              alive_e, alive_i, events, g, stages);
+    return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
+}
+
+template <bool ION, bool EVENTS>
+int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
+                    float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx,
+                    float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
+                    const cudapic_grid &g, cudaStream_t stream) {
+    auto kern = check_collisions_resident_kernel<ION, EVENTS>;
+    if (MR_SMEM > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_NOT_SUPPORTED, "check_collisions: shared memory");
+    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MR_SMEM),
+                             "cudaFuncSetAttribute(check_collisions resident)"));
+    const uint64_t chunks = ((uint64_t)g.capacity + MR_THREADS * MR_U - 1) / (MR_THREADS * MR_U);
+    kern<<<persistent_grid(1, chunks), MR_THREADS, MR_SMEM, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1,
+                                                                      r2, r3, ix, ivx, ivy, ivz, alive_e, alive_i,
+                                                                      events, g);
+    return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
+}
+
+// Variant choice: the bulk-copy kernel needs 16-byte aligned planes and a
+// capacity that is a multiple of 4; the resident-table kernel takes anything.
+template <bool ION>
+int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx,
+                      float *vy, float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix,
+                      float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
+                      const cudapic_grid &g, cudaStream_t stream) {
+    const bool bulk = tuning().mcc_variant == 2 && tma_ready(g.capacity, {vx, vy, vz, r0, r1, r2, r3});
+    if (bulk) {
+        if (events)
+            return launch_tma<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
+                                         alive_e, alive_i, events, g, stream);
+        return launch_tma<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
+                                      alive_e, alive_i, nullptr, g, stream);
+    }
+    if (events)
+        return launch_resident<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
+                                          alive_e, alive_i, events, g, stream);
+    return launch_resident<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
+                                       alive_e, alive_i, nullptr, g, stream);
+}
+
+}  // namespace
 
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
                         uint8_t *events, const cudapic_grid &g, cudaStream_t stream) {
-    if (events) {
-        auto k = check_collisions_e_kernel<true>;
-        k<<<mcc_grid(g.capacity, (const void *)k), MCC_THREADS, 0, stream>>>(
-            total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz, alive_e,
-            alive_i, events, g);
-    } else {
-        auto k = check_collisions_e_kernel<false>;
-        k<<<mcc_grid(g.capacity, (const void *)k), MCC_THREADS, 0, stream>>>(
-            total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz, alive_e,
-            alive_i, nullptr, g);
-    }
-    return check_launch("check_collisions_e");
+    return launch_collisions<false>(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
+                                    i_vz, alive_e, alive_i, events, g, stream);
 }
 
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
                         const cudapic_grid &g, cudaStream_t stream) {
-    if (events) {
-        auto k = check_collisions_i_kernel<true>;
-        k<<<mcc_grid(g.capacity, (const void *)k), MCC_THREADS, 0, stream>>>(total_cs_i, cs, active_i, vx, vy, vz,
-                                                                               rng0, rng1, rng2, rng3, events, g);
-    } else {
-        auto k = check_collisions_i_kernel<false>;
-        k<<<mcc_grid(g.capacity, (const void *)k), MCC_THREADS, 0, stream>>>(total_cs_i, cs, active_i, vx, vy, vz,
-                                                                               rng0, rng1, rng2, rng3, nullptr, g);
-    }
-    return check_launch("check_collisions_i");
+    return launch_collisions<true>(total_cs_i, cs, active_i, nullptr, vx, vy, vz, rng0, rng1, rng2, rng3, nullptr,
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream);
 }
 
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,

@@ -6,20 +6,22 @@
 // survivors appended to dst at a block base from one atomicAdd on
 // alive_counter; order across blocks is unspecified (as in the reference).
 //
-// B200 design (HBM-bound, 16 B read + 16 B written per survivor):
-//  * persistent grid, 256 threads, tiles of 2048 particles;
-//  * the four SoA input tiles (x, vx, vy, vz: 4 x 8 KB) are staged into
-//    shared memory by cp.async.bulk (TMA bulk copies) on an mbarrier,
-//    double-buffered so the next tile streams in while this one computes;
-//  * the field E[N_G] sits in shared memory for the gathers;
-//  * each thread takes 4 consecutive particles of each 1024-particle row
-//    (conflict-free float4 shared loads); per-thread survivor counts of
-//    both rows are packed into one int and scanned once across the block
-//    (warp shuffles + one warp over the 8 warp totals);
-//  * one atomicAdd per tile on alive_counter;
-//  * survivors are compacted into a shared output tile, then written with
-//    fully coalesced stores.
-// A simple one-particle-per-thread variant (ballot/popc, reference layout)
+// B200 design (HBM-bound: 16 B read per particle, 16 B written per survivor):
+//  * persistent grid, 256 threads, tiles of 1024 particles;
+//  * the four SoA input tiles (x, vx, vy, vz: 4 x 4 KB) are staged into
+//    shared memory by cp.async.bulk (TMA bulk copies) completing on an
+//    mbarrier, four stages deep, so three tiles stream in while one computes;
+//  * E[N_G] is held in shared memory for the gathers;
+//  * thread t owns particles t, t+256, t+512, t+768 of a tile (conflict-free
+//    shared loads); a warp ballot per row gives each surviving lane its rank,
+//    one warp scans the 4 x 8 (row, warp) counts, so a (row, warp)'s survivors
+//    are written to consecutive slots: coalesced stores straight from
+//    registers, no output staging;
+//  * two block barriers per tile; the tile's atomicAdd on alive_counter is
+//    issued at the end of one iteration and its result consumed in the next,
+//    after the next tile's wait and compute, so its latency is hidden.
+// Within a tile, survivors keep their order.
+// A one-particle-per-thread variant (ballot/popc, the reference's layout)
 // serves pointers that are not 16-byte aligned or capacities that are not
 // a multiple of 4.
 #include "common.cuh"
@@ -30,9 +32,9 @@ namespace cudapic {
 
 constexpr int MC_THREADS = 256;
 constexpr int MC_WARPS = MC_THREADS / 32;
-constexpr int MC_ROW = MC_THREADS * 4;   // 1024 particles per row
-constexpr int MC_TILE = 2 * MC_ROW;      // 2048 particles per tile
-constexpr int MC_STAGES = 2;
+constexpr int MC_U = 4;                          // particles per thread and tile
+constexpr int MC_TILE = MC_THREADS * MC_U;       // 1024
+constexpr int MC_MAX_STAGES = 6;                 // pipeline depth: cudapic_tuning.push_stages
 
 struct PushResult {
     float x, vx;
@@ -53,25 +55,32 @@ __device__ __forceinline__ PushResult push_one(float xi, float vxi, const float 
     return r;
 }
 
+// Survivors of one tile held in registers until their base is known.
+struct TileOut {
+    float x[MC_U], vx[MC_U], vy[MC_U], vz[MC_U];
+    uint32_t lane_off[MC_U];
+    uint32_t keep;  // bit u: particle of row u survives
+};
+
 __global__ void __launch_bounds__(MC_THREADS)
     move_and_compact_tma_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
                                 const float *__restrict__ svx, const float *__restrict__ svy,
                                 const float *__restrict__ svz, float *__restrict__ dx_,
                                 float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
-                                float factor, float dt, const cudapic_grid g, uint32_t ef_pad) {
+                                float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float *in = reinterpret_cast<float *>(smem);            // [STAGES][4][TILE]
-    float *out = in + MC_STAGES * 4 * MC_TILE;               // [4][TILE]
-    float *ef = out + 4 * MC_TILE;                           // [ef_pad]
+    float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
+    float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
     uint64_t *bar = reinterpret_cast<uint64_t *>(ef + ef_pad);
-    __shared__ uint32_t wsum[MC_WARPS];
-    __shared__ uint32_t s_base, s_tot0, s_total;
+    __shared__ uint32_t offs[2][MC_U * MC_WARPS];        // counts, then exclusive offsets
+    __shared__ uint32_t s_base[2];
     __shared__ int s_ready;
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
+    const unsigned lt = lanemask_lt();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     const uint32_t ntiles = (n + MC_TILE - 1) / MC_TILE;
     const float *src[4] = {sx, svx, svy, svz};
@@ -87,122 +96,107 @@ __global__ void __launch_bounds__(MC_THREADS)
     };
 
     if (tid == 0) {
-#pragma unroll
-        for (int s = 0; s < MC_STAGES; ++s) mbar_init(&bar[s], 1);
+        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
         fence_mbar_init();
     }
     for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
     __syncthreads();
     if (tid == 0) {
-        for (int s = 0; s < MC_STAGES; ++s) {
-            uint32_t tile = blockIdx.x + (uint32_t)s * gridDim.x;
+        for (int s = 0; s < stages; ++s) {
+            const uint32_t tile = blockIdx.x + (uint32_t)s * gridDim.x;
             if (tile < ntiles) issue(tile, s);
         }
     }
 
+    TileOut prev;
+    bool have_prev = false;
+    uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int s = (int)(it % MC_STAGES);
-        const uint32_t parity = (it / MC_STAGES) & 1u;
-        // One thread waits (bounded) on the stage's barrier and publishes the
-        // verdict, so that a timeout makes the whole CTA leave together.
+        const int s = (int)(it % (uint32_t)stages);
+        const uint32_t parity = (it / (uint32_t)stages) & 1u;
+        // (1) the stage's bulk copies have landed (one bounded waiter, uniform verdict)
         if (tid == 0) {
-            int ok = mbar_wait_bounded(&bar[s], parity) ? 1 : 0;
-            if (!ok) {
-                set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
-                // the other stage's copy, if one was issued, must land before exit
-                if (tile + gridDim.x < ntiles) mbar_wait_bounded(&bar[s ^ 1], ((it + 1) / MC_STAGES) & 1u);
-            }
+            const int ok = mbar_wait_bounded(&bar[s], parity) ? 1 : 0;
+            if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
             s_ready = ok;
         }
         __syncthreads();
         if (!s_ready) return;
+
         const uint32_t t0 = tile * MC_TILE;
         const uint32_t cnt = min((uint32_t)MC_TILE, n - t0);
         const float *bx = in + (s * 4 + 0) * MC_TILE;
         const float *bvx = in + (s * 4 + 1) * MC_TILE;
         const float *bvy = in + (s * 4 + 2) * MC_TILE;
         const float *bvz = in + (s * 4 + 3) * MC_TILE;
-
-        float ox[8], ovx[8], ovy[8], ovz[8];
-        uint32_t keep = 0;
+        TileOut cur;
+        cur.keep = 0;
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const uint32_t j = (uint32_t)r * MC_ROW + 4u * (uint32_t)tid;
-            const float4 X = *reinterpret_cast<const float4 *>(bx + j);
-            const float4 VX = *reinterpret_cast<const float4 *>(bvx + j);
-            const float4 VY = *reinterpret_cast<const float4 *>(bvy + j);
-            const float4 VZ = *reinterpret_cast<const float4 *>(bvz + j);
-            const float xs[4] = {X.x, X.y, X.z, X.w};
-            const float vxs[4] = {VX.x, VX.y, VX.z, VX.w};
-            const float vys[4] = {VY.x, VY.y, VY.z, VY.w};
-            const float vzs[4] = {VZ.x, VZ.y, VZ.z, VZ.w};
+        for (int u = 0; u < MC_U; ++u) {
+            const uint32_t j = (uint32_t)u * MC_THREADS + tid;
+            bool keep = false;
+            cur.x[u] = cur.vx[u] = cur.vy[u] = cur.vz[u] = 0.0f;
+            if (j < cnt) {
+                const PushResult pr = push_one(bx[j], bvx[j], ef, factor, dt, g);
+                keep = pr.keep;
+                cur.x[u] = pr.x;
+                cur.vx[u] = pr.vx;
+                cur.vy[u] = bvy[j];
+                cur.vz[u] = bvz[j];
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            cur.lane_off[u] = __popc(m & lt);
+            if (keep) cur.keep |= 1u << u;
+            if (lane == 0) offs[it & 1][u * MC_WARPS + warp] = __popc(m);
+        }
+        // publish the previous tile's base (its atomic had this iteration to return)
+        if (have_prev && warp == 0 && lane == 31) s_base[(it - 1) & 1] = pending_base;
+        __syncthreads();  // (2) counts and previous base visible; stage s consumed
+        if (tid == 0) {
+            const uint32_t next = tile + (uint32_t)stages * gridDim.x;
+            if (next < ntiles) issue(next, s);
+        }
+        if (have_prev) {
+            const uint32_t base = s_base[(it - 1) & 1];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int o = r * 4 + q;
-                if (j + q < cnt) {
-                    PushResult pr = push_one(xs[q], vxs[q], ef, factor, dt, g);
-                    ox[o] = pr.x;
-                    ovx[o] = pr.vx;
-                    ovy[o] = vys[q];
-                    ovz[o] = vzs[q];
-                    if (pr.keep) keep |= 1u << o;
-                } else {
-                    ox[o] = ovx[o] = ovy[o] = ovz[o] = 0.0f;
+            for (int u = 0; u < MC_U; ++u) {
+                if (prev.keep & (1u << u)) {
+                    const uint32_t slot = base + offs[(it - 1) & 1][u * MC_WARPS + warp] + prev.lane_off[u];
+                    dx_[slot] = prev.x[u];
+                    dvx[slot] = prev.vx[u];
+                    dvy[slot] = prev.vy[u];
+                    dvz[slot] = prev.vz[u];
                 }
             }
         }
-        const uint32_t packed = (uint32_t)__popc(keep & 0xfu) | ((uint32_t)__popc(keep >> 4) << 16);
-        uint32_t incl = packed;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) wsum[warp] = incl;
-        __syncthreads();  // (A) stage s fully read; warp totals visible
-        if (tid == 0) {
-            const uint32_t next = tile + (uint32_t)MC_STAGES * gridDim.x;
-            if (next < ntiles) issue(next, s);
-        }
         if (warp == 0) {
-            uint32_t w = lane < MC_WARPS ? wsum[lane] : 0u;
+            const uint32_t v = offs[it & 1][lane];   // MC_U * MC_WARPS == 32
+            uint32_t incl = v;
 #pragma unroll
-            for (int o = 1; o < MC_WARPS; o <<= 1) {
-                uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-            if (lane < MC_WARPS) wsum[lane] = w;
-            if (lane == MC_WARPS - 1) {
-                const uint32_t tot0 = w & 0xffffu;
-                const uint32_t total = tot0 + (w >> 16);
-                s_tot0 = tot0;
-                s_total = total;
-                s_base = total ? atomicAdd(alive, total) : 0u;
-            }
+            offs[it & 1][lane] = incl - v;
+            if (lane == 31) pending_base = incl ? atomicAdd(alive, incl) : 0u;
         }
-        __syncthreads();  // (B)
-        const uint32_t excl = incl - packed + (warp > 0 ? wsum[warp - 1] : 0u);
-        uint32_t off0 = excl & 0xffffu;
-        uint32_t off1 = s_tot0 + (excl >> 16);
+        prev = cur;
+        have_prev = true;
+    }
+    if (have_prev && warp == 0 && lane == 31) s_base[(it - 1) & 1] = pending_base;
+    __syncthreads();
+    if (have_prev) {
+        const uint32_t base = s_base[(it - 1) & 1];
 #pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            if (keep & (1u << o)) {
-                const uint32_t dst = o < 4 ? off0++ : off1++;
-                out[0 * MC_TILE + dst] = ox[o];
-                out[1 * MC_TILE + dst] = ovx[o];
-                out[2 * MC_TILE + dst] = ovy[o];
-                out[3 * MC_TILE + dst] = ovz[o];
+        for (int u = 0; u < MC_U; ++u) {
+            if (prev.keep & (1u << u)) {
+                const uint32_t slot = base + offs[(it - 1) & 1][u * MC_WARPS + warp] + prev.lane_off[u];
+                dx_[slot] = prev.x[u];
+                dvx[slot] = prev.vx[u];
+                dvy[slot] = prev.vy[u];
+                dvz[slot] = prev.vz[u];
             }
-        }
-        __syncthreads();  // (C)
-        const uint32_t total = s_total;
-        const uint32_t base = s_base;
-        for (uint32_t j = tid; j < total; j += MC_THREADS) {
-            dx_[base + j] = out[0 * MC_TILE + j];
-            dvx[base + j] = out[1 * MC_TILE + j];
-            dvy[base + j] = out[2 * MC_TILE + j];
-            dvz[base + j] = out[3 * MC_TILE + j];
         }
     }
 }
@@ -219,11 +213,11 @@ __global__ void __launch_bounds__(MCS_THREADS)
                                    float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                    uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
                                    float factor, float dt, const cudapic_grid g) {
-    extern __shared__ float ef[];
+    extern __shared__ float ef_s[];
     __shared__ uint32_t wsum[MCS_WARPS];
     __shared__ uint32_t s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (uint32_t k = tid; k < g.n_g; k += MCS_THREADS) ef[k] = efield[k];
+    for (uint32_t k = tid; k < g.n_g; k += MCS_THREADS) ef_s[k] = efield[k];
     __syncthreads();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     if (g.work && blockIdx.x == 0 && tid == 0) atomicAdd(g.work, (unsigned long long)n);
@@ -233,7 +227,7 @@ __global__ void __launch_bounds__(MCS_THREADS)
         PushResult pr = {0.0f, 0.0f, false};
         float vy = 0.0f, vz = 0.0f;
         if (i < n) {
-            pr = push_one(sx[i], svx[i], ef, factor, dt, g);
+            pr = push_one(sx[i], svx[i], ef_s, factor, dt, g);
             if (pr.keep) {
                 vy = svy[i];
                 vz = svz[i];
@@ -268,10 +262,10 @@ __global__ void __launch_bounds__(MCS_THREADS)
 
 namespace {
 
-size_t tma_smem_bytes(uint32_t n_g, uint32_t &ef_pad) {
+size_t tma_smem_bytes(uint32_t n_g, int stages, uint32_t &ef_pad) {
     ef_pad = (n_g + 3u) & ~3u;
-    return (size_t)(MC_STAGES * 4 + 4) * MC_TILE * sizeof(float) + (size_t)ef_pad * sizeof(float) +
-           MC_STAGES * sizeof(uint64_t);
+    return (size_t)(stages * 4) * MC_TILE * sizeof(float) + (size_t)ef_pad * sizeof(float) +
+           (size_t)stages * sizeof(uint64_t);
 }
 
 }  // namespace
@@ -283,8 +277,11 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
     const bool tma_ok = aligned16(sx) && aligned16(svx) && aligned16(svy) && aligned16(svz) &&
                         (g.capacity % 4u) == 0u;
     if (tma_ok) {
+        const cudapic_tuning t = tuning();
+        int stages = std::min(std::max(t.push_stages, 2), MC_MAX_STAGES);
         uint32_t ef_pad;
-        const size_t smem = tma_smem_bytes(g.n_g, ef_pad);
+        size_t smem = tma_smem_bytes(g.n_g, stages, ef_pad);
+        while (smem > (size_t)max_smem_optin() && stages > 2) smem = tma_smem_bytes(g.n_g, --stages, ef_pad);
         if (smem > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_ARG, "move_and_compact: n_g too large");
         CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(move_and_compact_tma_kernel,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -293,13 +290,12 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                                      &per_sm, move_and_compact_tma_kernel, MC_THREADS, smem),
                                  "occupancy(move_and_compact)"));
-        per_sm = std::max(per_sm, 1);
+        per_sm = std::min(std::max(per_sm, 1), t.push_ctas_per_sm);
         const uint64_t tiles_max = ((uint64_t)g.capacity + MC_TILE - 1) / MC_TILE;
-        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm,
-                                                                                tiles_max));
+        const unsigned grid = persistent_grid(per_sm, tiles_max);
         move_and_compact_tma_kernel<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy,
                                                                          dvz, alive, n_active, factor, dt, g,
-                                                                         ef_pad);
+                                                                         ef_pad, stages);
         return check_launch("move_and_compact_tma");
     }
     const size_t smem = (size_t)g.n_g * sizeof(float);

@@ -78,6 +78,10 @@ typedef struct cudapic_params {
 /* Poisson prefix sums in f32 as the reference does (default: FP64 sums,
  * f32 inputs/outputs). */
 #define CUDAPIC_FLAG_POISSON_F32_SCAN 0x1u
+/* Deposit with exact 32.32 fixed-point integer sums per CTA (order-
+ * independent within a thread-block cluster; default: the reference's shared
+ * f32 atomics, which are faster on B200). */
+#define CUDAPIC_FLAG_DEPOSIT_FIXED_POINT 0x2u
 
 /* Derived per-discharge constants handed to every drop-in kernel (by value
  * on the kernel side).  Built by cudapic_grid_from_params(); the fields are
@@ -113,6 +117,26 @@ typedef struct cudapic_grid {
 
 void cudapic_params_default(cudapic_params *p);
 int cudapic_grid_from_params(const cudapic_params *p, cudapic_grid *out);
+
+/* Launch shapes of the kernels (process-wide; set it before launching, not
+ * concurrently with launches).  Zero fields keep the built-in choice.
+ * The reference has no counterpart: its shapes are compile-time constants
+ * (Rust-CUDA/src/main.rs:84-88).  cudapic_b200.autotune sweeps these. */
+typedef struct cudapic_tuning {
+    int density_threads;      /* get_density CTA size: 256, 512 or 1024                 */
+    int density_ctas_per_sm;  /* resident CTAs per SM used (<= occupancy)               */
+    int density_copies;       /* warp-private shared histogram copies per CTA (1..32)    */
+    int density_cluster;      /* CTAs per thread-block cluster for the reduction: 1,2,4,8 */
+    int push_stages;          /* move_and_compact bulk-copy pipeline depth: 2..6         */
+    int push_ctas_per_sm;
+    int mcc_stages;           /* check_collisions_e/i pipeline depth: 2..4               */
+    int mcc_ctas_per_sm;
+    int mcc_variant;          /* 1: shared-memory resident sigma table (any alignment),
+                                 2: bulk-copy staged tiles (16-byte aligned pointers)    */
+} cudapic_tuning;
+
+int cudapic_get_tuning(cudapic_tuning *out);
+int cudapic_set_tuning(const cudapic_tuning *t);
 const char *cudapic_status_string(int status);
 const char *cudapic_last_error(void);
 int cudapic_version(void);

@@ -89,6 +89,19 @@ def test_math_accuracy_vs_libm(oracle, fn, lo, hi, ulps):
     assert np.max(np.abs(got - ref) / spacing) <= ulps
 
 
+def test_collision_fast_reject_bound(oracle):
+    """The kernels skip exp() when u >= fl(a + 5e-7), a = nu dt: valid because
+    the computed p = 1 - exp_det(-a) never exceeds a + 3.1e-7 (1 - e^-a <= a,
+    exp_det within 2 ulp, 1 - y exact for y >= 1/2).  Checked densely."""
+    a = np.concatenate([np.linspace(0.0, 1.0, 2_000_001), 10 ** np.linspace(-9, 0, 200_001)]).astype(np.float32)
+    y = oracle.math_apply("exp", -a)
+    p = (np.float32(1.0) - y).astype(np.float32)
+    thr = (a + np.float32(5e-7)).astype(np.float32)
+    assert np.all(p.astype(np.float64) < thr.astype(np.float64))
+    # and the bound is tight enough to matter: most u >= thr for the typical a ~ 4e-3
+    assert np.mean(thr[(a > 3e-3) & (a < 5e-3)]) < 6e-3
+
+
 def test_atan2_quadrants(oracle):
     rng = np.random.default_rng(8)
     y = rng.uniform(-3, 3, 100_000).astype(np.float32)
