@@ -324,7 +324,8 @@ def run_ours(args):
     elapsed_max, work_sum = reduce_max_sum(world, elapsed, work)
     value = work_sum / elapsed_max
     ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
-    launches = args.steps * (STEP * 4 + ion_steps * 3)
+    # fused driver: Poisson, push+deposit, electron MCC every step; ion push and MCC on ion steps
+    launches = args.steps * (STEP * 3 + ion_steps * 2)
 
     # ---------------- end to end through the C ABI with host buffers
     pinned = {}

@@ -101,6 +101,8 @@ SIGNATURES = {
     "cudapic_check_collisions_e": [_VP] * 17 + [_GP, _VP],
     "cudapic_check_collisions_i": [_VP] * 10 + [_GP, _VP],
     "cudapic_check_collisions_e_events": [_VP] * 18 + [_GP, _VP],
+    "cudapic_check_collisions_e_deposit": [_VP] * 19 + [_GP, _VP],
+    "cudapic_move_and_compact_deposit": [_VP] * 11 + [_F, _F, _VP, _GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
     "cudapic_accumulate_density": [_VP, _VP, _GP, _VP],
     "cudapic_accumulate_eepf": [_VP] * 7 + [_GP, _VP],
@@ -121,6 +123,7 @@ SIGNATURES = {
     "cudapic_state_download": [_VP, C.c_int, _VP, _VP, _VP, _VP, _U32, C.POINTER(_U32)],
     "cudapic_state_seed": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_set_measure": [_VP, C.c_int],
+    "cudapic_state_set_fused": [_VP, C.c_int],
     "cudapic_state_run_steps": [_VP, C.c_uint64],
     "cudapic_state_counts": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_device_error": [_VP, C.POINTER(_U32)],

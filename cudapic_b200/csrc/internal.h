@@ -34,16 +34,22 @@ cudapic_tuning tuning();
 unsigned persistent_grid(int per_sm, uint64_t units);
 
 // Launchers used by both the drop-in entry points and the driver.
+// zero_a / zero_b (may be null): n_g-float buffers the kernel clears after
+// reading the densities (the driver's next-step density accumulators).
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
-                   const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream);
+                   const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream,
+                   float *zero_a = nullptr, float *zero_b = nullptr);
+// dens_out (may be null): also deposit the survivors' new positions there.
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream);
+                            cudaStream_t stream, float *dens_out = nullptr);
+// dep_e / dep_i (may be null): next-step densities receiving the spawns.
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
-                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream);
+                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e = nullptr,
+                        float *dep_i = nullptr);
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
                         const cudapic_grid &g, cudaStream_t stream);

@@ -11,25 +11,26 @@
 //
 // B200 design: HBM-bound streaming (28 B read + 16 B RNG written per
 // particle; velocities written only by colliders, ~0.5 % of electrons per
-// step at the reference conditions):
-//  * persistent grid; the seven SoA input tiles of 512 particles (vx, vy,
-//    vz and the four RNG planes, 14 KB) are staged into shared memory by
-//    cp.async.bulk on an mbarrier, four stages deep;
-//  * pass 1 (every particle, uniform work): first draw(s), collision test;
-//    non-colliders store their advanced RNG state (coalesced);
-//  * colliders are appended to a shared-memory queue (index, RNG state,
-//    velocity, energy index); when it holds more than 256 entries, and at the
-//    end, the whole CTA drains it one collider per thread, so the long
-//    scattering path runs on full warps instead of one lane in 32;
-//  * sigma_tot gathers through the read-only path (the 4 MB table stays
-//    L2-resident); the per-process tables are read only by colliders;
+// step at the reference conditions).  Two kernels share the physics:
+//  * resident-table kernel (default, cudapic_tuning.mcc_variant = 1): one
+//    1024-thread CTA per SM keeps the first 32768 entries of sigma_tot in
+//    shared memory, every thread issues the loads of two particles before
+//    computing, and colliders go to warp-private queues drained 32 at a
+//    time -- no block barrier in the main loop;
+//  * bulk-copy kernel (mcc_variant = 2): tiles of the seven SoA arrays staged
+//    by cp.async.bulk on mbarriers, a CTA-wide collider queue.
+// Common to both:
+//  * the collision test of every particle is uniform work; the provably
+//    exact fast reject skips exp() for almost all of them; non-colliders
+//    store their advanced RNG state (coalesced);
+//  * a collider keeps its slot and its RNG state before the test; the drain
+//    re-runs the deterministic test and scatters it on a full warp (one
+//    collider per lane) instead of one lane in 32;
 //  * ionization spawns claim slots with one warp-aggregated atomicAdd per
 //    counter, bounded by capacity: a spawn that does not fit is dropped and
 //    flagged, never written out of bounds (the reference writes unbounded,
 //    :1132-1149);
 //  * transcendentals from detmath.cuh (bit-reproducible, see there).
-// One-particle-per-thread kernels without bulk copies serve pointers that
-// are not 16-byte aligned or capacities that are not a multiple of 4.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -141,14 +142,30 @@ __device__ __forceinline__ Test test_electron(float vxi, float vyi, float vzi, X
     return t;
 }
 
+// CIC deposit of one particle straight into a global density (boundary
+// nodes doubled per contribution, equal to doubling the node sum).
+__device__ __forceinline__ void deposit_global(float *dens, float xv, const cudapic_grid &g) {
+    const float pos = xv * g.inv_dx;
+    const int p = cell_of(pos, g.n_g);
+    const float rem = pos - (float)p;
+    float c1 = (1.0f - rem) * g.weight_factor;
+    float c2 = rem * g.weight_factor;
+    if (p == 0) c1 *= 2.0f;
+    if (p + 1 == (int)g.n_g - 1) c2 *= 2.0f;
+    atomicAdd(&dens[p], c1);
+    atomicAdd(&dens[p + 1], c2);
+}
+
 // collision_e, Rust-CUDA/src/main.rs:1035-1165: scatters electron i (state
 // rs already past the test draw), writes its velocity and any spawns;
-// returns the event (1 elastic, 2 excitation, 3 ionization).
+// returns the event (1 elastic, 2 excitation, 3 ionization).  dep_e / dep_i
+// (may be null): next-step densities that also receive the spawned
+// electron / ion.
 __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
                                                   Xoshiro128p &rs, const float *__restrict__ cs, float *x, float *vx,
                                                   float *vy, float *vz, float *ix, float *ivx, float *ivy,
                                                   float *ivz, uint32_t *alive_e, uint32_t *alive_i,
-                                                  const cudapic_grid &g) {
+                                                  const cudapic_grid &g, float *dep_e, float *dep_i) {
     const float exc_j = 11.5f * E_CHARGE_F;
     const float ion_j = 15.8f * E_CHARGE_F;
     float gx = vxi, gy = vyi, gz = vzi;
@@ -199,6 +216,7 @@ __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, floa
             vx[slot] = wx + g.f2 * ngx;
             vy[slot] = wy + g.f2 * ngy;
             vz[slot] = wz + g.f2 * ngz;
+            if (dep_e) deposit_global(dep_e, xi, g);
         } else {
             set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
         }
@@ -209,6 +227,7 @@ __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, floa
             ivx[slot] = a;
             ivy[slot] = b;
             ivz[slot] = c;
+            if (dep_i) deposit_global(dep_i, xi, g);
         } else {
             set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
         }
@@ -304,7 +323,8 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
                                 const uint32_t *__restrict__ active, float *x, float *vx, float *vy, float *vz,
                                 uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *ix,
                                 float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i,
-                                uint8_t *events, const __grid_constant__ cudapic_grid g, int stages) {
+                                uint8_t *events, const __grid_constant__ cudapic_grid g, int stages,
+                                float *dep_e, float *dep_i) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *in = reinterpret_cast<uint32_t *>(smem);             // [stages][7][TILE]
     uint32_t *queue = in + stages * MT_ARRAYS * MT_TILE;           // [5][QCAP]
@@ -344,7 +364,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
             } else {
                 const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
                 ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
-                                      alive_i, g);
+                                      alive_i, g, dep_e, dep_i);
             }
             rng0[i] = rs.s0;
             rng1[i] = rs.s1;
@@ -452,7 +472,8 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
                                      const uint32_t *__restrict__ active, float *x, float *vx, float *vy,
                                      float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                                      float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive_e,
-                                     uint32_t *alive_i, uint8_t *events, const __grid_constant__ cudapic_grid g) {
+                                     uint32_t *alive_i, uint8_t *events, const __grid_constant__ cudapic_grid g,
+                                     float *dep_e, float *dep_i) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *tab = reinterpret_cast<float *>(smem);
     const int tid = threadIdx.x;
@@ -479,7 +500,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
             } else {
                 const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
                 ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
-                                      alive_i, g);
+                                      alive_i, g, dep_e, dep_i);
             }
             rng0[i] = rs.s0;
             rng1[i] = rs.s1;
@@ -587,7 +608,7 @@ template <bool ION, bool EVENTS>
 int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
                float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx, float *ivy,
                float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events, const cudapic_grid &g,
-               cudaStream_t stream) {
+               cudaStream_t stream, float *dep_e, float *dep_i) {
     auto kern = check_collisions_tma_kernel<ION, EVENTS>;
     const cudapic_tuning t = tuning();
     const int stages = std::min(std::max(t.mcc_stages, 2), MT_MAX_STAGES);
@@ -601,7 +622,7 @@ int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, 
     const uint64_t tiles_max = ((uint64_t)g.capacity + MT_TILE - 1) / MT_TILE;
     const unsigned grid = persistent_grid(per_sm, tiles_max);
     kern<<<grid, MCC_THREADS, smem, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                              alive_e, alive_i, events, g, stages);
+                                              alive_e, alive_i, events, g, stages, dep_e, dep_i);
     return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
 }
 
@@ -609,7 +630,7 @@ template <bool ION, bool EVENTS>
 int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
                     float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx,
                     float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
-                    const cudapic_grid &g, cudaStream_t stream) {
+                    const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
     auto kern = check_collisions_resident_kernel<ION, EVENTS>;
     if (MR_SMEM > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_NOT_SUPPORTED, "check_collisions: shared memory");
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MR_SMEM),
@@ -617,7 +638,7 @@ int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *act
     const uint64_t chunks = ((uint64_t)g.capacity + MR_THREADS * MR_U - 1) / (MR_THREADS * MR_U);
     kern<<<persistent_grid(1, chunks), MR_THREADS, MR_SMEM, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1,
                                                                       r2, r3, ix, ivx, ivy, ivz, alive_e, alive_i,
-                                                                      events, g);
+                                                                      events, g, dep_e, dep_i);
     return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
 }
 
@@ -627,20 +648,20 @@ template <bool ION>
 int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx,
                       float *vy, float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix,
                       float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
-                      const cudapic_grid &g, cudaStream_t stream) {
+                      const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
     const bool bulk = tuning().mcc_variant == 2 && tma_ready(g.capacity, {vx, vy, vz, r0, r1, r2, r3});
     if (bulk) {
         if (events)
             return launch_tma<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                         alive_e, alive_i, events, g, stream);
+                                         alive_e, alive_i, events, g, stream, dep_e, dep_i);
         return launch_tma<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                      alive_e, alive_i, nullptr, g, stream);
+                                      alive_e, alive_i, nullptr, g, stream, dep_e, dep_i);
     }
     if (events)
         return launch_resident<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                          alive_e, alive_i, events, g, stream);
+                                          alive_e, alive_i, events, g, stream, dep_e, dep_i);
     return launch_resident<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                       alive_e, alive_i, nullptr, g, stream);
+                                       alive_e, alive_i, nullptr, g, stream, dep_e, dep_i);
 }
 
 }  // namespace
@@ -648,16 +669,16 @@ int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *a
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
-                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream) {
+                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
     return launch_collisions<false>(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
-                                    i_vz, alive_e, alive_i, events, g, stream);
+                                    i_vz, alive_e, alive_i, events, g, stream, dep_e, dep_i);
 }
 
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
                         const cudapic_grid &g, cudaStream_t stream) {
     return launch_collisions<true>(total_cs_i, cs, active_i, nullptr, vx, vy, vz, rng0, rng1, rng2, rng3, nullptr,
-                                   nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream);
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream, nullptr, nullptr);
 }
 
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
@@ -698,6 +719,20 @@ extern "C" int cudapic_check_collisions_e_events(const float *total_cs_e, const 
     CUDAPIC_REQUIRE(CUDAPIC_E_ARGS_NONNULL && events, "check_collisions_e_events: null pointer");
     return launch_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
                                i_vz, alive_e, alive_i, events, *grid, (cudaStream_t)stream);
+}
+
+extern "C" int cudapic_check_collisions_e_deposit(const float *total_cs_e, const float *cs,
+                                                  const uint32_t *active_e, float *x, float *vx, float *vy,
+                                                  float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
+                                                  uint32_t *rng3, float *i_x, float *i_vx, float *i_vy,
+                                                  float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
+                                                  float *e_next_density, float *i_next_density,
+                                                  const cudapic_grid *grid, cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(CUDAPIC_E_ARGS_NONNULL, "check_collisions_e_deposit: null pointer");
+    return launch_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
+                               i_vz, alive_e, alive_i, nullptr, *grid, (cudaStream_t)stream, e_next_density,
+                               i_next_density);
 }
 
 extern "C" int cudapic_check_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i,

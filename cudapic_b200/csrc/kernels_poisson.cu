@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
     poisson_kernel(const float *__restrict__ e_density, const float *__restrict__ i_density,
                    float *__restrict__ pot_out, float *__restrict__ efield_out, float pot0_arg,
                    const float *__restrict__ pot0_table, uint32_t *__restrict__ step_counter,
-                   const cudapic_grid g) {
+                   const cudapic_grid g, float *__restrict__ zero_a, float *__restrict__ zero_b) {
     constexpr int per_thread = PT;
     extern __shared__ unsigned char smem_raw[];
     T *pot_s = reinterpret_cast<T *>(smem_raw);        // n_g
@@ -74,6 +74,10 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
 
     const int n = (int)g.n_g;
     const int tid = threadIdx.x;
+    for (int k = tid; k < n; k += blockDim.x) {  // next-step accumulators of the driver
+        if (zero_a) zero_a[k] = 0.0f;
+        if (zero_b) zero_b[k] = 0.0f;
+    }
     if (tid == 0) {
         float p0 = pot0_arg;
         if (pot0_table) {
@@ -250,39 +254,40 @@ void poisson_shape(uint32_t n_g, int &threads, int &per_thread) {
 template <typename T, int PT>
 int launch_poisson_t(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                      const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, int threads,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, float *zero_a, float *zero_b) {
     size_t smem = (size_t)g.n_g * sizeof(T);
     auto kern = poisson_kernel<T, PT>;
     if (smem > 48 * 1024)
         CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                                  "cudaFuncSetAttribute(poisson)"));
-    kern<<<1, threads, smem, stream>>>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g);
+    kern<<<1, threads, smem, stream>>>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, zero_a,
+                                       zero_b);
     return check_launch("solve_poisson_scan");
 }
 
 template <typename T>
 int launch_poisson_pt(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                       const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, float *zero_a, float *zero_b) {
     int threads, pt;
     poisson_shape(g.n_g, threads, pt);
     switch (pt) {
-    case 1: return launch_poisson_t<T, 1>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
-    case 2: return launch_poisson_t<T, 2>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
-    case 4: return launch_poisson_t<T, 4>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
-    case 8: return launch_poisson_t<T, 8>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
-    default: return launch_poisson_t<T, 16>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream);
+    case 1: return launch_poisson_t<T, 1>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream, zero_a, zero_b);
+    case 2: return launch_poisson_t<T, 2>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream, zero_a, zero_b);
+    case 4: return launch_poisson_t<T, 4>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream, zero_a, zero_b);
+    case 8: return launch_poisson_t<T, 8>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream, zero_a, zero_b);
+    default: return launch_poisson_t<T, 16>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, threads, stream, zero_a, zero_b);
     }
 }
 
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, float *zero_a, float *zero_b) {
     if (g.n_g > (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD))
         return fail(CUDAPIC_ERR_ARG, "solve_poisson: n_g > 16384");
     if (g.flags & CUDAPIC_FLAG_POISSON_F32_SCAN)
-        return launch_poisson_pt<float>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream);
-    return launch_poisson_pt<double>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream);
+        return launch_poisson_pt<float>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream, zero_a, zero_b);
+    return launch_poisson_pt<double>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream, zero_a, zero_b);
 }
 
 }  // namespace cudapic

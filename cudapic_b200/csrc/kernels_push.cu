@@ -62,17 +62,23 @@ struct TileOut {
     uint32_t keep;  // bit u: particle of row u survives
 };
 
+// DEPOSIT: also deposit every survivor's new position into dens_out (the
+// charge density of the next time step; same CIC arithmetic as
+// get_density), through `copies` warp-private shared histograms.
+template <bool DEPOSIT>
 __global__ void __launch_bounds__(MC_THREADS)
     move_and_compact_tma_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
                                 const float *__restrict__ svx, const float *__restrict__ svy,
                                 const float *__restrict__ svz, float *__restrict__ dx_,
                                 float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
-                                float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages) {
+                                float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages,
+                                float *__restrict__ dens_out, int copies) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
     float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
-    uint64_t *bar = reinterpret_cast<uint64_t *>(ef + ef_pad);
+    float *hist = ef + ef_pad;                           // [copies][ef_pad] (DEPOSIT)
+    uint64_t *bar = reinterpret_cast<uint64_t *>(hist + (DEPOSIT ? copies * ef_pad : 0));
     __shared__ uint32_t offs[2][MC_U * MC_WARPS];        // counts, then exclusive offsets
     __shared__ uint32_t s_base[2];
     __shared__ int s_ready;
@@ -100,6 +106,9 @@ __global__ void __launch_bounds__(MC_THREADS)
         fence_mbar_init();
     }
     for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
+    if (DEPOSIT)
+        for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0.0f;
+    float *h = hist + (uint32_t)(warp % max(copies, 1)) * ef_pad;
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -144,6 +153,13 @@ __global__ void __launch_bounds__(MC_THREADS)
                 cur.vx[u] = pr.vx;
                 cur.vy[u] = bvy[j];
                 cur.vz[u] = bvz[j];
+            }
+            if (DEPOSIT && keep) {  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+                const float pos = cur.x[u] * g.inv_dx;
+                const int p = cell_of(pos, g.n_g);
+                const float rem = pos - (float)p;
+                atomicAdd(&h[p], (1.0f - rem) * g.weight_factor);
+                atomicAdd(&h[p + 1], rem * g.weight_factor);
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             cur.lane_off[u] = __popc(m & lt);
@@ -196,6 +212,17 @@ __global__ void __launch_bounds__(MC_THREADS)
                 dvx[slot] = prev.vx[u];
                 dvy[slot] = prev.vy[u];
                 dvz[slot] = prev.vz[u];
+            }
+        }
+    }
+    if (DEPOSIT) {  // sum the warp copies, one global atomic per non-empty node
+        __syncthreads();
+        for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) {
+            float sum = hist[k];
+            for (int c = 1; c < copies; ++c) sum += hist[(uint32_t)c * ef_pad + k];
+            if (sum != 0.0f) {
+                if (k == 0 || k == g.n_g - 1) sum *= 2.0f;
+                atomicAdd(&dens_out[k], sum);
             }
         }
     }
@@ -273,30 +300,38 @@ size_t tma_smem_bytes(uint32_t n_g, int stages, uint32_t &ef_pad) {
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, float *dens_out) {
     const bool tma_ok = aligned16(sx) && aligned16(svx) && aligned16(svy) && aligned16(svz) &&
                         (g.capacity % 4u) == 0u;
     if (tma_ok) {
         const cudapic_tuning t = tuning();
+        const bool dep = dens_out != nullptr;
+        const int copies = dep ? std::max(1, std::min(t.density_copies, MC_WARPS)) : 0;
         int stages = std::min(std::max(t.push_stages, 2), MC_MAX_STAGES);
         uint32_t ef_pad;
-        size_t smem = tma_smem_bytes(g.n_g, stages, ef_pad);
-        while (smem > (size_t)max_smem_optin() && stages > 2) smem = tma_smem_bytes(g.n_g, --stages, ef_pad);
+        auto bytes = [&](int st) {
+            return tma_smem_bytes(g.n_g, st, ef_pad) + (size_t)copies * ((g.n_g + 3u) & ~3u) * sizeof(float);
+        };
+        size_t smem = bytes(stages);
+        while (smem > (size_t)max_smem_optin() && stages > 2) smem = bytes(--stages);
         if (smem > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_ARG, "move_and_compact: n_g too large");
-        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(move_and_compact_tma_kernel,
-                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        auto kern = dep ? move_and_compact_tma_kernel<true> : move_and_compact_tma_kernel<false>;
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                                  "cudaFuncSetAttribute(move_and_compact)"));
         int per_sm = 0;
-        CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                     &per_sm, move_and_compact_tma_kernel, MC_THREADS, smem),
+        CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_THREADS, smem),
                                  "occupancy(move_and_compact)"));
         per_sm = std::min(std::max(per_sm, 1), t.push_ctas_per_sm);
         const uint64_t tiles_max = ((uint64_t)g.capacity + MC_TILE - 1) / MC_TILE;
         const unsigned grid = persistent_grid(per_sm, tiles_max);
-        move_and_compact_tma_kernel<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy,
-                                                                         dvz, alive, n_active, factor, dt, g,
-                                                                         ef_pad, stages);
+        kern<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active,
+                                                 factor, dt, g, ef_pad, stages, dens_out, copies);
         return check_launch("move_and_compact_tma");
+    }
+    if (dens_out) {  // unaligned buffers: separate deposit of the compacted survivors dst[0, *alive)
+        CUDAPIC_CHECK(launch_move_and_compact(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor,
+                                              dt, g, stream, nullptr));
+        return cudapic_get_density(dx_, dens_out, alive, &g, (cudapic_stream_t)stream);
     }
     const size_t smem = (size_t)g.n_g * sizeof(float);
     if (smem > 48 * 1024)
@@ -327,4 +362,20 @@ extern "C" int cudapic_move_and_compact(const float *efield, const float *src_x,
                     "move_and_compact: src and dst must be distinct buffers");
     return launch_move_and_compact(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz,
                                    alive_counter, n_active, factor, dt, *grid, (cudaStream_t)stream);
+}
+
+extern "C" int cudapic_move_and_compact_deposit(const float *efield, const float *src_x, const float *src_vx,
+                                                const float *src_vy, const float *src_vz, float *dst_x,
+                                                float *dst_vx, float *dst_vy, float *dst_vz,
+                                                uint32_t *alive_counter, const uint32_t *n_active, float factor,
+                                                float dt, float *next_density, const cudapic_grid *grid,
+                                                cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(efield && src_x && src_vx && src_vy && src_vz && dst_x && dst_vx && dst_vy && dst_vz &&
+                        alive_counter && n_active && next_density,
+                    "move_and_compact_deposit: null pointer");
+    CUDAPIC_REQUIRE(src_x != dst_x && src_vx != dst_vx && src_vy != dst_vy && src_vz != dst_vz,
+                    "move_and_compact_deposit: src and dst must be distinct buffers");
+    return launch_move_and_compact(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz,
+                                   alive_counter, n_active, factor, dt, *grid, (cudaStream_t)stream, next_density);
 }

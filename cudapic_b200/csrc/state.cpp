@@ -39,7 +39,15 @@ struct cudapic_state {
     uint32_t *rng[2][4] = {};
     // counters block: n_e, n_i, alive, step, dev_err, pad..., work (u64 at +32)
     uint32_t *counters = nullptr;
-    float *efield = nullptr, *pot = nullptr, *e_density = nullptr, *i_density = nullptr, *pot0_table = nullptr;
+    float *efield = nullptr, *pot = nullptr, *pot0_table = nullptr;
+    // Charge densities, double-buffered for the fused step: [cur] feeds the
+    // Poisson solve, [cur ^ 1] accumulates the next step's (electrons) or
+    // the next ion step's (ions) deposits.
+    float *e_dens[2] = {}, *i_dens[2] = {};
+    int e_cur = 0, i_cur = 0;
+    bool fused = true;        // deposit inside push / collisions (default)
+    bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
+    int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
     double *cumul_e = nullptr, *cumul_i = nullptr;
     uint32_t *eepf = nullptr;
@@ -56,6 +64,8 @@ struct cudapic_state {
     uint32_t *step_counter() const { return counters + 3; }
     uint32_t *dev_err() const { return counters + 4; }
     unsigned long long *work() const { return reinterpret_cast<unsigned long long *>(counters + 8); }
+    float *e_density() const { return e_dens[e_cur]; }
+    float *i_density() const { return i_dens[i_cur]; }
 };
 
 namespace {
@@ -95,25 +105,49 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     cudaStream_t st = s->stream;
     const int E = 0, I = 1;
     const uint32_t n_g = g.n_g;
+    const size_t nb = n_g * sizeof(float);
     int se = s->side[E], si = s->side[I];
+    const bool fused = s->fused;
+    float *e_next = nullptr, *i_acc = nullptr, *zero_b = nullptr;
 
-    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density, 0, n_g * sizeof(float), st), "memset e_density"));
-    CUDAPIC_CHECK(cudapic_get_density(s->x[E][se], s->e_density, s->n_e(), &g, (cudapic_stream_t)st));
-    if (ion_step) {
-        CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_density, 0, n_g * sizeof(float), st), "memset i_density"));
-        CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_density, s->n_i(), &g, (cudapic_stream_t)st));
+    if (!fused || !s->dens_valid) {
+        // the reference's deposit of the current positions (Rust-CUDA/src/main.rs:1729-1739)
+        CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density(), 0, nb, st), "memset e_density"));
+        CUDAPIC_CHECK(cudapic_get_density(s->x[E][se], s->e_density(), s->n_e(), &g, (cudapic_stream_t)st));
+        if (fused) {  // priming: both ion buffers hold the density of the present ions
+            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_dens[s->i_cur], 0, nb, st), "memset i_density"));
+            CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_dens[s->i_cur], s->n_i(), &g, (cudapic_stream_t)st));
+            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->i_dens[s->i_cur ^ 1], s->i_dens[s->i_cur], nb,
+                                                     cudaMemcpyDeviceToDevice, st), "copy i_density"));
+            s->dens_valid = true;
+        } else if (ion_step) {
+            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_density(), 0, nb, st), "memset i_density"));
+            CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_density(), s->n_i(), &g, (cudapic_stream_t)st));
+        }
     }
-    CUDAPIC_CHECK(launch_poisson(s->e_density, s->i_density, s->pot, s->efield, 0.0f, s->pot0_table,
-                                 s->step_counter(), g, st));
+    if (fused) {
+        // e_dens[e_cur] holds the density of the present electrons; the other
+        // buffer collects the next step's.  On an ion step the ion buffer
+        // that collected the period's deposits becomes current and the other
+        // one starts collecting.  The Poisson kernel clears the collectors.
+        e_next = s->e_dens[s->e_cur ^ 1];
+        if (ion_step) {
+            s->i_cur ^= 1;
+            zero_b = s->i_dens[s->i_cur ^ 1];
+        }
+        i_acc = s->i_dens[s->i_cur ^ 1];
+    }
+    CUDAPIC_CHECK(launch_poisson(s->e_density(), s->i_density(), s->pot, s->efield, 0.0f, s->pot0_table,
+                                 s->step_counter(), g, st, e_next, zero_b));
     if (s->measure) {
-        CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density, s->cumul_e, &g, (cudapic_stream_t)st));
-        if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density, s->cumul_i, &g, (cudapic_stream_t)st));
+        CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density(), s->cumul_e, &g, (cudapic_stream_t)st));
+        if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density(), s->cumul_i, &g, (cudapic_stream_t)st));
     }
     // electrons: push + compact into the other side
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
     CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
                                           s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
-                                          s->alive(), s->n_e(), g.factor_e, g.dt_e, g, st));
+                                          s->alive(), s->n_e(), g.factor_e, g.dt_e, g, st, e_next));
     se ^= 1;
     s->side[E] = se;
     CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
@@ -122,7 +156,8 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
         CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
         CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
                                               s->x[I][si ^ 1], s->vx[I][si ^ 1], s->vy[I][si ^ 1],
-                                              s->vz[I][si ^ 1], s->alive(), s->n_i(), g.factor_i, g.dt_i, g, st));
+                                              s->vz[I][si ^ 1], s->alive(), s->n_i(), g.factor_i, g.dt_i, g, st,
+                                              i_acc));
         si ^= 1;
         s->side[I] = si;
         CUDAPIC_CHECK(check_cuda(
@@ -133,9 +168,10 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     CUDAPIC_CHECK(launch_collisions_e(s->sigma_tot_e, s->cs, s->n_e(), s->x[E][se], s->vx[E][se], s->vy[E][se],
                                       s->vz[E][se], s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3],
                                       s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si], s->alive(), s->n_i(),
-                                      nullptr, g, st));
+                                      nullptr, g, st, e_next, i_acc));
     CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
                              "copy alive -> n_e"));
+    if (fused) s->e_cur ^= 1;
     if (ion_step) {
         CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
                                           s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
@@ -162,12 +198,20 @@ int build_graph(cudapic_state *s) {
     cudaGraph_t graph = nullptr;
     const uint64_t period = graph_period(s);
     const int side0[2] = {s->side[0], s->side[1]};
+    const int cur0[2] = {s->e_cur, s->i_cur};
     CUDAPIC_CHECK(check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
     int rc = CUDAPIC_OK;
     for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k) rc = enqueue_step(s, is_ion_step(s, s->steps_done + k));
     cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    // a graph of 2 N_SUB steps returns every ping-pong role to its start
     s->side[0] = side0[0];
     s->side[1] = side0[1];
+    s->e_cur = cur0[0];
+    s->i_cur = cur0[1];
+    s->graph_key[m][0] = side0[0];
+    s->graph_key[m][1] = side0[1];
+    s->graph_key[m][2] = cur0[0];
+    s->graph_key[m][3] = cur0[1];
     if (rc != CUDAPIC_OK) {
         if (graph) cudaGraphDestroy(graph);
         return rc;
@@ -226,7 +270,8 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
     }
     const size_t n_g = p->n_g;
     if ((rc = dalloc(s, &s->counters, 64)) || (rc = dalloc(s, &s->efield, n_g)) || (rc = dalloc(s, &s->pot, n_g)) ||
-        (rc = dalloc(s, &s->e_density, n_g)) || (rc = dalloc(s, &s->i_density, n_g)) ||
+        (rc = dalloc(s, &s->e_dens[0], n_g)) || (rc = dalloc(s, &s->e_dens[1], n_g)) ||
+        (rc = dalloc(s, &s->i_dens[0], n_g)) || (rc = dalloc(s, &s->i_dens[1], n_g)) ||
         (rc = dalloc(s, &s->pot0_table, p->n_t)) || (rc = dalloc(s, &s->cs, 5ull * CUDAPIC_CS_RANGES)) ||
         (rc = dalloc(s, &s->sigma_tot_e, CUDAPIC_CS_RANGES)) || (rc = dalloc(s, &s->sigma_tot_i, CUDAPIC_CS_RANGES)) ||
         (rc = dalloc(s, &s->cumul_e, n_g)) || (rc = dalloc(s, &s->cumul_i, n_g)) || (rc = dalloc(s, &s->eepf, 2000)))
@@ -243,8 +288,10 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
     if ((rc = check_cuda(cudaMemsetAsync(s->counters, 0, 64 * sizeof(uint32_t), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->efield, 0, n_g * sizeof(float), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->pot, 0, n_g * sizeof(float), s->stream), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(s->e_density, 0, n_g * sizeof(float), s->stream), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(s->i_density, 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->e_dens[0], 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->e_dens[1], 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->i_dens[0], 0, n_g * sizeof(float), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->i_dens[1], 0, n_g * sizeof(float), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "memset")))
@@ -323,8 +370,8 @@ extern "C" int cudapic_state_buffers(const cudapic_state *s, cudapic_buffers *o)
     o->alive_counter = s->alive();
     o->efield = s->efield;
     o->pot = s->pot;
-    o->e_density = s->e_density;
-    o->i_density = s->i_density;
+    o->e_density = s->e_density();
+    o->i_density = s->i_density();
     o->cs = s->cs;
     o->sigma_tot_e = s->sigma_tot_e;
     o->sigma_tot_i = s->sigma_tot_i;
@@ -344,6 +391,7 @@ extern "C" int cudapic_state_upload(cudapic_state *s, int species, const float *
     DeviceGuard dg(s->device);
     const int a = s->side[species];
     const size_t bytes = (size_t)n * sizeof(float);
+    s->dens_valid = false;  // the next step recomputes the densities from the particles
     if (n) {
         CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->x[species][a], x, bytes, cudaMemcpyHostToDevice, s->stream), "upload x"));
         CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->vx[species][a], vx, bytes, cudaMemcpyHostToDevice, s->stream), "upload vx"));
@@ -390,6 +438,16 @@ extern "C" int cudapic_state_seed(cudapic_state *s, const uint32_t e_master[4], 
     return CUDAPIC_OK;
 }
 
+extern "C" int cudapic_state_set_fused(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_fused: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_fused sync"));
+    s->fused = on != 0;
+    s->dens_valid = false;
+    destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
 extern "C" int cudapic_state_set_measure(cudapic_state *s, int on) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_measure: null state");
     DeviceGuard dg(s->device);
@@ -406,13 +464,20 @@ extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
     DeviceGuard dg(s->device);
     const uint64_t period = graph_period(s);
     while (n_steps > 0) {
-        if (s->graphs_enabled && (s->steps_done % period) == 0 && n_steps >= period) {
+        const bool primed = !s->fused || s->dens_valid;  // a priming step is never captured
+        if (s->graphs_enabled && primed && (s->steps_done % period) == 0 && n_steps >= period) {
+            const int m = s->measure ? 1 : 0;
+            const int key[4] = {s->side[0], s->side[1], s->e_cur, s->i_cur};
+            if (s->graph[m] && std::memcmp(key, s->graph_key[m], sizeof(key)) != 0) {
+                cudaGraphExecDestroy(s->graph[m]);  // buffer roles differ from the captured ones
+                s->graph[m] = nullptr;
+            }
             int rc = build_graph(s);
             if (rc != CUDAPIC_OK) {
                 s->graphs_enabled = false;  // fall back to direct launches
                 continue;
             }
-            CUDAPIC_CHECK(check_cuda(cudaGraphLaunch(s->graph[s->measure ? 1 : 0], s->stream), "cudaGraphLaunch"));
+            CUDAPIC_CHECK(check_cuda(cudaGraphLaunch(s->graph[m], s->stream), "cudaGraphLaunch"));
             s->steps_done += period;
             n_steps -= period;
             continue;

@@ -69,6 +69,24 @@ def move_and_compact(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_v
                                        _stream(stream, src_x)))
 
 
+def move_and_compact_deposit(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, alive_counter,
+                             n_active, factor, dt, next_density, grid, stream=None):
+    """move_and_compact fused with the deposit of the survivors' new
+    positions into next_density (no reference counterpart)."""
+    check(lib.cudapic_move_and_compact_deposit(_ptr(efield), _ptr(src_x), _ptr(src_vx), _ptr(src_vy),
+                                               _ptr(src_vz), _ptr(dst_x), _ptr(dst_vx), _ptr(dst_vy), _ptr(dst_vz),
+                                               _ptr(alive_counter), _ptr(n_active), float(factor), float(dt),
+                                               _ptr(next_density), _g(grid), _stream(stream, src_x)))
+
+
+def check_collisions_e_deposit(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
+                               i_vz, alive_e, alive_i, e_next_density, i_next_density, grid, stream=None):
+    """check_collisions_e whose spawns are also deposited (no reference counterpart)."""
+    args = [_ptr(a) for a in (total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
+                              i_vz, alive_e, alive_i, e_next_density, i_next_density)]
+    check(lib.cudapic_check_collisions_e_deposit(*args, _g(grid), _stream(stream, vx)))
+
+
 def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz,
                        alive_e, alive_i, grid, stream=None, events=None):
     """check_collisions_e (Rust-CUDA/src/main.rs:971-1165).  With `events`

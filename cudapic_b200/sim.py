@@ -133,6 +133,10 @@ class GpuSimState:
     def set_measure(self, on=True):
         check(lib.cudapic_state_set_measure(self._h, 1 if on else 0))
 
+    def set_fused(self, on=True):
+        """Deposit the next step's density inside push / collisions (default on)."""
+        check(lib.cudapic_state_set_fused(self._h, 1 if on else 0))
+
     def download_measurements(self):
         n_g = self.grid.n_g
         ce = np.zeros(n_g, np.float64)

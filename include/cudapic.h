@@ -174,6 +174,19 @@ int cudapic_move_and_compact(const float *efield, const float *src_x, const floa
                              const uint32_t *n_active, float factor, float dt,
                              const cudapic_grid *grid, cudapic_stream_t stream);
 
+/* move_and_compact fused with the next step's deposit: as
+ * cudapic_move_and_compact, and the CIC weights of every survivor's new
+ * position are ADDED to next_density[n_g] (boundary nodes doubled), i.e.
+ * get_density(dst) without re-reading the particles.  No reference
+ * counterpart: the reference recomputes the density from the particles at
+ * the start of every step (Rust-CUDA/src/main.rs:1729-1739), which gives
+ * the same values because collisions do not move particles. */
+int cudapic_move_and_compact_deposit(const float *efield, const float *src_x, const float *src_vx,
+                                     const float *src_vy, const float *src_vz, float *dst_x, float *dst_vx,
+                                     float *dst_vy, float *dst_vz, uint32_t *alive_counter,
+                                     const uint32_t *n_active, float factor, float dt, float *next_density,
+                                     const cudapic_grid *grid, cudapic_stream_t stream);
+
 /* check_collisions_e (Rust-CUDA/src/main.rs:971-1165): MCC of electrons
  * [0, *active_e) against the gas; ionization appends an electron at
  * atomicAdd(alive_e) and an ion at atomicAdd(alive_i) (bounded by capacity).
@@ -184,6 +197,17 @@ int cudapic_check_collisions_e(const float *total_cs_e, const float *cs, const u
                                float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e,
                                uint32_t *alive_i, const cudapic_grid *grid,
                                cudapic_stream_t stream);
+
+/* check_collisions_e whose spawned electrons / ions are also deposited
+ * into e_next_density / i_next_density (either may be NULL), completing the
+ * next-step densities of cudapic_move_and_compact_deposit.  No reference
+ * counterpart (see there). */
+int cudapic_check_collisions_e_deposit(const float *total_cs_e, const float *cs, const uint32_t *active_e,
+                                       float *x, float *vx, float *vy, float *vz, uint32_t *rng0,
+                                       uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *i_x, float *i_vx,
+                                       float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
+                                       float *e_next_density, float *i_next_density, const cudapic_grid *grid,
+                                       cudapic_stream_t stream);
 
 /* check_collisions_i (Rust-CUDA/src/main.rs:1167-1292): MCC of ions
  * [0, *active_i) against Maxwellian target atoms. */
@@ -292,6 +316,12 @@ int cudapic_state_set_measure(cudapic_state *s, int on);
 /* Enqueues n_steps reference-order time steps (Rust-CUDA/src/main.rs:1728-1807)
  * on the state's stream.  Asynchronous. */
 int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps);
+/* on (default): each step deposits the next step's charge density inside the
+ * push and collision kernels (cudapic_move_and_compact_deposit,
+ * cudapic_check_collisions_e_deposit) instead of re-reading every particle
+ * in a separate get_density launch; the first step after an upload runs
+ * the separate deposit.  off: the reference's launch sequence. */
+int cudapic_state_set_fused(cudapic_state *s, int on);
 /* Reads the counters (synchronises the state's stream). */
 int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i);
 /* Reads and returns the device error word (synchronises). */

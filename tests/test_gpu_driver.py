@@ -91,6 +91,41 @@ def test_graph_replay_equals_direct_launch_statistics(cudapic, cuda_device):
     b.close()
 
 
+@pytest.mark.parametrize("steps", [1, 137, 400])
+def test_fused_density_equals_fresh_deposit(cudapic, cuda_device, steps):
+    """In fused mode the density handed to the next Poisson solve was
+    accumulated by the previous push and collisions; it must equal a fresh
+    deposit of the electrons now present."""
+    import torch
+    st = _c0_state(cudapic)
+    st.run_steps(steps)
+    st.synchronize()
+    b, g = st.buffers(), st.grid
+    fresh = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
+    cudapic.kernels.get_density(b.x[0], fresh, b.n_electrons, g, stream=0)
+    used = torch.zeros(g.n_g, dtype=torch.float64, device="cuda")
+    cudapic.kernels.accumulate_density(b.e_density, used, g, stream=0)
+    torch.cuda.synchronize()
+    f, u = fresh.double().cpu().numpy(), used.cpu().numpy()
+    assert f.sum() > 0
+    assert np.linalg.norm(f - u) / np.linalg.norm(f) < 2e-5
+    st.close()
+
+
+def test_fused_and_reference_sequences_agree_statistically(cudapic, cuda_device):
+    a = _c0_state(cudapic)
+    b = _c0_state(cudapic)
+    b.set_fused(False)
+    a.run_cycles(4)
+    b.run_cycles(4)
+    na, nb = a.counts(), b.counts()
+    for x, y in zip(na, nb):
+        assert abs(x - y) <= 0.15 * max(x, y) + 50, (na, nb)
+    assert a.device_error() == 0 and b.device_error() == 0
+    a.close()
+    b.close()
+
+
 def test_measurement_accumulators(cudapic, cuda_device):
     st = _c0_state(cudapic)
     st.run_cycles(2)

@@ -268,6 +268,57 @@ def test_move_and_compact_bit_exact(cudapic, K, oracle, species, n, n_g):
     assert np.array_equal(sorted_rows(*got), sorted_rows(rx, rvx, rvy, rvz))
 
 
+@pytest.mark.parametrize("n,n_g", [(5, 400), (100_003, 400), (4_194_304, 400), (1_000_001, 4096)])
+def test_move_and_compact_deposit(cudapic, K, oracle, n, n_g):
+    """Fused push + deposit: survivors bit-exact, and the deposited density
+    equals get_density of the survivors (f32 restatement / FP64)."""
+    from cudapic_b200.workloads import field_profile
+    cap = (n + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_g=n_g, capacity=cap)
+    ph = oracle.phys_from_params(n_g=n_g, capacity=cap)
+    x, vx, vy, vz = _population(n, "e", n + 3, g.dt_e)
+    ef = field_profile(n_g)
+    src = [dev(np.concatenate([a, np.zeros(cap - n, np.float32)])) for a in (x, vx, vy, vz)]
+    dst = [zeros(cap) for _ in range(4)]
+    alive = counter(0)
+    nd = zeros(n_g)
+    K.move_and_compact_deposit(dev(ef), *src, *dst, alive, counter(n), g.factor_e, g.dt_e, nd, g)
+    m = int(host(alive)[0])
+    rx, rvx, rvy, rvz, _ = oracle.move_and_compact(ef, x, vx, vy, vz, g.factor_e, g.dt_e, ph)
+    assert m == rx.size
+    assert np.array_equal(sorted_rows(*[host(d)[:m] for d in dst]), sorted_rows(rx, rvx, rvy, rvz))
+    got = host(nd).astype(np.float64)
+    r32 = oracle.get_density_f32(rx, ph).astype(np.float64)
+    assert np.linalg.norm(got - r32) / np.linalg.norm(r32) < 2e-5
+    r64 = oracle.get_density_f64(rx, ph)
+    assert np.linalg.norm(got - r64) / np.linalg.norm(r64) < max(2e-5, 1.5 * n_g * 2.0 ** -24)
+
+
+def test_check_collisions_e_deposit_spawns(cudapic, K, oracle, dev_tables, tables):
+    """Spawned electrons and ions are deposited into the next-step densities."""
+    cs, se, si = tables
+    dcs, dse, _ = dev_tables
+    n = 300_001
+    cap = (2 * n + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=50, capacity=cap)
+    ph = oracle.phys_from_params(n_t=50, capacity=cap)
+    x, vx, vy, vz = _mcc_case(n, 60.0, 31, E_MASS)
+    pad = lambda a, dt=np.float32: np.concatenate([a, np.zeros(cap - len(a), dt)])  # noqa: E731
+    e_d = [dev(pad(a)) for a in (x, vx, vy, vz)]
+    i_d = [zeros(cap) for _ in range(4)]
+    r_d = [dev(pad(np.asarray(p), np.uint32)) for p in oracle.seed_streams([4, 4, 4, 4], n)]
+    ae, ai = counter(n), counter(0)
+    de, di = zeros(400), zeros(400)
+    K.check_collisions_e_deposit(dse, dcs, counter(n), *e_d, *r_d, *i_d, ae, ai, de, di, g)
+    ne, ni = int(host(ae)[0]), int(host(ai)[0])
+    assert ne - n == ni and ni > 1000
+    ex = host(e_d[0])[n:ne]
+    ix = host(i_d[0])[:ni]
+    for got, pos in ((host(de), ex), (host(di), ix)):
+        ref = oracle.get_density_f64(pos, ph)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
+
+
 def test_move_and_compact_unaligned_uses_reference_layout(cudapic, K, oracle):
     from cudapic_b200.workloads import field_profile
     n, n_g = 70_001, 400
