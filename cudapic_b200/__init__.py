@@ -20,7 +20,7 @@ import ctypes as _C
 
 from . import _lib
 from ._lib import (CS_RANGES, ELECTRONS, IONS, N_EEPF, Buffers, CudapicError, Grid, Params,  # noqa: F401
-                   FLAG_POISSON_F32_SCAN, FLAG_DEPOSIT_FIXED_POINT, DEVERR_SPAWN_E, DEVERR_SPAWN_I, DEVERR_POSITION,
+                   FLAG_POISSON_F32_SCAN, FLAG_DEPOSIT_FIXED_POINT, FLAG_DEPOSIT_F32, DEVERR_SPAWN_E, DEVERR_SPAWN_I, DEVERR_POSITION,
                    DEVERR_ACTIVE, DEVERR_TIMEOUT)
 
 lib = _lib.load()

@@ -26,6 +26,7 @@ DEVERR_TIMEOUT = 0x10
 
 FLAG_POISSON_F32_SCAN = 0x1
 FLAG_DEPOSIT_FIXED_POINT = 0x2
+FLAG_DEPOSIT_F32 = 0x4
 CS_RANGES = 1_000_000
 N_EEPF = 2000
 ELECTRONS = 0

@@ -2,7 +2,8 @@
 
 Sweeps, on the live GPU and a given population, the CTA size / CTAs per SM /
 warp-private histogram copies / cluster size of get_density, the bulk-copy
-pipeline depth and CTAs per SM of move_and_compact, and those of
+pipeline depth and CTAs per SM of move_and_compact (timed with the fused
+deposit of the driver step), and those of
 check_collisions_e; each candidate is timed with CUDA events (median of
 `reps` launches, L2 flushed before each launch) and the fastest is kept.
 
@@ -74,9 +75,13 @@ def tune(st, reps=5, verbose=True):
     def density():
         K.get_density(b.x[0], dens, ne_c, g, stream=s)
 
-    def push():
-        K.move_and_compact(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0],
-                           b.tmp_vz[0], alive, ne_c, g.factor_e, g.dt_e, g, stream=s)
+    def push():  # the fused driver's push: move_and_compact + deposit of the next density
+        K.move_and_compact_deposit(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], b.tmp_x[0], b.tmp_vx[0],
+                                   b.tmp_vy[0], b.tmp_vz[0], alive, ne_c, g.factor_e, g.dt_e, dens, g, stream=s)
+
+    def reset_push():
+        alive.zero_()
+        dens.zero_()
 
     def mcc():
         K.check_collisions_e(b.sigma_tot_e, b.cs, ne_c, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.x[1],
@@ -91,7 +96,7 @@ def tune(st, reps=5, verbose=True):
          [dict(density_threads=t, density_ctas_per_sm=c, density_copies=k, density_cluster=cl)
           for t, c, k, cl in itertools.product((256, 512, 1024), (1, 2, 4), (2, 4, 8, 16, 32), (1, 2, 4, 8))
           if k <= t // 32]),
-        ("move_and_compact", push, alive.zero_,
+        ("move_and_compact", push, reset_push,
          [dict(push_stages=st_, push_ctas_per_sm=c) for st_, c in itertools.product((2, 3, 4, 5, 6), (1, 2, 3, 4))]),
         ("check_collisions_e", mcc, reset_alive,
          [dict(mcc_variant=1)] +

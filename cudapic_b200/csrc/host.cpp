@@ -67,8 +67,8 @@ int max_smem_optin() { return device_info().smem_optin; }
 namespace {
 // Built-in launch shapes (chosen with cudapic_b200.autotune on B200).
 constexpr cudapic_tuning kDefaultTuning = {
-    /*density_threads*/ 512, /*density_ctas_per_sm*/ 2, /*density_copies*/ 16, /*density_cluster*/ 4,
-    /*push_stages*/ 3, /*push_ctas_per_sm*/ 4,
+    /*density_threads*/ 512, /*density_ctas_per_sm*/ 4, /*density_copies*/ 4, /*density_cluster*/ 4,
+    /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;

@@ -62,9 +62,57 @@ struct TileOut {
     uint32_t keep;  // bit u: particle of row u survives
 };
 
+// Fused deposit in 2^-20 fixed point.  A particle at rem = pos - p in [0, 1]
+// adds 2^20 - r to node p and r to node p + 1, r = round(rem * 2^20), with
+// 32-bit integer shared atomics (on sm_100a several times the throughput of
+// f32 or 64-bit shared atomics; the deposit is bound by that pipe).  The
+// quantum 2^-21 of a weight is below the f32 rounding of the position
+// x * inv_dx that the reference's f32 arithmetic already carries, and the
+// integer sums are exact and order-independent.  A node of one histogram
+// copy gains at most 2^20 per particle of its copy, so the copies are
+// drained into a per-CTA 64-bit accumulator before DEP_MAX_PER_COPY
+// particles have reached one copy.
+constexpr uint32_t DEP_Q = 20;
+constexpr uint32_t DEP_MAX_PER_COPY = (1u << (32 - DEP_Q)) - 1;
+
+__device__ __forceinline__ void dep_add(uint32_t *h, float x, const cudapic_grid &g) {
+    const float pos = x * g.inv_dx;
+    const int p = cell_of(pos, g.n_g);
+    const float rem = pos - (float)p;
+    // rem can exceed 1 by an ulp at x = L (pos rounds past N_G - 1): clamp, so no weight is negative
+    const uint32_t r = min(__float2uint_rn(rem * (float)(1u << DEP_Q)), 1u << DEP_Q);
+    atomicAdd(&h[p], (1u << DEP_Q) - r);
+    atomicAdd(&h[p + 1], r);
+}
+
+// acc[k] += sum of the copies of node k; the copies are cleared.  Each node is
+// owned by one thread: no atomics.  Callers synchronise before and after.
+__device__ __forceinline__ void dep_drain(uint32_t *hist, int copies, uint32_t stride, unsigned long long *acc,
+                                          uint32_t n_g) {
+    for (uint32_t k = threadIdx.x; k < n_g; k += blockDim.x) {
+        unsigned long long v = acc[k];
+        for (int c = 0; c < copies; ++c) {
+            v += hist[(uint32_t)c * stride + k];
+            hist[(uint32_t)c * stride + k] = 0u;
+        }
+        acc[k] = v;
+    }
+}
+
+// Adds the CTA's accumulated node weights to dens_out, boundary nodes doubled.
+__device__ __forceinline__ void dep_flush(const unsigned long long *acc, float *dens_out, const cudapic_grid &g) {
+    const double w = g.weight_factor_d * (1.0 / (double)(1u << DEP_Q));
+    for (uint32_t k = threadIdx.x; k < g.n_g; k += blockDim.x) {
+        if (acc[k] == 0ull) continue;
+        float f = (float)((double)acc[k] * w);
+        if (k == 0 || k == g.n_g - 1) f *= 2.0f;
+        atomicAdd(&dens_out[k], f);
+    }
+}
+
 // DEPOSIT: also deposit every survivor's new position into dens_out (the
-// charge density of the next time step; same CIC arithmetic as
-// get_density), through `copies` warp-private shared histograms.
+// charge density of the next time step), through `copies` warp-private
+// fixed-point shared histograms (see dep_add) drained every `epoch` tiles.
 template <bool DEPOSIT>
 __global__ void __launch_bounds__(MC_THREADS)
     move_and_compact_tma_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
@@ -73,11 +121,12 @@ __global__ void __launch_bounds__(MC_THREADS)
                                 float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
                                 float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages,
-                                float *__restrict__ dens_out, int copies) {
+                                float *__restrict__ dens_out, int copies, uint32_t epoch) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
     float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
-    float *hist = ef + ef_pad;                           // [copies][ef_pad] (DEPOSIT)
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);  // [ef_pad] (DEPOSIT)
+    uint32_t *hist = reinterpret_cast<uint32_t *>(acc + (DEPOSIT ? ef_pad : 0));     // [copies][ef_pad]
     uint64_t *bar = reinterpret_cast<uint64_t *>(hist + (DEPOSIT ? copies * ef_pad : 0));
     __shared__ uint32_t offs[2][MC_U * MC_WARPS];        // counts, then exclusive offsets
     __shared__ uint32_t s_base[2];
@@ -106,9 +155,11 @@ __global__ void __launch_bounds__(MC_THREADS)
         fence_mbar_init();
     }
     for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
-    if (DEPOSIT)
-        for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0.0f;
-    float *h = hist + (uint32_t)(warp % max(copies, 1)) * ef_pad;
+    if (DEPOSIT) {
+        for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0u;
+        for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) acc[k] = 0ull;
+    }
+    uint32_t *h = hist + (uint32_t)(warp % max(copies, 1)) * ef_pad;
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -122,6 +173,11 @@ __global__ void __launch_bounds__(MC_THREADS)
     uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        if (DEPOSIT && it != 0 && it % epoch == 0) {  // drain the copies before they can overflow
+            __syncthreads();
+            dep_drain(hist, copies, ef_pad, acc, g.n_g);
+            __syncthreads();
+        }
         const int s = (int)(it % (uint32_t)stages);
         const uint32_t parity = (it / (uint32_t)stages) & 1u;
         // (1) the stage's bulk copies have landed (one bounded waiter, uniform verdict)
@@ -154,13 +210,7 @@ __global__ void __launch_bounds__(MC_THREADS)
                 cur.vy[u] = bvy[j];
                 cur.vz[u] = bvz[j];
             }
-            if (DEPOSIT && keep) {  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
-                const float pos = cur.x[u] * g.inv_dx;
-                const int p = cell_of(pos, g.n_g);
-                const float rem = pos - (float)p;
-                atomicAdd(&h[p], (1.0f - rem) * g.weight_factor);
-                atomicAdd(&h[p + 1], rem * g.weight_factor);
-            }
+            if (DEPOSIT && keep) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             cur.lane_off[u] = __popc(m & lt);
             if (keep) cur.keep |= 1u << u;
@@ -217,14 +267,9 @@ __global__ void __launch_bounds__(MC_THREADS)
     }
     if (DEPOSIT) {  // sum the warp copies, one global atomic per non-empty node
         __syncthreads();
-        for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) {
-            float sum = hist[k];
-            for (int c = 1; c < copies; ++c) sum += hist[(uint32_t)c * ef_pad + k];
-            if (sum != 0.0f) {
-                if (k == 0 || k == g.n_g - 1) sum *= 2.0f;
-                atomicAdd(&dens_out[k], sum);
-            }
-        }
+        dep_drain(hist, copies, ef_pad, acc, g.n_g);
+        __syncthreads();
+        dep_flush(acc, dens_out, g);
     }
 }
 
@@ -306,14 +351,17 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
     if (tma_ok) {
         const cudapic_tuning t = tuning();
         const bool dep = dens_out != nullptr;
-        const int copies = dep ? std::max(1, std::min(t.density_copies, MC_WARPS)) : 0;
+        int copies = dep ? std::max(1, std::min(t.density_copies, MC_WARPS)) : 0;
         int stages = std::min(std::max(t.push_stages, 2), MC_MAX_STAGES);
         uint32_t ef_pad;
         auto bytes = [&](int st) {
-            return tma_smem_bytes(g.n_g, st, ef_pad) + (size_t)copies * ((g.n_g + 3u) & ~3u) * sizeof(float);
+            const size_t pad = (g.n_g + 3u) & ~3u;
+            return tma_smem_bytes(g.n_g, st, ef_pad) +
+                   (dep ? pad * sizeof(unsigned long long) + (size_t)copies * pad * sizeof(uint32_t) : 0);
         };
         size_t smem = bytes(stages);
         while (smem > (size_t)max_smem_optin() && stages > 2) smem = bytes(--stages);
+        while (smem > (size_t)max_smem_optin() && copies > 1) smem = bytes(copies = (copies + 1) / 2);
         if (smem > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_ARG, "move_and_compact: n_g too large");
         auto kern = dep ? move_and_compact_tma_kernel<true> : move_and_compact_tma_kernel<false>;
         CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -324,8 +372,11 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         per_sm = std::min(std::max(per_sm, 1), t.push_ctas_per_sm);
         const uint64_t tiles_max = ((uint64_t)g.capacity + MC_TILE - 1) / MC_TILE;
         const unsigned grid = persistent_grid(per_sm, tiles_max);
+        // tiles per drain: a copy receives the particles of ceil(MC_WARPS / copies) warps, MC_U * 32 per tile each
+        const uint32_t per_tile = (uint32_t)((MC_WARPS + std::max(copies, 1) - 1) / std::max(copies, 1)) * MC_U * 32u;
+        const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
         kern<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active,
-                                                 factor, dt, g, ef_pad, stages, dens_out, copies);
+                                                 factor, dt, g, ef_pad, stages, dens_out, copies, epoch);
         return check_launch("move_and_compact_tma");
     }
     if (dens_out) {  // unaligned buffers: separate deposit of the compacted survivors dst[0, *alive)

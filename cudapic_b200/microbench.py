@@ -3,16 +3,18 @@ L2 flushed before each launch): the target of the committed ncu captures.
 
     python -m cudapic_b200.microbench --kernel check_collisions_e [--particles N] [--reps 3]
 
-Kernels: get_density, solve_poisson, move_and_compact, check_collisions_e,
-check_collisions_i.  Prints one JSON line with the median time, the particle
+Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
+check_collisions_e, check_collisions_e_deposit, check_collisions_i (the
+*_deposit variants also deposit the next step's density, as the fused driver
+step does).  Prints one JSON line with the median time, the particle
 count and the algorithmic bytes per launch.
 """
 import argparse
 import json
 import statistics
 
-BYTES = {"get_density": 4, "move_and_compact": 32, "check_collisions_e": 44, "check_collisions_i": 44,
-         "solve_poisson": 0}
+BYTES = {"get_density": 4, "move_and_compact": 32, "move_and_compact_deposit": 32, "check_collisions_e": 44,
+         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0}
 
 
 def main():
@@ -57,6 +59,13 @@ def main():
                                                             b.vz[0], *b.rng[0], b.x[1], b.vx[1], b.vy[1], b.vz[1],
                                                             alive_e, alive_i, g, stream=s),
                                lambda: (alive_e.fill_(n_e), alive_i.fill_(n_i)), n_e),
+        "move_and_compact_deposit": (lambda: K.move_and_compact_deposit(
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], alive,
+            ne_c, g.factor_e, g.dt_e, dens, g, stream=s), lambda: (alive.zero_(), dens.zero_()), n_e),
+        "check_collisions_e_deposit": (lambda: K.check_collisions_e_deposit(
+            b.sigma_tot_e, b.cs, ne_c, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.x[1], b.vx[1], b.vy[1],
+            b.vz[1], alive_e, alive_i, dens, pot, g, stream=s), lambda: (alive_e.fill_(n_e), alive_i.fill_(n_i)),
+            n_e),
         "check_collisions_i": (lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                             *b.rng[1], g, stream=s), None, n_i),
     }

@@ -78,10 +78,16 @@ typedef struct cudapic_params {
 /* Poisson prefix sums in f32 as the reference does (default: FP64 sums,
  * f32 inputs/outputs). */
 #define CUDAPIC_FLAG_POISSON_F32_SCAN 0x1u
-/* Deposit with exact 32.32 fixed-point integer sums per CTA (order-
- * independent within a thread-block cluster; default: the reference's shared
- * f32 atomics, which are faster on B200). */
+/* Deposit arithmetic.  Default: CIC weights in 2^-20 fixed point summed
+ * with 32-bit integer shared atomics (exact, order-independent sums inside a
+ * thread-block cluster; a weight carries a quantum of 2^-21, below the f32
+ * rounding of x * inv_dx; the fastest shared atomic on B200).
+ * FIXED_POINT: 32.32 fixed-point weights summed with 64-bit shared atomics.
+ * F32: the reference's f32 weights summed with shared f32 atomics.  Where
+ * both are set, FIXED_POINT wins.  The fused deposits of the driver step
+ * (cudapic_move_and_compact_deposit) always use the default arithmetic. */
 #define CUDAPIC_FLAG_DEPOSIT_FIXED_POINT 0x2u
+#define CUDAPIC_FLAG_DEPOSIT_F32 0x4u
 
 /* Derived per-discharge constants handed to every drop-in kernel (by value
  * on the kernel side).  Built by cudapic_grid_from_params(); the fields are

@@ -77,10 +77,12 @@ def test_math_bit_exact_with_oracle(K, oracle, fn, lo, hi):
 
 # ---------------------------------------------------------------- deposit
 
+@pytest.mark.parametrize("arith", ["fixed20", "f32"])
 @pytest.mark.parametrize("n_g", [400, 4096])
 @pytest.mark.parametrize("n", [0, 1, 1001, 100_003, 4_194_304])
-def test_get_density_vs_fp64(cudapic, K, oracle, n_g, n):
-    g = cudapic.grid_from_params(n_g=n_g, capacity=max(n, 4))
+def test_get_density_vs_fp64(cudapic, K, oracle, n_g, n, arith):
+    flags = cudapic.FLAG_DEPOSIT_F32 if arith == "f32" else 0
+    g = cudapic.grid_from_params(n_g=n_g, capacity=max(n, 4), flags=flags)
     ph = oracle.phys_from_params(n_g=n_g, capacity=max(n, 4))
     rng = np.random.default_rng(n + n_g)
     x = (rng.random(n) * 0.025).astype(np.float32)
@@ -154,6 +156,44 @@ def test_get_density_fixed_point_is_exact_per_cta(cudapic, K, oracle):
         exp[0] *= 2
         exp[-1] *= 2
         assert np.max(np.abs(runs[0] - exp) / np.maximum(exp, 1e-30)) < 1.2e-7
+    finally:
+        cudapic.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("vec", [True, False])
+def test_get_density_fixed20_drains_are_exact(cudapic, K, vec):
+    """Default arithmetic at its limit: one histogram copy, one CTA per SM, no
+    cluster, particles in three cells with fractions up to ~1, so each copy
+    is drained every round.  Equals the exact CIC sum of the 2^-20-rounded
+    fractions."""
+    import torch
+    saved = cudapic.get_tuning()
+    try:
+        cudapic.set_tuning(density_copies=1, density_ctas_per_sm=1, density_cluster=1, density_threads=512)
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        n = 40 * sms * 512 * 4 + 3           # 40 rounds of float4 loads per CTA and a ragged tail
+        n_g = 400
+        g = cudapic.grid_from_params(n_g=n_g, capacity=n + 1)
+        xs = np.array([(200 + 0.9999) * g.dx, (37 + 0.5) * g.dx, (398 + 0.9995) * g.dx], np.float32)
+        x = np.resize(xs, n).astype(np.float32)
+        buf = dev(np.concatenate([[0.0], x]).astype(np.float32))
+        dens = zeros(n_g)
+        K.get_density(buf.data_ptr() + (0 if vec else 4), dens, counter(n), g)
+        if vec:
+            x = np.concatenate([[0.0], x[:-1]]).astype(np.float32)
+        pos = x * np.float32(g.inv_dx)
+        p = np.minimum(np.floor(pos).astype(np.int64), n_g - 2)
+        rem = (pos - p.astype(np.float32)).astype(np.float64)
+        r = np.minimum(np.rint(rem * 2.0 ** 20), 2.0 ** 20)
+        acc = np.zeros(n_g)
+        np.add.at(acc, p, 2.0 ** 20 - r)
+        np.add.at(acc, p + 1, r)
+        exp = acc * (g.weight_factor_d * 2.0 ** -20)
+        exp[0] *= 2.0
+        exp[-1] *= 2.0
+        got = host(dens).astype(np.float64)
+        # one CTA-sum per CTA rounded to f32, then f32 atomics across CTAs
+        assert np.allclose(got, exp, rtol=1e-5, atol=1e-6 * exp.max())
     finally:
         cudapic.set_tuning(**saved)
 
@@ -292,6 +332,43 @@ def test_move_and_compact_deposit(cudapic, K, oracle, n, n_g):
     assert np.linalg.norm(got - r32) / np.linalg.norm(r32) < 2e-5
     r64 = oracle.get_density_f64(rx, ph)
     assert np.linalg.norm(got - r64) / np.linalg.norm(r64) < max(2e-5, 1.5 * n_g * 2.0 ** -24)
+
+
+def test_move_and_compact_deposit_fixed_point_copies_do_not_overflow(cudapic, K):
+    """Worst case of the fixed-point fused deposit: one histogram copy, one
+    CTA per SM, the particles in three cells with fractions up to ~1, and
+    enough tiles per CTA that the 32-bit copies are drained many times.  The
+    deposit equals the exact FP64 CIC sum (2^-21 weight quantum)."""
+    saved = cudapic.get_tuning()
+    try:
+        cudapic.set_tuning(density_copies=1, push_ctas_per_sm=1)
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        n = 150 * sms * 1024                 # 150 tiles per CTA: 50 drains of 3 tiles
+        n_g = 400
+        g = cudapic.grid_from_params(n_g=n_g, capacity=n)
+        xs = np.array([(200 + 0.9999) * g.dx, (37 + 0.5) * g.dx, (398 + 0.9995) * g.dx], np.float32)
+        x = np.resize(xs, n).astype(np.float32)
+        z = np.zeros(n, np.float32)
+        src = [dev(a) for a in (x, z, z, z)]
+        dst = [zeros(n) for _ in range(4)]
+        alive = counter(0)
+        nd = zeros(n_g)
+        K.move_and_compact_deposit(zeros(n_g), *src, *dst, alive, counter(n), g.factor_e, g.dt_e, nd, g)
+        assert int(host(alive)[0]) == n
+        pos = x.astype(np.float32) * np.float32(g.inv_dx)
+        p = np.minimum(np.floor(pos).astype(np.int64), n_g - 2)
+        rem = (pos - p.astype(np.float32)).astype(np.float64)
+        exp = np.zeros(n_g)
+        np.add.at(exp, p, 1.0 - rem)
+        np.add.at(exp, p + 1, rem)
+        exp *= g.weight_factor_d
+        exp[0] *= 2.0
+        exp[-1] *= 2.0
+        got = host(nd).astype(np.float64)
+        assert np.allclose(got, exp, rtol=1e-5, atol=0.0), np.flatnonzero(~np.isclose(got, exp, rtol=1e-5))
+    finally:
+        cudapic.set_tuning(**saved)
 
 
 def test_check_collisions_e_deposit_spawns(cudapic, K, oracle, dev_tables, tables):
