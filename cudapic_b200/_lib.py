@@ -67,7 +67,8 @@ class Grid(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [(name, C.c_int) for name in (
         "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
-        "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant")]
+        "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant", "step_stages",
+        "step_ctas_per_sm")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -104,6 +105,7 @@ SIGNATURES = {
     "cudapic_check_collisions_e_events": [_VP] * 18 + [_GP, _VP],
     "cudapic_check_collisions_e_deposit": [_VP] * 19 + [_GP, _VP],
     "cudapic_move_and_compact_deposit": [_VP] * 11 + [_F, _F, _VP, _GP, _VP],
+    "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
     "cudapic_accumulate_density": [_VP, _VP, _GP, _VP],
     "cudapic_accumulate_eepf": [_VP] * 7 + [_GP, _VP],

@@ -51,6 +51,25 @@ __device__ __forceinline__ bool pos_in_range(float pos, uint32_t n_g) {
     return pos >= 0.0f && pos <= (float)(n_g - 1);
 }
 
+// End of a kernel that counted particles into link.src: the last CTA to
+// finish publishes the count (StepLink, internal.h).  Every thread fences its
+// own counter atomics before the CTA's ticket is taken.
+__device__ __forceinline__ void publish_count(uint32_t *ticket, uint32_t *dst, uint32_t *src, int clear_src,
+                                              uint32_t capacity) {
+    if (!ticket) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t t = atomicAdd(ticket, 1u);
+        if (t == gridDim.x - 1) {
+            __threadfence();
+            const uint32_t v = clear_src ? atomicExch(src, 0u) : atomicAdd(src, 0u);
+            *dst = v < capacity ? v : capacity;
+            *ticket = 0u;
+        }
+    }
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

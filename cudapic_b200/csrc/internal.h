@@ -33,6 +33,17 @@ cudapic_tuning tuning();
 // Grid of a persistent kernel: min(SMs x per_sm, work units), at least 1.
 unsigned persistent_grid(int per_sm, uint64_t units);
 
+// Publishes a particle count at the end of a kernel without a separate copy
+// node: the last CTA to finish (a ticket counter, zero between launches)
+// stores min(*src, capacity) into *dst and, with clear_src, zeroes *src.
+// ticket == nullptr: nothing published.
+struct StepLink {
+    uint32_t *ticket = nullptr;
+    uint32_t *dst = nullptr;
+    uint32_t *src = nullptr;
+    int clear_src = 0;
+};
+
 // Launchers used by both the drop-in entry points and the driver.
 // zero_a / zero_b (may be null): n_g-float buffers the kernel clears after
 // reading the densities (the driver's next-step density accumulators).
@@ -43,7 +54,20 @@ int launch_poisson(const float *e_density, const float *i_density, float *pot, f
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_out = nullptr);
+                            cudaStream_t stream, float *dens_out = nullptr, const StepLink &link = StepLink());
+// True when `count` planes are 16-byte aligned and the capacity is a multiple
+// of 4 (the bulk-copy tiles of the fused electron step).
+bool electron_step_eligible(const void *const *planes, int count, uint32_t capacity);
+// Fused electron step of the driver: push, compaction, collisions with the
+// RNG stream of each particle's source slot, next-step deposit (kernels_step.cu).
+// Returns CUDAPIC_ERR_NOT_SUPPORTED, recording nothing, when the buffers do not
+// meet its alignment rules (the caller then runs push and collisions apart).
+int launch_electron_step(const float *efield, const float *sx, const float *svx, const float *svy, const float *svz,
+                         float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *rng0, uint32_t *rng1,
+                         uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
+                         float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
+                         uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
+                         const StepLink &link);
 // dep_e / dep_i (may be null): next-step densities receiving the spawns.
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,

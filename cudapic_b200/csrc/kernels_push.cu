@@ -26,6 +26,7 @@
 // a multiple of 4.
 #include "common.cuh"
 #include "internal.h"
+#include "push.cuh"
 #include "tma.cuh"
 
 namespace cudapic {
@@ -36,79 +37,12 @@ constexpr int MC_U = 4;                          // particles per thread and til
 constexpr int MC_TILE = MC_THREADS * MC_U;       // 1024
 constexpr int MC_MAX_STAGES = 6;                 // pipeline depth: cudapic_tuning.push_stages
 
-struct PushResult {
-    float x, vx;
-    bool keep;
-};
-
-__device__ __forceinline__ PushResult push_one(float xi, float vxi, const float *ef, float factor, float dt,
-                                               const cudapic_grid &g) {
-    float pos = xi * g.inv_dx;
-    if (!(pos >= 0.0f && pos < (float)g.n_g - 0.5f)) set_dev_err(g.dev_err, CUDAPIC_DEVERR_POSITION);
-    int p = cell_of(pos, g.n_g);
-    float c2 = pos - (float)p;
-    float e_x = (1.0f - c2) * ef[p] + c2 * ef[p + 1];
-    PushResult r;
-    r.vx = vxi + factor * e_x;
-    r.x = xi + r.vx * dt;
-    r.keep = r.x >= 0.0f && r.x <= g.gap;
-    return r;
-}
-
 // Survivors of one tile held in registers until their base is known.
 struct TileOut {
     float x[MC_U], vx[MC_U], vy[MC_U], vz[MC_U];
     uint32_t lane_off[MC_U];
     uint32_t keep;  // bit u: particle of row u survives
 };
-
-// Fused deposit in 2^-20 fixed point.  A particle at rem = pos - p in [0, 1]
-// adds 2^20 - r to node p and r to node p + 1, r = round(rem * 2^20), with
-// 32-bit integer shared atomics (on sm_100a several times the throughput of
-// f32 or 64-bit shared atomics; the deposit is bound by that pipe).  The
-// quantum 2^-21 of a weight is below the f32 rounding of the position
-// x * inv_dx that the reference's f32 arithmetic already carries, and the
-// integer sums are exact and order-independent.  A node of one histogram
-// copy gains at most 2^20 per particle of its copy, so the copies are
-// drained into a per-CTA 64-bit accumulator before DEP_MAX_PER_COPY
-// particles have reached one copy.
-constexpr uint32_t DEP_Q = 20;
-constexpr uint32_t DEP_MAX_PER_COPY = (1u << (32 - DEP_Q)) - 1;
-
-__device__ __forceinline__ void dep_add(uint32_t *h, float x, const cudapic_grid &g) {
-    const float pos = x * g.inv_dx;
-    const int p = cell_of(pos, g.n_g);
-    const float rem = pos - (float)p;
-    // rem can exceed 1 by an ulp at x = L (pos rounds past N_G - 1): clamp, so no weight is negative
-    const uint32_t r = min(__float2uint_rn(rem * (float)(1u << DEP_Q)), 1u << DEP_Q);
-    atomicAdd(&h[p], (1u << DEP_Q) - r);
-    atomicAdd(&h[p + 1], r);
-}
-
-// acc[k] += sum of the copies of node k; the copies are cleared.  Each node is
-// owned by one thread: no atomics.  Callers synchronise before and after.
-__device__ __forceinline__ void dep_drain(uint32_t *hist, int copies, uint32_t stride, unsigned long long *acc,
-                                          uint32_t n_g) {
-    for (uint32_t k = threadIdx.x; k < n_g; k += blockDim.x) {
-        unsigned long long v = acc[k];
-        for (int c = 0; c < copies; ++c) {
-            v += hist[(uint32_t)c * stride + k];
-            hist[(uint32_t)c * stride + k] = 0u;
-        }
-        acc[k] = v;
-    }
-}
-
-// Adds the CTA's accumulated node weights to dens_out, boundary nodes doubled.
-__device__ __forceinline__ void dep_flush(const unsigned long long *acc, float *dens_out, const cudapic_grid &g) {
-    const double w = g.weight_factor_d * (1.0 / (double)(1u << DEP_Q));
-    for (uint32_t k = threadIdx.x; k < g.n_g; k += blockDim.x) {
-        if (acc[k] == 0ull) continue;
-        float f = (float)((double)acc[k] * w);
-        if (k == 0 || k == g.n_g - 1) f *= 2.0f;
-        atomicAdd(&dens_out[k], f);
-    }
-}
 
 // DEPOSIT: also deposit every survivor's new position into dens_out (the
 // charge density of the next time step), through `copies` warp-private
@@ -121,7 +55,7 @@ __global__ void __launch_bounds__(MC_THREADS)
                                 float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
                                 float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages,
-                                float *__restrict__ dens_out, int copies, uint32_t epoch) {
+                                float *__restrict__ dens_out, int copies, uint32_t epoch, const StepLink link) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
     float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
@@ -187,7 +121,7 @@ __global__ void __launch_bounds__(MC_THREADS)
             s_ready = ok;
         }
         __syncthreads();
-        if (!s_ready) return;
+        if (!s_ready) break;  // timed out: flagged; the counts are still published
 
         const uint32_t t0 = tile * MC_TILE;
         const uint32_t cnt = min((uint32_t)MC_TILE, n - t0);
@@ -271,6 +205,7 @@ __global__ void __launch_bounds__(MC_THREADS)
         __syncthreads();
         dep_flush(acc, dens_out, g);
     }
+    publish_count(link.ticket, link.dst, link.src, link.clear_src, g.capacity);
 }
 
 // Reference-layout variant: one particle per thread, warp ballot + popc,
@@ -345,7 +280,7 @@ size_t tma_smem_bytes(uint32_t n_g, int stages, uint32_t &ef_pad) {
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_out) {
+                            cudaStream_t stream, float *dens_out, const StepLink &link) {
     const bool tma_ok = aligned16(sx) && aligned16(svx) && aligned16(svy) && aligned16(svz) &&
                         (g.capacity % 4u) == 0u;
     if (tma_ok) {
@@ -376,13 +311,20 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         const uint32_t per_tile = (uint32_t)((MC_WARPS + std::max(copies, 1) - 1) / std::max(copies, 1)) * MC_U * 32u;
         const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
         kern<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active,
-                                                 factor, dt, g, ef_pad, stages, dens_out, copies, epoch);
+                                                 factor, dt, g, ef_pad, stages, dens_out, copies, epoch, link);
         return check_launch("move_and_compact_tma");
     }
-    if (dens_out) {  // unaligned buffers: separate deposit of the compacted survivors dst[0, *alive)
+    if (dens_out || link.ticket) {  // unaligned buffers: separate deposit and count copy
         CUDAPIC_CHECK(launch_move_and_compact(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor,
                                               dt, g, stream, nullptr));
-        return cudapic_get_density(dx_, dens_out, alive, &g, (cudapic_stream_t)stream);
+        if (dens_out) CUDAPIC_CHECK(cudapic_get_density(dx_, dens_out, alive, &g, (cudapic_stream_t)stream));
+        if (link.ticket) {
+            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(link.dst, link.src, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                                     stream), "publish count"));
+            if (link.clear_src)
+                CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(link.src, 0, sizeof(uint32_t), stream), "clear count"));
+        }
+        return CUDAPIC_OK;
     }
     const size_t smem = (size_t)g.n_g * sizeof(float);
     if (smem > 48 * 1024)

@@ -1,0 +1,271 @@
+// mcc.cuh -- Monte-Carlo collision physics shared by the collision kernels
+// (kernels_mcc.cu) and the fused electron step (kernels_step.cu).
+//
+// Reference: check_collisions_e / collision_e, Rust-CUDA/src/main.rs:971-1165,
+// check_collisions_i / collision_i, :1167-1292.  The RNG draw order of the
+// reference is kept exactly; transcendentals come from detmath.cuh.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "detmath.cuh"
+#include "rng.cuh"
+
+namespace cudapic {
+
+namespace cg = cooperative_groups;
+
+__device__ __forceinline__ uint32_t energy_index(float energy) {
+    float t = fminf(energy / DE_CS_F + 0.5f, (float)(CS_RANGES - 1));
+    return (uint32_t)t;
+}
+
+struct Euler {
+    float st, ct, sp, cp;
+};
+
+// Euler angles of (gx, gy, gz), Rust-CUDA/src/main.rs:1066-1090.
+__device__ __forceinline__ Euler euler_angles(float gx, float gy, float gz) {
+    float theta, phi;
+    if (gx == 0.0f) theta = 0.5f * PI_F;
+    else theta = dm::atan2f_det(sqrtf(gy * gy + gz * gz), gx);
+    if (gy == 0.0f) phi = (gz > 0.0f) ? 0.5f * PI_F : -0.5f * PI_F;
+    else phi = dm::atan2f_det(gz, gy);
+    Euler e;
+    dm::sincosf_det(theta, &e.st, &e.ct);
+    dm::sincosf_det(phi, &e.sp, &e.cp);
+    return e;
+}
+
+// Scattered relative velocity, Rust-CUDA/src/main.rs:1152-1158.
+__device__ __forceinline__ void rotate(float g, float sc, float cc, float se, float ce, const Euler &a, float &gx,
+                                       float &gy, float &gz) {
+    gx = g * (a.ct * cc - a.st * sc * ce);
+    gy = g * (a.st * a.cp * cc + a.ct * a.cp * sc * ce - a.sp * sc * se);
+    gz = g * (a.st * a.sp * cc + a.ct * a.sp * sc * ce + a.cp * sc * se);
+}
+
+// Claims one slot of `counter` for every lane of the calling coalesced
+// group with a single atomicAdd; never hands out a slot >= capacity.
+__device__ __forceinline__ bool claim_slot(uint32_t *counter, uint32_t capacity, uint32_t &slot) {
+    cg::coalesced_group grp = cg::coalesced_threads();
+    uint32_t base = 0, granted = 0;
+    if (grp.thread_rank() == 0) {
+        const uint32_t cnt = grp.size();
+        const uint32_t old = atomicAdd(counter, cnt);
+        granted = old >= capacity ? 0u : min(cnt, capacity - old);
+        if (granted < cnt) atomicSub(counter, cnt - granted);
+        base = old;
+    }
+    base = grp.shfl(base, 0);
+    granted = grp.shfl(granted, 0);
+    slot = base + grp.thread_rank();
+    return grp.thread_rank() < granted;
+}
+
+// Collision decision u < p with p = 1 - exp(-a), a = nu dt (the reference
+// evaluates exp(-nu * dt) with -nu * dt == -(nu * dt) exactly,
+// Rust-CUDA/src/main.rs:1011, 1196).  Since 1 - e^-a <= a, exp_det is
+// within 2 ulp and 1 - y is exact for y >= 1/2, the computed p never
+// exceeds a + 3.1e-7: any u >= fl(a + 5e-7) is a certain "no collision",
+// decided without evaluating exp (about 99 % of draws at the reference
+// conditions).  The decision is bit-identical to the full test.
+__device__ __forceinline__ bool collision_draw(float u, float a) {
+    if (u >= a + 5e-7f) return false;
+    const float p_coll = 1.0f - dm::expf_det(-a);
+    return u < p_coll;
+}
+
+// Outcome of the collision test of one particle.
+struct Test {
+    uint32_t idx;
+    bool collide;
+};
+
+// sigma_tot lookups: straight from the global table (read-only path), or
+// from a shared-memory copy of its first `resident` entries.
+struct GlobalTable {
+    const float *__restrict__ t;
+    __device__ __forceinline__ float operator()(uint32_t idx) const { return __ldg(t + idx); }
+};
+struct ResidentTable {
+    const float *__restrict__ t;   // global table
+    const float *s;                // shared copy of t[0 .. resident)
+    uint32_t resident;
+    __device__ __forceinline__ float operator()(uint32_t idx) const {
+        return idx < resident ? s[idx] : __ldg(t + idx);
+    }
+};
+
+// Electron collision test, Rust-CUDA/src/main.rs:992-1012 (one draw).
+template <typename Table>
+__device__ __forceinline__ Test test_electron(float vxi, float vyi, float vzi, Xoshiro128p &rs,
+                                              const Table &sigma_tot_e, const cudapic_grid &g) {
+    const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
+    const float energy = g.half_me_over_e * v2;
+    Test t;
+    t.idx = energy_index(energy);
+    const float velocity = sqrtf(v2);
+    const float nu = sigma_tot_e(t.idx) * velocity;
+    const float rand_val = rs.uniform();
+    t.collide = collision_draw(rand_val, nu * g.dt_e);
+    return t;
+}
+
+// CIC deposit of one particle straight into a global density (boundary
+// nodes doubled per contribution, equal to doubling the node sum).
+__device__ __forceinline__ void deposit_global(float *dens, float xv, const cudapic_grid &g) {
+    const float pos = xv * g.inv_dx;
+    const int p = cell_of(pos, g.n_g);
+    const float rem = pos - (float)p;
+    float c1 = (1.0f - rem) * g.weight_factor;
+    float c2 = rem * g.weight_factor;
+    if (p == 0) c1 *= 2.0f;
+    if (p + 1 == (int)g.n_g - 1) c2 *= 2.0f;
+    atomicAdd(&dens[p], c1);
+    atomicAdd(&dens[p + 1], c2);
+}
+
+// collision_e, Rust-CUDA/src/main.rs:1035-1165: scatters electron i (state
+// rs already past the test draw), writes its velocity and any spawns;
+// returns the event (1 elastic, 2 excitation, 3 ionization).  dep_e / dep_i
+// (may be null): next-step densities that also receive the spawned
+// electron / ion.
+static __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
+                                                  Xoshiro128p &rs, const float *__restrict__ cs, float *x, float *vx,
+                                                  float *vy, float *vz, float *ix, float *ivx, float *ivy,
+                                                  float *ivz, uint32_t *alive_e, uint32_t *alive_i,
+                                                  const cudapic_grid &g, float *dep_e, float *dep_i) {
+    const float exc_j = 11.5f * E_CHARGE_F;
+    const float ion_j = 15.8f * E_CHARGE_F;
+    float gx = vxi, gy = vyi, gz = vzi;
+    float gm = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float wx = g.f1 * vxi, wy = g.f1 * vyi, wz = g.f1 * vzi;
+    const float t0 = __ldg(cs + idx);
+    const float t1 = t0 + __ldg(cs + CS_RANGES + idx);
+    const float t2 = t1 + __ldg(cs + 2 * CS_RANGES + idx);
+    const Euler eu = euler_angles(gx, gy, gz);
+    float chi_s, chi_c, eta;
+    uint32_t ev;
+    const float rnd = rs.uniform();
+    if (rnd < t0 / t2) {
+        ev = 1;  // elastic
+        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        eta = TWO_PI_F * rs.uniform();
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    } else if (rnd < t1 / t2) {
+        ev = 2;  // excitation
+        float en = 0.5f * E_MASS_F * gm * gm;
+        en = fabsf(en - exc_j);
+        gm = sqrtf(2.0f * en / E_MASS_F);
+        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        eta = TWO_PI_F * rs.uniform();
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    } else {
+        ev = 3;  // ionization
+        float en = 0.5f * E_MASS_F * gm * gm;
+        en = fabsf(en - ion_j);
+        const float e_new =
+            10.0f * dm::tanf_det(rs.uniform() * dm::atanf_det(en / E_CHARGE_F / 20.0f)) * E_CHARGE_F;
+        const float e_orig = fabsf(en - e_new);
+        gm = sqrtf(2.0f * e_orig / E_MASS_F);
+        const float g_new = sqrtf(2.0f * e_new / E_MASS_F);
+        const float chi = dm::acosf_det(sqrtf(e_orig / en));
+        const float chi_new = dm::acosf_det(sqrtf(e_new / en));
+        eta = TWO_PI_F * rs.uniform();
+        const float eta_new = eta + PI_F;
+        float sc2, cc2, se2, ce2;
+        dm::sincosf_det(chi_new, &sc2, &cc2);
+        dm::sincosf_det(eta_new, &se2, &ce2);
+        float ngx, ngy, ngz;
+        rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
+        const float xi = x[i];
+        uint32_t slot;
+        if (claim_slot(alive_e, g.capacity, slot)) {
+            x[slot] = xi;
+            vx[slot] = wx + g.f2 * ngx;
+            vy[slot] = wy + g.f2 * ngy;
+            vz[slot] = wz + g.f2 * ngz;
+            if (dep_e) deposit_global(dep_e, xi, g);
+        } else {
+            set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
+        }
+        float a, b, c;
+        rs.three_normal(g.normal_range, a, b, c);
+        if (claim_slot(alive_i, g.capacity, slot)) {
+            ix[slot] = xi;
+            ivx[slot] = a;
+            ivy[slot] = b;
+            ivz[slot] = c;
+            if (dep_i) deposit_global(dep_i, xi, g);
+        } else {
+            set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
+        }
+        dm::sincosf_det(chi, &chi_s, &chi_c);
+    }
+    float se, ce;
+    dm::sincosf_det(eta, &se, &ce);
+    float ngx, ngy, ngz;
+    rotate(gm, chi_s, chi_c, se, ce, eu, ngx, ngy, ngz);
+    vx[i] = wx + g.f2 * ngx;
+    vy[i] = wy + g.f2 * ngy;
+    vz[i] = wz + g.f2 * ngz;
+    return ev;
+}
+
+struct IonTest {
+    uint32_t idx;
+    float vxa, vya, vza;
+    bool collide;
+};
+
+// Ion collision test with a Maxwellian target, Rust-CUDA/src/main.rs:1180-1197.
+template <typename Table>
+__device__ __forceinline__ IonTest test_ion(float vxi, float vyi, float vzi, Xoshiro128p &rs,
+                                            const Table &sigma_tot_i, const cudapic_grid &g) {
+    IonTest t;
+    rs.three_normal(g.normal_range, t.vxa, t.vya, t.vza);
+    const float gx = vxi - t.vxa, gy = vyi - t.vya, gz = vzi - t.vza;
+    const float g2 = gx * gx + gy * gy + gz * gz;
+    const float energy = g.half_mu_over_e * g2;
+    t.idx = energy_index(energy);
+    const float gmag = sqrtf(g2);
+    const float nu = sigma_tot_i(t.idx) * gmag;
+    const float rand_val = rs.uniform();
+    t.collide = collision_draw(rand_val, nu * g.dt_i);
+    return t;
+}
+
+// collision_i, Rust-CUDA/src/main.rs:1221-1292; returns 4 isotropic, 5 backscatter.
+static __device__ __noinline__ uint32_t collide_ion(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi, float vxa,
+                                             float vya, float vza, Xoshiro128p &rs, const float *__restrict__ cs,
+                                             float *vx, float *vy, float *vz, const cudapic_grid &g) {
+    const float gx = vxi - vxa, gy = vyi - vya, gz = vzi - vza;
+    const float t0 = __ldg(cs + 3 * CS_RANGES + idx);
+    const float t1 = t0 + __ldg(cs + 4 * CS_RANGES + idx);
+    const float gg = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float wx = 0.5f * (vxi + vxa), wy = 0.5f * (vyi + vya), wz = 0.5f * (vzi + vza);
+    const Euler eu = euler_angles(gx, gy, gz);
+    const float rnd = rs.uniform();
+    float chi;
+    uint32_t ev;
+    if (rnd < t0 / t1) {
+        ev = 4;
+        chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+    } else {
+        ev = 5;
+        chi = PI_F;
+    }
+    const float eta = TWO_PI_F * rs.uniform();
+    float sc, cc, se, ce;
+    dm::sincosf_det(chi, &sc, &cc);
+    dm::sincosf_det(eta, &se, &ce);
+    float ngx, ngy, ngz;
+    rotate(gg, sc, cc, se, ce, eu, ngx, ngy, ngz);
+    vx[i] = wx + 0.5f * ngx;
+    vy[i] = wy + 0.5f * ngy;
+    vz[i] = wz + 0.5f * ngz;
+    return ev;
+}
+
+}  // namespace cudapic

@@ -17,6 +17,7 @@
 //    steps) measures the work actually done.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -37,7 +38,7 @@ struct cudapic_state {
     float *x[2][2] = {}, *vx[2][2] = {}, *vy[2][2] = {}, *vz[2][2] = {};
     int side[2] = {0, 0};
     uint32_t *rng[2][4] = {};
-    // counters block: n_e, n_i, alive, step, dev_err, pad..., work (u64 at +32)
+    // counters block: n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work (u64 at +32)
     uint32_t *counters = nullptr;
     float *efield = nullptr, *pot = nullptr, *pot0_table = nullptr;
     // Charge densities, double-buffered for the fused step: [cur] feeds the
@@ -49,6 +50,7 @@ struct cudapic_state {
     bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
+    float sigma_max_e = 0.0f;  // largest entry of sigma_tot_e (the fused step's certain-rejection bound)
     double *cumul_e = nullptr, *cumul_i = nullptr;
     uint32_t *eepf = nullptr;
 
@@ -63,6 +65,8 @@ struct cudapic_state {
     uint32_t *alive() const { return counters + 2; }
     uint32_t *step_counter() const { return counters + 3; }
     uint32_t *dev_err() const { return counters + 4; }
+    uint32_t *alive_i() const { return counters + 5; }  // fused mode: ion push slot counter
+    uint32_t *ticket() const { return counters + 6; }   // fused mode: CTA completion ticket (StepLink)
     unsigned long long *work() const { return reinterpret_cast<unsigned long long *>(counters + 8); }
     float *e_density() const { return e_dens[e_cur]; }
     float *i_density() const { return i_dens[i_cur]; }
@@ -99,6 +103,58 @@ void destroy_graphs(cudapic_state *s) {
     }
 }
 
+// Particle part of a fused-mode step: [ion push] -> fused electron step ->
+// [ion collisions] -> [measurement]; the kernels publish the particle counts
+// themselves (StepLink), so the step holds no copy or memset node.  The
+// electrons draw from the RNG stream of their source slot (kernels_step.cu).
+// Returns CUDAPIC_ERR_NOT_SUPPORTED, having enqueued nothing, when the
+// electron planes are not aligned for the fused kernel.
+int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, float *i_acc) {
+    const cudapic_grid &g = s->grid;
+    cudaStream_t st = s->stream;
+    const int E = 0, I = 1;
+    int se = s->side[E], si = s->side[I];
+    const void *planes[8] = {s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
+                             s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3]};
+    if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
+    if (ion_step) {
+        StepLink li;
+        li.ticket = s->ticket();
+        li.dst = s->n_i();
+        li.src = s->alive_i();
+        li.clear_src = 1;
+        CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
+                                              s->x[I][si ^ 1], s->vx[I][si ^ 1], s->vy[I][si ^ 1],
+                                              s->vz[I][si ^ 1], s->alive_i(), s->n_i(), g.factor_i, g.dt_i, g, st,
+                                              i_acc, li));
+        si ^= 1;
+        s->side[I] = si;
+    }
+    StepLink le;
+    le.ticket = s->ticket();
+    le.dst = s->n_e();
+    le.src = s->alive();
+    le.clear_src = 1;
+    CUDAPIC_CHECK(launch_electron_step(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
+                                       s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
+                                       s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3], s->sigma_tot_e, s->cs,
+                                       s->sigma_max_e, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
+                                       s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le));
+    se ^= 1;
+    s->side[E] = se;
+    s->e_cur ^= 1;
+    if (ion_step) {
+        CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
+                                          s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
+                                          nullptr, g, st));
+    }
+    if (s->measure) {
+        CUDAPIC_CHECK(launch_eepf(s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->efield, s->n_e(),
+                                  s->eepf, g, st));
+    }
+    return CUDAPIC_OK;
+}
+
 // One reference time step (Rust-CUDA/src/main.rs:1728-1807).
 int enqueue_step(cudapic_state *s, bool ion_step) {
     const cudapic_grid &g = s->grid;
@@ -115,6 +171,9 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
         CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density(), 0, nb, st), "memset e_density"));
         CUDAPIC_CHECK(cudapic_get_density(s->x[E][se], s->e_density(), s->n_e(), &g, (cudapic_stream_t)st));
         if (fused) {  // priming: both ion buffers hold the density of the present ions
+            // the published-count kernels expect their slot counters and ticket at zero
+            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
+            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive_i(), 0, 2 * sizeof(uint32_t), st), "memset alive_i"));
             CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_dens[s->i_cur], 0, nb, st), "memset i_density"));
             CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_dens[s->i_cur], s->n_i(), &g, (cudapic_stream_t)st));
             CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->i_dens[s->i_cur ^ 1], s->i_dens[s->i_cur], nb,
@@ -142,6 +201,10 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     if (s->measure) {
         CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density(), s->cumul_e, &g, (cudapic_stream_t)st));
         if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density(), s->cumul_i, &g, (cudapic_stream_t)st));
+    }
+    if (fused) {
+        const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc);
+        if (rc != CUDAPIC_ERR_NOT_SUPPORTED) return rc;  // else: buffers not aligned for the fused kernel
     }
     // electrons: push + compact into the other side
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
@@ -304,6 +367,7 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
     // cross sections (host, all threads), Rust-CUDA/src/main.rs:1649, 1378-1444
     std::vector<float> cs(5ull * CUDAPIC_CS_RANGES), se(CUDAPIC_CS_RANGES), si(CUDAPIC_CS_RANGES);
     if ((rc = cudapic_cross_sections(grid.gas_density, cs.data(), se.data(), si.data()))) return cleanup(rc);
+    s->sigma_max_e = *std::max_element(se.begin(), se.end());
     if ((rc = check_cuda(cudaMemcpyAsync(s->pot0_table, table.data(), table.size() * sizeof(float),
                                          cudaMemcpyHostToDevice, s->stream), "upload pot0 table")) ||
         (rc = check_cuda(cudaMemcpyAsync(s->cs, cs.data(), cs.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream),

@@ -87,6 +87,18 @@ def check_collisions_e_deposit(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rn
     check(lib.cudapic_check_collisions_e_deposit(*args, _g(grid), _stream(stream, vx)))
 
 
+def step_electrons(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, rng0, rng1, rng2, rng3,
+                   total_cs_e, cs, sigma_max_e, i_x, i_vx, i_vy, i_vz, alive_counter, n_e, n_i, e_next_density,
+                   i_next_density, grid, stream=None):
+    """Fused electron step: push, collisions with the RNG stream of each
+    electron's source slot, compaction and next-step deposit in one launch
+    (does the work of move_and_compact + check_collisions_e + get_density)."""
+    head = [_ptr(a) for a in (efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, rng0, rng1, rng2,
+                              rng3, total_cs_e, cs)]
+    tail = [_ptr(a) for a in (i_x, i_vx, i_vy, i_vz, alive_counter, n_e, n_i, e_next_density, i_next_density)]
+    check(lib.cudapic_step_electrons(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, src_x)))
+
+
 def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz,
                        alive_e, alive_i, grid, stream=None, events=None):
     """check_collisions_e (Rust-CUDA/src/main.rs:971-1165).  With `events`

@@ -139,6 +139,8 @@ typedef struct cudapic_tuning {
     int mcc_ctas_per_sm;
     int mcc_variant;          /* 1: shared-memory resident sigma table (any alignment),
                                  2: bulk-copy staged tiles (16-byte aligned pointers)    */
+    int step_stages;          /* fused electron step bulk-copy pipeline depth: 2..4      */
+    int step_ctas_per_sm;
 } cudapic_tuning;
 
 int cudapic_get_tuning(cudapic_tuning *out);
@@ -214,6 +216,26 @@ int cudapic_check_collisions_e_deposit(const float *total_cs_e, const float *cs,
                                        float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
                                        float *e_next_density, float *i_next_density, const cudapic_grid *grid,
                                        cudapic_stream_t stream);
+
+/* Fused electron step: one launch doing the work of move_and_compact
+ * (Rust-CUDA/src/main.rs:566-678), check_collisions_e (:971-1165) and the
+ * next step's get_density (:356-406); no single reference counterpart.
+ * Electron k of src[0, *n_e) is pushed in `efield` (factor_e, dt_e of the
+ * grid); a survivor is tested for a collision with the RNG stream of slot k
+ * (the planes are updated in place), scattered, and written with any
+ * spawned electron to dst[0, *alive_counter) (*alive_counter must be 0 on
+ * entry; order unspecified); spawned ions are appended at *n_i (bounded by
+ * capacity).  Survivors and spawned electrons are added to e_next_density,
+ * spawned ions to i_next_density (both accumulate).  sigma_max_e must be
+ * the largest entry of total_cs_e: it bounds the collision probability so
+ * that most electrons skip the table (decisions are bit-identical).  The
+ * eight planes must be 16-byte aligned and the capacity a multiple of 4. */
+int cudapic_step_electrons(const float *efield, const float *src_x, const float *src_vx, const float *src_vy,
+                           const float *src_vz, float *dst_x, float *dst_vx, float *dst_vy, float *dst_vz,
+                           uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, const float *total_cs_e,
+                           const float *cs, float sigma_max_e, float *i_x, float *i_vx, float *i_vy, float *i_vz,
+                           uint32_t *alive_counter, const uint32_t *n_e, uint32_t *n_i, float *e_next_density,
+                           float *i_next_density, const cudapic_grid *grid, cudapic_stream_t stream);
 
 /* check_collisions_i (Rust-CUDA/src/main.rs:1167-1292): MCC of ions
  * [0, *active_i) against Maxwellian target atoms. */

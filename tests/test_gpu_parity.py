@@ -500,6 +500,73 @@ def test_check_collisions_e_bit_exact(cudapic, K, oracle, dev_tables, tables, n,
     assert np.array_equal(sorted_rows(*[a[n_i0:ni] for a in gi_arr]), sorted_rows(*[h[n_i0:ni] for h in i_h]))
 
 
+@pytest.mark.parametrize("n,n_t,temp", [(1, 4000, 30.0), (4099, 200, 30.0), (300_001, 100, 60.0),
+                                        (1_000_003, 20, 80.0), (4_194_304, 4000, 3.0)])
+def test_step_electrons_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp):
+    """Fused electron step against the oracle's move_and_compact followed by
+    its check_collisions_e over the survivors, each survivor drawing from the
+    RNG stream of its source slot: RNG planes bit-exact (every slot), the
+    electron and ion sets bit-exact, densities within the deposit tolerance."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    cs, se, si = tables
+    dcs, dse, _ = dev_tables
+    n_i0 = 1000
+    cap = (2 * n + 4096 + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=n_t, capacity=cap)
+    ph = oracle.phys_from_params(n_t=n_t, capacity=cap)
+    x, vx, vy, vz = steady_state(n, E_MASS, temp, dt=g.dt_e, seed=n + 11)
+    ef = field_profile(400)
+    pad = lambda a, dt=np.float32: np.concatenate([a, np.zeros(cap - len(a), dt)])  # noqa: E731
+    rng = [pad(np.asarray(p), np.uint32) for p in oracle.seed_streams([3, 1, 4, 1], cap)[:4]]
+    # oracle: push, then collisions of the survivors with their source slots' streams
+    rx, rvx, rvy, rvz, src = oracle.move_and_compact(ef, x, vx, vy, vz, g.factor_e, g.dt_e, ph)
+    m = rx.size
+    e_h = [pad(a) for a in (rx, rvx, rvy, rvz)]
+    r_sub = [pad(p[src], np.uint32) for p in rng]
+    i_h = [pad(np.full(n_i0, 0.0125, np.float32)) for _ in range(4)]
+    _, ne_ref, ni_ref, dropped = oracle.check_collisions_e(se, cs, m, e_h, r_sub, i_h, m, n_i0, ph)
+    assert dropped == 0
+    r_ref = [p.copy() for p in rng]
+    for k in range(4):
+        r_ref[k][src] = r_sub[k][:m]
+    # GPU
+    src_d = [dev(pad(a)) for a in (x, vx, vy, vz)]
+    dst_d = [zeros(cap) for _ in range(4)]
+    r_d = [dev(p) for p in rng]
+    i_d = [dev(pad(np.full(n_i0, 0.0125, np.float32))) for _ in range(4)]
+    alive, n_i = counter(0), counter(n_i0)
+    de, di = zeros(400), zeros(400)
+    K.step_electrons(dev(ef), *src_d, *dst_d, *r_d, dse, dcs, float(se.max()), *i_d, alive, counter(n), n_i, de, di,
+                     g)
+    ne, ni = int(host(alive)[0]), int(host(n_i)[0])
+    assert (ne, ni) == (ne_ref, ni_ref)
+    if n > 100_000 and n_t <= 100:
+        assert m < n and ne_ref > m        # absorption and ionization both exercised
+    for d, h in zip(r_d, r_ref):
+        assert np.array_equal(host(d), h)
+    got = [host(d)[:ne] for d in dst_d]
+    assert np.array_equal(sorted_rows(*got), sorted_rows(*[h[:ne] for h in e_h]))
+    gi = [host(d) for d in i_d]
+    assert np.array_equal(sorted_rows(*[a[n_i0:ni] for a in gi]), sorted_rows(*[h[n_i0:ni] for h in i_h]))
+    ref_e = oracle.get_density_f64(got[0], ph)
+    assert np.linalg.norm(host(de) - ref_e) / np.linalg.norm(ref_e) < 2e-5
+    if ni > n_i0:
+        ref_i = oracle.get_density_f64(gi[0][n_i0:ni], ph)
+        assert np.linalg.norm(host(di) - ref_i) / np.linalg.norm(ref_i) < 2e-5
+
+
+def test_step_electrons_rejects_unaligned_planes(cudapic, K, dev_tables, tables):
+    _, se, _ = tables
+    dcs, dse, _ = dev_tables
+    g = cudapic.grid_from_params(capacity=1024)
+    b = [zeros(1025) for _ in range(8)]
+    r = [zeros(1025, np.uint32) for _ in range(4)]
+    with pytest.raises(cudapic.CudapicError):
+        K.step_electrons(zeros(400), *[t.data_ptr() + 4 for t in b[:4]], *b[4:], *r, dse, dcs, float(se.max()),
+                         *[zeros(1024) for _ in range(4)], counter(0), counter(10), counter(0), zeros(400),
+                         zeros(400), g)
+
+
 @pytest.mark.parametrize("layout", ["aligned", "unaligned"])
 @pytest.mark.parametrize("n,n_t,temp", [(1, 4000, 1.0), (65_537, 4000, 0.03), (300_001, 200, 2.0),
                                         (300_001, 20, 20.0), (4_194_304, 4000, 0.03)])
