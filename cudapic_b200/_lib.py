@@ -60,7 +60,7 @@ class Grid(C.Structure):
         ("eepf_half_kick", C.c_float),
         ("dx", C.c_double), ("weight_factor_d", C.c_double), ("gas_density", C.c_double),
         ("voltage", C.c_double),
-        ("dev_err", C.c_void_p), ("work", C.c_void_p),
+        ("dev_err", C.c_void_p), ("work", C.c_void_p), ("sigma_max_e", C.c_float),
     ]
 
 
@@ -68,7 +68,7 @@ class Tuning(C.Structure):
     _fields_ = [(name, C.c_int) for name in (
         "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
         "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant", "step_stages",
-        "step_ctas_per_sm")]
+        "step_ctas_per_sm", "step_rows")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -86,7 +86,7 @@ class Buffers(C.Structure):
         ("efield", C.c_void_p), ("pot", C.c_void_p), ("e_density", C.c_void_p), ("i_density", C.c_void_p),
         ("cs", C.c_void_p), ("sigma_tot_e", C.c_void_p), ("sigma_tot_i", C.c_void_p),
         ("cumul_e_density", C.c_void_p), ("cumul_i_density", C.c_void_p), ("eepf", C.c_void_p),
-        ("dev_err", C.c_void_p), ("work", C.c_void_p),
+        ("dev_err", C.c_void_p), ("work", C.c_void_p), ("sigma_max_e", C.c_float),
     ]
 
 

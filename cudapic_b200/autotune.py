@@ -3,8 +3,8 @@
 Sweeps, on the live GPU and a given population, the CTA size / CTAs per SM /
 warp-private histogram copies / cluster size of get_density, the bulk-copy
 pipeline depth and CTAs per SM of move_and_compact (timed with the fused
-deposit of the driver step), and those of
-check_collisions_e; each candidate is timed with CUDA events (median of
+deposit of the driver step), those of check_collisions_e and those of the
+fused electron step; each candidate is timed with CUDA events (median of
 `reps` launches, L2 flushed before each launch) and the fastest is kept.
 
     python -m cudapic_b200.autotune [--particles N] [--n-g 400] [--out tuning.json]
@@ -70,7 +70,7 @@ def tune(st, reps=5, verbose=True):
     alive = u32(0)
     alive_e, alive_i = u32(n_e), u32(n_i)
     base = cp.get_tuning()
-    results = {"get_density": [], "move_and_compact": [], "check_collisions_e": []}
+    results = {"get_density": [], "move_and_compact": [], "check_collisions_e": [], "step_electrons": []}
 
     def density():
         K.get_density(b.x[0], dens, ne_c, g, stream=s)
@@ -91,6 +91,18 @@ def tune(st, reps=5, verbose=True):
         alive_e.fill_(n_e)
         alive_i.fill_(n_i)
 
+    dens_i = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
+
+    def step_e():  # the fused driver's electron kernel
+        K.step_electrons(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0],
+                         b.tmp_vz[0], *b.rng[0], b.sigma_tot_e, b.cs, b.sigma_max_e, b.x[1], b.vx[1], b.vy[1],
+                         b.vz[1], alive, ne_c, alive_i, dens, dens_i, g, stream=s)
+
+    def reset_step():
+        alive.zero_()
+        alive_i.fill_(n_i)
+        dens.zero_()
+
     sweeps = [
         ("get_density", density, None,
          [dict(density_threads=t, density_ctas_per_sm=c, density_copies=k, density_cluster=cl)
@@ -101,6 +113,9 @@ def tune(st, reps=5, verbose=True):
         ("check_collisions_e", mcc, reset_alive,
          [dict(mcc_variant=1)] +
          [dict(mcc_variant=2, mcc_stages=st_, mcc_ctas_per_sm=c) for st_, c in itertools.product((2, 3, 4), (2, 3, 4))]),
+        ("step_electrons", step_e, reset_step,
+         [dict(step_rows=r, step_stages=st_, step_ctas_per_sm=c)
+          for r, st_, c in itertools.product((2, 4), (2, 3, 4, 5, 6), (1, 2, 3, 4))]),
     ]
     best = dict(base)
     for name, fn, pre, configs in sweeps:

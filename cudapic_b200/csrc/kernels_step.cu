@@ -16,8 +16,8 @@
 //
 // B200 design (HBM-bound: 16 B of particle and 16 B of RNG state read, the
 // same written per survivor -- 64 B against 76 B for push + collisions):
-//  * persistent grid, 256 threads, tiles of 1024 particles; the eight SoA
-//    planes of a tile (x, vx, vy, vz, rng0..3: 32 KB) are staged by
+//  * persistent grid, 256 threads, tiles of 512 or 1024 particles; the eight
+//    SoA planes of a tile (x, vx, vy, vz, rng0..3: 16 or 32 KB) are staged by
 //    cp.async.bulk on an mbarrier pipeline;
 //  * certain rejection without the cross-section table: the exact test
 //    (mcc.cuh) decides "no collision" whenever u >= fl(a + 5e-7) with
@@ -49,17 +49,23 @@ namespace cudapic {
 
 constexpr int ES_THREADS = 256;
 constexpr int ES_WARPS = ES_THREADS / 32;
-constexpr int ES_U = 4;                       // particles per thread and tile
-constexpr int ES_TILE = ES_THREADS * ES_U;    // 1024
 constexpr int ES_PLANES = 8;                  // x, vx, vy, vz, rng0..3
-constexpr int ES_MAX_STAGES = 4;              // pipeline depth: cudapic_tuning.step_stages
-constexpr int ES_QCAP = 32 + 32 * ES_U;       // a warp drains at 32; one tile adds <= 128
-static_assert(ES_U * ES_WARPS == 32, "one warp scans the (row, warp) counts");
+constexpr int ES_MAX_STAGES = 6;              // pipeline depth: cudapic_tuning.step_stages
+// U (cudapic_tuning.step_rows, 2 or 4): particles per thread and tile, so a
+// tile holds 256 U particles (8 KB U of staged planes); a warp's collider
+// queue holds 31 + 32 U entries at most.
+template <int U>
+struct StepShape {
+    static constexpr int TILE = ES_THREADS * U;
+    static constexpr int QCAP = 32 + 32 * U;
+    static_assert(U * ES_WARPS <= 32, "one warp scans the (row, warp) counts");
+};
 
 // Survivors of one tile held in registers until their base is known.
+template <int U>
 struct StepOut {
-    float x[ES_U], vx[ES_U], vy[ES_U], vz[ES_U];
-    uint32_t lane_off[ES_U];
+    float x[U], vx[U], vy[U], vz[U];
+    uint32_t lane_off[U];
     uint32_t keep;  // bit u: the particle of row u is written by the tile
 };
 
@@ -69,6 +75,7 @@ __device__ __forceinline__ bool may_collide(float u, float velocity, float sigma
     return u < sigma_max * velocity * dt + 5e-7f;
 }
 
+template <int U>
 __global__ void __launch_bounds__(ES_THREADS)
     electron_step_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
                          const float *__restrict__ svx, const float *__restrict__ svy,
@@ -79,6 +86,9 @@ __global__ void __launch_bounds__(ES_THREADS)
                          const uint32_t *__restrict__ n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                          const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int stages, int copies,
                          uint32_t epoch, const StepLink link) {
+    constexpr int ES_TILE = StepShape<U>::TILE;
+    constexpr int ES_QCAP = StepShape<U>::QCAP;
+    constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *in = reinterpret_cast<uint32_t *>(smem);                                   // [stages][8][TILE]
     float *ef = reinterpret_cast<float *>(in + stages * ES_PLANES * ES_TILE);             // [ef_pad]
@@ -86,7 +96,7 @@ __global__ void __launch_bounds__(ES_THREADS)
     uint32_t *hist = reinterpret_cast<uint32_t *>(acc + ef_pad);                          // [copies][ef_pad]
     uint32_t *queue = hist + (uint32_t)copies * ef_pad;                                   // [WARPS][QCAP]
     uint64_t *bar = reinterpret_cast<uint64_t *>(queue + ES_WARPS * ES_QCAP);             // [stages]
-    __shared__ uint32_t offs[2][ES_U * ES_WARPS];  // counts, then exclusive offsets
+    __shared__ uint32_t offs[2][NSEG];  // counts, then exclusive offsets
     __shared__ uint32_t s_base[2];
     __shared__ int s_ready;
 
@@ -152,7 +162,7 @@ __global__ void __launch_bounds__(ES_THREADS)
         __syncwarp();
     };
 
-    StepOut prev;
+    StepOut<U> prev;
     bool have_prev = false;
     uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
     uint32_t qn = 0;            // this warp's queued colliders (warp-uniform)
@@ -176,10 +186,10 @@ __global__ void __launch_bounds__(ES_THREADS)
         const uint32_t t0 = tile * ES_TILE;
         const uint32_t cnt = min((uint32_t)ES_TILE, n - t0);
         const uint32_t *b = in + s * ES_PLANES * ES_TILE;
-        StepOut cur;
+        StepOut<U> cur;
         cur.keep = 0;
 #pragma unroll
-        for (int u = 0; u < ES_U; ++u) {
+        for (int u = 0; u < U; ++u) {
             const uint32_t j = (uint32_t)u * ES_THREADS + tid;
             bool stay = false, collide = false;
             cur.x[u] = cur.vx[u] = cur.vy[u] = cur.vz[u] = 0.0f;
@@ -231,7 +241,7 @@ __global__ void __launch_bounds__(ES_THREADS)
         if (have_prev) {
             const uint32_t base = s_base[(it - 1) & 1];
 #pragma unroll
-            for (int u = 0; u < ES_U; ++u) {
+            for (int u = 0; u < U; ++u) {
                 if (prev.keep & (1u << u)) {
                     const uint32_t slot = base + offs[(it - 1) & 1][u * ES_WARPS + warp] + prev.lane_off[u];
                     if (slot < g.capacity) {
@@ -246,14 +256,14 @@ __global__ void __launch_bounds__(ES_THREADS)
             }
         }
         if (warp == 0) {
-            const uint32_t v = offs[it & 1][lane];
+            const uint32_t v = lane < NSEG ? offs[it & 1][lane] : 0u;
             uint32_t incl = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += t;
             }
-            offs[it & 1][lane] = incl - v;
+            if (lane < NSEG) offs[it & 1][lane] = incl - v;
             if (lane == 31) pending_base = incl ? atomicAdd(alive, incl) : 0u;
         }
         prev = cur;
@@ -268,7 +278,7 @@ __global__ void __launch_bounds__(ES_THREADS)
     if (have_prev) {
         const uint32_t base = s_base[(it - 1) & 1];
 #pragma unroll
-        for (int u = 0; u < ES_U; ++u) {
+        for (int u = 0; u < U; ++u) {
             if (prev.keep & (1u << u)) {
                 const uint32_t slot = base + offs[(it - 1) & 1][u * ES_WARPS + warp] + prev.lane_off[u];
                 if (slot < g.capacity) {
@@ -297,15 +307,18 @@ bool electron_step_eligible(const void *const *planes, int count, uint32_t capac
     return true;
 }
 
-int launch_electron_step(const float *efield, const float *sx, const float *svx, const float *svy, const float *svz,
-                         float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *rng0, uint32_t *rng1,
-                         uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
-                         float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
-                         uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
-                         const StepLink &link) {
-    const void *planes[8] = {sx, svx, svy, svz, rng0, rng1, rng2, rng3};
-    if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
-    const cudapic_tuning t = tuning();
+namespace {
+
+template <int U>
+int launch_electron_step_t(const float *efield, const float *sx, const float *svx, const float *svy,
+                           const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *rng0,
+                           uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs,
+                           float sigma_max_e, float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
+                           const uint32_t *n_active, uint32_t *n_i, float *dens_e, float *dens_i,
+                           const cudapic_grid &g, cudaStream_t stream, const StepLink &link,
+                           const cudapic_tuning &t) {
+    constexpr int ES_TILE = StepShape<U>::TILE;
+    constexpr int ES_QCAP = StepShape<U>::QCAP;
     int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
     int copies = std::max(1, std::min(t.density_copies, ES_WARPS));
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
@@ -318,7 +331,7 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
     while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "step_electrons: n_g too large");
     const size_t smem = bytes();
-    auto kern = electron_step_kernel;
+    auto kern = electron_step_kernel<U>;
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                              "cudaFuncSetAttribute(step_electrons)"));
     int per_sm = 0;
@@ -328,12 +341,28 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
     const uint64_t tiles_max = ((uint64_t)g.capacity + ES_TILE - 1) / ES_TILE;
     const unsigned grid = persistent_grid(per_sm, tiles_max);
     // tiles per deposit drain: a copy receives ceil(WARPS / copies) warps x 128 particles per tile
-    const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * ES_U * 32u;
+    const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
     const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
     kern<<<grid, ES_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3,
                                              sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz, alive, n_active, n_i,
                                              dens_e, dens_i, g, ef_pad, stages, copies, epoch, link);
     return check_launch("step_electrons");
+}
+
+}  // namespace
+
+int launch_electron_step(const float *efield, const float *sx, const float *svx, const float *svy, const float *svz,
+                         float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *rng0, uint32_t *rng1,
+                         uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
+                         float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
+                         uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
+                         const StepLink &link) {
+    const void *planes[8] = {sx, svx, svy, svz, rng0, rng1, rng2, rng3};
+    if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
+    const cudapic_tuning t = tuning();
+    auto launch = t.step_rows == 4 ? launch_electron_step_t<4> : launch_electron_step_t<2>;
+    return launch(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e,
+                  ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, t);
 }
 
 }  // namespace cudapic

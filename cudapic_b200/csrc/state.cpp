@@ -429,6 +429,7 @@ extern "C" int cudapic_state_buffers(const cudapic_state *s, cudapic_buffers *o)
         o->tmp_vz[sp] = s->vz[sp][b];
         for (int k = 0; k < 4; ++k) o->rng[sp][k] = s->rng[sp][k];
     }
+    o->sigma_max_e = s->sigma_max_e;
     o->n_electrons = s->n_e();
     o->n_ions = s->n_i();
     o->alive_counter = s->alive();

@@ -4,9 +4,9 @@ L2 flushed before each launch): the target of the committed ncu captures.
     python -m cudapic_b200.microbench --kernel check_collisions_e [--particles N] [--reps 3]
 
 Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
-check_collisions_e, check_collisions_e_deposit, check_collisions_i (the
-*_deposit variants also deposit the next step's density, as the fused driver
-step does).  Prints one JSON line with the median time, the particle
+check_collisions_e, check_collisions_e_deposit, check_collisions_i and
+step_electrons (the *_deposit variants also deposit the next step's density;
+step_electrons is the fused driver's electron kernel).  Prints one JSON line with the median time, the particle
 count and the algorithmic bytes per launch.
 """
 import argparse
@@ -14,7 +14,7 @@ import json
 import statistics
 
 BYTES = {"get_density": 4, "move_and_compact": 32, "move_and_compact_deposit": 32, "check_collisions_e": 44,
-         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0}
+         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0, "step_electrons": 64}
 
 
 def main():
@@ -66,6 +66,10 @@ def main():
             b.sigma_tot_e, b.cs, ne_c, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.x[1], b.vx[1], b.vy[1],
             b.vz[1], alive_e, alive_i, dens, pot, g, stream=s), lambda: (alive_e.fill_(n_e), alive_i.fill_(n_i)),
             n_e),
+        "step_electrons": (lambda: K.step_electrons(
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], *b.rng[0],
+            b.sigma_tot_e, b.cs, b.sigma_max_e, b.x[1], b.vx[1], b.vy[1], b.vz[1], alive, ne_c, alive_i, dens, pot, g,
+            stream=s), lambda: (alive.zero_(), alive_i.fill_(n_i), dens.zero_()), n_e),
         "check_collisions_i": (lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                             *b.rng[1], g, stream=s), None, n_i),
     }

@@ -85,7 +85,8 @@ typedef struct cudapic_params {
  * FIXED_POINT: 32.32 fixed-point weights summed with 64-bit shared atomics.
  * F32: the reference's f32 weights summed with shared f32 atomics.  Where
  * both are set, FIXED_POINT wins.  The fused deposits of the driver step
- * (cudapic_move_and_compact_deposit) always use the default arithmetic. */
+ * (cudapic_move_and_compact_deposit, cudapic_step_electrons) always use the
+ * default arithmetic. */
 #define CUDAPIC_FLAG_DEPOSIT_FIXED_POINT 0x2u
 #define CUDAPIC_FLAG_DEPOSIT_F32 0x4u
 
@@ -139,8 +140,9 @@ typedef struct cudapic_tuning {
     int mcc_ctas_per_sm;
     int mcc_variant;          /* 1: shared-memory resident sigma table (any alignment),
                                  2: bulk-copy staged tiles (16-byte aligned pointers)    */
-    int step_stages;          /* fused electron step bulk-copy pipeline depth: 2..4      */
+    int step_stages;          /* fused electron step bulk-copy pipeline depth: 2..6      */
     int step_ctas_per_sm;
+    int step_rows;            /* fused electron step particles per thread and tile: 2, 4 */
 } cudapic_tuning;
 
 int cudapic_get_tuning(cudapic_tuning *out);
@@ -314,6 +316,7 @@ typedef struct cudapic_buffers {
     uint32_t *eepf;
     uint32_t *dev_err;
     unsigned long long *work;
+    float sigma_max_e;                       /* largest entry of sigma_tot_e        */
 } cudapic_buffers;
 
 #define CUDAPIC_ELECTRONS 0

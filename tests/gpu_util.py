@@ -37,3 +37,48 @@ def sorted_rows(*cols):
         return r
     order = np.lexsort(r.T[::-1])
     return r[order]
+
+
+def check_step_electrons(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, cap, seed=(3, 1, 4, 1), n_i0=1000):
+    """Runs the fused electron step through the C ABI and checks it against
+    the oracle's move_and_compact followed by its check_collisions_e over the
+    survivors, each survivor drawing from the RNG stream of its source slot.
+    RNG planes (every slot), electron and ion sets bit-exact; densities within
+    the deposit tolerance.  Returns (survivors, electrons after, ions after)."""
+    cs, se, _ = tables
+    dcs, dse, _ = dev_tables
+    n = len(x)
+    pad = lambda a, dt=np.float32: np.concatenate([a, np.zeros(cap - len(a), dt)])  # noqa: E731
+    rng = [pad(np.asarray(p), np.uint32) for p in oracle.seed_streams(list(seed), cap)]
+    rx, rvx, rvy, rvz, src = oracle.move_and_compact(ef, x, vx, vy, vz, g.factor_e, g.dt_e, ph)
+    m = rx.size
+    e_h = [pad(a) for a in (rx, rvx, rvy, rvz)]
+    r_sub = [pad(p[src], np.uint32) for p in rng]
+    i_h = [pad(np.full(n_i0, 0.0125, np.float32)) for _ in range(4)]
+    _, ne_ref, ni_ref, dropped = oracle.check_collisions_e(se, cs, m, e_h, r_sub, i_h, m, n_i0, ph)
+    assert dropped == 0
+    r_ref = [p.copy() for p in rng]
+    for k in range(4):
+        r_ref[k][src] = r_sub[k][:m]
+    src_d = [dev(pad(a)) for a in (x, vx, vy, vz)]
+    dst_d = [zeros(cap) for _ in range(4)]
+    r_d = [dev(p) for p in rng]
+    i_d = [dev(pad(np.full(n_i0, 0.0125, np.float32))) for _ in range(4)]
+    alive, n_i = counter(0), counter(n_i0)
+    de, di = zeros(len(ef)), zeros(len(ef))
+    K.step_electrons(dev(ef), *src_d, *dst_d, *r_d, dse, dcs, float(se.max()), *i_d, alive, counter(n), n_i, de, di,
+                     g)
+    ne, ni = int(host(alive)[0]), int(host(n_i)[0])
+    assert (ne, ni) == (ne_ref, ni_ref)
+    for d, h in zip(r_d, r_ref):
+        assert np.array_equal(host(d), h)
+    got = [host(d)[:ne] for d in dst_d]
+    assert np.array_equal(sorted_rows(*got), sorted_rows(*[h[:ne] for h in e_h]))
+    gi = [host(d) for d in i_d]
+    assert np.array_equal(sorted_rows(*[a[n_i0:ni] for a in gi]), sorted_rows(*[h[n_i0:ni] for h in i_h]))
+    ref_e = oracle.get_density_f64(got[0], ph)
+    assert np.linalg.norm(host(de) - ref_e) / np.linalg.norm(ref_e) < 2e-5
+    if ni > n_i0:
+        ref_i = oracle.get_density_f64(gi[0][n_i0:ni], ph)
+        assert np.linalg.norm(host(di) - ref_i) / np.linalg.norm(ref_i) < 2e-5
+    return m, ne, ni

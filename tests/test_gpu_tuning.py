@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from gpu_util import counter, dev, host, sorted_rows, zeros
+from gpu_util import check_step_electrons, counter, dev, host, sorted_rows, zeros
 
 pytestmark = pytest.mark.gpu
 
@@ -11,11 +11,14 @@ E_MASS = 9.10938356e-31
 
 SHAPES = [
     dict(density_threads=256, density_ctas_per_sm=1, density_copies=2, density_cluster=1, push_stages=2,
-         push_ctas_per_sm=1, mcc_stages=2, mcc_ctas_per_sm=1, mcc_variant=2),
+         push_ctas_per_sm=1, mcc_stages=2, mcc_ctas_per_sm=1, mcc_variant=2, step_rows=2, step_stages=2,
+         step_ctas_per_sm=1),
     dict(density_threads=1024, density_ctas_per_sm=4, density_copies=32, density_cluster=8, push_stages=6,
-         push_ctas_per_sm=2, mcc_stages=4, mcc_ctas_per_sm=2, mcc_variant=2),
+         push_ctas_per_sm=2, mcc_stages=4, mcc_ctas_per_sm=2, mcc_variant=2, step_rows=4, step_stages=6,
+         step_ctas_per_sm=4),
     dict(density_threads=512, density_ctas_per_sm=2, density_copies=8, density_cluster=2, push_stages=5,
-         push_ctas_per_sm=3, mcc_stages=3, mcc_ctas_per_sm=3, mcc_variant=1),
+         push_ctas_per_sm=3, mcc_stages=3, mcc_ctas_per_sm=3, mcc_variant=1, step_rows=2, step_stages=5,
+         step_ctas_per_sm=3),
 ]
 
 
@@ -67,3 +70,10 @@ def test_kernels_exact_under_every_shape(cudapic, oracle, tables, cuda_device, r
     assert int(host(ae)[0]) == ne_ref and int(host(ai)[0]) == ni_ref
     for d, h in zip(r_d, r_h):
         assert np.array_equal(host(d)[:n], h[:n])
+
+    # the fused electron step under the same shape
+    dev_tables = (dev(cs), dev(se), dev(si))
+    cap2 = (2 * n + 4096 + 3) // 4 * 4
+    g2 = cudapic.grid_from_params(capacity=cap2, n_t=100)
+    ph2 = oracle.phys_from_params(capacity=cap2, n_t=100)
+    check_step_electrons(K, oracle, tables, dev_tables, g2, ph2, x, vx, vy, vz, ef, cap2)
