@@ -25,7 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I", ROOT, "-Xcompiler", "-fPIC,-ff
           "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "--expt-relaxed-constexpr"]
 
 SOURCES = ["host.cpp", "state.cpp", "kernels_density.cu", "kernels_poisson.cu", "kernels_push.cu",
-           "kernels_mcc.cu", "kernels_step.cu", "kernels_misc.cu"]
+           "kernels_mcc.cu", "kernels_step.cu", "kernels_misc.cu",
+           "noalloc.cu"]
 
 
 def _newer(target, deps):

@@ -99,6 +99,18 @@ def step_electrons(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy,
     check(lib.cudapic_step_electrons(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, src_x)))
 
 
+def step_electrons_noalloc(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, rng0, rng1, rng2,
+                           rng3, total_cs_e, cs, sigma_max_e, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density,
+                           i_next_density, grid, stream=None):
+    """step_electrons for callers that cannot allocate device memory: no
+    slot counter is passed (the library keeps it in a static device array)
+    and the new electron count is written into n_e in place."""
+    head = [_ptr(a) for a in (efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, rng0, rng1, rng2,
+                              rng3, total_cs_e, cs)]
+    tail = [_ptr(a) for a in (i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density)]
+    check(lib.cudapic_step_electrons_noalloc(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, src_x)))
+
+
 def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz,
                        alive_e, alive_i, grid, stream=None, events=None):
     """check_collisions_e (Rust-CUDA/src/main.rs:971-1165).  With `events`

@@ -239,6 +239,32 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
                            uint32_t *alive_counter, const uint32_t *n_e, uint32_t *n_i, float *e_next_density,
                            float *i_next_density, const cudapic_grid *grid, cudapic_stream_t stream);
 
+/* cudapic_step_electrons for callers that cannot allocate device memory
+ * (a host whose device memory belongs to its own pool or framework and that
+ * hands this library only its particle buffers, or code that must not call
+ * cudaMalloc because it synchronises the device).  It has no counterpart in
+ * the reference.  Same arguments and results as cudapic_step_electrons
+ * except that no alive_counter is passed: the kernel's slot counter and
+ * completion ticket live in a library-owned static device array of
+ * CUDAPIC_NOALLOC_SCRATCH_BYTES (held by every GPU that loads the library
+ * until exit), and the new electron count is written into *n_e in place.
+ * The call allocates nothing; it clears the two counters on `stream` before
+ * the launch.  The first call on a device looks up the array's address with
+ * that device current; make it before any stream capture.  Every call shares
+ * the array: calls whose kernels overlap on one GPU race.  Rejects (with
+ * CUDAPIC_ERR_ARG) a capacity above CUDAPIC_NOALLOC_MAX_CAPACITY, where the
+ * shared 32-bit slot counter could wrap, besides the checks of
+ * cudapic_step_electrons. */
+#define CUDAPIC_NOALLOC_SCRATCH_BYTES 256u
+#define CUDAPIC_NOALLOC_MAX_CAPACITY 0x80000000u
+int cudapic_step_electrons_noalloc(const float *efield, const float *src_x, const float *src_vx,
+                                   const float *src_vy, const float *src_vz, float *dst_x, float *dst_vx,
+                                   float *dst_vy, float *dst_vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
+                                   uint32_t *rng3, const float *total_cs_e, const float *cs, float sigma_max_e,
+                                   float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *n_e, uint32_t *n_i,
+                                   float *e_next_density, float *i_next_density, const cudapic_grid *grid,
+                                   cudapic_stream_t stream);
+
 /* check_collisions_i (Rust-CUDA/src/main.rs:1167-1292): MCC of ions
  * [0, *active_i) against Maxwellian target atoms. */
 int cudapic_check_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i,

@@ -80,6 +80,15 @@ def test_argument_validation_without_device(cudapic):
         cudapic.grid_from_params(n_g=1)
     with pytest.raises(cudapic.CudapicError):
         cudapic.grid_from_params(capacity=0)
+    # the no-alloc fused step: checks come before any device work
+    ptrs = list(range(256, 256 + 16 * 15, 16))
+    tail = list(range(4096, 4096 + 16 * 8, 16))
+    assert lib.cudapic_step_electrons_noalloc(*ptrs, C.c_float(1.0), *tail[:4], None, *tail[5:], C.byref(g),
+                                              None) == _lib.ERR_ARG
+    big = cudapic.grid_from_params()
+    big.capacity = 0x80000004
+    assert lib.cudapic_step_electrons_noalloc(*ptrs, C.c_float(1.0), *tail, C.byref(big), None) == _lib.ERR_ARG
+    assert b"CUDAPIC_NOALLOC_MAX_CAPACITY" in lib.cudapic_last_error()
 
 
 def test_state_create_reports_missing_device(cudapic):
