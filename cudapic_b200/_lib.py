@@ -128,6 +128,7 @@ SIGNATURES = {
     "cudapic_state_seed": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_set_measure": [_VP, C.c_int],
     "cudapic_state_set_fused": [_VP, C.c_int],
+    "cudapic_state_set_overlap": [_VP, C.c_int],
     "cudapic_state_run_steps": [_VP, C.c_uint64],
     "cudapic_state_counts": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_device_error": [_VP, C.POINTER(_U32)],

@@ -51,6 +51,15 @@ __device__ __forceinline__ bool pos_in_range(float pos, uint32_t n_g) {
     return pos >= 0.0f && pos <= (float)(n_g - 1);
 }
 
+// Programmatic dependent launch: waits until the grids this one depends on
+// have completed and their memory is visible (a no-op for a launch without
+// the PDL attribute), then lets the next kernel of the stream be scheduled.
+// Called before the first global access that another kernel may touch.
+__device__ __forceinline__ void grid_dep_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // End of a kernel that counted particles into link.src: the last CTA to
 // finish publishes the count (StepLink, internal.h).  Every thread fences its
 // own counter atomics before the CTA's ticket is taken.

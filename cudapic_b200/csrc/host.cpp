@@ -70,10 +70,18 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*density_threads*/ 512, /*density_ctas_per_sm*/ 4, /*density_copies*/ 4, /*density_cluster*/ 4,
     /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1,
-    /*step_stages*/ 2, /*step_ctas_per_sm*/ 2, /*step_rows*/ 4};
+    /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
 }  // namespace
+
+namespace {
+thread_local bool t_pdl = false;
+}
+
+bool pdl_enabled() { return t_pdl; }
+PdlScope::PdlScope(bool on) : prev(t_pdl) { t_pdl = on; }
+PdlScope::~PdlScope() { t_pdl = prev; }
 
 cudapic_tuning tuning() {
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 
 #include "../../include/cudapic.h"
 
@@ -29,6 +30,42 @@ int validate_grid(const cudapic_grid *g);
 
 // Current launch shapes (defaults filled in for zero fields).
 cudapic_tuning tuning();
+
+// Programmatic dependent launch (PDL).  Inside a PdlScope the kernel
+// launches of the calling thread carry cudaLaunchAttributeProgrammatic-
+// StreamSerialization, so a kernel may be scheduled while the previous one
+// drains.  Every kernel of this library executes grid_dep_wait()
+// (common.cuh) before it reads or writes global data another kernel may
+// touch, so only its prologue (shared-memory set-up, static tables) overlaps.
+// The driver opens a scope around its own steps; the drop-in entry points
+// never do, because a caller's preceding kernel may write what a prologue reads.
+bool pdl_enabled();
+struct PdlScope {
+    bool prev;
+    explicit PdlScope(bool on);
+    ~PdlScope();
+};
+
+// Launches `kern` on `stream` (with the PDL attribute inside a PdlScope).
+template <typename... KArgs, typename... Args>
+int launch_kernel(const char *name, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                  Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    if (pdl_enabled()) {
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+    if (e != cudaSuccess) return check_cuda(e, name);
+    return check_launch(name);
+}
 
 // Grid of a persistent kernel: min(SMs x per_sm, work units), at least 1.
 unsigned persistent_grid(int per_sm, uint64_t units);

@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(BLOCK)
     const int tid = threadIdx.x;
     for (uint32_t k = tid; k < (uint32_t)copies * n_g; k += BLOCK) hist[k] = Acc(0);
     __syncthreads();
+    grid_dep_wait();
 
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     Acc *h = hist + (uint32_t)((tid >> 5) % copies) * n_g;
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(BLOCK)
     for (uint32_t k = tid; k < (uint32_t)copies * n_g; k += BLOCK) hist[k] = 0u;
     for (uint32_t k = tid; k < n_g; k += BLOCK) acc[k] = 0ull;
     __syncthreads();
+    grid_dep_wait();
 
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     uint32_t *h = hist + (uint32_t)((tid >> 5) % copies) * n_g;
@@ -229,6 +231,7 @@ __global__ void __launch_bounds__(BLOCK)
 // accumulate_density, Rust-CUDA/src/main.rs:1294-1299.
 __global__ void accumulate_density_kernel(const float *__restrict__ density, double *__restrict__ cumul,
                                           uint32_t n_g) {
+    grid_dep_wait();
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n_g) cumul[k] += (double)density[k];
 }
@@ -242,7 +245,7 @@ int launch_clustered(Kern kern, int block, size_t smem, const cudapic_grid &g, c
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                              "cudaFuncSetAttribute(get_density)"));
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)t.density_cluster;
     attr[0].val.clusterDim.y = 1;
@@ -263,6 +266,11 @@ int launch_clustered(Kern kern, int block, size_t smem, const cudapic_grid &g, c
     const uint64_t clusters = std::min(std::min((uint64_t)max_clusters, std::max<uint64_t>(1, want)),
                                        std::max<uint64_t>(1, (need + cl - 1) / cl));
     cfg.gridDim = dim3((unsigned)(clusters * cl));
+    if (pdl_enabled()) {
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.numAttrs = 2;
+    }
     CUDAPIC_CHECK(check_cuda(cudaLaunchKernelEx(&cfg, kern, args...), "launch get_density"));
     return CUDAPIC_OK;
 }
@@ -353,7 +361,6 @@ extern "C" int cudapic_accumulate_density(const float *density, double *cumul, c
     CUDAPIC_CHECK(validate_grid(grid));
     CUDAPIC_REQUIRE(density && cumul, "accumulate_density: null pointer");
     const int block = 256;
-    accumulate_density_kernel<<<(grid->n_g + block - 1) / block, block, 0, (cudaStream_t)stream>>>(
-        density, cumul, grid->n_g);
-    return check_launch("accumulate_density");
+    return launch_kernel("accumulate_density", accumulate_density_kernel, dim3((grid->n_g + block - 1) / block),
+                         dim3(block), 0, (cudaStream_t)stream, density, cumul, grid->n_g);
 }

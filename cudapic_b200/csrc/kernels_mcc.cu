@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
     __shared__ int s_ready;
 
     const int tid = threadIdx.x;
+    grid_dep_wait();
     const uint32_t n = load_count(active, g.capacity, g.dev_err);
     const uint32_t ntiles = (n + MT_TILE - 1) / MT_TILE;
     const void *src[MT_ARRAYS] = {vx, vy, vz, rng0, rng1, rng2, rng3};
@@ -224,8 +225,11 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
     uint32_t *wq = reinterpret_cast<uint32_t *>(tab + MR_RESIDENT) + (size_t)warp * 5 * MR_QCAP;  // [5][QCAP]
     const unsigned lt = lanemask_lt();
 
+    // the table is read before the wait: under PDL (the driver) it was
+    // written when the state was created, long before any dependent grid
     for (uint32_t k = tid; k < MR_RESIDENT; k += MR_THREADS) tab[k] = __ldg(sigma_tot + k);
     __syncthreads();
+    grid_dep_wait();
     const ResidentTable table{sigma_tot, tab, MR_RESIDENT};
     const uint32_t n = load_count(active, g.capacity, g.dev_err);
 
@@ -317,6 +321,7 @@ __global__ void __launch_bounds__(256)
     __shared__ uint32_t h[N_EEPF];
     for (uint32_t k = threadIdx.x; k < N_EEPF; k += blockDim.x) h[k] = 0;
     __syncthreads();
+    grid_dep_wait();
     const uint32_t n = load_count(active_e, g.capacity, g.dev_err);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float xi = x[i];
@@ -363,9 +368,9 @@ int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, 
     per_sm = std::min(std::max(per_sm, 1), t.mcc_ctas_per_sm);
     const uint64_t tiles_max = ((uint64_t)g.capacity + MT_TILE - 1) / MT_TILE;
     const unsigned grid = persistent_grid(per_sm, tiles_max);
-    kern<<<grid, MCC_THREADS, smem, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                              alive_e, alive_i, events, g, stages, dep_e, dep_i);
-    return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
+    return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(grid), dim3(MCC_THREADS), smem,
+                         stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz, alive_e,
+                         alive_i, events, g, stages, dep_e, dep_i);
 }
 
 template <bool ION, bool EVENTS>
@@ -378,10 +383,9 @@ int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *act
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MR_SMEM),
                              "cudaFuncSetAttribute(check_collisions resident)"));
     const uint64_t chunks = ((uint64_t)g.capacity + MR_THREADS * MR_U - 1) / (MR_THREADS * MR_U);
-    kern<<<persistent_grid(1, chunks), MR_THREADS, MR_SMEM, stream>>>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1,
-                                                                      r2, r3, ix, ivx, ivy, ivz, alive_e, alive_i,
-                                                                      events, g, dep_e, dep_i);
-    return check_launch(ION ? "check_collisions_i" : "check_collisions_e");
+    return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(persistent_grid(1, chunks)),
+                         dim3(MR_THREADS), MR_SMEM, stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix,
+                         ivx, ivy, ivz, alive_e, alive_i, events, g, dep_e, dep_i);
 }
 
 // Variant choice: the bulk-copy kernel needs 16-byte aligned planes and a
@@ -427,8 +431,8 @@ int launch_eepf(const float *x, const float *vx, const float *vy, const float *v
                 const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream) {
     const uint64_t need = ((uint64_t)g.capacity + 255) / 256;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * 2, need));
-    accumulate_eepf_kernel<<<grid, 256, 0, stream>>>(x, vx, vy, vz, efield, active_e, eepf, g);
-    return check_launch("accumulate_eepf");
+    return launch_kernel("accumulate_eepf", accumulate_eepf_kernel, dim3(grid), dim3(256), 0, stream, x, vx, vy, vz,
+                         efield, active_e, eepf, g);
 }
 
 }  // namespace cudapic

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
 
     const int n = (int)g.n_g;
     const int tid = threadIdx.x;
+    grid_dep_wait();
     for (int k = tid; k < n; k += blockDim.x) {  // next-step accumulators of the driver
         if (zero_a) zero_a[k] = 0.0f;
         if (zero_b) zero_b[k] = 0.0f;
@@ -260,9 +261,8 @@ int launch_poisson_t(const float *e_density, const float *i_density, float *pot,
     if (smem > 48 * 1024)
         CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                                  "cudaFuncSetAttribute(poisson)"));
-    kern<<<1, threads, smem, stream>>>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, zero_a,
-                                       zero_b);
-    return check_launch("solve_poisson_scan");
+    return launch_kernel("solve_poisson_scan", kern, dim3(1), dim3(threads), smem, stream, e_density, i_density, pot,
+                         efield, pot0, pot0_table, step_counter, g, zero_a, zero_b);
 }
 
 template <typename T>

@@ -70,6 +70,15 @@ __global__ void __launch_bounds__(MC_THREADS)
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const unsigned lt = lanemask_lt();
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    if (DEPOSIT) {
+        for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0u;
+        for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) acc[k] = 0ull;
+    }
+    grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     const uint32_t ntiles = (n + MC_TILE - 1) / MC_TILE;
     const float *src[4] = {sx, svx, svy, svz};
@@ -84,15 +93,7 @@ __global__ void __launch_bounds__(MC_THREADS)
         for (int a = 0; a < 4; ++a) bulk_load(in + (stage * 4 + a) * MC_TILE, src[a] + t0, bytes, &bar[stage]);
     };
 
-    if (tid == 0) {
-        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
-        fence_mbar_init();
-    }
     for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
-    if (DEPOSIT) {
-        for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0u;
-        for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) acc[k] = 0ull;
-    }
     uint32_t *h = hist + (uint32_t)(warp % max(copies, 1)) * ef_pad;
     __syncthreads();
     if (tid == 0) {
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(MCS_THREADS)
     __shared__ uint32_t wsum[MCS_WARPS];
     __shared__ uint32_t s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    grid_dep_wait();
     for (uint32_t k = tid; k < g.n_g; k += MCS_THREADS) ef_s[k] = efield[k];
     __syncthreads();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
@@ -310,9 +312,9 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         // tiles per drain: a copy receives the particles of ceil(MC_WARPS / copies) warps, MC_U * 32 per tile each
         const uint32_t per_tile = (uint32_t)((MC_WARPS + std::max(copies, 1) - 1) / std::max(copies, 1)) * MC_U * 32u;
         const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
-        kern<<<grid, MC_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active,
-                                                 factor, dt, g, ef_pad, stages, dens_out, copies, epoch, link);
-        return check_launch("move_and_compact_tma");
+        return launch_kernel("move_and_compact_tma", kern, dim3(grid), dim3(MC_THREADS), smem, stream, efield, sx, svx,
+                             svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g, ef_pad, stages, dens_out,
+                             copies, epoch, link);
     }
     if (dens_out || link.ticket) {  // unaligned buffers: separate deposit and count copy
         CUDAPIC_CHECK(launch_move_and_compact(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor,
@@ -333,9 +335,8 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
                                  "cudaFuncSetAttribute(move_and_compact_simple)"));
     const uint64_t blocks_max = ((uint64_t)g.capacity + MCS_THREADS - 1) / MCS_THREADS;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * 4, blocks_max));
-    move_and_compact_simple_kernel<<<grid, MCS_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy,
-                                                                        dvz, alive, n_active, factor, dt, g);
-    return check_launch("move_and_compact_simple");
+    return launch_kernel("move_and_compact_simple", move_and_compact_simple_kernel, dim3(grid), dim3(MCS_THREADS), smem,
+                         stream, efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g);
 }
 
 }  // namespace cudapic

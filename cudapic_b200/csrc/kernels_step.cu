@@ -25,6 +25,8 @@
 //    the largest table entry, u >= fl(fl(fl(sigma_max |v|) dt) + 5e-7)
 //    implies it: the energy index and the table gather are skipped for
 //    almost every electron, the decision is bit-identical;
+//  * every thread waits on the stage's mbarrier itself, so a tile has one
+//    block barrier (after the counts), not a barrier for the data as well;
 //  * non-colliding survivors store their advanced RNG state in place
 //    (coalesced) and are compacted as in move_and_compact: warp ballots, one
 //    warp scan per tile, one atomicAdd per tile whose result is consumed a
@@ -96,14 +98,23 @@ __global__ void __launch_bounds__(ES_THREADS)
     uint32_t *hist = reinterpret_cast<uint32_t *>(acc + ef_pad);                          // [copies][ef_pad]
     uint32_t *queue = hist + (uint32_t)copies * ef_pad;                                   // [WARPS][QCAP]
     uint64_t *bar = reinterpret_cast<uint64_t *>(queue + ES_WARPS * ES_QCAP);             // [stages]
-    __shared__ uint32_t offs[2][NSEG];  // counts, then exclusive offsets
-    __shared__ uint32_t s_base[2];
-    __shared__ int s_ready;
+    // Per tile: (row, warp) counts, then exclusive offsets; the tile's base.
+    // Three buffers, because a tile's counts are written while slower warps
+    // may still be storing the tile before the previous one.
+    __shared__ uint32_t offs[3][NSEG];
+    __shared__ uint32_t s_base[3];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const unsigned lt = lanemask_lt();
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += ES_THREADS) hist[k] = 0u;
+    for (uint32_t k = tid; k < ef_pad; k += ES_THREADS) acc[k] = 0ull;
+    grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     const uint32_t ntiles = (n + ES_TILE - 1) / ES_TILE;
     const uint32_t *src[ES_PLANES] = {reinterpret_cast<const uint32_t *>(sx), reinterpret_cast<const uint32_t *>(svx),
@@ -121,13 +132,7 @@ __global__ void __launch_bounds__(ES_THREADS)
             bulk_load(in + (stage * ES_PLANES + a) * ES_TILE, src[a] + t0, bytes, &bar[stage]);
     };
 
-    if (tid == 0) {
-        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
-        fence_mbar_init();
-    }
     for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) ef[k] = efield[k];
-    for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += ES_THREADS) hist[k] = 0u;
-    for (uint32_t k = tid; k < ef_pad; k += ES_THREADS) acc[k] = 0ull;
     uint32_t *h = hist + (uint32_t)(warp % copies) * ef_pad;
     uint32_t *wq = queue + warp * ES_QCAP;
     __syncthreads();
@@ -175,75 +180,104 @@ __global__ void __launch_bounds__(ES_THREADS)
         }
         const int s = (int)(it % (uint32_t)stages);
         const uint32_t parity = (it / (uint32_t)stages) & 1u;
-        if (tid == 0) {
-            const int ok = mbar_wait_bounded(&bar[s], parity) ? 1 : 0;
-            if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
-            s_ready = ok;
-        }
-        __syncthreads();
-        if (!s_ready) break;  // timed out: flagged; the count is still published
+        const uint32_t r3 = it % 3u, p3 = (it + 2u) % 3u;  // buffers of this tile and of the previous one
+        // every thread waits for the stage's bulk copies itself (bounded)
+        const bool ok = mbar_wait_bounded(&bar[s], parity);
+        if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
 
         const uint32_t t0 = tile * ES_TILE;
-        const uint32_t cnt = min((uint32_t)ES_TILE, n - t0);
+        const uint32_t cnt = ok ? min((uint32_t)ES_TILE, n - t0) : 0u;
         const uint32_t *b = in + s * ES_PLANES * ES_TILE;
+        // The rows of a tile are independent; the work is split into phases
+        // over all rows so that the scheduler can interleave them.
         StepOut<U> cur;
         cur.keep = 0;
+        uint32_t st[U][4];     // RNG states after the test draw
+        uint32_t keep = 0, may = 0, coll = 0;  // bit u: row u survives / may collide / collides
+        // (1) push (Rust-CUDA/src/main.rs:596-620); rows past the tile's end
+        //     push a harmless stand-in and are masked
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-            bool stay = false, collide = false;
-            cur.x[u] = cur.vx[u] = cur.vy[u] = cur.vz[u] = 0.0f;
-            if (j < cnt) {
-                const PushResult pr = push_one(__uint_as_float(b[j]), __uint_as_float(b[ES_TILE + j]), ef, g.factor_e,
-                                               g.dt_e, g);
-                if (pr.keep) {
-                    const float vy = __uint_as_float(b[2 * ES_TILE + j]);
-                    const float vz = __uint_as_float(b[3 * ES_TILE + j]);
-                    dep_add(h, pr.x, g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            const bool valid = j < cnt;
+            const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * g.gap;
+            const float v0 = valid ? __uint_as_float(b[ES_TILE + j]) : 0.0f;
+            const PushResult pr = push_one(x0, v0, ef, g.factor_e, g.dt_e, g);
+            if (valid && pr.keep) keep |= 1u << u;
+            cur.x[u] = pr.x;
+            cur.vx[u] = pr.vx;
+        }
+        // (2) test_electron (mcc.cuh, Rust-CUDA/src/main.rs:992-1012) up to the
+        //     certain rejection, which needs no table
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+            cur.vy[u] = __uint_as_float(b[2 * ES_TILE + j]);
+            cur.vz[u] = __uint_as_float(b[3 * ES_TILE + j]);
+            Xoshiro128p rs{b[4 * ES_TILE + j], b[5 * ES_TILE + j], b[6 * ES_TILE + j], b[7 * ES_TILE + j]};
+            const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
+            const float velocity = sqrtf(v2);
+            const float rnd = rs.uniform();
+            if ((keep >> u & 1u) && may_collide(rnd, velocity, sigma_max, g.dt_e)) may |= 1u << u;
+            st[u][0] = rs.s0;
+            st[u][1] = rs.s1;
+            st[u][2] = rs.s2;
+            st[u][3] = rs.s3;
+        }
+        // (3) the exact test where the bound cannot decide (a few per cent)
+        if (may) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (may >> u & 1u) {
+                    const uint32_t j = (uint32_t)u * ES_THREADS + tid;
                     Xoshiro128p rs{b[4 * ES_TILE + j], b[5 * ES_TILE + j], b[6 * ES_TILE + j], b[7 * ES_TILE + j]};
-                    // test_electron (mcc.cuh), Rust-CUDA/src/main.rs:992-1012, with the certain rejection first
-                    const float v2 = pr.vx * pr.vx + vy * vy + vz * vz;
+                    const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
                     const float velocity = sqrtf(v2);
                     const float rnd = rs.uniform();
-                    if (may_collide(rnd, velocity, sigma_max, g.dt_e)) {
-                        const uint32_t idx = energy_index(g.half_me_over_e * v2);
-                        collide = collision_draw(rnd, __ldg(sigma_tot_e + idx) * velocity * g.dt_e);
-                    }
-                    if (!collide) {
-                        const uint32_t i = t0 + j;
-                        rng0[i] = rs.s0;
-                        rng1[i] = rs.s1;
-                        rng2[i] = rs.s2;
-                        rng3[i] = rs.s3;
-                        stay = true;
-                        cur.x[u] = pr.x;
-                        cur.vx[u] = pr.vx;
-                        cur.vy[u] = vy;
-                        cur.vz[u] = vz;
-                    }
+                    const uint32_t idx = energy_index(g.half_me_over_e * v2);
+                    if (collision_draw(rnd, __ldg(sigma_tot_e + idx) * velocity * g.dt_e)) coll |= 1u << u;
                 }
+            }
+        }
+        // (4) deposit every survivor; non-colliders store their RNG state and
+        //     are compacted, colliders are queued
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+            const bool kept = keep >> u & 1u;
+            const bool collide = coll >> u & 1u;
+            const bool stay = kept && !collide;
+            if (kept) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            if (stay) {
+                const uint32_t i = t0 + j;
+                rng0[i] = st[u][0];
+                rng1[i] = st[u][1];
+                rng2[i] = st[u][2];
+                rng3[i] = st[u][3];
             }
             const unsigned m = __ballot_sync(0xffffffffu, stay);
             cur.lane_off[u] = __popc(m & lt);
             if (stay) cur.keep |= 1u << u;
-            if (lane == 0) offs[it & 1][u * ES_WARPS + warp] = __popc(m);
+            if (lane == 0) offs[r3][u * ES_WARPS + warp] = __popc(m);
             const unsigned cm = __ballot_sync(0xffffffffu, collide);
             if (collide) wq[qn + __popc(cm & lt)] = t0 + j;
             qn += __popc(cm);
         }
         // publish the previous tile's base (its atomic had this iteration to return)
-        if (have_prev && warp == 0 && lane == 31) s_base[(it - 1) & 1] = pending_base;
-        __syncthreads();  // counts and previous base visible; stage s consumed
+        if (have_prev && warp == 0 && lane == 31) s_base[p3] = pending_base;
+        // the one block barrier of a tile: counts and previous base visible,
+        // stage s consumed; a timeout anywhere ends the loop of every thread
+        if (__syncthreads_or(!ok)) break;
         if (tid == 0) {
             const uint32_t next = tile + (uint32_t)stages * gridDim.x;
             if (next < ntiles) issue(next, s);
         }
         if (have_prev) {
-            const uint32_t base = s_base[(it - 1) & 1];
+            const uint32_t base = s_base[p3];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (prev.keep & (1u << u)) {
-                    const uint32_t slot = base + offs[(it - 1) & 1][u * ES_WARPS + warp] + prev.lane_off[u];
+                    const uint32_t slot = base + offs[p3][u * ES_WARPS + warp] + prev.lane_off[u];
                     if (slot < g.capacity) {
                         dx_[slot] = prev.x[u];
                         dvx[slot] = prev.vx[u];
@@ -256,14 +290,14 @@ __global__ void __launch_bounds__(ES_THREADS)
             }
         }
         if (warp == 0) {
-            const uint32_t v = lane < NSEG ? offs[it & 1][lane] : 0u;
+            const uint32_t v = lane < NSEG ? offs[r3][lane] : 0u;
             uint32_t incl = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += t;
             }
-            if (lane < NSEG) offs[it & 1][lane] = incl - v;
+            if (lane < NSEG) offs[r3][lane] = incl - v;
             if (lane == 31) pending_base = incl ? atomicAdd(alive, incl) : 0u;
         }
         prev = cur;
@@ -273,14 +307,15 @@ __global__ void __launch_bounds__(ES_THREADS)
             drain(qn, 32);
         }
     }
-    if (have_prev && warp == 0 && lane == 31) s_base[(it - 1) & 1] = pending_base;
+    const uint32_t pl = (it + 2u) % 3u;  // buffers of the last tile with survivors held in registers
+    if (have_prev && warp == 0 && lane == 31) s_base[pl] = pending_base;
     __syncthreads();
     if (have_prev) {
-        const uint32_t base = s_base[(it - 1) & 1];
+        const uint32_t base = s_base[pl];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (prev.keep & (1u << u)) {
-                const uint32_t slot = base + offs[(it - 1) & 1][u * ES_WARPS + warp] + prev.lane_off[u];
+                const uint32_t slot = base + offs[pl][u * ES_WARPS + warp] + prev.lane_off[u];
                 if (slot < g.capacity) {
                     dx_[slot] = prev.x[u];
                     dvx[slot] = prev.vx[u];
@@ -343,10 +378,9 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     // tiles per deposit drain: a copy receives ceil(WARPS / copies) warps x 128 particles per tile
     const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
     const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
-    kern<<<grid, ES_THREADS, smem, stream>>>(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3,
-                                             sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz, alive, n_active, n_i,
-                                             dens_e, dens_i, g, ef_pad, stages, copies, epoch, link);
-    return check_launch("step_electrons");
+    return launch_kernel("step_electrons", kern, dim3(grid), dim3(ES_THREADS), smem, stream, efield, sx, svx, svy, svz,
+                         dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz,
+                         alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link);
 }
 
 }  // namespace

@@ -47,6 +47,7 @@ struct cudapic_state {
     float *e_dens[2] = {}, *i_dens[2] = {};
     int e_cur = 0, i_cur = 0;
     bool fused = true;        // deposit inside push / collisions (default)
+    bool overlap = true;      // programmatic dependent launch between the step's kernels (default)
     bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
@@ -157,6 +158,7 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
 
 // One reference time step (Rust-CUDA/src/main.rs:1728-1807).
 int enqueue_step(cudapic_state *s, bool ion_step) {
+    PdlScope pdl(s->overlap);
     const cudapic_grid &g = s->grid;
     cudaStream_t st = s->stream;
     const int E = 0, I = 1;
@@ -500,6 +502,15 @@ extern "C" int cudapic_state_seed(cudapic_state *s, const uint32_t e_master[4], 
                                                   s->rng[0][2], s->rng[0][3], (cudapic_stream_t)s->stream));
     CUDAPIC_CHECK(cudapic_xoshiro128_seed_streams(i_master, s->params.capacity, s->rng[1][0], s->rng[1][1],
                                                   s->rng[1][2], s->rng[1][3], (cudapic_stream_t)s->stream));
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_set_overlap(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_overlap: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_overlap sync"));
+    s->overlap = on != 0;
+    destroy_graphs(s);
     return CUDAPIC_OK;
 }
 

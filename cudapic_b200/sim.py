@@ -134,8 +134,14 @@ class GpuSimState:
         check(lib.cudapic_state_set_measure(self._h, 1 if on else 0))
 
     def set_fused(self, on=True):
-        """Deposit the next step's density inside push / collisions (default on)."""
+        """Fused driver step: the electron kernel pushes, collides and deposits
+        the next density in one launch (default on); off: the reference's
+        launch sequence."""
         check(lib.cudapic_state_set_fused(self._h, 1 if on else 0))
+
+    def set_overlap(self, on=True):
+        """Programmatic dependent launch between the step's kernels (default on)."""
+        check(lib.cudapic_state_set_overlap(self._h, 1 if on else 0))
 
     def download_measurements(self):
         n_g = self.grid.n_g

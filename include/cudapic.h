@@ -373,12 +373,20 @@ int cudapic_state_set_measure(cudapic_state *s, int on);
 /* Enqueues n_steps reference-order time steps (Rust-CUDA/src/main.rs:1728-1807)
  * on the state's stream.  Asynchronous. */
 int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps);
-/* on (default): each step deposits the next step's charge density inside the
- * push and collision kernels (cudapic_move_and_compact_deposit,
- * cudapic_check_collisions_e_deposit) instead of re-reading every particle
- * in a separate get_density launch; the first step after an upload runs
- * the separate deposit.  off: the reference's launch sequence. */
+/* on (default): each step runs the fused electron kernel
+ * (cudapic_step_electrons: push, collisions and the next step's deposit in
+ * one launch, electrons drawing from their source slot's RNG stream) and the
+ * ion push deposits the ions' next density (cudapic_move_and_compact_deposit);
+ * the kernels publish the particle counts themselves.  The first step after
+ * an upload runs the separate deposit.  Planes that are not 16-byte aligned
+ * (or a capacity that is not a multiple of 4) fall back to push + deposit and
+ * cudapic_check_collisions_e_deposit.  off: the reference's launch sequence. */
 int cudapic_state_set_fused(cudapic_state *s, int on);
+/* on (default): the driver launches its kernels with programmatic dependent
+ * launch, so a kernel's launch and prologue overlap the previous kernel's
+ * tail (every kernel waits for its predecessor before touching global data).
+ * off: plain stream order.  The captured graphs are rebuilt. */
+int cudapic_state_set_overlap(cudapic_state *s, int on);
 /* Reads the counters (synchronises the state's stream). */
 int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i);
 /* Reads and returns the device error word (synchronises). */

@@ -91,13 +91,16 @@ def test_graph_replay_equals_direct_launch_statistics(cudapic, cuda_device):
     b.close()
 
 
+@pytest.mark.parametrize("overlap", [True, False])
 @pytest.mark.parametrize("steps", [1, 137, 400])
-def test_fused_density_equals_fresh_deposit(cudapic, cuda_device, steps):
+def test_fused_density_equals_fresh_deposit(cudapic, cuda_device, steps, overlap):
     """In fused mode the density handed to the next Poisson solve was
-    accumulated by the previous push and collisions; it must equal a fresh
-    deposit of the electrons now present."""
+    accumulated by the previous electron step; it must equal a fresh deposit
+    of the electrons now present (with and without programmatic dependent
+    launch between the kernels)."""
     import torch
     st = _c0_state(cudapic)
+    st.set_overlap(overlap)
     st.run_steps(steps)
     st.synchronize()
     b, g = st.buffers(), st.grid
@@ -109,7 +112,23 @@ def test_fused_density_equals_fresh_deposit(cudapic, cuda_device, steps):
     f, u = fresh.double().cpu().numpy(), used.cpu().numpy()
     assert f.sum() > 0
     assert np.linalg.norm(f - u) / np.linalg.norm(f) < 2e-5
+    assert st.device_error() == 0
     st.close()
+
+
+def test_overlap_on_and_off_agree_statistically(cudapic, cuda_device):
+    a = _c0_state(cudapic)
+    b = _c0_state(cudapic)
+    b.set_overlap(False)
+    a.run_cycles(3)
+    b.run_cycles(3)
+    na, nb = a.counts(), b.counts()
+    for x, y in zip(na, nb):
+        assert abs(x - y) <= 0.15 * max(x, y) + 50, (na, nb)
+    assert a.device_error() == 0 and b.device_error() == 0
+    assert a.steps_done() == b.steps_done() == 3 * 4000
+    a.close()
+    b.close()
 
 
 def test_fused_and_reference_sequences_agree_statistically(cudapic, cuda_device):
