@@ -116,16 +116,22 @@ __global__ void __launch_bounds__(ES_THREADS)
     for (uint32_t k = tid; k < ef_pad; k += ES_THREADS) acc[k] = 0ull;
     grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
-    const uint32_t ntiles = (n + ES_TILE - 1) / ES_TILE;
+    // Balanced partition: CTA c owns the particles [beg, end), an equal share
+    // (a multiple of 4, so every tile start stays 16-byte aligned) cut into
+    // tiles; every CTA then finishes after the same work, whatever n is.
+    const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 3u) & ~3u;
+    const uint32_t beg = min(n, blockIdx.x * chunk);
+    const uint32_t end = min(n, beg + chunk);
+    const uint32_t ntiles = (end - beg + ES_TILE - 1) / ES_TILE;  // this CTA's tiles
     const uint32_t *src[ES_PLANES] = {reinterpret_cast<const uint32_t *>(sx), reinterpret_cast<const uint32_t *>(svx),
                                       reinterpret_cast<const uint32_t *>(svy), reinterpret_cast<const uint32_t *>(svz),
                                       rng0, rng1, rng2, rng3};
     if (g.work && blockIdx.x == 0 && tid == 0) atomicAdd(g.work, (unsigned long long)n);
 
-    auto issue = [&](uint32_t tile, int stage) {
-        const uint32_t t0 = tile * ES_TILE;
-        const uint32_t cnt = min((uint32_t)ES_TILE, n - t0);
-        const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;  // capacity is a multiple of 4
+    auto issue = [&](uint32_t tile, int stage) {  // tile: index within this CTA's share
+        const uint32_t t0 = beg + tile * ES_TILE;
+        const uint32_t cnt = min((uint32_t)ES_TILE, end - t0);
+        const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;  // beg is a multiple of 4; so is the capacity
         mbar_arrive_expect_tx(&bar[stage], ES_PLANES * bytes);
 #pragma unroll
         for (int a = 0; a < ES_PLANES; ++a)
@@ -137,10 +143,8 @@ __global__ void __launch_bounds__(ES_THREADS)
     uint32_t *wq = queue + warp * ES_QCAP;
     __syncthreads();
     if (tid == 0) {
-        for (int s = 0; s < stages; ++s) {
-            const uint32_t tile = blockIdx.x + (uint32_t)s * gridDim.x;
-            if (tile < ntiles) issue(tile, s);
-        }
+        for (int s = 0; s < stages; ++s)
+            if ((uint32_t)s < ntiles) issue((uint32_t)s, s);
     }
 
     // Scatters wq[first, first + count), one collider per lane.
@@ -172,7 +176,7 @@ __global__ void __launch_bounds__(ES_THREADS)
     uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
     uint32_t qn = 0;            // this warp's queued colliders (warp-uniform)
     uint32_t it = 0;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    for (uint32_t tile = 0; tile < ntiles; ++tile, ++it) {
         if (it != 0 && it % epoch == 0) {  // drain the deposit copies before they can overflow
             __syncthreads();
             dep_drain(hist, copies, ef_pad, acc, g.n_g);
@@ -185,8 +189,8 @@ __global__ void __launch_bounds__(ES_THREADS)
         const bool ok = mbar_wait_bounded(&bar[s], parity);
         if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
 
-        const uint32_t t0 = tile * ES_TILE;
-        const uint32_t cnt = ok ? min((uint32_t)ES_TILE, n - t0) : 0u;
+        const uint32_t t0 = beg + tile * ES_TILE;
+        const uint32_t cnt = ok ? min((uint32_t)ES_TILE, end - t0) : 0u;
         const uint32_t *b = in + s * ES_PLANES * ES_TILE;
         // The rows of a tile are independent; the work is split into phases
         // over all rows so that the scheduler can interleave them.
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(ES_THREADS)
         // stage s consumed; a timeout anywhere ends the loop of every thread
         if (__syncthreads_or(!ok)) break;
         if (tid == 0) {
-            const uint32_t next = tile + (uint32_t)stages * gridDim.x;
+            const uint32_t next = tile + (uint32_t)stages;
             if (next < ntiles) issue(next, s);
         }
         if (have_prev) {

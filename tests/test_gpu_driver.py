@@ -116,33 +116,36 @@ def test_fused_density_equals_fresh_deposit(cudapic, cuda_device, steps, overlap
     st.close()
 
 
-def test_overlap_on_and_off_agree_statistically(cudapic, cuda_device):
-    a = _c0_state(cudapic)
-    b = _c0_state(cudapic)
-    b.set_overlap(False)
-    a.run_cycles(3)
-    b.run_cycles(3)
-    na, nb = a.counts(), b.counts()
-    for x, y in zip(na, nb):
-        assert abs(x - y) <= 0.15 * max(x, y) + 50, (na, nb)
-    assert a.device_error() == 0 and b.device_error() == 0
-    assert a.steps_done() == b.steps_done() == 3 * 4000
-    a.close()
-    b.close()
+def _c0_counts_after(cudapic, mode, seed, cycles=4):
+    st = _c0_state(cudapic, seed=seed)
+    st.seed(e_master=(0x12345678 + seed, 0x11112222, 0x22223333, 0x33334444))
+    if mode == "reference":
+        st.set_fused(False)
+    elif mode == "no_overlap":
+        st.set_overlap(False)
+    st.run_cycles(cycles)
+    counts = st.counts()
+    assert st.device_error() == 0
+    assert st.steps_done() == cycles * 4000
+    st.close()
+    return counts
 
 
-def test_fused_and_reference_sequences_agree_statistically(cudapic, cuda_device):
-    a = _c0_state(cudapic)
-    b = _c0_state(cudapic)
-    b.set_fused(False)
-    a.run_cycles(4)
-    b.run_cycles(4)
-    na, nb = a.counts(), b.counts()
-    for x, y in zip(na, nb):
-        assert abs(x - y) <= 0.15 * max(x, y) + 50, (na, nb)
-    assert a.device_error() == 0 and b.device_error() == 0
-    a.close()
-    b.close()
+@pytest.mark.parametrize("mode", ["reference", "no_overlap"])
+def test_fused_driver_agrees_statistically(cudapic, cuda_device, mode):
+    """The fused driver (electrons drawing from their source slot's stream,
+    programmatic dependent launch) against the reference launch sequence and
+    against itself without PDL: mean electron and ion counts after 4 RF
+    cycles of the igniting C0 discharge over 6 seeds agree within 3 standard
+    errors.  (Single realisations of this growth phase spread by ~5 %, so a
+    pair of runs alone cannot tell a bias from noise.)"""
+    seeds = range(6)
+    fused = np.array([_c0_counts_after(cudapic, "fused", k) for k in seeds], np.float64)
+    other = np.array([_c0_counts_after(cudapic, mode, k) for k in seeds], np.float64)
+    for col in range(2):
+        f, o = fused[:, col], other[:, col]
+        se = np.sqrt(f.var(ddof=1) / len(f) + o.var(ddof=1) / len(o))
+        assert abs(f.mean() - o.mean()) <= 3.0 * se + 0.01 * o.mean(), (col, fused, other)
 
 
 def test_measurement_accumulators(cudapic, cuda_device):
