@@ -74,6 +74,21 @@ class Tuning(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+N_IFED = 200
+
+
+class WallCounters(C.Structure):
+    """cudapic_wall_counters: particles absorbed at each electrode and the
+    ion flux-energy distributions (1 eV bins)."""
+    _fields_ = [("abs_pow", C.c_ulonglong), ("abs_gnd", C.c_ulonglong),
+                ("ifed_pow", C.c_uint32 * N_IFED), ("ifed_gnd", C.c_uint32 * N_IFED)]
+
+    def as_dict(self):
+        import numpy as np
+        return {"abs_pow": int(self.abs_pow), "abs_gnd": int(self.abs_gnd),
+                "ifed_pow": np.array(self.ifed_pow, np.uint32), "ifed_gnd": np.array(self.ifed_gnd, np.uint32)}
+
+
 _P2 = C.c_void_p * 2
 
 
@@ -105,6 +120,8 @@ SIGNATURES = {
     "cudapic_check_collisions_e_events": [_VP] * 18 + [_GP, _VP],
     "cudapic_check_collisions_e_deposit": [_VP] * 19 + [_GP, _VP],
     "cudapic_move_and_compact_deposit": [_VP] * 11 + [_F, _F, _VP, _GP, _VP],
+    "cudapic_move_and_compact_wall": [_VP] * 11 + [_F, _F, _VP, C.c_int, _GP, _VP],
+    "cudapic_state_wall_counters": [_VP, _VP],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],

@@ -18,6 +18,8 @@ constexpr float TWO_PI_F = 6.28318530717958647692f;
 // Physical constants as f32 (`E_MASS as Real`, ... in Rust-CUDA/src/main.rs).
 constexpr float E_MASS_F = 9.10938356e-31f;
 constexpr float E_CHARGE_F = 1.60217662e-19f;
+// 1/2 M_Ar / e as f32: the ion energy in eV of the flux-energy distributions
+constexpr float HALF_MI_OVER_E = (float)(0.5 * 6.63352090e-26 / 1.60217662e-19);
 
 __device__ __forceinline__ void set_dev_err(uint32_t *err, uint32_t bits) {
     if (err) atomicOr(err, bits);

@@ -87,11 +87,13 @@ struct StepLink {
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream,
                    float *zero_a = nullptr, float *zero_b = nullptr);
-// dens_out (may be null): also deposit the survivors' new positions there.
+// dens_out (may be null): also deposit the survivors' new positions there;
+// wall (may be null): count the absorbed particles (with IFEDs for ions).
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_out = nullptr, const StepLink &link = StepLink());
+                            cudaStream_t stream, float *dens_out = nullptr, const StepLink &link = StepLink(),
+                            cudapic_wall_counters *wall = nullptr, bool wall_ions = false);
 // True when `count` planes are 16-byte aligned and the capacity is a multiple
 // of 4 (the bulk-copy tiles of the fused electron step).
 bool electron_step_eligible(const void *const *planes, int count, uint32_t capacity);
@@ -104,7 +106,7 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
                          uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
                          uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
-                         const StepLink &link);
+                         const StepLink &link, cudapic_wall_counters *wall = nullptr);
 // dep_e / dep_i (may be null): next-step densities receiving the spawns.
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,

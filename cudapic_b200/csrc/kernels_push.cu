@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(MC_THREADS)
                                 float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
                                 float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages,
-                                float *__restrict__ dens_out, int copies, uint32_t epoch, const StepLink link) {
+                                float *__restrict__ dens_out, int copies, uint32_t epoch, const StepLink link,
+                                cudapic_wall_counters *wall, int wall_ions) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
     float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(MC_THREADS)
                 cur.vz[u] = bvz[j];
             }
             if (DEPOSIT && keep) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            if (wall) count_wall(wall, wall_ions, j < cnt && !keep, cur.x[u], cur.vx[u], cur.vy[u], cur.vz[u], g.gap);
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             cur.lane_off[u] = __popc(m & lt);
             if (keep) cur.keep |= 1u << u;
@@ -220,7 +222,8 @@ __global__ void __launch_bounds__(MCS_THREADS)
                                    const float *__restrict__ svz, float *__restrict__ dx_,
                                    float *__restrict__ dvx, float *__restrict__ dvy, float *__restrict__ dvz,
                                    uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
-                                   float factor, float dt, const cudapic_grid g) {
+                                   float factor, float dt, const cudapic_grid g, cudapic_wall_counters *wall,
+                                   int wall_ions) {
     extern __shared__ float ef_s[];
     __shared__ uint32_t wsum[MCS_WARPS];
     __shared__ uint32_t s_base;
@@ -237,11 +240,12 @@ __global__ void __launch_bounds__(MCS_THREADS)
         float vy = 0.0f, vz = 0.0f;
         if (i < n) {
             pr = push_one(sx[i], svx[i], ef_s, factor, dt, g);
-            if (pr.keep) {
+            if (pr.keep || wall) {
                 vy = svy[i];
                 vz = svz[i];
             }
         }
+        if (wall) count_wall(wall, wall_ions, i < n && !pr.keep, pr.x, pr.vx, vy, vz, g.gap);
         const unsigned mask = __ballot_sync(0xffffffffu, pr.keep);
         const uint32_t lane_off = __popc(mask & lanemask_lt());
         if (lane == 0) wsum[warp] = __popc(mask);
@@ -282,7 +286,8 @@ size_t tma_smem_bytes(uint32_t n_g, int stages, uint32_t &ef_pad) {
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,
                             const float *svz, float *dx_, float *dvx, float *dvy, float *dvz, uint32_t *alive,
                             const uint32_t *n_active, float factor, float dt, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_out, const StepLink &link) {
+                            cudaStream_t stream, float *dens_out, const StepLink &link,
+                            cudapic_wall_counters *wall, bool wall_ions) {
     const bool tma_ok = aligned16(sx) && aligned16(svx) && aligned16(svy) && aligned16(svz) &&
                         (g.capacity % 4u) == 0u;
     if (tma_ok) {
@@ -314,11 +319,11 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
         return launch_kernel("move_and_compact_tma", kern, dim3(grid), dim3(MC_THREADS), smem, stream, efield, sx, svx,
                              svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g, ef_pad, stages, dens_out,
-                             copies, epoch, link);
+                             copies, epoch, link, wall, (int)wall_ions);
     }
     if (dens_out || link.ticket) {  // unaligned buffers: separate deposit and count copy
         CUDAPIC_CHECK(launch_move_and_compact(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor,
-                                              dt, g, stream, nullptr));
+                                              dt, g, stream, nullptr, StepLink(), wall, wall_ions));
         if (dens_out) CUDAPIC_CHECK(cudapic_get_density(dx_, dens_out, alive, &g, (cudapic_stream_t)stream));
         if (link.ticket) {
             CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(link.dst, link.src, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
@@ -336,7 +341,8 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
     const uint64_t blocks_max = ((uint64_t)g.capacity + MCS_THREADS - 1) / MCS_THREADS;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * 4, blocks_max));
     return launch_kernel("move_and_compact_simple", move_and_compact_simple_kernel, dim3(grid), dim3(MCS_THREADS), smem,
-                         stream, efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g);
+                         stream, efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g, wall,
+                         (int)wall_ions);
 }
 
 }  // namespace cudapic
@@ -372,4 +378,21 @@ extern "C" int cudapic_move_and_compact_deposit(const float *efield, const float
                     "move_and_compact_deposit: src and dst must be distinct buffers");
     return launch_move_and_compact(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz,
                                    alive_counter, n_active, factor, dt, *grid, (cudaStream_t)stream, next_density);
+}
+
+extern "C" int cudapic_move_and_compact_wall(const float *efield, const float *src_x, const float *src_vx,
+                                             const float *src_vy, const float *src_vz, float *dst_x, float *dst_vx,
+                                             float *dst_vy, float *dst_vz, uint32_t *alive_counter,
+                                             const uint32_t *n_active, float factor, float dt,
+                                             cudapic_wall_counters *wall, int ions, const cudapic_grid *grid,
+                                             cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(efield && src_x && src_vx && src_vy && src_vz && dst_x && dst_vx && dst_vy && dst_vz &&
+                        alive_counter && n_active && wall,
+                    "move_and_compact_wall: null pointer");
+    CUDAPIC_REQUIRE(src_x != dst_x && src_vx != dst_vx && src_vy != dst_vy && src_vz != dst_vz,
+                    "move_and_compact_wall: src and dst must be distinct buffers");
+    return launch_move_and_compact(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz,
+                                   alive_counter, n_active, factor, dt, *grid, (cudaStream_t)stream, nullptr,
+                                   StepLink(), wall, ions != 0);
 }

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(ES_THREADS)
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
                          const uint32_t *__restrict__ n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                          const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int stages, int copies,
-                         uint32_t epoch, const StepLink link) {
+                         uint32_t epoch, const StepLink link, cudapic_wall_counters *wall) {
     constexpr int ES_TILE = StepShape<U>::TILE;
     constexpr int ES_QCAP = StepShape<U>::QCAP;
     constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
@@ -208,6 +208,7 @@ __global__ void __launch_bounds__(ES_THREADS)
             const float v0 = valid ? __uint_as_float(b[ES_TILE + j]) : 0.0f;
             const PushResult pr = push_one(x0, v0, ef, g.factor_e, g.dt_e, g);
             if (valid && pr.keep) keep |= 1u << u;
+            if (wall) count_wall(wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, g.gap);
             cur.x[u] = pr.x;
             cur.vx[u] = pr.vx;
         }
@@ -355,7 +356,7 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
                            float sigma_max_e, float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
                            const uint32_t *n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                            const cudapic_grid &g, cudaStream_t stream, const StepLink &link,
-                           const cudapic_tuning &t) {
+                           cudapic_wall_counters *wall, const cudapic_tuning &t) {
     constexpr int ES_TILE = StepShape<U>::TILE;
     constexpr int ES_QCAP = StepShape<U>::QCAP;
     int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
@@ -384,7 +385,7 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
     return launch_kernel("step_electrons", kern, dim3(grid), dim3(ES_THREADS), smem, stream, efield, sx, svx, svy, svz,
                          dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz,
-                         alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link);
+                         alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link, wall);
 }
 
 }  // namespace
@@ -394,13 +395,13 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
                          uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
                          uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
-                         const StepLink &link) {
+                         const StepLink &link, cudapic_wall_counters *wall) {
     const void *planes[8] = {sx, svx, svy, svz, rng0, rng1, rng2, rng3};
     if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
     const cudapic_tuning t = tuning();
     auto launch = t.step_rows == 4 ? launch_electron_step_t<4> : launch_electron_step_t<2>;
     return launch(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e,
-                  ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, t);
+                  ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, wall, t);
 }
 
 }  // namespace cudapic

@@ -31,6 +31,27 @@ __device__ __forceinline__ PushResult push_one(float xi, float vxi, const float 
     return r;
 }
 
+// Boundary check of C/eduPIC.cc:623-667 for one row of a warp (every lane
+// calls it): particles with a pushed position x < 0 count at the powered
+// electrode, x > L at the grounded one, one atomic per electrode and row;
+// with ions, the energy 1/2 M v^2 / e of an absorbed ion goes to the 1 eV bin
+// of that electrode's IFED (below 200 eV).
+__device__ __forceinline__ void count_wall(cudapic_wall_counters *w, bool ions, bool valid, float x, float vx,
+                                           float vy, float vz, float gap) {
+    const bool at_pow = valid && x < 0.0f;
+    const bool at_gnd = valid && x > gap;
+    const unsigned mp = __ballot_sync(0xffffffffu, at_pow);
+    const unsigned mg = __ballot_sync(0xffffffffu, at_gnd);
+    if ((threadIdx.x & 31) == 0) {
+        if (mp) atomicAdd(&w->abs_pow, (unsigned long long)__popc(mp));
+        if (mg) atomicAdd(&w->abs_gnd, (unsigned long long)__popc(mg));
+    }
+    if (ions && (at_pow || at_gnd)) {
+        const float e = HALF_MI_OVER_E * (vx * vx + vy * vy + vz * vz);
+        if (e < (float)CUDAPIC_N_IFED) atomicAdd(at_pow ? &w->ifed_pow[(int)e] : &w->ifed_gnd[(int)e], 1u);
+    }
+}
+
 // Fused deposit in 2^-20 fixed point.  A particle at rem = pos - p in [0, 1]
 // adds 2^20 - r to node p and r to node p + 1, r = round(rem * 2^20), with
 // 32-bit integer shared atomics (on sm_100a several times the throughput of

@@ -53,6 +53,7 @@ struct cudapic_state {
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
     float sigma_max_e = 0.0f;  // largest entry of sigma_tot_e (the fused step's certain-rejection bound)
     double *cumul_e = nullptr, *cumul_i = nullptr;
+    cudapic_wall_counters *wall = nullptr;  // [0] electrons, [1] ions (measurement window)
     uint32_t *eepf = nullptr;
 
     bool measure = false;
@@ -127,7 +128,7 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
         CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
                                               s->x[I][si ^ 1], s->vx[I][si ^ 1], s->vy[I][si ^ 1],
                                               s->vz[I][si ^ 1], s->alive_i(), s->n_i(), g.factor_i, g.dt_i, g, st,
-                                              i_acc, li));
+                                              i_acc, li, s->measure ? s->wall + 1 : nullptr, true));
         si ^= 1;
         s->side[I] = si;
     }
@@ -140,7 +141,8 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
                                        s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
                                        s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3], s->sigma_tot_e, s->cs,
                                        s->sigma_max_e, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
-                                       s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le));
+                                       s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le,
+                                       s->measure ? s->wall : nullptr));
     se ^= 1;
     s->side[E] = se;
     s->e_cur ^= 1;
@@ -212,7 +214,8 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
     CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
                                           s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
-                                          s->alive(), s->n_e(), g.factor_e, g.dt_e, g, st, e_next));
+                                          s->alive(), s->n_e(), g.factor_e, g.dt_e, g, st, e_next, StepLink(),
+                                          s->measure ? s->wall : nullptr, false));
     se ^= 1;
     s->side[E] = se;
     CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
@@ -222,7 +225,7 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
         CUDAPIC_CHECK(launch_move_and_compact(s->efield, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
                                               s->x[I][si ^ 1], s->vx[I][si ^ 1], s->vy[I][si ^ 1],
                                               s->vz[I][si ^ 1], s->alive(), s->n_i(), g.factor_i, g.dt_i, g, st,
-                                              i_acc));
+                                              i_acc, StepLink(), s->measure ? s->wall + 1 : nullptr, true));
         si ^= 1;
         s->side[I] = si;
         CUDAPIC_CHECK(check_cuda(
@@ -339,7 +342,8 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
         (rc = dalloc(s, &s->i_dens[0], n_g)) || (rc = dalloc(s, &s->i_dens[1], n_g)) ||
         (rc = dalloc(s, &s->pot0_table, p->n_t)) || (rc = dalloc(s, &s->cs, 5ull * CUDAPIC_CS_RANGES)) ||
         (rc = dalloc(s, &s->sigma_tot_e, CUDAPIC_CS_RANGES)) || (rc = dalloc(s, &s->sigma_tot_i, CUDAPIC_CS_RANGES)) ||
-        (rc = dalloc(s, &s->cumul_e, n_g)) || (rc = dalloc(s, &s->cumul_i, n_g)) || (rc = dalloc(s, &s->eepf, 2000)))
+        (rc = dalloc(s, &s->cumul_e, n_g)) || (rc = dalloc(s, &s->cumul_i, n_g)) || (rc = dalloc(s, &s->eepf, 2000)) ||
+        (rc = dalloc(s, &s->wall, 2)))
         return cleanup(rc);
     s->grid.dev_err = s->dev_err();
     s->grid.work = s->work();
@@ -358,6 +362,7 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
         (rc = check_cuda(cudaMemsetAsync(s->i_dens[0], 0, n_g * sizeof(float), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->i_dens[1], 0, n_g * sizeof(float), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->wall, 0, 2 * sizeof(cudapic_wall_counters), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "memset")))
         return cleanup(rc);
@@ -531,6 +536,7 @@ extern "C" int cudapic_state_set_measure(cudapic_state *s, int on) {
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "zero cumul_e"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "zero cumul_i"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "zero eepf"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->wall, 0, 2 * sizeof(cudapic_wall_counters), s->stream), "zero wall"));
     s->measure = on != 0;
     return CUDAPIC_OK;
 }
@@ -606,6 +612,14 @@ extern "C" int cudapic_state_synchronize(cudapic_state *s) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_synchronize: null state");
     DeviceGuard dg(s->device);
     return check_cuda(cudaStreamSynchronize(s->stream), "state_synchronize");
+}
+
+extern "C" int cudapic_state_wall_counters(cudapic_state *s, cudapic_wall_counters out[2]) {
+    if (!s || !out) return fail(CUDAPIC_ERR_ARG, "state_wall_counters: null pointer");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(out, s->wall, 2 * sizeof(cudapic_wall_counters), cudaMemcpyDeviceToHost,
+                                             s->stream), "download wall counters"));
+    return check_cuda(cudaStreamSynchronize(s->stream), "wall counters sync");
 }
 
 extern "C" int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, double *cumul_i,

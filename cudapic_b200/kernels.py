@@ -87,6 +87,17 @@ def check_collisions_e_deposit(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rn
     check(lib.cudapic_check_collisions_e_deposit(*args, _g(grid), _stream(stream, vx)))
 
 
+def move_and_compact_wall(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, alive_counter,
+                          n_active, factor, dt, wall, ions, grid, stream=None):
+    """move_and_compact that also counts the particles absorbed at each
+    electrode into the device block `wall` (cudapic_wall_counters; ions also
+    fill the IFEDs), the boundary check of C/eduPIC.cc:623-667."""
+    check(lib.cudapic_move_and_compact_wall(_ptr(efield), _ptr(src_x), _ptr(src_vx), _ptr(src_vy), _ptr(src_vz),
+                                            _ptr(dst_x), _ptr(dst_vx), _ptr(dst_vy), _ptr(dst_vz),
+                                            _ptr(alive_counter), _ptr(n_active), float(factor), float(dt), _ptr(wall),
+                                            1 if ions else 0, _g(grid), _stream(stream, src_x)))
+
+
 def step_electrons(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx, dst_vy, dst_vz, rng0, rng1, rng2, rng3,
                    total_cs_e, cs, sigma_max_e, i_x, i_vx, i_vy, i_vz, alive_counter, n_e, n_i, e_next_density,
                    i_next_density, grid, stream=None):

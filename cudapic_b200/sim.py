@@ -143,6 +143,13 @@ class GpuSimState:
         """Programmatic dependent launch between the step's kernels (default on)."""
         check(lib.cudapic_state_set_overlap(self._h, 1 if on else 0))
 
+    def wall_counters(self):
+        """Electrode counters of the measurement window:
+        {"e": {...}, "i": {...}} with abs_pow, abs_gnd, ifed_pow, ifed_gnd."""
+        out = (_lib.WallCounters * 2)()
+        check(lib.cudapic_state_wall_counters(self._h, out))
+        return {"e": out[0].as_dict(), "i": out[1].as_dict()}
+
     def download_measurements(self):
         n_g = self.grid.n_g
         ce = np.zeros(n_g, np.float64)

@@ -318,6 +318,30 @@ int cudapic_xoshiro128_seed_streams(const uint32_t master[4], uint32_t n, uint32
 #define CUDAPIC_CS_RANGES 1000000u
 int cudapic_cross_sections(double gas_density, float *cs, float *sigma_tot_e, float *sigma_tot_i);
 
+/* Particles absorbed at the electrodes (C/eduPIC.cc:623-667; the GPU
+ * reference keeps none, Rust-CUDA has no counterpart): a particle whose
+ * pushed position is x < 0 counts at the powered electrode, x > L at the
+ * grounded one.  Ions also add their energy 1/2 M v^2 / e (f32, v after the
+ * push) to the ion flux-energy distribution of that electrode: 1 eV bins,
+ * energies of 200 eV and above not binned (C/eduPIC.cc:118-119, 645-657).
+ * A device-memory block; the counters only grow (zero it to restart). */
+#define CUDAPIC_N_IFED 200
+typedef struct cudapic_wall_counters {
+    unsigned long long abs_pow;          /* absorbed at x < 0 (powered electrode)  */
+    unsigned long long abs_gnd;          /* absorbed at x > L (grounded electrode) */
+    uint32_t ifed_pow[CUDAPIC_N_IFED];   /* ions: counts per 1 eV energy bin       */
+    uint32_t ifed_gnd[CUDAPIC_N_IFED];
+} cudapic_wall_counters;
+
+/* move_and_compact that also counts the absorbed particles into `wall`
+ * (device pointer); ions != 0 also fills its IFEDs.  No single reference
+ * counterpart: the boundary check of C/eduPIC.cc:623-667 fused into the push. */
+int cudapic_move_and_compact_wall(const float *efield, const float *src_x, const float *src_vx,
+                                  const float *src_vy, const float *src_vz, float *dst_x, float *dst_vx,
+                                  float *dst_vy, float *dst_vz, uint32_t *alive_counter, const uint32_t *n_active,
+                                  float factor, float dt, cudapic_wall_counters *wall, int ions,
+                                  const cudapic_grid *grid, cudapic_stream_t stream);
+
 /* Evaluates the kernels' f32 transcendental functions on device arrays
  * (fn: 0 exp, 1 log, 2 sin, 3 cos, 4 tan, 5 atan, 6 acos, 7 atan2(in, in2)).
  * No reference counterpart: a diagnostic for the bit-exactness tests. */
@@ -397,6 +421,10 @@ int cudapic_state_steps_done(const cudapic_state *s, uint64_t *steps);
 int cudapic_state_synchronize(cudapic_state *s);
 int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, double *cumul_i,
                                         uint32_t *eepf);
+/* The electrode counters of the measurement window (zeroed by
+ * cudapic_state_set_measure(s, 1)): out[0] electrons, out[1] ions, host
+ * memory (synchronises). */
+int cudapic_state_wall_counters(cudapic_state *s, cudapic_wall_counters out[2]);
 
 #ifdef __cplusplus
 }

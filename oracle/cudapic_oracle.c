@@ -392,6 +392,35 @@ uint32_t orc_move_and_compact(const float *efield,
     return m;
 }
 
+/* Boundary check of C/eduPIC.cc:623-667 on the pushed particles of
+ * orc_move_and_compact: counts[0] += absorbed at x < 0 (powered electrode),
+ * counts[1] += absorbed at x > L (grounded); with ions, the ion energy
+ * 1/2 M v^2 / e in f32 (HALF_MI_OVER_E, v after the push) goes to the 1 eV
+ * bin floor(E) of that electrode's IFED when below 200 eV (:118-119, :645-657). */
+static const float HALF_MI_OVER_E = (float)(0.5 * ORC_AR_MASS / ORC_E_CHARGE);
+
+void orc_wall_count(const float *efield, const float *sx, const float *svx, const float *svy, const float *svz,
+                    uint32_t n, float factor, float dt, const orc_phys *ph, int ions, uint64_t counts[2],
+                    uint32_t *ifed_pow, uint32_t *ifed_gnd) {
+    for (uint32_t i = 0; i < n; ++i) {
+        float xi = sx[i];
+        float vxi = svx[i];
+        float pos = xi * ph->inv_dx;
+        int p = cell_of(pos, ph->n_g);
+        float c2 = pos - (float)p;
+        float e_x = (1.0f - c2) * efield[p] + c2 * efield[p + 1];
+        float nvx = vxi + factor * e_x;
+        float nx = xi + nvx * dt;
+        int side = nx < 0.0f ? 0 : (nx > ph->gap ? 1 : -1);
+        if (side < 0) continue;
+        counts[side] += 1;
+        if (ions) {
+            float e = HALF_MI_OVER_E * (nvx * nvx + svy[i] * svy[i] + svz[i] * svz[i]);
+            if (e < (float)ORC_N_IFED) (side == 0 ? ifed_pow : ifed_gnd)[(int)e] += 1;
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* MCC                                                                 */
 /* ------------------------------------------------------------------ */

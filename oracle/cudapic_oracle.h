@@ -35,6 +35,7 @@ extern "C" {
 #define ORC_EPSILON0    8.85418781e-12
 #define ORC_CS_RANGES   1000000
 #define ORC_N_EEPF      2000
+#define ORC_N_IFED      200
 
 /* Runtime replacement of the reference's compile-time simulation constants
  * (Rust-CUDA/src/main.rs:40-50, 53-59, 79-82). */
@@ -128,6 +129,9 @@ void orc_poisson_dps_flexible_f64(const double *source, double *pot, uint32_t n,
                                   double psi_left, double psi_right, double dx);
 
 /* ---- push + absorb + compact (Rust-CUDA/src/main.rs:566-678), stable order ---- */
+void orc_wall_count(const float *efield, const float *sx, const float *svx, const float *svy, const float *svz,
+                    uint32_t n, float factor, float dt, const orc_phys *ph, int ions, uint64_t counts[2],
+                    uint32_t *ifed_pow, uint32_t *ifed_gnd);
 uint32_t orc_move_and_compact(const float *efield,
                               const float *sx, const float *svx, const float *svy, const float *svz,
                               float *dx_, float *dvx, float *dvy, float *dvz,

@@ -15,9 +15,10 @@ _LIB_PATH = os.path.join(_HERE, "libcudapic_oracle.so")
 REF_DIR = os.path.join(_HERE, "_ref")
 CS_RANGES = 1_000_000
 N_EEPF = 2000
+N_IFED = 200
 
 __all__ = [
-    "lib", "build", "OrcParams", "OrcPhys", "default_params", "phys_from_params",
+    "lib", "build", "OrcParams", "OrcPhys", "default_params", "phys_from_params", "wall_count", "N_IFED",
     "xoshiro_stream", "u32_to_real", "jump", "seed_streams", "math_apply",
     "cross_sections", "get_density_f32", "get_density_f64", "poisson_thomas_f64",
     "poisson_scan_f32", "poisson_dps_flexible_f64", "move_and_compact",
@@ -74,6 +75,7 @@ def lib():
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
@@ -99,6 +101,9 @@ def _declare(L):
     L.orc_move_and_compact.argtypes = [_f32p] + [_f32p] * 8 + [C.c_uint32, C.c_float, C.c_float,
                                                               P(OrcPhys), _u32p]
     L.orc_move_and_compact.restype = C.c_uint32
+    L.orc_wall_count.argtypes = [_f32p] * 5 + [C.c_uint32, C.c_float, C.c_float, P(OrcPhys), C.c_int,
+                                               _u64p, _u32p, _u32p]
+    L.orc_wall_count.restype = None
     L.orc_check_collisions_e.argtypes = ([_f32p, _f32p, C.c_uint32] + [_f32p] * 4 + [_u32p] * 4 +
                                          [_f32p] * 4 + [P(C.c_uint32), P(C.c_uint32), P(OrcPhys),
                                                         _u8p, P(C.c_uint32)])
@@ -217,6 +222,17 @@ def move_and_compact(efield, x, vx, vy, vz, factor, dt, ph):
     m = lib().orc_move_and_compact(_f32(efield), _f32(x), _f32(vx), _f32(vy), _f32(vz), *out,
                                    n, float(factor), float(dt), C.byref(ph), idx)
     return tuple(a[:m] for a in out) + (idx[:m],)
+
+
+def wall_count(efield, x, vx, vy, vz, factor, dt, ph, ions):
+    """Absorption counts (powered, grounded) and IFEDs of one push
+    (C/eduPIC.cc:623-667)."""
+    counts = np.zeros(2, np.uint64)
+    ifed_pow = np.zeros(N_IFED, np.uint32)
+    ifed_gnd = np.zeros(N_IFED, np.uint32)
+    lib().orc_wall_count(_f32(efield), _f32(x), _f32(vx), _f32(vy), _f32(vz), len(x), float(factor), float(dt),
+                         C.byref(ph), 1 if ions else 0, counts, ifed_pow, ifed_gnd)
+    return counts, ifed_pow, ifed_gnd
 
 
 def check_collisions_e(sigma_tot_e, cs, n_active, e, rng, ions, n_e, n_i, ph):

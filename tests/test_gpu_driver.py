@@ -9,6 +9,9 @@ from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
+E_MASS = 9.10938356e-31
+AR_MASS = 6.63352090e-26
+
 
 def _c0_state(cudapic, seed=0, **kw):
     from cudapic_b200.sim import GpuSimState, ParticlesSoA
@@ -146,6 +149,42 @@ def test_fused_driver_agrees_statistically(cudapic, cuda_device, mode):
         f, o = fused[:, col], other[:, col]
         se = np.sqrt(f.var(ddof=1) / len(f) + o.var(ddof=1) / len(o))
         assert abs(f.mean() - o.mean()) <= 3.0 * se + 0.01 * o.mean(), (col, fused, other)
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_wall_counters_of_one_step_match_the_oracle(cudapic, oracle, cuda_device, fused):
+    """Measurement of one step (an ion step) from an uploaded population:
+    electrons and ions absorbed at each electrode, and the ion IFEDs, equal
+    the oracle's boundary check of the same push in the same field."""
+    import torch
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    from cudapic_b200.workloads import steady_state
+    n = 200_000
+    st = GpuSimState(capacity=2 * n, weight=7.0e4 * 120000 / n)
+    st.set_fused(fused)
+    g = st.grid
+    pe = steady_state(n, E_MASS, 3.0, dt=g.dt_e, edge_fraction=0.02, seed=11)
+    pi = steady_state(n, AR_MASS, 20.0, dt=g.dt_i, edge_fraction=0.02, seed=12)
+    st.upload_electrons(ParticlesSoA(*pe))
+    st.upload_ions(ParticlesSoA(*pi))
+    st.seed()
+    st.set_measure(True)
+    st.run_steps(1)
+    w = st.wall_counters()
+    b = st.buffers()
+    ef64 = torch.zeros(g.n_g, dtype=torch.float64, device="cuda")
+    cudapic.kernels.accumulate_density(b.efield, ef64, g, stream=0)   # the field of step 0, exactly
+    ef = ef64.cpu().numpy().astype(np.float32)
+    ph = oracle.phys_from_params(capacity=2 * n, weight=7.0e4 * 120000 / n)
+    ce, _, _ = oracle.wall_count(ef, *pe, g.factor_e, g.dt_e, ph, False)
+    ci, ip, ig = oracle.wall_count(ef, *pi, g.factor_i, g.dt_i, ph, True)
+    assert (w["e"]["abs_pow"], w["e"]["abs_gnd"]) == (int(ce[0]), int(ce[1]))
+    assert (w["i"]["abs_pow"], w["i"]["abs_gnd"]) == (int(ci[0]), int(ci[1]))
+    assert np.array_equal(w["i"]["ifed_pow"], ip) and np.array_equal(w["i"]["ifed_gnd"], ig)
+    assert ce.min() > 100 and ci.min() > 100
+    st.set_measure(True)                                  # a new window starts from zero
+    assert st.wall_counters()["e"]["abs_pow"] == 0
+    st.close()
 
 
 def test_measurement_accumulators(cudapic, cuda_device):

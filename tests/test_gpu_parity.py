@@ -396,6 +396,55 @@ def test_check_collisions_e_deposit_spawns(cudapic, K, oracle, dev_tables, table
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-5
 
 
+def _wall_block():
+    import ctypes as C
+    import torch
+    from cudapic_b200 import _lib
+    return torch.zeros(C.sizeof(_lib.WallCounters) // 4, dtype=torch.int32, device="cuda")
+
+
+def _wall_read(t):
+    import ctypes as C
+    from cudapic_b200 import _lib
+    raw = host(t).view(np.uint32).tobytes()
+    return _lib.WallCounters.from_buffer_copy(raw).as_dict()
+
+
+@pytest.mark.parametrize("species", ["e", "i"])
+@pytest.mark.parametrize("layout", ["aligned", "unaligned"])
+def test_move_and_compact_wall_bit_exact(cudapic, K, oracle, species, layout):
+    """Absorption counters and IFEDs fused into the push (C/eduPIC.cc:623-667)
+    equal the oracle's count of the same push; called twice, they add up."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    n = 300_001
+    cap = (n + 3) // 4 * 4
+    g = cudapic.grid_from_params(capacity=cap + 4)
+    ph = oracle.phys_from_params(capacity=cap + 4)
+    mass, temp = (E_MASS, 4.0) if species == "e" else (AR_MASS, 30.0)   # hot ions: IFED bins up to ~100 eV
+    factor, dt = (g.factor_e, g.dt_e) if species == "e" else (g.factor_i, g.dt_i)
+    x, vx, vy, vz = steady_state(n, mass, temp, dt=dt, edge_fraction=0.02, seed=5)
+    ef = field_profile(400)
+    if layout == "aligned":
+        src = [dev(np.concatenate([a, np.zeros(cap + 4 - n, np.float32)])) for a in (x, vx, vy, vz)]
+        ptrs = src
+    else:
+        src = [dev(np.concatenate([[0.0], a, np.zeros(cap + 3 - n)]).astype(np.float32)) for a in (x, vx, vy, vz)]
+        ptrs = [t.data_ptr() + 4 for t in src]
+    wall = _wall_block()
+    for rep in range(2):
+        dst = [zeros(cap + 4) for _ in range(4)]
+        K.move_and_compact_wall(dev(ef), *ptrs, *dst, counter(0), counter(n), factor, dt, wall, species == "i", g)
+    got = _wall_read(wall)
+    counts, ip, ig = oracle.wall_count(ef, x, vx, vy, vz, factor, dt, ph, species == "i")
+    assert counts.min() > 1000
+    assert (got["abs_pow"], got["abs_gnd"]) == (2 * int(counts[0]), 2 * int(counts[1]))
+    if species == "i":
+        assert ip.sum() > 1000 and ig.sum() > 1000
+        assert np.array_equal(got["ifed_pow"], 2 * ip) and np.array_equal(got["ifed_gnd"], 2 * ig)
+    else:
+        assert not got["ifed_pow"].any() and not got["ifed_gnd"].any()
+
+
 def test_move_and_compact_unaligned_uses_reference_layout(cudapic, K, oracle):
     from cudapic_b200.workloads import field_profile
     n, n_g = 70_001, 400

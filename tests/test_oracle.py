@@ -213,3 +213,27 @@ def test_collision_decisions_vs_exact(oracle, tables):
     assert got.sum() > 100
     assert ne - n == np.sum(events == 3) and ni == np.sum(events == 3)
     assert dropped == 0
+
+
+def test_wall_count_known_answers(oracle):
+    """Boundary check of C/eduPIC.cc:623-667: sides by the pushed position,
+    ion energies binned at floor(1/2 M v^2 / e) below 200 eV."""
+    import numpy as np
+    ph = oracle.phys_from_params()
+    L = ph.gap
+    m_half = 0.5 * 6.63352090e-26 / 1.60217662e-19
+    v_of = lambda e: np.sqrt(e / m_half)  # noqa: E731
+    x = np.array([-1e-6, -1e-6, L + 1e-6, L + 1e-6, 0.5 * L, 0.0, L], np.float32)
+    vx = np.array([-v_of(10.5), -v_of(250.0), v_of(3.2), 0.0, 0.0, 0.0, 0.0], np.float32)
+    z = np.zeros_like(x)
+    counts, ip, ig = oracle.wall_count(np.zeros(400, np.float32), x, vx, z, z, 0.0, 0.0, ph, True)
+    assert list(counts) == [2, 2]                       # x = 0 and x = L stay
+    assert ip.sum() == 1 and ip[10] == 1                 # the 250 eV ion is counted but not binned
+    assert ig.sum() == 2 and ig[3] == 1 and ig[0] == 1
+    # electrons: counts only; every absorbed particle is one not kept by the push
+    from cudapic_b200.workloads import field_profile, steady_state
+    xs, vxs, vys, vzs = steady_state(20000, 9.10938356e-31, 5.0, dt=1.8e-11, edge_fraction=0.02, seed=3)
+    ef = field_profile(400)
+    c, _, _ = oracle.wall_count(ef, xs, vxs, vys, vzs, -3.2e4, 1.8e-11, ph, False)
+    kept = oracle.move_and_compact(ef, xs, vxs, vys, vzs, -3.2e4, 1.8e-11, ph)[0].size
+    assert int(c.sum()) == 20000 - kept and c.min() > 0
