@@ -122,6 +122,11 @@ SIGNATURES = {
     "cudapic_move_and_compact_deposit": [_VP] * 11 + [_F, _F, _VP, _GP, _VP],
     "cudapic_move_and_compact_wall": [_VP] * 11 + [_F, _F, _VP, C.c_int, _GP, _VP],
     "cudapic_state_wall_counters": [_VP, _VP],
+    "cudapic_picdata_write": [C.c_char_p, C.c_double, _U32, _VP, _U32, _VP, _U32],
+    "cudapic_picdata_read_header": [C.c_char_p, _VP, _VP, _VP, _VP],
+    "cudapic_picdata_read": [C.c_char_p, _VP, _U32, _VP, _U32],
+    "cudapic_state_save": [_VP, C.c_char_p],
+    "cudapic_state_load": [_VP, C.c_char_p],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "../../include/cudapic.h"
 
@@ -118,6 +119,12 @@ int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t
                         const cudapic_grid &g, cudaStream_t stream);
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
                 const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream);
+
+// RNG sidecar of a checkpoint (<path>.rng, checkpoint.cpp): both species'
+// four planes over `capacity` slots.  read: CUDAPIC_ERR_NOT_SUPPORTED,
+// nothing recorded, when the file does not exist.
+int rng_sidecar_write(const char *path, uint32_t capacity, const std::vector<uint32_t> planes[2][4]);
+int rng_sidecar_read(const char *path, uint32_t capacity, std::vector<uint32_t> planes[2][4]);
 
 }  // namespace cudapic
 

@@ -510,6 +510,78 @@ extern "C" int cudapic_state_seed(cudapic_state *s, const uint32_t e_master[4], 
     return CUDAPIC_OK;
 }
 
+// eduPIC's time step DT_E = 1 / (f N_T) in double (C/eduPIC.cc:65-69).
+static double dt_e_double(const cudapic_state *s) {
+    return 1.0 / (s->params.frequency * (double)s->params.n_t);
+}
+
+extern "C" int cudapic_state_save(cudapic_state *s, const char *path) {
+    if (!s || !path) return fail(CUDAPIC_ERR_ARG, "state_save: null pointer");
+    DeviceGuard dg(s->device);
+    const uint32_t cap = s->params.capacity;
+    std::vector<float> e[4], i[4];
+    for (int a = 0; a < 4; ++a) {
+        e[a].resize(cap);
+        i[a].resize(cap);
+    }
+    uint32_t ne = 0, ni = 0;
+    CUDAPIC_CHECK(cudapic_state_download(s, 0, e[0].data(), e[1].data(), e[2].data(), e[3].data(), cap, &ne));
+    CUDAPIC_CHECK(cudapic_state_download(s, 1, i[0].data(), i[1].data(), i[2].data(), i[3].data(), cap, &ni));
+    const float *ep[4] = {e[0].data(), e[1].data(), e[2].data(), e[3].data()};
+    const float *ip[4] = {i[0].data(), i[1].data(), i[2].data(), i[3].data()};
+    const double time = (double)s->steps_done * dt_e_double(s);  // eduPIC's Time
+    CUDAPIC_CHECK(cudapic_picdata_write(path, time, (uint32_t)(s->steps_done / s->params.n_t), ep, ne, ip, ni));
+    std::vector<uint32_t> planes[2][4];
+    for (int sp = 0; sp < 2; ++sp)
+        for (int k = 0; k < 4; ++k) {
+            planes[sp][k].resize(cap);
+            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(planes[sp][k].data(), s->rng[sp][k], cap * sizeof(uint32_t),
+                                                     cudaMemcpyDeviceToHost, s->stream), "state_save: download rng"));
+        }
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_save sync"));
+    return rng_sidecar_write(path, cap, planes);
+}
+
+extern "C" int cudapic_state_load(cudapic_state *s, const char *path) {
+    if (!s || !path) return fail(CUDAPIC_ERR_ARG, "state_load: null pointer");
+    DeviceGuard dg(s->device);
+    double time = 0.0;
+    uint32_t cycles = 0, ne = 0, ni = 0;
+    CUDAPIC_CHECK(cudapic_picdata_read_header(path, &time, &cycles, &ne, &ni));
+    const uint32_t cap = s->params.capacity;
+    if (ne > cap || ni > cap) return fail(CUDAPIC_ERR_CAPACITY, "state_load: more particles than the capacity");
+    std::vector<float> e[4], i[4];
+    for (int a = 0; a < 4; ++a) {
+        e[a].resize(std::max<uint32_t>(ne, 1));
+        i[a].resize(std::max<uint32_t>(ni, 1));
+    }
+    float *ep[4] = {e[0].data(), e[1].data(), e[2].data(), e[3].data()};
+    float *ip[4] = {i[0].data(), i[1].data(), i[2].data(), i[3].data()};
+    CUDAPIC_CHECK(cudapic_picdata_read(path, ep, ne, ip, ni));
+    CUDAPIC_CHECK(cudapic_state_upload(s, 0, ep[0], ep[1], ep[2], ep[3], ne));
+    CUDAPIC_CHECK(cudapic_state_upload(s, 1, ip[0], ip[1], ip[2], ip[3], ni));
+    // the step count (and with it the RF phase and the ion subcycle) from eduPIC's Time
+    const double steps = time > 0.0 ? std::floor(time / dt_e_double(s) + 0.5) : 0.0;
+    s->steps_done = (uint64_t)steps;
+    const uint32_t counter = (uint32_t)(s->steps_done & 0xffffffffu);
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->step_counter(), &counter, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                             s->stream), "state_load: step counter"));
+    std::vector<uint32_t> planes[2][4];
+    const int rc = rng_sidecar_read(path, cap, planes);
+    if (rc == CUDAPIC_ERR_NOT_SUPPORTED) {  // an eduPIC file: fresh streams from the reference master seeds
+        const uint32_t em[4] = {0x12345678u, 0x11112222u, 0x22223333u, 0x33334444u};
+        const uint32_t im[4] = {0x44445555u, 0x55556666u, 0x66667777u, 0x77778888u};
+        CUDAPIC_CHECK(cudapic_state_seed(s, em, im));
+    } else {
+        CUDAPIC_CHECK(rc);
+        for (int sp = 0; sp < 2; ++sp)
+            for (int k = 0; k < 4; ++k)
+                CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->rng[sp][k], planes[sp][k].data(), cap * sizeof(uint32_t),
+                                                         cudaMemcpyHostToDevice, s->stream), "state_load: rng"));
+    }
+    return check_cuda(cudaStreamSynchronize(s->stream), "state_load sync");
+}
+
 extern "C" int cudapic_state_set_overlap(cudapic_state *s, int on) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_overlap: null state");
     DeviceGuard dg(s->device);

@@ -143,6 +143,14 @@ class GpuSimState:
         """Programmatic dependent launch between the step's kernels (default on)."""
         check(lib.cudapic_state_set_overlap(self._h, 1 if on else 0))
 
+    def save(self, path):
+        """Checkpoint in eduPIC's picdata.bin format (plus ``path``.rng)."""
+        check(lib.cudapic_state_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        """Resume from a picdata.bin (this library's or eduPIC's)."""
+        check(lib.cudapic_state_load(self._h, str(path).encode()))
+
     def wall_counters(self):
         """Electrode counters of the measurement window:
         {"e": {...}, "i": {...}} with abs_pow, abs_gnd, ifed_pow, ifed_gnd."""

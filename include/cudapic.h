@@ -348,6 +348,19 @@ int cudapic_move_and_compact_wall(const float *efield, const float *src_x, const
 int cudapic_math_eval(int fn, const float *in, const float *in2, float *out, uint32_t n,
                       cudapic_stream_t stream);
 
+/* eduPIC's particle checkpoint file picdata.bin (save_particle_data /
+ * load_particle_data, C/eduPIC.cc:726-781): doubles [Time, cycles_done, N_e,
+ * x_e[N_e], vx_e, vy_e, vz_e, N_i, x_i[N_i], vx_i, vy_i, vz_i].  Host
+ * pointers; e[4] / i[4] are the x, vx, vy, vz planes.  Writing widens the
+ * f32 values exactly; reading rounds to the nearest f32; read rejects
+ * (CUDAPIC_ERR_CAPACITY) more particles than max_e / max_i. */
+int cudapic_picdata_write(const char *path, double time, uint32_t cycles_done, const float *const e[4],
+                          uint32_t n_e, const float *const i[4], uint32_t n_i);
+int cudapic_picdata_read_header(const char *path, double *time, uint32_t *cycles_done, uint32_t *n_e,
+                                uint32_t *n_i);
+int cudapic_picdata_read(const char *path, float *const e[4], uint32_t max_e, float *const i[4],
+                         uint32_t max_i);
+
 /* ------------------------------------------------------------------ */
 /* 2. simulation state and driver                                      */
 /* ------------------------------------------------------------------ */
@@ -425,6 +438,15 @@ int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, doubl
  * cudapic_state_set_measure(s, 1)): out[0] electrons, out[1] ions, host
  * memory (synchronises). */
 int cudapic_state_wall_counters(cudapic_state *s, cudapic_wall_counters out[2]);
+/* Checkpoint: the particles of both species in eduPIC's picdata.bin format
+ * at `path` (Time = steps done x DT_E, cycles_done = whole RF periods), and
+ * the RNG planes of every slot in `path`.rng.  Synchronises. */
+int cudapic_state_save(cudapic_state *s, const char *path);
+/* Resume from a picdata.bin (this library's or eduPIC's own): uploads both
+ * species, sets the steps done (and the RF phase) from its Time, and
+ * restores the RNG planes from `path`.rng, or seeds the reference's master
+ * streams when there is none (a file written by eduPIC).  Synchronises. */
+int cudapic_state_load(cudapic_state *s, const char *path);
 
 #ifdef __cplusplus
 }

@@ -187,6 +187,53 @@ def test_wall_counters_of_one_step_match_the_oracle(cudapic, oracle, cuda_device
     st.close()
 
 
+def test_checkpoint_save_load_resumes_the_discharge(cudapic, cuda_device, tmp_path):
+    """save -> load into a fresh state restores the particles, the steps done
+    (RF phase) and every RNG plane: saving the loaded state again gives the
+    same files; both states then step on alike."""
+    from cudapic_b200.sim import GpuSimState
+    a = _c0_state(cudapic)
+    a.run_steps(1010)
+    a.save(tmp_path / "a.bin")
+    b = GpuSimState()
+    b.load(tmp_path / "a.bin")
+    assert b.steps_done() == 1010 and b.counts() == a.counts()
+    b.save(tmp_path / "b.bin")
+    assert (tmp_path / "a.bin").read_bytes() == (tmp_path / "b.bin").read_bytes()
+    assert (tmp_path / "a.bin.rng").read_bytes() == (tmp_path / "b.bin.rng").read_bytes()
+    a.set_fused(False)          # both now deposit afresh and run the same launch sequence
+    b.set_fused(False)
+    a.run_steps(1)
+    b.run_steps(1)
+    (na, ni_a), (nb, ni_b) = a.counts(), b.counts()
+    assert abs(na - nb) <= 2 and abs(ni_a - ni_b) <= 2   # f32 atomic order may flip a borderline particle
+    a.close()
+    b.close()
+
+
+def test_state_resumes_from_an_edupic_checkpoint(cudapic, cuda_device, tmp_path):
+    """A picdata.bin written by eduPIC itself (its initialising cycle):
+    loaded with its counts, one RF period done, fresh reference streams."""
+    import os
+    import subprocess
+    from cudapic_b200.checkpoint import read_picdata
+    from cudapic_b200.sim import GpuSimState
+    exe = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "eduPIC")
+    if not os.path.exists(exe):
+        pytest.skip("eduPIC not built")
+    out = subprocess.run([os.path.abspath(exe), "0"], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    _, _, e, i = read_picdata(tmp_path / "picdata.bin")
+    st = GpuSimState()
+    st.load(tmp_path / "picdata.bin")
+    assert st.counts() == (len(e[0]), len(i[0])) and st.steps_done() == 4000
+    ge, _ = st.download_electrons()
+    assert np.array_equal(ge.x, e[0])
+    st.run_cycles(1)
+    assert st.device_error() == 0 and st.counts()[0] > 0
+    st.close()
+
+
 def test_measurement_accumulators(cudapic, cuda_device):
     st = _c0_state(cudapic)
     st.run_cycles(2)
