@@ -77,5 +77,15 @@ def set_tuning(**fields):
     return get_tuning()
 
 
+def stability_precheck(params=None, **overrides):
+    """The accuracy conditions that follow from the parameters alone
+    (cudapic_stability_precheck): max collision frequency x time step for
+    electrons and ions, and the CFL energy limit."""
+    p = params if params is not None else default_params(**overrides)
+    out = _lib.Precheck()
+    check(lib.cudapic_stability_precheck(_C.byref(p), _C.byref(out)))
+    return out.as_dict()
+
+
 from . import kernels  # noqa: E402,F401
 from . import sim  # noqa: E402,F401

@@ -89,6 +89,27 @@ class WallCounters(C.Structure):
                 "ifed_pow": np.array(self.ifed_pow, np.uint32), "ifed_gnd": np.array(self.ifed_gnd, np.uint32)}
 
 
+class Precheck(C.Structure):
+    """cudapic_precheck: the parameter-only accuracy conditions."""
+    _fields_ = [("max_e_coll_dt_e", C.c_double), ("max_i_coll_dt_i", C.c_double), ("cfl_max_energy", C.c_double),
+                ("conditions_ok", C.c_int)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Report(C.Structure):
+    """cudapic_report: eduPIC's simulation report of a measurement window."""
+    _fields_ = [("steps_measured", C.c_uint64)] + [(n, C.c_double) for n in (
+        "density_center", "plasma_freq", "mean_energy_center", "debye_length", "e_coll_freq", "i_coll_freq",
+        "wp_dt_e", "dx_over_debye", "max_e_coll_dt_e", "max_i_coll_dt_i")] + [("conditions_ok", C.c_int)] + [
+        (n, C.c_double) for n in ("cfl_max_energy", "ion_flux_pow", "ion_flux_gnd", "mean_ion_energy_pow",
+                                  "mean_ion_energy_gnd", "e_flux_pow", "e_flux_gnd")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _P2 = C.c_void_p * 2
 
 
@@ -126,6 +147,9 @@ SIGNATURES = {
     "cudapic_picdata_read_header": [C.c_char_p, _VP, _VP, _VP, _VP],
     "cudapic_picdata_read": [C.c_char_p, _VP, _U32, _VP, _U32],
     "cudapic_state_save": [_VP, C.c_char_p],
+    "cudapic_stability_precheck": [_VP, _VP],
+    "cudapic_state_report": [_VP, _VP],
+    "cudapic_state_write_info": [_VP, C.c_char_p],
     "cudapic_state_load": [_VP, C.c_char_p],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],

@@ -107,18 +107,26 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
                          uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
                          uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
-                         const StepLink &link, cudapic_wall_counters *wall = nullptr);
-// dep_e / dep_i (may be null): next-step densities receiving the spawns.
+                         const StepLink &link, cudapic_wall_counters *wall = nullptr,
+                         unsigned long long *coll = nullptr);
+// dep_e / dep_i (may be null): next-step densities receiving the spawns;
+// coll (may be null): += collision events.
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
                         uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e = nullptr,
-                        float *dep_i = nullptr);
+                        float *dep_i = nullptr, unsigned long long *coll = nullptr);
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
-                        const cudapic_grid &g, cudaStream_t stream);
+                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll = nullptr);
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
-                const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream);
+                const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream,
+                double *esum = nullptr, unsigned long long *ecount = nullptr);
+
+// Largest electron / ion collision frequencies of the total tables [1/s]
+// (C/eduPIC.cc:252-276) and the CFL energy limit [eV] (report.cpp).
+void table_coll_freqs(const float *sigma_tot_e, const float *sigma_tot_i, double *max_e, double *max_i);
+double cfl_max_energy(const cudapic_params &p);
 
 // RNG sidecar of a checkpoint (<path>.rng, checkpoint.cpp): both species'
 // four planes over `capacity` slots.  read: CUDAPIC_ERR_NOT_SUPPORTED,

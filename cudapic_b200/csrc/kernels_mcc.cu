@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
                                 uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *ix,
                                 float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i,
                                 uint8_t *events, const __grid_constant__ cudapic_grid g, int stages,
-                                float *dep_e, float *dep_i) {
+                                float *dep_e, float *dep_i, unsigned long long *coll) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *in = reinterpret_cast<uint32_t *>(smem);             // [stages][7][TILE]
     uint32_t *queue = in + stages * MT_ARRAYS * MT_TILE;           // [5][QCAP]
@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
     // Drains the collider queue: one collider per thread, full warps.
     auto drain = [&]() {
         const uint32_t qn = s_q;
+        if (coll && tid == 0 && qn) atomicAdd(coll, (unsigned long long)qn);  // collision events (measurement)
         for (uint32_t q = tid; q < qn; q += MCC_THREADS) {
             const uint32_t i = queue[0 * MT_QCAP + q];
             Xoshiro128p rs{queue[1 * MT_QCAP + q], queue[2 * MT_QCAP + q], queue[3 * MT_QCAP + q],
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
                                      float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                                      float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive_e,
                                      uint32_t *alive_i, uint8_t *events, const __grid_constant__ cudapic_grid g,
-                                     float *dep_e, float *dep_i) {
+                                     float *dep_e, float *dep_i, unsigned long long *coll) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *tab = reinterpret_cast<float *>(smem);
     const int tid = threadIdx.x;
@@ -234,6 +235,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
     const uint32_t n = load_count(active, g.capacity, g.dev_err);
 
     auto drain = [&](uint32_t first, uint32_t count) {  // lanes < count take entries first + lane
+        if (coll && lane == 0) atomicAdd(coll, (unsigned long long)count);  // collision events (measurement)
         if ((uint32_t)lane < count) {
             const uint32_t q = first + lane;
             const uint32_t i = wq[0 * MR_QCAP + q];
@@ -317,12 +319,14 @@ __global__ void __launch_bounds__(256)
     accumulate_eepf_kernel(const float *__restrict__ x, const float *__restrict__ vx, const float *__restrict__ vy,
                            const float *__restrict__ vz, const float *__restrict__ efield,
                            const uint32_t *__restrict__ active_e, uint32_t *__restrict__ eepf,
-                           const cudapic_grid g) {
+                           const cudapic_grid g, double *esum, unsigned long long *ecount) {
     __shared__ uint32_t h[N_EEPF];
     for (uint32_t k = threadIdx.x; k < N_EEPF; k += blockDim.x) h[k] = 0;
     __syncthreads();
     grid_dep_wait();
     const uint32_t n = load_count(active_e, g.capacity, g.dev_err);
+    double e_sum = 0.0;
+    unsigned long long e_cnt = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float xi = x[i];
         if (xi <= g.min_x || xi >= g.max_x) continue;
@@ -336,6 +340,18 @@ __global__ void __launch_bounds__(256)
         const float energy = g.half_me_over_e * v2;
         const float binf = energy / DE_EEPF_F;
         if (binf < (float)N_EEPF) atomicAdd(&h[(uint32_t)binf], 1u);
+        e_sum += (double)energy;
+        ++e_cnt;
+    }
+    if (esum) {  // mean energy of the sampled electrons (the report's centre energy)
+        for (int o = 16; o > 0; o >>= 1) {
+            e_sum += __shfl_down_sync(0xffffffffu, e_sum, o);
+            e_cnt += __shfl_down_sync(0xffffffffu, e_cnt, o);
+        }
+        if ((threadIdx.x & 31) == 0 && e_cnt) {
+            atomicAdd(esum, e_sum);
+            atomicAdd(ecount, e_cnt);
+        }
     }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < N_EEPF; k += blockDim.x)
@@ -355,7 +371,7 @@ template <bool ION, bool EVENTS>
 int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
                float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx, float *ivy,
                float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events, const cudapic_grid &g,
-               cudaStream_t stream, float *dep_e, float *dep_i) {
+               cudaStream_t stream, float *dep_e, float *dep_i, unsigned long long *coll) {
     auto kern = check_collisions_tma_kernel<ION, EVENTS>;
     const cudapic_tuning t = tuning();
     const int stages = std::min(std::max(t.mcc_stages, 2), MT_MAX_STAGES);
@@ -370,14 +386,15 @@ int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, 
     const unsigned grid = persistent_grid(per_sm, tiles_max);
     return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(grid), dim3(MCC_THREADS), smem,
                          stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz, alive_e,
-                         alive_i, events, g, stages, dep_e, dep_i);
+                         alive_i, events, g, stages, dep_e, dep_i, coll);
 }
 
 template <bool ION, bool EVENTS>
 int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
                     float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx,
                     float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
-                    const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
+                    const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i,
+                    unsigned long long *coll) {
     auto kern = check_collisions_resident_kernel<ION, EVENTS>;
     if (MR_SMEM > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_NOT_SUPPORTED, "check_collisions: shared memory");
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MR_SMEM),
@@ -385,7 +402,7 @@ int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *act
     const uint64_t chunks = ((uint64_t)g.capacity + MR_THREADS * MR_U - 1) / (MR_THREADS * MR_U);
     return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(persistent_grid(1, chunks)),
                          dim3(MR_THREADS), MR_SMEM, stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix,
-                         ivx, ivy, ivz, alive_e, alive_i, events, g, dep_e, dep_i);
+                         ivx, ivy, ivz, alive_e, alive_i, events, g, dep_e, dep_i, coll);
 }
 
 // Variant choice: the bulk-copy kernel needs 16-byte aligned planes and a
@@ -394,20 +411,21 @@ template <bool ION>
 int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx,
                       float *vy, float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix,
                       float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
-                      const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
+                      const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i,
+                      unsigned long long *coll) {
     const bool bulk = tuning().mcc_variant == 2 && tma_ready(g.capacity, {vx, vy, vz, r0, r1, r2, r3});
     if (bulk) {
         if (events)
             return launch_tma<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                         alive_e, alive_i, events, g, stream, dep_e, dep_i);
+                                         alive_e, alive_i, events, g, stream, dep_e, dep_i, coll);
         return launch_tma<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                      alive_e, alive_i, nullptr, g, stream, dep_e, dep_i);
+                                      alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll);
     }
     if (events)
         return launch_resident<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                          alive_e, alive_i, events, g, stream, dep_e, dep_i);
+                                          alive_e, alive_i, events, g, stream, dep_e, dep_i, coll);
     return launch_resident<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                       alive_e, alive_i, nullptr, g, stream, dep_e, dep_i);
+                                       alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll);
 }
 
 }  // namespace
@@ -415,24 +433,27 @@ int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *a
 int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t *active_e, float *x, float *vx,
                         float *vy, float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
-                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i) {
+                        uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i,
+                        unsigned long long *coll) {
     return launch_collisions<false>(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy,
-                                    i_vz, alive_e, alive_i, events, g, stream, dep_e, dep_i);
+                                    i_vz, alive_e, alive_i, events, g, stream, dep_e, dep_i, coll);
 }
 
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
-                        const cudapic_grid &g, cudaStream_t stream) {
+                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll) {
     return launch_collisions<true>(total_cs_i, cs, active_i, nullptr, vx, vy, vz, rng0, rng1, rng2, rng3, nullptr,
-                                   nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream, nullptr, nullptr);
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream, nullptr, nullptr,
+                                   coll);
 }
 
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
-                const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream) {
+                const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream,
+                double *esum, unsigned long long *ecount) {
     const uint64_t need = ((uint64_t)g.capacity + 255) / 256;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * 2, need));
     return launch_kernel("accumulate_eepf", accumulate_eepf_kernel, dim3(grid), dim3(256), 0, stream, x, vx, vy, vz,
-                         efield, active_e, eepf, g);
+                         efield, active_e, eepf, g, esum, ecount);
 }
 
 }  // namespace cudapic

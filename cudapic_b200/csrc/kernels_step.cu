@@ -87,7 +87,8 @@ __global__ void __launch_bounds__(ES_THREADS)
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
                          const uint32_t *__restrict__ n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                          const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int stages, int copies,
-                         uint32_t epoch, const StepLink link, cudapic_wall_counters *wall) {
+                         uint32_t epoch, const StepLink link, cudapic_wall_counters *wall,
+                         unsigned long long *coll) {
     constexpr int ES_TILE = StepShape<U>::TILE;
     constexpr int ES_QCAP = StepShape<U>::QCAP;
     constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
@@ -149,6 +150,7 @@ __global__ void __launch_bounds__(ES_THREADS)
 
     // Scatters wq[first, first + count), one collider per lane.
     auto drain = [&](uint32_t first, uint32_t count) {
+        if (coll && lane == 0) atomicAdd(coll, (unsigned long long)count);  // collision events (measurement)
         if ((uint32_t)lane < count) {
             const uint32_t i = wq[first + lane];
             const PushResult pr = push_one(sx[i], svx[i], ef, g.factor_e, g.dt_e, g);
@@ -356,7 +358,7 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
                            float sigma_max_e, float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
                            const uint32_t *n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                            const cudapic_grid &g, cudaStream_t stream, const StepLink &link,
-                           cudapic_wall_counters *wall, const cudapic_tuning &t) {
+                           cudapic_wall_counters *wall, unsigned long long *coll, const cudapic_tuning &t) {
     constexpr int ES_TILE = StepShape<U>::TILE;
     constexpr int ES_QCAP = StepShape<U>::QCAP;
     int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
@@ -385,7 +387,7 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
     return launch_kernel("step_electrons", kern, dim3(grid), dim3(ES_THREADS), smem, stream, efield, sx, svx, svy, svz,
                          dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz,
-                         alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link, wall);
+                         alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link, wall, coll);
 }
 
 }  // namespace
@@ -395,13 +397,13 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
                          uint32_t *rng2, uint32_t *rng3, const float *sigma_tot_e, const float *cs, float sigma_max_e,
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive, const uint32_t *n_active,
                          uint32_t *n_i, float *dens_e, float *dens_i, const cudapic_grid &g, cudaStream_t stream,
-                         const StepLink &link, cudapic_wall_counters *wall) {
+                         const StepLink &link, cudapic_wall_counters *wall, unsigned long long *coll) {
     const void *planes[8] = {sx, svx, svy, svz, rng0, rng1, rng2, rng3};
     if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
     const cudapic_tuning t = tuning();
     auto launch = t.step_rows == 4 ? launch_electron_step_t<4> : launch_electron_step_t<2>;
     return launch(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e,
-                  ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, wall, t);
+                  ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, wall, coll, t);
 }
 
 }  // namespace cudapic

@@ -19,7 +19,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <new>
 #include <vector>
 
@@ -54,6 +56,12 @@ struct cudapic_state {
     float sigma_max_e = 0.0f;  // largest entry of sigma_tot_e (the fused step's certain-rejection bound)
     double *cumul_e = nullptr, *cumul_i = nullptr;
     cudapic_wall_counters *wall = nullptr;  // [0] electrons, [1] ions (measurement window)
+    // measurement window: [0] electron and [1] ion collision events, [2] EEPF
+    // electrons sampled; esum: their energies [eV]; measure_steps on the host
+    unsigned long long *mcount = nullptr;
+    double *esum = nullptr;
+    uint64_t measure_steps = 0;
+    double max_e_coll_freq = 0.0, max_i_coll_freq = 0.0;  // of the tables [1/s]
     uint32_t *eepf = nullptr;
 
     bool measure = false;
@@ -142,18 +150,18 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
                                        s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3], s->sigma_tot_e, s->cs,
                                        s->sigma_max_e, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
                                        s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le,
-                                       s->measure ? s->wall : nullptr));
+                                       s->measure ? s->wall : nullptr, s->measure ? s->mcount : nullptr));
     se ^= 1;
     s->side[E] = se;
     s->e_cur ^= 1;
     if (ion_step) {
         CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
                                           s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
-                                          nullptr, g, st));
+                                          nullptr, g, st, s->measure ? s->mcount + 1 : nullptr));
     }
     if (s->measure) {
         CUDAPIC_CHECK(launch_eepf(s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->efield, s->n_e(),
-                                  s->eepf, g, st));
+                                  s->eepf, g, st, s->esum, s->mcount + 2));
     }
     return CUDAPIC_OK;
 }
@@ -236,18 +244,18 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     CUDAPIC_CHECK(launch_collisions_e(s->sigma_tot_e, s->cs, s->n_e(), s->x[E][se], s->vx[E][se], s->vy[E][se],
                                       s->vz[E][se], s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3],
                                       s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si], s->alive(), s->n_i(),
-                                      nullptr, g, st, e_next, i_acc));
+                                      nullptr, g, st, e_next, i_acc, s->measure ? s->mcount : nullptr));
     CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->n_e(), s->alive(), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st),
                              "copy alive -> n_e"));
     if (fused) s->e_cur ^= 1;
     if (ion_step) {
         CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
                                           s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
-                                          nullptr, g, st));
+                                          nullptr, g, st, s->measure ? s->mcount + 1 : nullptr));
     }
     if (s->measure) {
         CUDAPIC_CHECK(launch_eepf(s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->efield, s->n_e(),
-                                  s->eepf, g, st));
+                                  s->eepf, g, st, s->esum, s->mcount + 2));
     }
     return CUDAPIC_OK;
 }
@@ -343,7 +351,7 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
         (rc = dalloc(s, &s->pot0_table, p->n_t)) || (rc = dalloc(s, &s->cs, 5ull * CUDAPIC_CS_RANGES)) ||
         (rc = dalloc(s, &s->sigma_tot_e, CUDAPIC_CS_RANGES)) || (rc = dalloc(s, &s->sigma_tot_i, CUDAPIC_CS_RANGES)) ||
         (rc = dalloc(s, &s->cumul_e, n_g)) || (rc = dalloc(s, &s->cumul_i, n_g)) || (rc = dalloc(s, &s->eepf, 2000)) ||
-        (rc = dalloc(s, &s->wall, 2)))
+        (rc = dalloc(s, &s->wall, 2)) || (rc = dalloc(s, &s->mcount, 3)) || (rc = dalloc(s, &s->esum, 1)))
         return cleanup(rc);
     s->grid.dev_err = s->dev_err();
     s->grid.work = s->work();
@@ -363,6 +371,8 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
         (rc = check_cuda(cudaMemsetAsync(s->i_dens[1], 0, n_g * sizeof(float), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->wall, 0, 2 * sizeof(cudapic_wall_counters), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->mcount, 0, 3 * sizeof(unsigned long long), s->stream), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(s->esum, 0, sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "memset")))
         return cleanup(rc);
@@ -375,6 +385,7 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
     std::vector<float> cs(5ull * CUDAPIC_CS_RANGES), se(CUDAPIC_CS_RANGES), si(CUDAPIC_CS_RANGES);
     if ((rc = cudapic_cross_sections(grid.gas_density, cs.data(), se.data(), si.data()))) return cleanup(rc);
     s->sigma_max_e = *std::max_element(se.begin(), se.end());
+    table_coll_freqs(se.data(), si.data(), &s->max_e_coll_freq, &s->max_i_coll_freq);
     if ((rc = check_cuda(cudaMemcpyAsync(s->pot0_table, table.data(), table.size() * sizeof(float),
                                          cudaMemcpyHostToDevice, s->stream), "upload pot0 table")) ||
         (rc = check_cuda(cudaMemcpyAsync(s->cs, cs.data(), cs.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream),
@@ -609,6 +620,9 @@ extern "C" int cudapic_state_set_measure(cudapic_state *s, int on) {
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "zero cumul_i"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "zero eepf"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->wall, 0, 2 * sizeof(cudapic_wall_counters), s->stream), "zero wall"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->mcount, 0, 3 * sizeof(unsigned long long), s->stream), "zero counts"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->esum, 0, sizeof(double), s->stream), "zero esum"));
+    s->measure_steps = 0;
     s->measure = on != 0;
     return CUDAPIC_OK;
 }
@@ -633,11 +647,13 @@ extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
             }
             CUDAPIC_CHECK(check_cuda(cudaGraphLaunch(s->graph[m], s->stream), "cudaGraphLaunch"));
             s->steps_done += period;
+            if (s->measure) s->measure_steps += period;
             n_steps -= period;
             continue;
         }
         CUDAPIC_CHECK(enqueue_step(s, is_ion_step(s, s->steps_done)));
         s->steps_done += 1;
+        if (s->measure) s->measure_steps += 1;
         n_steps -= 1;
     }
     return CUDAPIC_OK;
@@ -684,6 +700,123 @@ extern "C" int cudapic_state_synchronize(cudapic_state *s) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_synchronize: null state");
     DeviceGuard dg(s->device);
     return check_cuda(cudaStreamSynchronize(s->stream), "state_synchronize");
+}
+
+extern "C" int cudapic_state_report(cudapic_state *s, cudapic_report *out) {
+    if (!s || !out) return fail(CUDAPIC_ERR_ARG, "state_report: null pointer");
+    DeviceGuard dg(s->device);
+    const cudapic_params &p = s->params;
+    const uint32_t n_g = p.n_g;
+    std::vector<double> cumul(n_g);
+    cudapic_wall_counters wall[2];
+    unsigned long long mc[3];
+    double esum = 0.0;
+    uint32_t counts[2];
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(cumul.data(), s->cumul_e, n_g * sizeof(double), cudaMemcpyDeviceToHost,
+                                             s->stream), "report: density"));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(wall, s->wall, sizeof(wall), cudaMemcpyDeviceToHost, s->stream),
+                             "report: wall"));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(mc, s->mcount, sizeof(mc), cudaMemcpyDeviceToHost, s->stream),
+                             "report: counts"));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(&esum, s->esum, sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+                             "report: energy"));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(counts, s->counters, sizeof(counts), cudaMemcpyDeviceToHost, s->stream),
+                             "report: particle counts"));
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "report sync"));
+    // eduPIC's formulas (C/eduPIC.cc:930-1008), with its constants
+    const double e_charge = 1.60217662e-19, e_mass = 9.10938356e-31, eps0 = 8.85418781e-12;
+    const double dt_e = dt_e_double(s), dt_i = dt_e * (double)p.n_sub;
+    const double dx = p.gap / (double)(n_g - 1);
+    const uint64_t steps = s->measure_steps;
+    const double sim_time = (double)steps * dt_e;
+    cudapic_report r{};
+    r.steps_measured = steps;
+    r.density_center = steps ? cumul[n_g / 2] / (double)steps : 0.0;
+    r.plasma_freq = e_charge * std::sqrt(r.density_center / eps0 / e_mass);
+    r.mean_energy_center = mc[2] ? esum / (double)mc[2] : NAN;
+    const double kT = 2.0 * r.mean_energy_center * e_charge / 3.0;
+    r.debye_length = std::sqrt(eps0 * kT / r.density_center) / e_charge;
+    const double n_e = std::min(counts[0], p.capacity), n_i = std::min(counts[1], p.capacity);
+    r.e_coll_freq = (double)mc[0] / sim_time / n_e;
+    r.i_coll_freq = (double)mc[1] / sim_time / n_i;
+    r.wp_dt_e = r.plasma_freq * dt_e;
+    r.dx_over_debye = dx / r.debye_length;
+    r.max_e_coll_dt_e = s->max_e_coll_freq * dt_e;
+    r.max_i_coll_dt_i = s->max_i_coll_freq * dt_i;
+    r.conditions_ok = !(r.wp_dt_e > 0.2) && !(r.dx_over_debye > 1.0) && !(r.max_e_coll_dt_e > 0.05) &&
+                      !(r.max_i_coll_dt_i > 0.05);
+    r.cfl_max_energy = cfl_max_energy(p);
+    const double flux = p.weight / p.electrode_area / sim_time;
+    r.ion_flux_pow = (double)wall[1].abs_pow * flux;
+    r.ion_flux_gnd = (double)wall[1].abs_gnd * flux;
+    r.e_flux_pow = (double)wall[0].abs_pow * flux;
+    r.e_flux_gnd = (double)wall[0].abs_gnd * flux;
+    double hp = 0.0, hg = 0.0, mp = 0.0, mg = 0.0;  // save_ifed, :824-844 (1 eV bins)
+    for (int k = 0; k < CUDAPIC_N_IFED; ++k) {
+        hp += wall[1].ifed_pow[k];
+        hg += wall[1].ifed_gnd[k];
+        mp += (k + 0.5) * wall[1].ifed_pow[k];
+        mg += (k + 0.5) * wall[1].ifed_gnd[k];
+    }
+    r.mean_ion_energy_pow = hp > 0.0 ? mp / hp : NAN;
+    r.mean_ion_energy_gnd = hg > 0.0 ? mg / hg : NAN;
+    *out = r;
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_write_info(cudapic_state *s, const char *path) {
+    if (!s || !path) return fail(CUDAPIC_ERR_ARG, "state_write_info: null pointer");
+    cudapic_report r;
+    CUDAPIC_CHECK(cudapic_state_report(s, &r));
+    const cudapic_params &p = s->params;
+    FILE *f = std::fopen(path, "w");
+    if (!f) return fail(CUDAPIC_ERR_ARG, std::string("state_write_info: cannot open ") + path);
+    const char *rule = "--------------------------------------------------------------------------------\n";
+    // the lines of check_and_save_info, C/eduPIC.cc:940-1008
+    std::fprintf(f, "########################## eduPIC simulation report ############################\n");
+    std::fprintf(f, "Simulation parameters:\n");
+    std::fprintf(f, "Gap distance                          = %12.3e [m]\n", p.gap);
+    std::fprintf(f, "# of grid divisions                   = %12d\n", (int)p.n_g);
+    std::fprintf(f, "Frequency                             = %12.3e [Hz]\n", p.frequency);
+    std::fprintf(f, "# of time steps / period              = %12d\n", (int)p.n_t);
+    std::fprintf(f, "# of electron / ion time steps        = %12d\n", (int)p.n_sub);
+    std::fprintf(f, "Voltage amplitude                     = %12.3e [V]\n", p.voltage);
+    std::fprintf(f, "Pressure (Ar)                         = %12.3e [Pa]\n", p.pressure);
+    std::fprintf(f, "Temperature                           = %12.3e [K]\n", p.temperature);
+    std::fprintf(f, "Superparticle weight                  = %12.3e\n", p.weight);
+    std::fprintf(f, "# of simulation cycles in this run    = %12d\n", (int)(r.steps_measured / p.n_t));
+    std::fprintf(f, "%s", rule);
+    std::fprintf(f, "Plasma characteristics:\n");
+    std::fprintf(f, "Electron density @ center             = %12.3e [m^{-3}]\n", r.density_center);
+    std::fprintf(f, "Plasma frequency @ center             = %12.3e [rad/s]\n", r.plasma_freq);
+    std::fprintf(f, "Debye length @ center                 = %12.3e [m]\n", r.debye_length);
+    std::fprintf(f, "Electron collision frequency          = %12.3e [1/s]\n", r.e_coll_freq);
+    std::fprintf(f, "Ion collision frequency               = %12.3e [1/s]\n", r.i_coll_freq);
+    std::fprintf(f, "%s", rule);
+    std::fprintf(f, "Stability and accuracy conditions:\n");
+    std::fprintf(f, "Plasma frequency @ center * DT_E      = %12.3f (OK if less than 0.20)\n", r.wp_dt_e);
+    std::fprintf(f, "DX / Debye length @ center            = %12.3f (OK if less than 1.00)\n", r.dx_over_debye);
+    std::fprintf(f, "Max. electron coll. frequency * DT_E  = %12.3f (OK if less than 0.05)\n", r.max_e_coll_dt_e);
+    std::fprintf(f, "Max. ion coll. frequency * DT_I       = %12.3f (OK if less than 0.05)\n", r.max_i_coll_dt_i);
+    if (!r.conditions_ok) {
+        std::fprintf(f, "%s", rule);
+        std::fprintf(f, "** STABILITY AND ACCURACY CONDITION(S) VIOLATED - REFINE SIMULATION SETTINGS! **\n");
+        std::fprintf(f, "%s", rule);
+    } else {
+        std::fprintf(f, "Max e- energy for CFL condition       = %12.3f [eV]\n", r.cfl_max_energy);
+        std::fprintf(f, "Check EEPF to ensure that CFL is fulfilled for the majority of the electrons!\n");
+        std::fprintf(f, "%s", rule);
+        std::fprintf(f, "Particle characteristics at the electrodes:\n");
+        std::fprintf(f, "Ion flux at powered electrode         = %12.3e [m^{-2} s^{-1}]\n", r.ion_flux_pow);
+        std::fprintf(f, "Ion flux at grounded electrode        = %12.3e [m^{-2} s^{-1}]\n", r.ion_flux_gnd);
+        std::fprintf(f, "Mean ion energy at powered electrode  = %12.3e [eV]\n", r.mean_ion_energy_pow);
+        std::fprintf(f, "Mean ion energy at grounded electrode = %12.3e [eV]\n", r.mean_ion_energy_gnd);
+        std::fprintf(f, "Electron flux at powered electrode    = %12.3e [m^{-2} s^{-1}]\n", r.e_flux_pow);
+        std::fprintf(f, "Electron flux at grounded electrode   = %12.3e [m^{-2} s^{-1}]\n", r.e_flux_gnd);
+        std::fprintf(f, "%s", rule);
+    }
+    const bool ok = std::fclose(f) == 0;
+    return ok ? CUDAPIC_OK : fail(CUDAPIC_ERR_ARG, std::string("state_write_info: write failed: ") + path);
 }
 
 extern "C" int cudapic_state_wall_counters(cudapic_state *s, cudapic_wall_counters out[2]) {

@@ -151,6 +151,16 @@ class GpuSimState:
         """Resume from a picdata.bin (this library's or eduPIC's)."""
         check(lib.cudapic_state_load(self._h, str(path).encode()))
 
+    def report(self):
+        """eduPIC's simulation report of the measurement window (dict)."""
+        r = _lib.Report()
+        check(lib.cudapic_state_report(self._h, C.byref(r)))
+        return r.as_dict()
+
+    def write_info(self, path):
+        """The report as eduPIC's info.txt."""
+        check(lib.cudapic_state_write_info(self._h, str(path).encode()))
+
     def wall_counters(self):
         """Electrode counters of the measurement window:
         {"e": {...}, "i": {...}} with abs_pow, abs_gnd, ifed_pow, ifed_gnd."""

@@ -361,6 +361,21 @@ int cudapic_picdata_read_header(const char *path, double *time, uint32_t *cycles
 int cudapic_picdata_read(const char *path, float *const e[4], uint32_t max_e, float *const i[4],
                          uint32_t max_i);
 
+/* The accuracy conditions that follow from the parameters alone
+ * (check_and_save_info, C/eduPIC.cc:925-1030): the largest collision
+ * frequency of the cross-section tables times the time step, for electrons
+ * and ions (each OK below 0.05; max_electron_coll_freq / max_ion_coll_freq,
+ * :252-276), and the largest electron energy [eV] for which the CFL
+ * condition holds.  Host only; lets a parameter sweep flag a discharge
+ * before it runs.  conditions_ok: both frequencies within their bound. */
+typedef struct cudapic_precheck {
+    double max_e_coll_dt_e;
+    double max_i_coll_dt_i;
+    double cfl_max_energy;
+    int conditions_ok;
+} cudapic_precheck;
+int cudapic_stability_precheck(const cudapic_params *p, cudapic_precheck *out);
+
 /* ------------------------------------------------------------------ */
 /* 2. simulation state and driver                                      */
 /* ------------------------------------------------------------------ */
@@ -438,6 +453,36 @@ int cudapic_state_download_measurements(cudapic_state *s, double *cumul_e, doubl
  * cudapic_state_set_measure(s, 1)): out[0] electrons, out[1] ions, host
  * memory (synchronises). */
 int cudapic_state_wall_counters(cudapic_state *s, cudapic_wall_counters out[2]);
+/* eduPIC's simulation report (check_and_save_info, C/eduPIC.cc:925-1030)
+ * for the measurement window (since cudapic_state_set_measure(s, 1)):
+ * plasma characteristics at the centre, the stability and accuracy
+ * conditions, and the particle fluxes at the electrodes.  The centre
+ * density is the window's average of the electron density at node N_G/2;
+ * the mean energy is that of the electrons the EEPF samples; collision
+ * frequencies are events per second per particle present; fluxes are
+ * absorbed particles x weight / electrode area / window time; mean ion
+ * energies are those of the IFEDs (NaN without absorbed ions). */
+typedef struct cudapic_report {
+    uint64_t steps_measured;
+    double density_center;        /* m^-3                                     */
+    double plasma_freq;           /* rad/s                                    */
+    double mean_energy_center;    /* eV                                       */
+    double debye_length;          /* m                                        */
+    double e_coll_freq;           /* 1/s                                      */
+    double i_coll_freq;
+    double wp_dt_e;               /* plasma frequency x DT_E     (OK < 0.20)  */
+    double dx_over_debye;         /* DX / Debye length           (OK < 1.00)  */
+    double max_e_coll_dt_e;       /* max e coll. frequency x DT_E (OK < 0.05) */
+    double max_i_coll_dt_i;       /* max ion coll. frequency x DT_I (< 0.05)  */
+    int conditions_ok;
+    double cfl_max_energy;        /* eV                                       */
+    double ion_flux_pow, ion_flux_gnd;   /* m^-2 s^-1                         */
+    double mean_ion_energy_pow, mean_ion_energy_gnd;   /* eV                  */
+    double e_flux_pow, e_flux_gnd;       /* m^-2 s^-1                         */
+} cudapic_report;
+int cudapic_state_report(cudapic_state *s, cudapic_report *out);
+/* Writes the report as eduPIC's info.txt (same lines and number formats). */
+int cudapic_state_write_info(cudapic_state *s, const char *path);
 /* Checkpoint: the particles of both species in eduPIC's picdata.bin format
  * at `path` (Time = steps done x DT_E, cycles_done = whole RF periods), and
  * the RNG planes of every slot in `path`.rng.  Synchronises. */

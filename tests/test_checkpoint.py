@@ -69,3 +69,33 @@ def test_edupic_continues_from_a_file_written_here(cudapic, tmp_path):
         (len(e2[0]), len(i2[0]), 2)
     assert t == pytest.approx(4000 / (13.56e6 * 4000), rel=1e-9)   # one period of DT_E steps
     assert np.all((e2[0] >= 0) & (e2[0] <= 0.025)) and len(e2[0]) > 0
+
+
+@pytest.mark.skipif(not os.path.exists(EDUPIC), reason="eduPIC not built (make -C oracle ref)")
+def test_stability_precheck_matches_edupics_report(cudapic, tmp_path):
+    """The parameter-only lines of eduPIC's info.txt (max collision frequency
+    x time step for electrons and ions, the CFL energy) equal the precheck
+    to the printed digits."""
+    exe = os.path.abspath(EDUPIC)
+    for args in (["0"], ["1", "m"]):
+        out = subprocess.run([exe] + args, cwd=tmp_path, capture_output=True, text=True, timeout=120)
+        assert out.returncode == 0, out.stdout + out.stderr
+    info = (tmp_path / "info.txt").read_text()
+
+    def value(label):
+        return float(re.search(re.escape(label) + r"\s*=\s*(\S+)", info).group(1))
+
+    pc = cudapic.stability_precheck()
+    assert round(pc["max_e_coll_dt_e"], 3) == value("Max. electron coll. frequency * DT_E")
+    assert round(pc["max_i_coll_dt_i"], 3) == value("Max. ion coll. frequency * DT_I")
+    assert round(pc["cfl_max_energy"], 3) == value("Max e- energy for CFL condition")
+    assert pc["conditions_ok"] == 1
+
+
+def test_stability_precheck_scales_with_density_and_step(cudapic):
+    base = cudapic.stability_precheck()
+    hi = cudapic.stability_precheck(pressure=50.0, n_t=1000)   # 5x the gas density, 4x the time step
+    assert hi["max_e_coll_dt_e"] == pytest.approx(20 * base["max_e_coll_dt_e"], rel=1e-6)
+    assert hi["max_i_coll_dt_i"] == pytest.approx(20 * base["max_i_coll_dt_i"], rel=1e-6)
+    assert hi["cfl_max_energy"] == pytest.approx(base["cfl_max_energy"] / 16, rel=1e-12)
+    assert hi["conditions_ok"] == 0

@@ -234,6 +234,37 @@ def test_state_resumes_from_an_edupic_checkpoint(cudapic, cuda_device, tmp_path)
     st.close()
 
 
+def test_report_of_a_measurement_window(cudapic, cuda_device, tmp_path):
+    """eduPIC's report from the window's accumulators: the centre density is
+    the window average at node N_G/2, fluxes are the electrode counts over
+    weight / area / time, the table numbers equal the precheck; the
+    info.txt carries eduPIC's lines."""
+    st = _c0_state(cudapic)
+    st.run_cycles(3)
+    st.set_measure(True)
+    st.run_cycles(1)
+    r = st.report()
+    ce, _, eepf = st.download_measurements()
+    w = st.wall_counters()
+    p = st.params
+    t = 4000 / p.frequency / p.n_t
+    assert r["steps_measured"] == 4000
+    assert r["density_center"] == ce[p.n_g // 2] / 4000
+    assert r["e_flux_pow"] == pytest.approx(w["e"]["abs_pow"] * p.weight / p.electrode_area / t, rel=1e-12)
+    assert r["ion_flux_gnd"] == pytest.approx(w["i"]["abs_gnd"] * p.weight / p.electrode_area / t, rel=1e-12)
+    pc = cudapic.stability_precheck()
+    assert r["max_e_coll_dt_e"] == pytest.approx(pc["max_e_coll_dt_e"], rel=1e-5)
+    assert r["max_i_coll_dt_i"] == pytest.approx(pc["max_i_coll_dt_i"], rel=1e-5)
+    assert r["conditions_ok"] == 1 and eepf.sum() > 0
+    assert 0.5 < r["mean_energy_center"] < 20.0
+    assert r["e_coll_freq"] > 0 and r["i_coll_freq"] > 0
+    assert 0.0 < r["mean_ion_energy_pow"] < 200.0
+    st.write_info(tmp_path / "info.txt")
+    info = (tmp_path / "info.txt").read_text()
+    assert "Electron flux at grounded electrode" in info and "Max. ion coll. frequency * DT_I" in info
+    st.close()
+
+
 def test_measurement_accumulators(cudapic, cuda_device):
     st = _c0_state(cudapic)
     st.run_cycles(2)
