@@ -21,6 +21,13 @@ electron advanced by one electron step, or one ion by one ion step, counts
 Each timed step touches > 190 MB (electron SoA source + destination + RNG
 planes), more than the 126 MB L2, so no L2 flush is needed between steps.
 
+--workload c2 runs the batched path instead: the 256-discharge sweep of the
+reference's batched configuration (V ~ U(100, 500) V, p ~ logU(5, 50) Pa,
+L ~ U(15, 40) mm, N_G in {200, 400, 800}, 1e4..1e6 particles per species,
+seeded), every discharge a state on its own stream, sharded over the ranks
+of an N-GPU job; the line also reports the same discharges run one at a
+time (a sample) as the plain comparison.
+
 --impl reference times the reference's own CPU implementation of the path,
 eduPIC 1.0 (C/eduPIC.cc, built from the reference tree into oracle/_ref/),
 on all host cores, each core running an independent share of the same
@@ -60,6 +67,11 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-breakdown", action="store_true")
+    ap.add_argument("--workload", choices=["c1", "c2"], default="c1",
+                    help="c1: one 4M+4M discharge (plain path); c2: the 256-discharge sweep (batched path)")
+    ap.add_argument("--discharges", type=int, default=256)
+    ap.add_argument("--plain-sample", type=int, default=12,
+                    help="c2: discharges also timed one at a time for the plain comparison")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -163,15 +175,8 @@ def dist_setup(args):
 
 
 def reduce_max_sum(world, elapsed, work):
-    if world == 1:
-        return elapsed, work
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-    w = torch.tensor([float(work)], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dist.all_reduce(w, op=dist.ReduceOp.SUM)
-    return t.item(), w.item()
+    from cudapic_b200.batch import reduce_max_sum as rms
+    return rms(world, elapsed, work)
 
 
 def barrier(world):
@@ -442,7 +447,8 @@ def run_ours(args):
         "config": workload_config(args),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_wall},
-        "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+        "roofline": roofline, "cpu_baseline": cpu, "stated_error": STATED_ERROR, "clocks": clk.summary(),
+        "gpu_launches": launches,
         "kernels": breakdown, "population_end": [n_e_end, n_i_end], "device_error_bits": dev_err,
     }
     print(json.dumps(line))
@@ -463,6 +469,112 @@ def ncu_traffic(kernel, n):
     return k["dram_bytes"] * n / k["n"]
 
 
+STATED_ERROR = {"kernels": "RNG, push/compaction, collisions bit-exact with the CPU restatement of the reference",
+                "deposit": "relative L2 <= 2e-5 vs FP64", "poisson": "relative L2 <= 1e-6 vs FP64 Thomas (FP64 sums)"}
+
+
+def run_batched(args):
+    """The C2 sweep through cudapic_b200.batch (see the module docstring)."""
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    from cudapic_b200.batch import Batch, c2_specs, gather, shard
+    specs = c2_specs(n=args.discharges)
+    mine = [specs[k] for k in shard(specs, world)[rank]]
+    batch = Batch(mine, device=local)
+    batch.run_steps(STEP * args.warmup)
+    batch.synchronize()
+    barrier(world)
+    with ClockSampler(local) as clk:
+        elapsed, work = batch.timed_steps(STEP * args.steps)
+    barrier(world)
+    elapsed_max, work_sum = reduce_max_sum(world, elapsed, work)
+    value = work_sum / elapsed_max
+    errors = batch.device_errors()
+    flagged = [k for k, pc in enumerate(batch.prechecks()) if not pc["conditions_ok"]]
+
+    # end to end through the public API: every discharge re-uploaded from
+    # pinned host memory, the steps, every discharge's counts read back
+    from cudapic_b200.batch import initial_population
+    pinned = []
+    for st, spec in zip(batch.states, mine):
+        e, i = initial_population(spec, st.grid.dt_e, st.grid.dt_i)
+        pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*e, *i)])
+    lib = __import__("cudapic_b200").lib
+    barrier(world)
+    batch.synchronize()
+    w0 = batch.work()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for st, arrs in zip(batch.states, pinned):
+        n = arrs[0].numel()
+        for sp in (0, 1):
+            __import__("cudapic_b200").check(lib.cudapic_state_upload(
+                st.handle, sp, *(t.data_ptr() for t in arrs[4 * sp:4 * sp + 4]), n))
+            h2d += 16 * n
+    batch.run_steps(STEP * args.steps)
+    for st in batch.states:
+        st.counts()
+        d2h += 8
+    e2e_wall = time.perf_counter() - t0
+    e2e_work = batch.work() - w0
+    e2e_max, e2e_sum = reduce_max_sum(world, e2e_wall, e2e_work)
+
+    # the plain comparison: a sample of the same discharges, one at a time
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        order = sorted(range(len(specs)), key=lambda k: specs[k].particles)
+        pick = [order[int(j * (len(order) - 1) / max(1, args.plain_sample - 1))] for j in range(args.plain_sample)]
+        t_sum = w_sum = 0.0
+        for k in pick:
+            with Batch([specs[k]], device=local) as one:
+                one.run_steps(STEP * args.warmup)
+                t, w = one.timed_steps(STEP * args.steps)
+            t_sum += t
+            w_sum += w
+        plain = {"value": w_sum / t_sum, "unit": UNIT, "sample": "%d of the %d discharges across the size range, "
+                 "each alone, %d PIC steps each" % (len(pick), len(specs), STEP * args.steps)}
+    per_rank = gather({"discharges": len(mine), "errors": sum(1 for e in errors if e)}, world)
+    batch.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peaks()
+    ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched path: %d discharges of the C2 sweep (V, p, L, N_G, 1e4..1e6 particles per "
+                               "species sampled, seeded), every discharge a state on its own stream; 1 step = %d PIC "
+                               "steps" % (len(specs), STEP),
+                   "discharges": len(specs), "particles_total": int(sum(s.particles for s in specs)),
+                   "l2": "inputs larger than L2 in aggregate, no flush",
+                   "parallelism": "discharges sharded over %d rank(s), no collective" % world},
+        "plain_sequential": plain,
+        "speedup_vs_plain": value / plain["value"] if plain else None,
+        "e2e": {"value": e2e_sum / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_max},
+        "roofline": {"bound": "hbm", "kernel": "all (batch aggregate, 64 B per particle-step)",
+                     "achieved": 64.0 * work_sum / elapsed_max / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": 64.0 * work_sum / elapsed_max / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+        "stated_error": STATED_ERROR, "clocks": clk.summary(),
+        "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2) * len(specs),
+        "discharges_with_device_errors": sum(r["errors"] for r in per_rank),
+        "precheck_flagged": len(flagged),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 if __name__ == "__main__":
     a = parse()
-    sys.exit(run_reference(a) if a.impl == "reference" else run_ours(a))
+    if a.workload == "c2":
+        # one hardware work queue per stream up to the maximum, so that the
+        # discharges' streams do not share (and serialise on) the default 8
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+    if a.impl == "reference":
+        sys.exit(run_reference(a))
+    sys.exit(run_batched(a) if a.workload == "c2" else run_ours(a))

@@ -1,0 +1,194 @@
+"""Batched discharges: many independent discharges stepped concurrently.
+
+A parameter sweep (the C2 workload: 256 argon CCP discharges with sampled
+voltage, pressure, gap, grid and particle count) leaves most of a B200 idle
+when its small discharges run one after another: a discharge of 1e4
+particles fills a few dozen of the 148 SMs for a few microseconds per step.
+``Batch`` gives every discharge its own ``GpuSimState`` on its own stream;
+each state replays its step graph there, so the kernels of all discharges
+run side by side.  Throughput is timed on the device: a start event on a
+coordinating stream that every state stream waits for, and an end event
+after every state stream has finished.
+
+Streams beyond the device's hardware work queues share them and serialise:
+set CUDA_DEVICE_MAX_CONNECTIONS=32 (the maximum) in the environment before
+CUDA starts when batching many discharges.
+
+``shard`` spreads discharges over the ranks of a multi-GPU job (no
+collective during the run: the discharges are independent); ``gather``
+collects per-rank results on every rank through ``torch.distributed``.
+"""
+import math
+from dataclasses import asdict, dataclass
+
+import numpy as np
+
+E_MASS = 9.10938356e-31
+AR_MASS = 6.63352090e-26
+
+
+@dataclass
+class DischargeSpec:
+    """One discharge of a sweep (argon CCP, eduPIC physics)."""
+    voltage: float      # RF amplitude [V]
+    pressure: float     # [Pa]
+    gap: float          # electrode gap [m]
+    n_g: int            # grid points
+    particles: int      # initial electrons (and ions)
+    seed: int
+
+    def params(self, capacity_factor=2.0):
+        import cudapic_b200 as cp
+        cap = int(math.ceil(self.particles * capacity_factor / 4.0)) * 4
+        # superparticle weight of the reference steady state scaled to the particle count
+        return cp.default_params(voltage=self.voltage, pressure=self.pressure, gap=self.gap, n_g=self.n_g,
+                                 capacity=cap, weight=7.0e4 * 120000 / self.particles)
+
+
+def c2_specs(n=256, seed=0x5EED):
+    """The C2 sweep: V ~ U(100, 500) V, p ~ logU(5, 50) Pa, L ~ U(15, 40) mm,
+    N_G in {200, 400, 800}, particles per species ~ logU(1e4, 1e6)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(n):
+        specs.append(DischargeSpec(
+            voltage=float(rng.uniform(100.0, 500.0)),
+            pressure=float(math.exp(rng.uniform(math.log(5.0), math.log(50.0)))),
+            gap=float(rng.uniform(0.015, 0.040)),
+            n_g=int(rng.choice([200, 400, 800])),
+            particles=int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6))))),
+            seed=int(seed) * 1000 + k))
+    return specs
+
+
+def shard(specs, world):
+    """Indices of the discharges of each rank: largest first onto the rank
+    with the fewest particles so far (balanced by particle count)."""
+    order = sorted(range(len(specs)), key=lambda k: -specs[k].particles)
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += specs[k].particles
+    return [sorted(p) for p in parts]
+
+
+def gather(local, world):
+    """All ranks' results (any picklable object) on every rank, rank order."""
+    if world == 1:
+        return [local]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, local)
+    return out
+
+
+def reduce_max_sum(world, elapsed, work):
+    """(max over ranks of elapsed, sum over ranks of work): the job's time and
+    its total work.  Tensors live on the GPU for NCCL, on the host for gloo."""
+    if world == 1:
+        return elapsed, work
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    w = torch.tensor([float(work)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return t.item(), w.item()
+
+
+def initial_population(spec, dt_e, dt_i):
+    """Maxwellian electrons (3 eV) and ions (0.03 eV) uniform in the gap."""
+    from cudapic_b200.workloads import steady_state
+    e = steady_state(spec.particles, E_MASS, 3.0, gap=spec.gap, dt=dt_e, seed=spec.seed)
+    i = steady_state(spec.particles, AR_MASS, 0.03, gap=spec.gap, dt=dt_i, seed=spec.seed + 1)
+    return e, i
+
+
+class Batch:
+    """Every discharge of ``specs`` as a GpuSimState on its own stream."""
+
+    def __init__(self, specs, device=0, capacity_factor=2.0):
+        from cudapic_b200.sim import GpuSimState, ParticlesSoA
+        self.specs = list(specs)
+        self.states = []
+        try:
+            for k, spec in enumerate(self.specs):
+                st = GpuSimState(spec.params(capacity_factor), device=device)
+                self.states.append(st)
+                g = st.grid
+                e, i = initial_population(spec, g.dt_e, g.dt_i)
+                st.upload_electrons(ParticlesSoA(*e))
+                st.upload_ions(ParticlesSoA(*i))
+                st.seed(e_master=(0x12345678 ^ spec.seed, 0x11112222, 0x22223333, 0x33334444),
+                        i_master=(0x44445555 ^ spec.seed, 0x55556666, 0x66667777, 0x77778888))
+        except Exception:
+            self.close()
+            raise
+
+    def run_steps(self, n_steps):
+        """Enqueues n_steps on every discharge (asynchronous)."""
+        for st in self.states:
+            st.run_steps(n_steps)
+
+    def run_cycles(self, n_cycles):
+        for st in self.states:
+            st.run_cycles(n_cycles)
+
+    def synchronize(self):
+        for st in self.states:
+            st.synchronize()
+
+    def work(self):
+        return sum(st.work() for st in self.states)
+
+    def timed_steps(self, n_steps):
+        """Runs n_steps on every discharge; returns (device seconds, particle-steps)."""
+        import torch
+        w0 = self.work()
+        self.synchronize()
+        coord = torch.cuda.Stream()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(coord):
+            # a bounded sleep holds the start while the host enqueues every
+            # discharge, so the device clock measures the batch, not the host
+            torch.cuda._sleep(int(2e8))
+        start.record(coord)
+        streams = [torch.cuda.ExternalStream(st.stream) for st in self.states]
+        for s in streams:
+            s.wait_event(start)
+        self.run_steps(n_steps)
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            coord.wait_event(ev)
+        end.record(coord)
+        end.synchronize()
+        return start.elapsed_time(end) * 1e-3, self.work() - w0
+
+    def counts(self):
+        return [st.counts() for st in self.states]
+
+    def device_errors(self):
+        return [st.device_error() for st in self.states]
+
+    def prechecks(self):
+        import cudapic_b200 as cp
+        return [cp.stability_precheck(st.params) for st in self.states]
+
+    def describe(self):
+        return [asdict(s) for s in self.specs]
+
+    def close(self):
+        for st in self.states:
+            st.close()
+        self.states = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
