@@ -24,9 +24,11 @@ planes), more than the 126 MB L2, so no L2 flush is needed between steps.
 --workload c2 runs the batched path instead: the 256-discharge sweep of the
 reference's batched configuration (V ~ U(100, 500) V, p ~ logU(5, 50) Pa,
 L ~ U(15, 40) mm, N_G in {200, 400, 800}, 1e4..1e6 particles per species,
-seeded), every discharge a state on its own stream, sharded over the ranks
-of an N-GPU job; the line also reports the same discharges run one at a
-time (a sample) as the plain comparison.
+seeded), every kernel of a step one launch over all discharges of a rank
+(libcudapic's batch driver), discharges sharded over the ranks of an N-GPU
+job; the line also reports the same discharges run one at a time through
+the reference's launch sequence (the plain path) and through the
+one-discharge fused driver.
 
 --impl reference times the reference's own CPU implementation of the path,
 eduPIC 1.0 (C/eduPIC.cc, built from the reference tree into oracle/_ref/),
@@ -70,8 +72,8 @@ def parse():
     ap.add_argument("--workload", choices=["c1", "c2"], default="c1",
                     help="c1: one 4M+4M discharge (plain path); c2: the 256-discharge sweep (batched path)")
     ap.add_argument("--discharges", type=int, default=256)
-    ap.add_argument("--plain-sample", type=int, default=12,
-                    help="c2: discharges also timed one at a time for the plain comparison")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="c2: discharges also timed one at a time for the plain comparisons (0: all of them)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -520,20 +522,49 @@ def run_batched(args):
     e2e_work = batch.work() - w0
     e2e_max, e2e_sum = reduce_max_sum(world, e2e_wall, e2e_work)
 
-    # the plain comparison: a sample of the same discharges, one at a time
-    plain = None
-    if rank == 0 and args.plain_sample > 0:
-        order = sorted(range(len(specs)), key=lambda k: specs[k].particles)
-        pick = [order[int(j * (len(order) - 1) / max(1, args.plain_sample - 1))] for j in range(args.plain_sample)]
-        t_sum = w_sum = 0.0
-        for k in pick:
-            with Batch([specs[k]], device=local) as one:
-                one.run_steps(STEP * args.warmup)
-                t, w = one.timed_steps(STEP * args.steps)
-            t_sum += t
-            w_sum += w
-        plain = {"value": w_sum / t_sum, "unit": UNIT, "sample": "%d of the %d discharges across the size range, "
-                 "each alone, %d PIC steps each" % (len(pick), len(specs), STEP * args.steps)}
+    # the single-simulation comparisons, rank 0's discharges one at a time
+    # (the same states, continuing from where the batch left them):
+    #  * plain: the reference's launch sequence, every step launched from the
+    #    host (no fusion, no graph, no programmatic dependent launch);
+    #  * fused: this library's one-discharge driver (fused step, graphs, PDL).
+    plain = fused = None
+    if rank == 0:
+        order = sorted(range(len(mine)), key=lambda k: mine[k].particles)
+        if 0 < args.plain_sample < len(order):
+            order = [order[int(j * (len(order) - 1) / max(1, args.plain_sample - 1))] for j in range(args.plain_sample)]
+        batch.synchronize()
+
+        def alone(st, k_steps):
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s = torch.cuda.ExternalStream(st.stream)
+            w0 = st.work()
+            ev0.record(s)
+            st.run_steps(k_steps)
+            ev1.record(s)
+            ev1.synchronize()
+            return ev0.elapsed_time(ev1) * 1e-3, st.work() - w0
+
+        sums = {"plain": [0.0, 0.0], "fused": [0.0, 0.0]}
+        for k in order:
+            st = batch.states[k]
+            for mode in ("plain", "fused"):
+                on = mode == "fused"
+                st.set_fused(on)
+                st.set_graphs(on)
+                st.set_overlap(on)
+                st.run_steps(STEP * args.warmup)
+                st.synchronize()
+                t, w = alone(st, STEP * args.steps)
+                sums[mode][0] += t
+                sums[mode][1] += w
+        what = "%d of the %d discharges, each alone in turn, %d PIC steps each" % (len(order), len(specs),
+                                                                                 STEP * args.steps)
+        plain = {"value": sums["plain"][1] / sums["plain"][0], "unit": UNIT,
+                 "path": "reference launch sequence (get_density, Poisson, move_and_compact, check_collisions), "
+                         "every step launched from the host", "sample": what}
+        fused = {"value": sums["fused"][1] / sums["fused"][0], "unit": UNIT,
+                 "path": "one-discharge fused driver (fused electron step, CUDA graph of 2 N_SUB steps, PDL)",
+                 "sample": what}
     per_rank = gather({"discharges": len(mine), "errors": sum(1 for e in errors if e)}, world)
     batch.close()
     if world > 1:
@@ -548,20 +579,24 @@ def run_batched(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "batched path: %d discharges of the C2 sweep (V, p, L, N_G, 1e4..1e6 particles per "
-                               "species sampled, seeded), every discharge a state on its own stream; 1 step = %d PIC "
-                               "steps" % (len(specs), STEP),
+                               "species sampled, seeded), one launch per kernel for all discharges, graph of 2 N_SUB "
+                               "steps; 1 step = %d PIC steps" % (len(specs), STEP),
+                   "precision": "f32 particles and push, 2^-20 fixed-point deposits summed exactly in 64-bit "
+                                "integers, FP64 Poisson scans and time averages",
                    "discharges": len(specs), "particles_total": int(sum(s.particles for s in specs)),
                    "l2": "inputs larger than L2 in aggregate, no flush",
                    "parallelism": "discharges sharded over %d rank(s), no collective" % world},
         "plain_sequential": plain,
+        "fused_sequential": fused,
         "speedup_vs_plain": value / plain["value"] if plain else None,
+        "speedup_vs_fused_single": value / fused["value"] if fused else None,
         "e2e": {"value": e2e_sum / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_max},
         "roofline": {"bound": "hbm", "kernel": "all (batch aggregate, 64 B per particle-step)",
                      "achieved": 64.0 * work_sum / elapsed_max / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": 64.0 * work_sum / elapsed_max / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
         "stated_error": STATED_ERROR, "clocks": clk.summary(),
-        "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2) * len(specs),
+        "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2),
         "discharges_with_device_errors": sum(r["errors"] for r in per_rank),
         "precheck_flagged": len(flagged),
     }

@@ -175,6 +175,7 @@ SIGNATURES = {
     "cudapic_state_set_measure": [_VP, C.c_int],
     "cudapic_state_set_fused": [_VP, C.c_int],
     "cudapic_state_set_overlap": [_VP, C.c_int],
+    "cudapic_state_set_graphs": [_VP, C.c_int],
     "cudapic_state_run_steps": [_VP, C.c_uint64],
     "cudapic_state_counts": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_device_error": [_VP, C.POINTER(_U32)],
@@ -182,12 +183,17 @@ SIGNATURES = {
     "cudapic_state_steps_done": [_VP, C.POINTER(C.c_uint64)],
     "cudapic_state_synchronize": [_VP],
     "cudapic_state_download_measurements": [_VP, _VP, _VP, _VP],
+    "cudapic_batch_create": [C.POINTER(_VP), _U32, C.POINTER(_VP)],
+    "cudapic_batch_destroy": [_VP],
+    "cudapic_batch_run_steps": [_VP, C.c_uint64],
+    "cudapic_batch_synchronize": [_VP],
 }
 OTHER = {
     "cudapic_params_default": (None, [C.POINTER(Params)]),
     "cudapic_status_string": (C.c_char_p, [C.c_int]),
     "cudapic_last_error": (C.c_char_p, []),
     "cudapic_state_stream": (_VP, [_VP]),
+    "cudapic_batch_stream": (_VP, [_VP]),
 }
 
 

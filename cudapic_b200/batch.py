@@ -3,16 +3,12 @@
 A parameter sweep (the C2 workload: 256 argon CCP discharges with sampled
 voltage, pressure, gap, grid and particle count) leaves most of a B200 idle
 when its small discharges run one after another: a discharge of 1e4
-particles fills a few dozen of the 148 SMs for a few microseconds per step.
-``Batch`` gives every discharge its own ``GpuSimState`` on its own stream;
-each state replays its step graph there, so the kernels of all discharges
-run side by side.  Throughput is timed on the device: a start event on a
-coordinating stream that every state stream waits for, and an end event
-after every state stream has finished.
-
-Streams beyond the device's hardware work queues share them and serialise:
-set CUDA_DEVICE_MAX_CONNECTIONS=32 (the maximum) in the environment before
-CUDA starts when batching many discharges.
+particles fills a few of the 148 SMs for a few microseconds per step.
+``Batch`` gives every discharge its own ``GpuSimState`` and steps them all
+through one ``GpuBatch``: each kernel of a step is ONE persistent launch over
+the concatenated particles of every discharge (libcudapic's batch driver,
+kernels_batch.cu), 2 N_SUB steps per captured CUDA graph.  Throughput is
+timed on the device with events on the batch's stream.
 
 ``shard`` spreads discharges over the ranks of a multi-GPU job (no
 collective during the run: the discharges are independent); ``gather``
@@ -108,14 +104,15 @@ def initial_population(spec, dt_e, dt_i):
 
 
 class Batch:
-    """Every discharge of ``specs`` as a GpuSimState on its own stream."""
+    """Every discharge of ``specs`` as a GpuSimState, stepped by one GpuBatch."""
 
     def __init__(self, specs, device=0, capacity_factor=2.0):
-        from cudapic_b200.sim import GpuSimState, ParticlesSoA
+        from cudapic_b200.sim import GpuBatch, GpuSimState, ParticlesSoA
         self.specs = list(specs)
         self.states = []
+        self.batch = None
         try:
-            for k, spec in enumerate(self.specs):
+            for spec in self.specs:
                 st = GpuSimState(spec.params(capacity_factor), device=device)
                 self.states.append(st)
                 g = st.grid
@@ -124,20 +121,20 @@ class Batch:
                 st.upload_ions(ParticlesSoA(*i))
                 st.seed(e_master=(0x12345678 ^ spec.seed, 0x11112222, 0x22223333, 0x33334444),
                         i_master=(0x44445555 ^ spec.seed, 0x55556666, 0x66667777, 0x77778888))
+            self.batch = GpuBatch(self.states)
         except Exception:
             self.close()
             raise
 
     def run_steps(self, n_steps):
-        """Enqueues n_steps on every discharge (asynchronous)."""
-        for st in self.states:
-            st.run_steps(n_steps)
+        """Enqueues n_steps of every discharge (asynchronous)."""
+        self.batch.run_steps(n_steps)
 
     def run_cycles(self, n_cycles):
-        for st in self.states:
-            st.run_cycles(n_cycles)
+        self.batch.run_cycles(n_cycles)
 
     def synchronize(self):
+        self.batch.synchronize()
         for st in self.states:
             st.synchronize()
 
@@ -149,23 +146,16 @@ class Batch:
         import torch
         w0 = self.work()
         self.synchronize()
-        coord = torch.cuda.Stream()
+        s = torch.cuda.ExternalStream(self.batch.stream)
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(coord):
-            # a bounded sleep holds the start while the host enqueues every
-            # discharge, so the device clock measures the batch, not the host
-            torch.cuda._sleep(int(2e8))
-        start.record(coord)
-        streams = [torch.cuda.ExternalStream(st.stream) for st in self.states]
-        for s in streams:
-            s.wait_event(start)
+        with torch.cuda.stream(s):
+            # a bounded sleep holds the start while the host enqueues, so the
+            # device clock measures the batch, not the host
+            torch.cuda._sleep(int(5e7))
+        start.record(s)
         self.run_steps(n_steps)
-        for s in streams:
-            ev = torch.cuda.Event()
-            ev.record(s)
-            coord.wait_event(ev)
-        end.record(coord)
+        end.record(s)
         end.synchronize()
         return start.elapsed_time(end) * 1e-3, self.work() - w0
 
@@ -183,6 +173,9 @@ class Batch:
         return [asdict(s) for s in self.specs]
 
     def close(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
         for st in self.states:
             st.close()
         self.states = []

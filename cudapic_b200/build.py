@@ -24,9 +24,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I", ROOT, "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
           "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "--expt-relaxed-constexpr"]
 
-SOURCES = ["host.cpp", "state.cpp", "checkpoint.cpp", "report.cpp", "kernels_density.cu", "kernels_poisson.cu", "kernels_push.cu",
-           "kernels_mcc.cu", "kernels_step.cu", "kernels_misc.cu",
-           "noalloc.cu"]
+SOURCES = ["host.cpp", "state.cpp", "batch.cpp", "checkpoint.cpp", "report.cpp", "kernels_density.cu",
+           "kernels_poisson.cu", "kernels_push.cu", "kernels_mcc.cu", "kernels_step.cu", "kernels_batch.cu",
+           "kernels_misc.cu", "noalloc.cu"]
 
 
 def _newer(target, deps):

@@ -1,0 +1,442 @@
+// kernels_batch.cu -- the particle kernels of a batch of discharges.
+//
+// The reference steps one discharge per process (Rust-CUDA/src/main.rs:
+// 1725-1808); a parameter sweep of small discharges leaves most of a B200
+// idle between launches.  Here one persistent launch per kernel of the step
+// covers every discharge of a batch:
+//  * the particles of all discharges form one index space, each discharge's
+//    count rounded up to a multiple of 4 (so every segment starts 16-byte
+//    aligned); CTA c owns an equal contiguous share of it, which cuts into at
+//    most a few discharges: its segments;
+//  * per segment the CTA loads that discharge's descriptor (buffers, grid
+//    constants, tables) into shared memory and runs the same tile pipeline
+//    as the one-discharge fused step (step.cuh), with the discharge's own
+//    slot counters, density and E-field;
+//  * each discharge's count is published by the last CTA to finish it (its
+//    own ticket, expecting the CTAs whose shares meet the discharge).
+// The plan (a prefix over the counts) is recomputed by every CTA from the
+// counts the batched Poisson kernel wrote, so no extra launch is needed.
+#include <algorithm>
+
+#include "batch_internal.h"
+#include "internal.h"
+#include "step.cuh"
+
+namespace cudapic {
+
+namespace {
+
+__device__ __forceinline__ uint32_t round4(uint32_t n) { return (n + 3u) & ~3u; }
+
+// P[d] = sum_{k<d} round4(count(k)) for d in [0, D]; one call by the whole
+// CTA (ES_THREADS threads), which synchronises before returning.
+template <typename Count>
+__device__ __forceinline__ void plan_prefix(Count count, uint32_t D, uint32_t *P, uint32_t *wsum) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t per = (D + ES_THREADS - 1) / ES_THREADS;
+    uint32_t sum = 0;
+    for (uint32_t j = 0; j < per; ++j) {
+        const uint32_t d = (uint32_t)tid * per + j;
+        if (d < D) sum += round4(count(d));
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < ES_WARPS ? wsum[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < ES_WARPS) wsum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = incl - sum + (warp > 0 ? wsum[warp - 1] : 0u);
+    for (uint32_t j = 0; j < per; ++j) {
+        const uint32_t d = (uint32_t)tid * per + j;
+        if (d < D) {
+            P[d] = run;
+            run += round4(count(d));
+        }
+    }
+    if (tid == 0) P[D] = wsum[ES_WARPS - 1];
+    __syncthreads();
+}
+
+// Smallest d with P[d + 1] > x (D when there is none).
+__device__ __forceinline__ uint32_t first_discharge(const uint32_t *P, uint32_t D, uint32_t x) {
+    uint32_t lo = 0, hi = D;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (P[mid + 1] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// The CTA's share [beg, end) of the batch's index space (a multiple of 4 long).
+__device__ __forceinline__ void cta_share(uint32_t total, uint32_t &chunk, uint32_t &beg, uint32_t &end) {
+    chunk = ((total + gridDim.x - 1) / gridDim.x + 3u) & ~3u;
+    beg = min(total, blockIdx.x * chunk);
+    end = min(total, beg + chunk);
+}
+
+// Publishes a discharge's count: the CTA whose ticket is the last of the
+// `expected` CTAs that processed the discharge stores min(*src, capacity)
+// into *dst and clears *src and the ticket (publish_count with a count).
+__device__ __forceinline__ void publish_count_of(uint32_t *ticket, uint32_t *dst, uint32_t *src, uint32_t capacity,
+                                                 uint32_t expected) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t t = atomicAdd(ticket, 1u);
+        if (t == expected - 1) {
+            __threadfence();
+            const uint32_t v = atomicExch(src, 0u);
+            *dst = v < capacity ? v : capacity;
+            *ticket = 0u;
+        }
+    }
+}
+
+}  // namespace
+
+// MCC: the fused electron step of every discharge; !MCC: the ion push with
+// the deposit of the next ion density.  MINB: resident CTAs per SM the
+// register allocation is bounded for (cudapic_tuning.step_ctas_per_sm: 3
+// caps it at 80 registers, 2 leaves it free).
+template <int U, bool MCC, int MINB>
+__global__ void __launch_bounds__(ES_THREADS, MINB)
+    batch_step_kernel(const BatchDisc *__restrict__ desc, const uint32_t *__restrict__ counts, uint32_t D,
+                      const StepRoles r, uint32_t ef_pad, int stages, int copies, uint32_t epoch) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint32_t offs[3][StepShape<U, MCC>::NSEG];
+    __shared__ uint32_t s_base[3];
+    __shared__ uint32_t wsum[ES_WARPS];
+    __shared__ StepIO s_io;
+    __shared__ cudapic_grid s_g;
+    const StepSmem<U, MCC> sm(smem, stages, copies, ef_pad, offs, s_base);
+    uint32_t *P = reinterpret_cast<uint32_t *>(sm.end(stages));  // [D + 1]
+    step_smem_init(sm, stages, copies, ef_pad);
+    grid_dep_wait();
+    plan_prefix([&](uint32_t d) { return counts[d]; }, D, P, wsum);
+    uint32_t chunk, beg, end;
+    cta_share(P[D], chunk, beg, end);
+    const int sp = MCC ? 0 : 1;
+    uint32_t it = 0;
+    bool ok = true;
+    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
+        const uint32_t n = counts[d];
+        const uint32_t lo = max(beg, P[d]) - P[d];
+        const uint32_t hi = min(end, P[d] + n) - P[d];
+        if (lo >= hi) continue;
+        const BatchDisc &dd = desc[d];
+        if (threadIdx.x == 0) {
+            s_g = dd.g;
+            StepIO io;
+            io.efield = dd.efield;
+            io.sx = dd.x[sp][r.src];
+            io.svx = dd.vx[sp][r.src];
+            io.svy = dd.vy[sp][r.src];
+            io.svz = dd.vz[sp][r.src];
+            io.dx = dd.x[sp][r.dst];
+            io.dvx = dd.vx[sp][r.dst];
+            io.dvy = dd.vy[sp][r.dst];
+            io.dvz = dd.vz[sp][r.dst];
+            io.rng0 = dd.rng[sp][0];
+            io.rng1 = dd.rng[sp][1];
+            io.rng2 = dd.rng[sp][2];
+            io.rng3 = dd.rng[sp][3];
+            io.sigma_tot = MCC ? dd.sigma_tot_e : dd.sigma_tot_i;
+            io.cs = dd.cs;
+            io.sigma_max = dd.sigma_max_e;
+            io.factor = MCC ? dd.g.factor_e : dd.g.factor_i;
+            io.dt = MCC ? dd.g.dt_e : dd.g.dt_i;
+            io.ix = dd.x[1][r.ion_side];
+            io.ivx = dd.vx[1][r.ion_side];
+            io.ivy = dd.vy[1][r.ion_side];
+            io.ivz = dd.vz[1][r.ion_side];
+            io.alive = dd.counters + (MCC ? 2 : 5);
+            io.n_i = dd.counters + 1;
+            io.dens = MCC ? dd.e_dens[r.dens] : dd.i_dens[r.dens];
+            io.dens_i = dd.i_dens[r.dens_i];
+            io.wall = r.measure ? dd.wall + sp : nullptr;
+            io.coll = r.measure && MCC ? dd.mcount : nullptr;
+            s_io = io;
+            if (lo == 0 && dd.g.work) atomicAdd(dd.g.work, (unsigned long long)n);
+        }
+        __syncthreads();
+        if (ok) ok = step_segment<U, MCC>(s_io, s_g, lo, hi, sm, stages, copies, ef_pad, epoch, it);
+        const uint32_t expected = (P[d] + n - 1) / chunk - P[d] / chunk + 1;
+        publish_count_of(dd.counters + 6, dd.counters + (MCC ? 0 : 1), dd.counters + (MCC ? 2 : 5), s_g.capacity,
+                         expected);
+        __syncthreads();  // s_io and s_g are rewritten for the next segment
+    }
+}
+
+// check_collisions_i / collision_i (Rust-CUDA/src/main.rs:1167-1292) of every
+// discharge, in place.  Plain coalesced loads; colliders go to warp-private
+// queues (slot and RNG state before the test) drained 32 at a time, as in
+// the resident-table kernel of kernels_mcc.cu, with each discharge's table
+// read from global memory.
+constexpr int BC_U = 2;
+constexpr int BC_QCAP = 32 + 32 * BC_U;
+
+struct IonCollIO {
+    float *vx, *vy, *vz;
+    uint32_t *rng0, *rng1, *rng2, *rng3;
+    const float *sigma_tot, *cs;
+    unsigned long long *coll;
+};
+
+__global__ void __launch_bounds__(ES_THREADS)
+    batch_collisions_i_kernel(const BatchDisc *__restrict__ desc, uint32_t D, int side, int measure) {
+    extern __shared__ __align__(16) uint32_t bc_smem[];
+    uint32_t *P = bc_smem;                                   // [D + 1]
+    __shared__ uint32_t queue[ES_WARPS][5][BC_QCAP];
+    __shared__ uint32_t wsum[ES_WARPS];
+    __shared__ IonCollIO s_io;
+    __shared__ cudapic_grid s_g;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = lanemask_lt();
+    grid_dep_wait();
+    auto count = [&](uint32_t d) {
+        const BatchDisc &dd = desc[d];
+        return min(*(volatile uint32_t *)(dd.counters + 1), dd.g.capacity);
+    };
+    plan_prefix(count, D, P, wsum);
+    uint32_t chunk, beg, end;
+    cta_share(P[D], chunk, beg, end);
+    uint32_t (*wq)[BC_QCAP] = queue[warp];
+    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
+        const uint32_t n = count(d);  // unchanged during the kernel
+        const uint32_t lo = max(beg, P[d]) - P[d];
+        const uint32_t hi = min(end, P[d] + n) - P[d];
+        if (lo >= hi) continue;
+        const BatchDisc &dd = desc[d];
+        if (tid == 0) {
+            s_g = dd.g;
+            IonCollIO io;
+            io.vx = dd.vx[1][side];
+            io.vy = dd.vy[1][side];
+            io.vz = dd.vz[1][side];
+            io.rng0 = dd.rng[1][0];
+            io.rng1 = dd.rng[1][1];
+            io.rng2 = dd.rng[1][2];
+            io.rng3 = dd.rng[1][3];
+            io.sigma_tot = dd.sigma_tot_i;
+            io.cs = dd.cs;
+            io.coll = measure ? dd.mcount + 1 : nullptr;
+            s_io = io;
+        }
+        __syncthreads();
+        const IonCollIO &io = s_io;
+        const cudapic_grid &g = s_g;
+        const GlobalTable table{io.sigma_tot};
+        auto drain = [&](uint32_t first, uint32_t cnt) {
+            if (io.coll && lane == 0) atomicAdd(io.coll, (unsigned long long)cnt);
+            if ((uint32_t)lane < cnt) {
+                const uint32_t q = first + lane;
+                const uint32_t i = wq[0][q];
+                Xoshiro128p rs{wq[1][q], wq[2][q], wq[3][q], wq[4][q]};
+                const float vxi = io.vx[i], vyi = io.vy[i], vzi = io.vz[i];
+                const IonTest t = test_ion(vxi, vyi, vzi, rs, table, g);
+                collide_ion(i, t.idx, vxi, vyi, vzi, t.vxa, t.vya, t.vza, rs, io.cs, io.vx, io.vy, io.vz, g);
+                io.rng0[i] = rs.s0;
+                io.rng1[i] = rs.s1;
+                io.rng2[i] = rs.s2;
+                io.rng3[i] = rs.s3;
+            }
+            __syncwarp();
+        };
+        uint32_t qn = 0;
+        for (uint32_t b0 = lo; b0 < hi; b0 += ES_THREADS * BC_U) {
+            uint32_t s[BC_U][4];
+            float v[BC_U][3];
+#pragma unroll
+            for (int u = 0; u < BC_U; ++u) {
+                const uint32_t i = b0 + (uint32_t)u * ES_THREADS + tid;
+                if (i < hi) {
+                    s[u][0] = io.rng0[i];
+                    s[u][1] = io.rng1[i];
+                    s[u][2] = io.rng2[i];
+                    s[u][3] = io.rng3[i];
+                    v[u][0] = io.vx[i];
+                    v[u][1] = io.vy[i];
+                    v[u][2] = io.vz[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BC_U; ++u) {
+                const uint32_t i = b0 + (uint32_t)u * ES_THREADS + tid;
+                bool collide = false;
+                if (i < hi) {
+                    Xoshiro128p rs{s[u][0], s[u][1], s[u][2], s[u][3]};
+                    collide = test_ion(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
+                    if (!collide) {
+                        io.rng0[i] = rs.s0;
+                        io.rng1[i] = rs.s1;
+                        io.rng2[i] = rs.s2;
+                        io.rng3[i] = rs.s3;
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, collide);
+                if (collide) {
+                    const uint32_t q = qn + __popc(m & lt);
+                    wq[0][q] = i;
+                    wq[1][q] = s[u][0];
+                    wq[2][q] = s[u][1];
+                    wq[3][q] = s[u][2];
+                    wq[4][q] = s[u][3];
+                }
+                qn += __popc(m);
+            }
+            __syncwarp();
+            while (qn >= 32) {
+                qn -= 32;
+                drain(qn, 32);
+            }
+        }
+        if (qn) drain(0, qn);
+        __syncthreads();  // s_io and s_g are rewritten for the next segment
+    }
+}
+
+// accumulate_eepf (Rust-CUDA/src/main.rs:1301-1339) of every discharge with
+// the centre-energy sums of the report; one shared histogram per segment.
+__global__ void __launch_bounds__(ES_THREADS)
+    batch_eepf_kernel(const BatchDisc *__restrict__ desc, uint32_t D, int side) {
+    extern __shared__ __align__(16) uint32_t be_smem[];
+    uint32_t *P = be_smem;  // [D + 1]
+    __shared__ uint32_t hist[N_EEPF];
+    __shared__ uint32_t wsum[ES_WARPS];
+    const int tid = threadIdx.x;
+    for (uint32_t k = tid; k < N_EEPF; k += ES_THREADS) hist[k] = 0u;
+    grid_dep_wait();
+    auto count = [&](uint32_t d) {
+        const BatchDisc &dd = desc[d];
+        return min(*(volatile uint32_t *)(dd.counters + 0), dd.g.capacity);
+    };
+    plan_prefix(count, D, P, wsum);
+    uint32_t chunk, beg, end;
+    cta_share(P[D], chunk, beg, end);
+    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
+        const uint32_t n = count(d);  // unchanged during the kernel
+        const uint32_t lo = max(beg, P[d]) - P[d];
+        const uint32_t hi = min(end, P[d] + n) - P[d];
+        if (lo >= hi) continue;
+        const BatchDisc &dd = desc[d];
+        const cudapic_grid &g = dd.g;
+        const float *x = dd.x[0][side], *vx = dd.vx[0][side], *vy = dd.vy[0][side], *vz = dd.vz[0][side];
+        const float *ef = dd.efield;
+        const float min_x = g.min_x, max_x = g.max_x, inv_dx = g.inv_dx, kick = g.eepf_half_kick;
+        const float half_me = g.half_me_over_e;
+        const uint32_t n_g = g.n_g;
+        double e_sum = 0.0;
+        unsigned long long e_cnt = 0;
+        for (uint32_t i = lo + tid; i < hi; i += ES_THREADS) {
+            const float xi = x[i];
+            if (xi <= min_x || xi >= max_x) continue;
+            const float pos = xi * inv_dx;
+            const int p = cell_of(pos, n_g);
+            const float c2 = pos - (float)p;
+            const float e_x = (1.0f - c2) * __ldg(ef + p) + c2 * __ldg(ef + p + 1);
+            const float mvx = vx[i] - 0.5f * e_x * kick;
+            const float vyi = vy[i], vzi = vz[i];
+            const float v2 = mvx * mvx + vyi * vyi + vzi * vzi;
+            const float energy = half_me * v2;
+            const float binf = energy / DE_EEPF_F;
+            if (binf < (float)N_EEPF) atomicAdd(&hist[(uint32_t)binf], 1u);
+            e_sum += (double)energy;
+            ++e_cnt;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            e_sum += __shfl_down_sync(0xffffffffu, e_sum, o);
+            e_cnt += __shfl_down_sync(0xffffffffu, e_cnt, o);
+        }
+        if ((tid & 31) == 0 && e_cnt) {
+            atomicAdd(dd.esum, e_sum);
+            atomicAdd(dd.mcount + 2, e_cnt);
+        }
+        __syncthreads();
+        for (uint32_t k = tid; k < N_EEPF; k += ES_THREADS) {
+            if (hist[k]) {
+                atomicAdd(&dd.eepf[k], hist[k]);
+                hist[k] = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+namespace {
+
+template <int U, bool MCC, int MINB>
+int launch_batch_step_t(const BatchDisc *desc, const uint32_t *counts, uint32_t D, uint64_t cap_sum,
+                        uint32_t max_n_g, const StepRoles &r, cudaStream_t stream, const cudapic_tuning &t) {
+    constexpr int TILE = StepShape<U, MCC>::TILE;
+    int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
+    int copies = std::max(1, std::min(t.density_copies, ES_WARPS));
+    const uint32_t ef_pad = (max_n_g + 3u) & ~3u;
+    const size_t plan = (size_t)(D + 1) * sizeof(uint32_t);
+    auto bytes = [&]() { return step_smem_bytes<U, MCC>(stages, copies, ef_pad) + plan; };
+    const size_t budget = (size_t)max_smem_optin();
+    while (bytes() > budget && stages > 2) --stages;
+    while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
+    if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "batch step: n_g too large");
+    const size_t smem = bytes();
+    auto kern = batch_step_kernel<U, MCC, MINB>;
+    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                             "cudaFuncSetAttribute(batch step)"));
+    int per_sm = 0;
+    CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ES_THREADS, smem),
+                             "occupancy(batch step)"));
+    per_sm = std::min(std::max(per_sm, 1), t.step_ctas_per_sm);
+    const unsigned grid = persistent_grid(per_sm, (cap_sum + TILE - 1) / TILE);
+    const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
+    const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
+    return launch_kernel(MCC ? "batch_step_electrons" : "batch_push_ions", kern, dim3(grid), dim3(ES_THREADS), smem,
+                         stream, desc, counts, D, r, ef_pad, stages, copies, epoch);
+}
+
+}  // namespace
+
+int launch_batch_step(bool mcc, const BatchDisc *desc, const uint32_t *counts, uint32_t D, uint64_t cap_sum,
+                      uint32_t max_n_g, const StepRoles &r, cudaStream_t stream) {
+    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch step: bad discharge count");
+    const cudapic_tuning t = tuning();
+    const bool three = t.step_ctas_per_sm >= 3;
+    if (mcc) {
+        if (t.step_rows == 4)
+            return three ? launch_batch_step_t<4, true, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                         : launch_batch_step_t<4, true, 2>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
+        return three ? launch_batch_step_t<2, true, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                     : launch_batch_step_t<2, true, 2>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
+    }
+    return t.step_rows == 4 ? launch_batch_step_t<4, false, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                            : launch_batch_step_t<2, false, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
+}
+
+int launch_batch_collisions_i(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, int measure,
+                              cudaStream_t stream) {
+    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch collisions: bad discharge count");
+    const size_t smem = (size_t)(D + 1) * sizeof(uint32_t);
+    const unsigned grid = persistent_grid(4, (cap_sum + ES_THREADS * BC_U - 1) / (ES_THREADS * BC_U));
+    return launch_kernel("batch_collisions_i", batch_collisions_i_kernel, dim3(grid), dim3(ES_THREADS), smem, stream,
+                         desc, D, side, measure);
+}
+
+int launch_batch_eepf(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, cudaStream_t stream) {
+    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch eepf: bad discharge count");
+    const size_t smem = (size_t)(D + 1) * sizeof(uint32_t);
+    const unsigned grid = persistent_grid(2, (cap_sum + ES_THREADS - 1) / ES_THREADS);
+    return launch_kernel("batch_eepf", batch_eepf_kernel, dim3(grid), dim3(ES_THREADS), smem, stream, desc, D, side);
+}
+
+}  // namespace cudapic

@@ -19,6 +19,7 @@
 // The driver variant reads pot0 from a device table indexed by a device
 // step counter (so that one captured CUDA graph serves every RF phase) and
 // advances the counter.
+#include "batch_internal.h"
 #include "common.cuh"
 #include "internal.h"
 
@@ -58,13 +59,15 @@ __device__ __forceinline__ T block_excl_scan(T v, T *wsum, T &total) {
     return excl;
 }
 
+// The solve of one discharge by one CTA (after grid_dep_wait), shared by
+// poisson_kernel and the batched solve (kernels_batch.cu).
 // T: arithmetic type of the scans (double or float); PT: nodes per thread.
 template <typename T, int PT>
-__global__ void __launch_bounds__(POIS_MAX_THREADS)
-    poisson_kernel(const float *__restrict__ e_density, const float *__restrict__ i_density,
-                   float *__restrict__ pot_out, float *__restrict__ efield_out, float pot0_arg,
-                   const float *__restrict__ pot0_table, uint32_t *__restrict__ step_counter,
-                   const cudapic_grid g, float *__restrict__ zero_a, float *__restrict__ zero_b) {
+__device__ __forceinline__ void poisson_body(const float *__restrict__ e_density, const float *__restrict__ i_density,
+                                             float *__restrict__ pot_out, float *__restrict__ efield_out,
+                                             float pot0_arg, const float *__restrict__ pot0_table,
+                                             uint32_t *__restrict__ step_counter, const cudapic_grid &g,
+                                             float *__restrict__ zero_a, float *__restrict__ zero_b) {
     constexpr int per_thread = PT;
     extern __shared__ unsigned char smem_raw[];
     T *pot_s = reinterpret_cast<T *>(smem_raw);        // n_g
@@ -74,7 +77,6 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
 
     const int n = (int)g.n_g;
     const int tid = threadIdx.x;
-    grid_dep_wait();
     for (int k = tid; k < n; k += blockDim.x) {  // next-step accumulators of the driver
         if (zero_a) zero_a[k] = 0.0f;
         if (zero_b) zero_b[k] = 0.0f;
@@ -178,6 +180,17 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
             }
         }
     }
+}
+
+template <typename T, int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    poisson_kernel(const float *__restrict__ e_density, const float *__restrict__ i_density,
+                   float *__restrict__ pot_out, float *__restrict__ efield_out, float pot0_arg,
+                   const float *__restrict__ pot0_table, uint32_t *__restrict__ step_counter,
+                   const cudapic_grid g, float *__restrict__ zero_a, float *__restrict__ zero_b) {
+    grid_dep_wait();
+    poisson_body<T, PT>(e_density, i_density, pot_out, efield_out, pot0_arg, pot0_table, step_counter, g, zero_a,
+                        zero_b);
 }
 
 // solve_poisson_dps_flexible: the same closed form with runtime n, dx and
@@ -288,6 +301,72 @@ int launch_poisson(const float *e_density, const float *i_density, float *pot, f
     if (g.flags & CUDAPIC_FLAG_POISSON_F32_SCAN)
         return launch_poisson_pt<float>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream, zero_a, zero_b);
     return launch_poisson_pt<double>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g, stream, zero_a, zero_b);
+}
+
+// Batched solve: CTA d solves discharge d of the batch (the driver variant
+// above, with the discharge's own step counter and RF table), writes its
+// clamped particle counts for the batched particle kernels and, when
+// measuring, adds the densities it read to the time averages
+// (accumulate_density, Rust-CUDA/src/main.rs:1294-1299).
+template <typename T, int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    batch_poisson_kernel(const BatchDisc *__restrict__ desc, uint32_t *__restrict__ counts, uint32_t D, int e_read,
+                         int i_read, int ion_step, int measure) {
+    __shared__ cudapic_grid s_g;
+    const BatchDisc &dd = desc[blockIdx.x];
+    if (threadIdx.x == 0) s_g = dd.g;
+    __syncthreads();
+    grid_dep_wait();
+    uint32_t *ctr = dd.counters;
+    if (threadIdx.x == 0) {
+        counts[blockIdx.x] = load_count(ctr + 0, s_g.capacity, s_g.dev_err);
+        counts[D + blockIdx.x] = load_count(ctr + 1, s_g.capacity, s_g.dev_err);
+    }
+    const float *e_dens = dd.e_dens[e_read];
+    const float *i_dens = dd.i_dens[i_read];
+    if (measure) {
+        for (uint32_t k = threadIdx.x; k < s_g.n_g; k += blockDim.x) {
+            dd.cumul_e[k] += (double)e_dens[k];
+            if (ion_step) dd.cumul_i[k] += (double)i_dens[k];
+        }
+    }
+    poisson_body<T, PT>(e_dens, i_dens, dd.pot, dd.efield, 0.0f, dd.pot0_table, ctr + 3, s_g, dd.e_dens[e_read ^ 1],
+                        ion_step ? dd.i_dens[i_read ^ 1] : nullptr);
+}
+
+template <typename T, int PT>
+int launch_batch_poisson_t(const BatchDisc *desc, uint32_t *counts, uint32_t D, uint32_t max_n_g, int threads,
+                           int e_read, int i_read, int ion_step, int measure, cudaStream_t stream) {
+    const size_t smem = (size_t)max_n_g * sizeof(T);
+    auto kern = batch_poisson_kernel<T, PT>;
+    if (smem > 48 * 1024)
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                 "cudaFuncSetAttribute(batch poisson)"));
+    return launch_kernel("batch_solve_poisson", kern, dim3(D), dim3(threads), smem, stream, desc, counts, D, e_read,
+                         i_read, ion_step, measure);
+}
+
+template <typename T>
+int launch_batch_poisson_pt(const BatchDisc *desc, uint32_t *counts, uint32_t D, uint32_t max_n_g, int e_read,
+                            int i_read, int ion_step, int measure, cudaStream_t stream) {
+    int threads, pt;
+    poisson_shape(max_n_g, threads, pt);
+    switch (pt) {
+    case 1: return launch_batch_poisson_t<T, 1>(desc, counts, D, max_n_g, threads, e_read, i_read, ion_step, measure, stream);
+    case 2: return launch_batch_poisson_t<T, 2>(desc, counts, D, max_n_g, threads, e_read, i_read, ion_step, measure, stream);
+    case 4: return launch_batch_poisson_t<T, 4>(desc, counts, D, max_n_g, threads, e_read, i_read, ion_step, measure, stream);
+    case 8: return launch_batch_poisson_t<T, 8>(desc, counts, D, max_n_g, threads, e_read, i_read, ion_step, measure, stream);
+    default: return launch_batch_poisson_t<T, 16>(desc, counts, D, max_n_g, threads, e_read, i_read, ion_step, measure, stream);
+    }
+}
+
+int launch_batch_poisson(const BatchDisc *desc, uint32_t *counts, uint32_t D, uint32_t max_n_g, uint32_t flags,
+                         int e_read, int i_read, int ion_step, int measure, cudaStream_t stream) {
+    if (max_n_g > (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD))
+        return fail(CUDAPIC_ERR_ARG, "batch: n_g > 16384");
+    if (flags & CUDAPIC_FLAG_POISSON_F32_SCAN)
+        return launch_batch_poisson_pt<float>(desc, counts, D, max_n_g, e_read, i_read, ion_step, measure, stream);
+    return launch_batch_poisson_pt<double>(desc, counts, D, max_n_g, e_read, i_read, ion_step, measure, stream);
 }
 
 }  // namespace cudapic

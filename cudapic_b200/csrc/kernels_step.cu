@@ -41,41 +41,10 @@
 //  * the last CTA to finish publishes the electron count (StepLink).
 #include <algorithm>
 
-#include "common.cuh"
 #include "internal.h"
-#include "mcc.cuh"
-#include "push.cuh"
-#include "tma.cuh"
+#include "step.cuh"
 
 namespace cudapic {
-
-constexpr int ES_THREADS = 256;
-constexpr int ES_WARPS = ES_THREADS / 32;
-constexpr int ES_PLANES = 8;                  // x, vx, vy, vz, rng0..3
-constexpr int ES_MAX_STAGES = 6;              // pipeline depth: cudapic_tuning.step_stages
-// U (cudapic_tuning.step_rows, 2 or 4): particles per thread and tile, so a
-// tile holds 256 U particles (8 KB U of staged planes); a warp's collider
-// queue holds 31 + 32 U entries at most.
-template <int U>
-struct StepShape {
-    static constexpr int TILE = ES_THREADS * U;
-    static constexpr int QCAP = 32 + 32 * U;
-    static_assert(U * ES_WARPS <= 32, "one warp scans the (row, warp) counts");
-};
-
-// Survivors of one tile held in registers until their base is known.
-template <int U>
-struct StepOut {
-    float x[U], vx[U], vy[U], vz[U];
-    uint32_t lane_off[U];
-    uint32_t keep;  // bit u: the particle of row u is written by the tile
-};
-
-// True unless u certainly exceeds the collision probability at speed
-// `velocity` (see the file comment; same operation order as test_electron).
-__device__ __forceinline__ bool may_collide(float u, float velocity, float sigma_max, float dt) {
-    return u < sigma_max * velocity * dt + 5e-7f;
-}
 
 template <int U>
 __global__ void __launch_bounds__(ES_THREADS)
@@ -89,32 +58,14 @@ __global__ void __launch_bounds__(ES_THREADS)
                          const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int stages, int copies,
                          uint32_t epoch, const StepLink link, cudapic_wall_counters *wall,
                          unsigned long long *coll) {
-    constexpr int ES_TILE = StepShape<U>::TILE;
-    constexpr int ES_QCAP = StepShape<U>::QCAP;
-    constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
     extern __shared__ __align__(128) unsigned char smem[];
-    uint32_t *in = reinterpret_cast<uint32_t *>(smem);                                   // [stages][8][TILE]
-    float *ef = reinterpret_cast<float *>(in + stages * ES_PLANES * ES_TILE);             // [ef_pad]
-    unsigned long long *acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);        // [ef_pad]
-    uint32_t *hist = reinterpret_cast<uint32_t *>(acc + ef_pad);                          // [copies][ef_pad]
-    uint32_t *queue = hist + (uint32_t)copies * ef_pad;                                   // [WARPS][QCAP]
-    uint64_t *bar = reinterpret_cast<uint64_t *>(queue + ES_WARPS * ES_QCAP);             // [stages]
     // Per tile: (row, warp) counts, then exclusive offsets; the tile's base.
     // Three buffers, because a tile's counts are written while slower warps
     // may still be storing the tile before the previous one.
-    __shared__ uint32_t offs[3][NSEG];
+    __shared__ uint32_t offs[3][StepShape<U, true>::NSEG];
     __shared__ uint32_t s_base[3];
-
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const unsigned lt = lanemask_lt();
-    if (tid == 0) {
-        for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
-        fence_mbar_init();
-    }
-    for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += ES_THREADS) hist[k] = 0u;
-    for (uint32_t k = tid; k < ef_pad; k += ES_THREADS) acc[k] = 0ull;
+    const StepSmem<U, true> sm(smem, stages, copies, ef_pad, offs, s_base);
+    step_smem_init(sm, stages, copies, ef_pad);
     grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     // Balanced partition: CTA c owns the particles [beg, end), an equal share
@@ -123,222 +74,38 @@ __global__ void __launch_bounds__(ES_THREADS)
     const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 3u) & ~3u;
     const uint32_t beg = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, beg + chunk);
-    const uint32_t ntiles = (end - beg + ES_TILE - 1) / ES_TILE;  // this CTA's tiles
-    const uint32_t *src[ES_PLANES] = {reinterpret_cast<const uint32_t *>(sx), reinterpret_cast<const uint32_t *>(svx),
-                                      reinterpret_cast<const uint32_t *>(svy), reinterpret_cast<const uint32_t *>(svz),
-                                      rng0, rng1, rng2, rng3};
-    if (g.work && blockIdx.x == 0 && tid == 0) atomicAdd(g.work, (unsigned long long)n);
-
-    auto issue = [&](uint32_t tile, int stage) {  // tile: index within this CTA's share
-        const uint32_t t0 = beg + tile * ES_TILE;
-        const uint32_t cnt = min((uint32_t)ES_TILE, end - t0);
-        const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;  // beg is a multiple of 4; so is the capacity
-        mbar_arrive_expect_tx(&bar[stage], ES_PLANES * bytes);
-#pragma unroll
-        for (int a = 0; a < ES_PLANES; ++a)
-            bulk_load(in + (stage * ES_PLANES + a) * ES_TILE, src[a] + t0, bytes, &bar[stage]);
-    };
-
-    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) ef[k] = efield[k];
-    uint32_t *h = hist + (uint32_t)(warp % copies) * ef_pad;
-    uint32_t *wq = queue + warp * ES_QCAP;
-    __syncthreads();
-    if (tid == 0) {
-        for (int s = 0; s < stages; ++s)
-            if ((uint32_t)s < ntiles) issue((uint32_t)s, s);
-    }
-
-    // Scatters wq[first, first + count), one collider per lane.
-    auto drain = [&](uint32_t first, uint32_t count) {
-        if (coll && lane == 0) atomicAdd(coll, (unsigned long long)count);  // collision events (measurement)
-        if ((uint32_t)lane < count) {
-            const uint32_t i = wq[first + lane];
-            const PushResult pr = push_one(sx[i], svx[i], ef, g.factor_e, g.dt_e, g);
-            const float vy = svy[i], vz = svz[i];
-            Xoshiro128p rs{rng0[i], rng1[i], rng2[i], rng3[i]};
-            const Test t = test_electron(pr.vx, vy, vz, rs, GlobalTable{sigma_tot_e}, g);  // collides, as before
-            uint32_t slot;
-            if (claim_slot(alive, g.capacity, slot)) {
-                dx_[slot] = pr.x;
-                collide_electron(slot, t.idx, pr.vx, vy, vz, rs, cs, dx_, dvx, dvy, dvz, ix, ivx, ivy, ivz, alive,
-                                 n_i, g, dens_e, dens_i);
-            } else {
-                set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
-            }
-            rng0[i] = rs.s0;
-            rng1[i] = rs.s1;
-            rng2[i] = rs.s2;
-            rng3[i] = rs.s3;
-        }
-        __syncwarp();
-    };
-
-    StepOut<U> prev;
-    bool have_prev = false;
-    uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
-    uint32_t qn = 0;            // this warp's queued colliders (warp-uniform)
+    if (g.work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(g.work, (unsigned long long)n);
+    StepIO io;
+    io.efield = efield;
+    io.sx = sx;
+    io.svx = svx;
+    io.svy = svy;
+    io.svz = svz;
+    io.dx = dx_;
+    io.dvx = dvx;
+    io.dvy = dvy;
+    io.dvz = dvz;
+    io.rng0 = rng0;
+    io.rng1 = rng1;
+    io.rng2 = rng2;
+    io.rng3 = rng3;
+    io.sigma_tot = sigma_tot_e;
+    io.cs = cs;
+    io.sigma_max = sigma_max;
+    io.factor = g.factor_e;
+    io.dt = g.dt_e;
+    io.ix = ix;
+    io.ivx = ivx;
+    io.ivy = ivy;
+    io.ivz = ivz;
+    io.alive = alive;
+    io.n_i = n_i;
+    io.dens = dens_e;
+    io.dens_i = dens_i;
+    io.wall = wall;
+    io.coll = coll;
     uint32_t it = 0;
-    for (uint32_t tile = 0; tile < ntiles; ++tile, ++it) {
-        if (it != 0 && it % epoch == 0) {  // drain the deposit copies before they can overflow
-            __syncthreads();
-            dep_drain(hist, copies, ef_pad, acc, g.n_g);
-            __syncthreads();
-        }
-        const int s = (int)(it % (uint32_t)stages);
-        const uint32_t parity = (it / (uint32_t)stages) & 1u;
-        const uint32_t r3 = it % 3u, p3 = (it + 2u) % 3u;  // buffers of this tile and of the previous one
-        // every thread waits for the stage's bulk copies itself (bounded)
-        const bool ok = mbar_wait_bounded(&bar[s], parity);
-        if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
-
-        const uint32_t t0 = beg + tile * ES_TILE;
-        const uint32_t cnt = ok ? min((uint32_t)ES_TILE, end - t0) : 0u;
-        const uint32_t *b = in + s * ES_PLANES * ES_TILE;
-        // The rows of a tile are independent; the work is split into phases
-        // over all rows so that the scheduler can interleave them.
-        StepOut<U> cur;
-        cur.keep = 0;
-        uint32_t st[U][4];     // RNG states after the test draw
-        uint32_t keep = 0, may = 0, coll = 0;  // bit u: row u survives / may collide / collides
-        // (1) push (Rust-CUDA/src/main.rs:596-620); rows past the tile's end
-        //     push a harmless stand-in and are masked
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-            const bool valid = j < cnt;
-            const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * g.gap;
-            const float v0 = valid ? __uint_as_float(b[ES_TILE + j]) : 0.0f;
-            const PushResult pr = push_one(x0, v0, ef, g.factor_e, g.dt_e, g);
-            if (valid && pr.keep) keep |= 1u << u;
-            if (wall) count_wall(wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, g.gap);
-            cur.x[u] = pr.x;
-            cur.vx[u] = pr.vx;
-        }
-        // (2) test_electron (mcc.cuh, Rust-CUDA/src/main.rs:992-1012) up to the
-        //     certain rejection, which needs no table
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-            cur.vy[u] = __uint_as_float(b[2 * ES_TILE + j]);
-            cur.vz[u] = __uint_as_float(b[3 * ES_TILE + j]);
-            Xoshiro128p rs{b[4 * ES_TILE + j], b[5 * ES_TILE + j], b[6 * ES_TILE + j], b[7 * ES_TILE + j]};
-            const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
-            const float velocity = sqrtf(v2);
-            const float rnd = rs.uniform();
-            if ((keep >> u & 1u) && may_collide(rnd, velocity, sigma_max, g.dt_e)) may |= 1u << u;
-            st[u][0] = rs.s0;
-            st[u][1] = rs.s1;
-            st[u][2] = rs.s2;
-            st[u][3] = rs.s3;
-        }
-        // (3) the exact test where the bound cannot decide (a few per cent)
-        if (may) {
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (may >> u & 1u) {
-                    const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-                    Xoshiro128p rs{b[4 * ES_TILE + j], b[5 * ES_TILE + j], b[6 * ES_TILE + j], b[7 * ES_TILE + j]};
-                    const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
-                    const float velocity = sqrtf(v2);
-                    const float rnd = rs.uniform();
-                    const uint32_t idx = energy_index(g.half_me_over_e * v2);
-                    if (collision_draw(rnd, __ldg(sigma_tot_e + idx) * velocity * g.dt_e)) coll |= 1u << u;
-                }
-            }
-        }
-        // (4) deposit every survivor; non-colliders store their RNG state and
-        //     are compacted, colliders are queued
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-            const bool kept = keep >> u & 1u;
-            const bool collide = coll >> u & 1u;
-            const bool stay = kept && !collide;
-            if (kept) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
-            if (stay) {
-                const uint32_t i = t0 + j;
-                rng0[i] = st[u][0];
-                rng1[i] = st[u][1];
-                rng2[i] = st[u][2];
-                rng3[i] = st[u][3];
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, stay);
-            cur.lane_off[u] = __popc(m & lt);
-            if (stay) cur.keep |= 1u << u;
-            if (lane == 0) offs[r3][u * ES_WARPS + warp] = __popc(m);
-            const unsigned cm = __ballot_sync(0xffffffffu, collide);
-            if (collide) wq[qn + __popc(cm & lt)] = t0 + j;
-            qn += __popc(cm);
-        }
-        // publish the previous tile's base (its atomic had this iteration to return)
-        if (have_prev && warp == 0 && lane == 31) s_base[p3] = pending_base;
-        // the one block barrier of a tile: counts and previous base visible,
-        // stage s consumed; a timeout anywhere ends the loop of every thread
-        if (__syncthreads_or(!ok)) break;
-        if (tid == 0) {
-            const uint32_t next = tile + (uint32_t)stages;
-            if (next < ntiles) issue(next, s);
-        }
-        if (have_prev) {
-            const uint32_t base = s_base[p3];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (prev.keep & (1u << u)) {
-                    const uint32_t slot = base + offs[p3][u * ES_WARPS + warp] + prev.lane_off[u];
-                    if (slot < g.capacity) {
-                        dx_[slot] = prev.x[u];
-                        dvx[slot] = prev.vx[u];
-                        dvy[slot] = prev.vy[u];
-                        dvz[slot] = prev.vz[u];
-                    } else {
-                        set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
-                    }
-                }
-            }
-        }
-        if (warp == 0) {
-            const uint32_t v = lane < NSEG ? offs[r3][lane] : 0u;
-            uint32_t incl = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            if (lane < NSEG) offs[r3][lane] = incl - v;
-            if (lane == 31) pending_base = incl ? atomicAdd(alive, incl) : 0u;
-        }
-        prev = cur;
-        have_prev = true;
-        while (qn >= 32) {  // full-warp drains from the top of the queue
-            qn -= 32;
-            drain(qn, 32);
-        }
-    }
-    const uint32_t pl = (it + 2u) % 3u;  // buffers of the last tile with survivors held in registers
-    if (have_prev && warp == 0 && lane == 31) s_base[pl] = pending_base;
-    __syncthreads();
-    if (have_prev) {
-        const uint32_t base = s_base[pl];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (prev.keep & (1u << u)) {
-                const uint32_t slot = base + offs[pl][u * ES_WARPS + warp] + prev.lane_off[u];
-                if (slot < g.capacity) {
-                    dx_[slot] = prev.x[u];
-                    dvx[slot] = prev.vx[u];
-                    dvy[slot] = prev.vy[u];
-                    dvz[slot] = prev.vz[u];
-                } else {
-                    set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
-                }
-            }
-        }
-    }
-    if (qn) drain(0, qn);
-    __syncthreads();
-    dep_drain(hist, copies, ef_pad, acc, g.n_g);
-    __syncthreads();
-    dep_flush(acc, dens_e, g);
+    step_segment<U, true>(io, g, beg, end, sm, stages, copies, ef_pad, epoch, it);
     publish_count(link.ticket, link.dst, link.src, link.clear_src, g.capacity);
 }
 
@@ -359,15 +126,11 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
                            const uint32_t *n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                            const cudapic_grid &g, cudaStream_t stream, const StepLink &link,
                            cudapic_wall_counters *wall, unsigned long long *coll, const cudapic_tuning &t) {
-    constexpr int ES_TILE = StepShape<U>::TILE;
-    constexpr int ES_QCAP = StepShape<U>::QCAP;
+    constexpr int ES_TILE = StepShape<U, true>::TILE;
     int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
     int copies = std::max(1, std::min(t.density_copies, ES_WARPS));
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
-    auto bytes = [&]() {
-        return (size_t)stages * ES_PLANES * ES_TILE * 4 + (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 +
-               (size_t)ES_WARPS * ES_QCAP * 4 + (size_t)stages * sizeof(uint64_t);
-    };
+    auto bytes = [&]() { return step_smem_bytes<U, true>(stages, copies, ef_pad); };
     const size_t budget = (size_t)max_smem_optin();
     while (bytes() > budget && stages > 2) --stages;
     while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;

@@ -26,74 +26,38 @@
 #include <vector>
 
 #include "internal.h"
+#include "state_impl.h"
 
 using namespace cudapic;
 
-struct cudapic_state {
-    int device = 0;
-    cudapic_params params{};
-    cudapic_grid grid{};
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
+namespace cudapic {
 
-    // [species][side]
-    float *x[2][2] = {}, *vx[2][2] = {}, *vy[2][2] = {}, *vz[2][2] = {};
-    int side[2] = {0, 0};
-    uint32_t *rng[2][4] = {};
-    // counters block: n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work (u64 at +32)
-    uint32_t *counters = nullptr;
-    float *efield = nullptr, *pot = nullptr, *pot0_table = nullptr;
-    // Charge densities, double-buffered for the fused step: [cur] feeds the
-    // Poisson solve, [cur ^ 1] accumulates the next step's (electrons) or
-    // the next ion step's (ions) deposits.
-    float *e_dens[2] = {}, *i_dens[2] = {};
-    int e_cur = 0, i_cur = 0;
-    bool fused = true;        // deposit inside push / collisions (default)
-    bool overlap = true;      // programmatic dependent launch between the step's kernels (default)
-    bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
-    int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
-    float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
-    float sigma_max_e = 0.0f;  // largest entry of sigma_tot_e (the fused step's certain-rejection bound)
-    double *cumul_e = nullptr, *cumul_i = nullptr;
-    cudapic_wall_counters *wall = nullptr;  // [0] electrons, [1] ions (measurement window)
-    // measurement window: [0] electron and [1] ion collision events, [2] EEPF
-    // electrons sampled; esum: their energies [eV]; measure_steps on the host
-    unsigned long long *mcount = nullptr;
-    double *esum = nullptr;
-    uint64_t measure_steps = 0;
-    double max_e_coll_freq = 0.0, max_i_coll_freq = 0.0;  // of the tables [1/s]
-    uint32_t *eepf = nullptr;
+int state_prime_fused(cudapic_state *s, cudaStream_t st) {
+    const cudapic_grid &g = s->grid;
+    const size_t nb = g.n_g * sizeof(float);
+    const int E = 0, I = 1;
+    // the reference's deposit of the current positions (Rust-CUDA/src/main.rs:1729-1739)
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density(), 0, nb, st), "memset e_density"));
+    CUDAPIC_CHECK(cudapic_get_density(s->x[E][s->side[E]], s->e_density(), s->n_e(), &g, (cudapic_stream_t)st));
+    // the published-count kernels expect their slot counters and ticket at zero
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive_i(), 0, 2 * sizeof(uint32_t), st), "memset alive_i"));
+    // both ion buffers hold the density of the present ions
+    CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_dens[s->i_cur], 0, nb, st), "memset i_density"));
+    CUDAPIC_CHECK(cudapic_get_density(s->x[I][s->side[I]], s->i_dens[s->i_cur], s->n_i(), &g, (cudapic_stream_t)st));
+    CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->i_dens[s->i_cur ^ 1], s->i_dens[s->i_cur], nb,
+                                             cudaMemcpyDeviceToDevice, st), "copy i_density"));
+    s->dens_valid = true;
+    return CUDAPIC_OK;
+}
 
-    bool measure = false;
-    uint64_t steps_done = 0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
-    bool graphs_enabled = true;
-    std::vector<void *> allocations;
+bool state_is_ion_step(const cudapic_state *s, uint64_t step) {
+    return ((step % s->params.n_t) % s->params.n_sub) == 0;
+}
 
-    uint32_t *n_e() const { return counters + 0; }
-    uint32_t *n_i() const { return counters + 1; }
-    uint32_t *alive() const { return counters + 2; }
-    uint32_t *step_counter() const { return counters + 3; }
-    uint32_t *dev_err() const { return counters + 4; }
-    uint32_t *alive_i() const { return counters + 5; }  // fused mode: ion push slot counter
-    uint32_t *ticket() const { return counters + 6; }   // fused mode: CTA completion ticket (StepLink)
-    unsigned long long *work() const { return reinterpret_cast<unsigned long long *>(counters + 8); }
-    float *e_density() const { return e_dens[e_cur]; }
-    float *i_density() const { return i_dens[i_cur]; }
-};
+}  // namespace cudapic
 
 namespace {
-
-struct DeviceGuard {
-    int prev = 0;
-    bool ok = false;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(dev) == cudaSuccess) ok = true;
-    }
-    ~DeviceGuard() {
-        if (ok) cudaSetDevice(prev);
-    }
-};
 
 template <typename T>
 int dalloc(cudapic_state *s, T **p, size_t count) {
@@ -178,20 +142,13 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     const bool fused = s->fused;
     float *e_next = nullptr, *i_acc = nullptr, *zero_b = nullptr;
 
-    if (!fused || !s->dens_valid) {
+    if (fused && !s->dens_valid) {
+        CUDAPIC_CHECK(state_prime_fused(s, st));
+    } else if (!fused) {
         // the reference's deposit of the current positions (Rust-CUDA/src/main.rs:1729-1739)
         CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->e_density(), 0, nb, st), "memset e_density"));
         CUDAPIC_CHECK(cudapic_get_density(s->x[E][se], s->e_density(), s->n_e(), &g, (cudapic_stream_t)st));
-        if (fused) {  // priming: both ion buffers hold the density of the present ions
-            // the published-count kernels expect their slot counters and ticket at zero
-            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive(), 0, sizeof(uint32_t), st), "memset alive"));
-            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->alive_i(), 0, 2 * sizeof(uint32_t), st), "memset alive_i"));
-            CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_dens[s->i_cur], 0, nb, st), "memset i_density"));
-            CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_dens[s->i_cur], s->n_i(), &g, (cudapic_stream_t)st));
-            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(s->i_dens[s->i_cur ^ 1], s->i_dens[s->i_cur], nb,
-                                                     cudaMemcpyDeviceToDevice, st), "copy i_density"));
-            s->dens_valid = true;
-        } else if (ion_step) {
+        if (ion_step) {
             CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->i_density(), 0, nb, st), "memset i_density"));
             CUDAPIC_CHECK(cudapic_get_density(s->x[I][si], s->i_density(), s->n_i(), &g, (cudapic_stream_t)st));
         }
@@ -260,9 +217,7 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     return CUDAPIC_OK;
 }
 
-bool is_ion_step(const cudapic_state *s, uint64_t step) {
-    return ((step % s->params.n_t) % s->params.n_sub) == 0;
-}
+bool is_ion_step(const cudapic_state *s, uint64_t step) { return state_is_ion_step(s, step); }
 
 // Graph period: 2 * N_SUB steps returns both species to their starting
 // side; requires N_T % N_SUB == 0 so that the ion-step pattern repeats.
@@ -609,6 +564,15 @@ extern "C" int cudapic_state_set_fused(cudapic_state *s, int on) {
     s->fused = on != 0;
     s->dens_valid = false;
     destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_set_graphs(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_graphs: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_graphs sync"));
+    destroy_graphs(s);
+    s->graphs_enabled = on != 0 && (s->params.n_t % s->params.n_sub) == 0;
     return CUDAPIC_OK;
 }
 

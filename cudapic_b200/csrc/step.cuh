@@ -1,0 +1,387 @@
+// step.cuh -- the tile pipeline of the fused particle steps, shared by the
+// one-discharge kernel (kernels_step.cu) and the batched kernels
+// (kernels_batch.cu).
+//
+// A segment is a contiguous range [beg, end) of one species of one
+// discharge.  step_segment<U, MCC> streams its SoA planes through shared
+// memory with cp.async.bulk on an mbarrier ring, pushes every particle
+// (Rust-CUDA/src/main.rs:596-620), compacts the survivors into the other
+// side (ballots, one warp scan and one atomicAdd per tile, :566-678) and
+// deposits them into the next density in 2^-20 fixed point (push.cuh).
+// With MCC (electrons) it also runs the collision test and the scattering
+// (check_collisions_e / collision_e, :971-1165) with the RNG stream of each
+// particle's source slot; without (ions) it is the ion push of the driver.
+#pragma once
+#include "common.cuh"
+#include "mcc.cuh"
+#include "push.cuh"
+#include "tma.cuh"
+
+namespace cudapic {
+
+constexpr int ES_THREADS = 256;
+constexpr int ES_WARPS = ES_THREADS / 32;
+constexpr int ES_MAX_STAGES = 6;  // pipeline depth: cudapic_tuning.step_stages
+
+// U (cudapic_tuning.step_rows, 2 or 4): particles per thread and tile, so a
+// tile holds 256 U particles; a warp's collider queue holds 31 + 32 U
+// entries at most.  Planes: x, vx, vy, vz (+ rng0..3 with MCC).
+template <int U, bool MCC>
+struct StepShape {
+    static constexpr int TILE = ES_THREADS * U;
+    static constexpr int PLANES = MCC ? 8 : 4;
+    static constexpr int QCAP = MCC ? 32 + 32 * U : 0;
+    static constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
+    static_assert(U * ES_WARPS <= 32, "one warp scans the (row, warp) counts");
+};
+
+// Dynamic shared memory: [stages][PLANES][TILE] staged planes, E[ef_pad],
+// the 64-bit deposit accumulator [ef_pad], [copies][ef_pad] fixed-point
+// histograms, the warps' collider queues, the stage mbarriers.
+template <int U, bool MCC>
+__host__ __device__ constexpr size_t step_smem_bytes(int stages, int copies, uint32_t ef_pad) {
+    using S = StepShape<U, MCC>;
+    return (size_t)stages * S::PLANES * S::TILE * 4 + (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 +
+           (size_t)ES_WARPS * S::QCAP * 4 + (size_t)stages * sizeof(uint64_t);
+}
+
+// Buffers of one segment.
+struct StepIO {
+    const float *efield;
+    const float *sx, *svx, *svy, *svz;        // source side
+    float *dx, *dvx, *dvy, *dvz;              // destination side
+    uint32_t *rng0, *rng1, *rng2, *rng3;      // MCC: RNG planes (by source slot)
+    const float *sigma_tot, *cs;              // MCC: total and per-process cross sections
+    float sigma_max;                          // MCC: largest entry of sigma_tot
+    float factor, dt;                         // push constants of the species
+    float *ix, *ivx, *ivy, *ivz;              // MCC: ion side receiving ionization spawns
+    uint32_t *alive;                          // destination slot counter
+    uint32_t *n_i;                            // MCC: ion count (spawn slots)
+    float *dens;                              // next density of the species (survivors)
+    float *dens_i;                            // MCC: next ion density (spawned ions)
+    cudapic_wall_counters *wall;              // absorbed particles (may be null)
+    unsigned long long *coll;                 // MCC: collision events (may be null)
+};
+
+template <int U, bool MCC>
+struct StepSmem {
+    uint32_t *in;
+    float *ef;
+    unsigned long long *acc;
+    uint32_t *hist;
+    uint32_t *queue;
+    uint64_t *bar;
+    uint32_t (*offs)[StepShape<U, MCC>::NSEG];  // [3][NSEG]
+    uint32_t *s_base;                            // [3]
+
+    __device__ __forceinline__ StepSmem(unsigned char *smem, int stages, int copies, uint32_t ef_pad,
+                                        uint32_t (*offs_)[StepShape<U, MCC>::NSEG], uint32_t *s_base_) {
+        using S = StepShape<U, MCC>;
+        in = reinterpret_cast<uint32_t *>(smem);
+        ef = reinterpret_cast<float *>(in + stages * S::PLANES * S::TILE);
+        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);
+        hist = reinterpret_cast<uint32_t *>(acc + ef_pad);
+        queue = hist + (uint32_t)copies * ef_pad;
+        bar = reinterpret_cast<uint64_t *>(queue + ES_WARPS * S::QCAP);
+        offs = offs_;
+        s_base = s_base_;
+    }
+    // end of the carved region (the batched kernels put their plan there)
+    __device__ __forceinline__ unsigned char *end(int stages) const {
+        return reinterpret_cast<unsigned char *>(bar + stages);
+    }
+};
+
+// Survivors of one tile held in registers until their base is known.
+template <int U>
+struct StepOut {
+    float x[U], vx[U], vy[U], vz[U];
+    uint32_t lane_off[U];
+    uint32_t keep;  // bit u: the particle of row u is written by the tile
+};
+
+// True unless u certainly exceeds the collision probability at speed
+// `velocity` (same operation order as test_electron): the exact test
+// decides "no collision" whenever u >= fl(a + 5e-7), a = fl(fl(sigma(E) |v|)
+// dt); rounding is monotone, so with sigma_max the largest table entry
+// u >= fl(fl(fl(sigma_max |v|) dt) + 5e-7) implies it.
+__device__ __forceinline__ bool may_collide(float u, float velocity, float sigma_max, float dt) {
+    return u < sigma_max * velocity * dt + 5e-7f;
+}
+
+// Initialises the stage mbarriers (thread 0) and clears the deposit
+// accumulators; the caller synchronises before the first segment.
+template <int U, bool MCC>
+__device__ __forceinline__ void step_smem_init(const StepSmem<U, MCC> &sm, int stages, int copies, uint32_t ef_pad) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) mbar_init(&sm.bar[s], 1);
+        fence_mbar_init();
+    }
+    for (uint32_t k = threadIdx.x; k < (uint32_t)copies * ef_pad; k += ES_THREADS) sm.hist[k] = 0u;
+    for (uint32_t k = threadIdx.x; k < ef_pad; k += ES_THREADS) sm.acc[k] = 0ull;
+}
+
+// Processes the particles [beg, end) of one species of one discharge.  On
+// entry the histograms and the accumulator are zero; on return they are
+// zero again (drained, the accumulator flushed into io.dens and cleared).
+// `it` counts the tiles this CTA has run through the stage ring (it selects
+// the stage and its mbarrier phase) and is advanced by the segment's tiles.
+// Returns false when a stage wait timed out (CUDAPIC_DEVERR_TIMEOUT set);
+// the survivors held so far are still written and the deposits flushed.
+template <int U, bool MCC>
+__device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_grid &g, uint32_t beg, uint32_t end,
+                                             const StepSmem<U, MCC> &sm, int stages, int copies, uint32_t ef_pad,
+                                             uint32_t epoch, uint32_t &it) {
+    using S = StepShape<U, MCC>;
+    constexpr int TILE = S::TILE;
+    constexpr int PLANES = S::PLANES;
+    constexpr int QCAP = S::QCAP;
+    constexpr int NSEG = S::NSEG;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const unsigned lt = lanemask_lt();
+    const uint32_t it0 = it;
+    const uint32_t ntiles = (end - beg + TILE - 1) / TILE;  // this segment's tiles
+
+    auto issue = [&](uint32_t tile, int stage) {  // tile: index within the segment
+        const uint32_t t0 = beg + tile * TILE;
+        const uint32_t cnt = min((uint32_t)TILE, end - t0);
+        const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;  // beg is a multiple of 4; so is the capacity
+        mbar_arrive_expect_tx(&sm.bar[stage], PLANES * bytes);
+        bulk_load(sm.in + (stage * PLANES + 0) * TILE, io.sx + t0, bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 1) * TILE, io.svx + t0, bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 2) * TILE, io.svy + t0, bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 3) * TILE, io.svz + t0, bytes, &sm.bar[stage]);
+        if (MCC) {
+            bulk_load(sm.in + (stage * PLANES + 4) * TILE, io.rng0 + t0, bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 5) * TILE, io.rng1 + t0, bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 6) * TILE, io.rng2 + t0, bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 7) * TILE, io.rng3 + t0, bytes, &sm.bar[stage]);
+        }
+    };
+
+    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.ef[k] = io.efield[k];
+    uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
+    uint32_t *wq = sm.queue + warp * QCAP;
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s)
+            if ((uint32_t)s < ntiles) issue((uint32_t)s, (int)((it0 + (uint32_t)s) % (uint32_t)stages));
+    }
+
+    // Scatters wq[first, first + count), one collider per lane.
+    auto drain = [&](uint32_t first, uint32_t count) {
+        if (io.coll && lane == 0) atomicAdd(io.coll, (unsigned long long)count);  // collision events (measurement)
+        if ((uint32_t)lane < count) {
+            const uint32_t i = wq[first + lane];
+            const PushResult pr = push_one(io.sx[i], io.svx[i], sm.ef, io.factor, io.dt, g);
+            const float vy = io.svy[i], vz = io.svz[i];
+            Xoshiro128p rs{io.rng0[i], io.rng1[i], io.rng2[i], io.rng3[i]};
+            const Test t = test_electron(pr.vx, vy, vz, rs, GlobalTable{io.sigma_tot}, g);  // collides, as before
+            uint32_t slot;
+            if (claim_slot(io.alive, g.capacity, slot)) {
+                io.dx[slot] = pr.x;
+                collide_electron(slot, t.idx, pr.vx, vy, vz, rs, io.cs, io.dx, io.dvx, io.dvy, io.dvz, io.ix, io.ivx,
+                                 io.ivy, io.ivz, io.alive, io.n_i, g, io.dens, io.dens_i);
+            } else {
+                set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
+            }
+            io.rng0[i] = rs.s0;
+            io.rng1[i] = rs.s1;
+            io.rng2[i] = rs.s2;
+            io.rng3[i] = rs.s3;
+        }
+        __syncwarp();
+    };
+
+    StepOut<U> prev;
+    bool have_prev = false;
+    bool ok = true;
+    uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
+    uint32_t qn = 0;            // this warp's queued colliders (warp-uniform)
+    uint32_t tile = 0;
+    for (; tile < ntiles; ++tile) {
+        const uint32_t k = it0 + tile;  // position in the stage ring
+        if (tile != 0 && k % epoch == 0) {  // drain the deposit copies before they can overflow
+            __syncthreads();
+            dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
+            __syncthreads();
+        }
+        const int s = (int)(k % (uint32_t)stages);
+        const uint32_t parity = (k / (uint32_t)stages) & 1u;
+        const uint32_t r3 = k % 3u, p3 = (k + 2u) % 3u;  // buffers of this tile and of the previous one
+        // every thread waits for the stage's bulk copies itself (bounded)
+        ok = mbar_wait_bounded(&sm.bar[s], parity);
+        if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
+
+        const uint32_t t0 = beg + tile * TILE;
+        const uint32_t cnt = ok ? min((uint32_t)TILE, end - t0) : 0u;
+        const uint32_t *b = sm.in + s * PLANES * TILE;
+        // The rows of a tile are independent; the work is split into phases
+        // over all rows so that the scheduler can interleave them.
+        StepOut<U> cur;
+        cur.keep = 0;
+        uint32_t st[U][4];     // MCC: RNG states after the test draw
+        uint32_t keep = 0, may = 0, coll = 0;  // bit u: row u survives / may collide / collides
+        // (1) push (Rust-CUDA/src/main.rs:596-620); rows past the tile's end
+        //     push a harmless stand-in and are masked
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+            const bool valid = j < cnt;
+            const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * g.gap;
+            const float v0 = valid ? __uint_as_float(b[TILE + j]) : 0.0f;
+            const PushResult pr = push_one(x0, v0, sm.ef, io.factor, io.dt, g);
+            if (valid && pr.keep) keep |= 1u << u;
+            cur.x[u] = pr.x;
+            cur.vx[u] = pr.vx;
+            if (!MCC) {
+                cur.vy[u] = __uint_as_float(b[2 * TILE + j]);
+                cur.vz[u] = __uint_as_float(b[3 * TILE + j]);
+                if (io.wall) count_wall(io.wall, true, valid && !pr.keep, pr.x, pr.vx, cur.vy[u], cur.vz[u], g.gap);
+            } else if (io.wall) {
+                count_wall(io.wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, g.gap);
+            }
+        }
+        if (MCC) {
+            // (2) test_electron (mcc.cuh, Rust-CUDA/src/main.rs:992-1012) up to
+            //     the certain rejection, which needs no table
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+                cur.vy[u] = __uint_as_float(b[2 * TILE + j]);
+                cur.vz[u] = __uint_as_float(b[3 * TILE + j]);
+                Xoshiro128p rs{b[4 * TILE + j], b[5 * TILE + j], b[6 * TILE + j], b[7 * TILE + j]};
+                const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
+                const float velocity = sqrtf(v2);
+                const float rnd = rs.uniform();
+                if ((keep >> u & 1u) && may_collide(rnd, velocity, io.sigma_max, io.dt)) may |= 1u << u;
+                st[u][0] = rs.s0;
+                st[u][1] = rs.s1;
+                st[u][2] = rs.s2;
+                st[u][3] = rs.s3;
+            }
+            // (3) the exact test where the bound cannot decide (a few per cent)
+            if (may) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (may >> u & 1u) {
+                        const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+                        Xoshiro128p rs{b[4 * TILE + j], b[5 * TILE + j], b[6 * TILE + j], b[7 * TILE + j]};
+                        const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
+                        const float velocity = sqrtf(v2);
+                        const float rnd = rs.uniform();
+                        const uint32_t idx = energy_index(g.half_me_over_e * v2);
+                        if (collision_draw(rnd, __ldg(io.sigma_tot + idx) * velocity * io.dt)) coll |= 1u << u;
+                    }
+                }
+            }
+        }
+        // (4) deposit every survivor; non-colliders (MCC: store their RNG
+        //     state) are compacted, colliders are queued
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = (uint32_t)u * ES_THREADS + tid;
+            const bool kept = keep >> u & 1u;
+            const bool collide = MCC && (coll >> u & 1u);
+            const bool stay = kept && !collide;
+            if (kept) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            if (MCC && stay) {
+                const uint32_t i = t0 + j;
+                io.rng0[i] = st[u][0];
+                io.rng1[i] = st[u][1];
+                io.rng2[i] = st[u][2];
+                io.rng3[i] = st[u][3];
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, stay);
+            cur.lane_off[u] = __popc(m & lt);
+            if (stay) cur.keep |= 1u << u;
+            if (lane == 0) sm.offs[r3][u * ES_WARPS + warp] = __popc(m);
+            if (MCC) {
+                const unsigned cm = __ballot_sync(0xffffffffu, collide);
+                if (collide) wq[qn + __popc(cm & lt)] = t0 + j;
+                qn += __popc(cm);
+            }
+        }
+        // publish the previous tile's base (its atomic had this iteration to return)
+        if (have_prev && warp == 0 && lane == 31) sm.s_base[p3] = pending_base;
+        // the one block barrier of a tile: counts and previous base visible,
+        // stage s consumed; a timeout anywhere ends the loop of every thread
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) {
+            const uint32_t next = tile + (uint32_t)stages;
+            if (next < ntiles) issue(next, s);
+        }
+        if (have_prev) {
+            const uint32_t base = sm.s_base[p3];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (prev.keep & (1u << u)) {
+                    const uint32_t slot = base + sm.offs[p3][u * ES_WARPS + warp] + prev.lane_off[u];
+                    if (slot < g.capacity) {
+                        io.dx[slot] = prev.x[u];
+                        io.dvx[slot] = prev.vx[u];
+                        io.dvy[slot] = prev.vy[u];
+                        io.dvz[slot] = prev.vz[u];
+                    } else {
+                        set_dev_err(g.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
+                    }
+                }
+            }
+        }
+        if (warp == 0) {
+            const uint32_t v = lane < NSEG ? sm.offs[r3][lane] : 0u;
+            uint32_t incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane < NSEG) sm.offs[r3][lane] = incl - v;
+            if (lane == 31) pending_base = incl ? atomicAdd(io.alive, incl) : 0u;
+        }
+        prev = cur;
+        have_prev = true;
+        if (MCC) {
+            while (qn >= 32) {  // full-warp drains from the top of the queue
+                qn -= 32;
+                drain(qn, 32);
+            }
+        }
+    }
+    const uint32_t pl = (it0 + tile + 2u) % 3u;  // buffers of the last tile with survivors held in registers
+    if (have_prev && warp == 0 && lane == 31) sm.s_base[pl] = pending_base;
+    __syncthreads();
+    if (have_prev) {
+        const uint32_t base = sm.s_base[pl];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (prev.keep & (1u << u)) {
+                const uint32_t slot = base + sm.offs[pl][u * ES_WARPS + warp] + prev.lane_off[u];
+                if (slot < g.capacity) {
+                    io.dx[slot] = prev.x[u];
+                    io.dvx[slot] = prev.vx[u];
+                    io.dvy[slot] = prev.vy[u];
+                    io.dvz[slot] = prev.vz[u];
+                } else {
+                    set_dev_err(g.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
+                }
+            }
+        }
+    }
+    if (MCC && qn) drain(0, qn);
+    __syncthreads();
+    dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
+    __syncthreads();
+    dep_flush(sm.acc, io.dens, g);
+    // the thread that flushed a node clears it (same node ownership as dep_flush)
+    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.acc[k] = 0ull;
+    it = it0 + tile;
+    return ok;
+}
+
+}  // namespace cudapic

@@ -139,6 +139,10 @@ class GpuSimState:
         launch sequence."""
         check(lib.cudapic_state_set_fused(self._h, 1 if on else 0))
 
+    def set_graphs(self, on=True):
+        """Replay captured CUDA graphs (default) or launch every step from the host."""
+        check(lib.cudapic_state_set_graphs(self._h, 1 if on else 0))
+
     def set_overlap(self, on=True):
         """Programmatic dependent launch between the step's kernels (default on)."""
         check(lib.cudapic_state_set_overlap(self._h, 1 if on else 0))
@@ -209,3 +213,47 @@ class GpuSimState:
 
     def synchronize(self):
         check(lib.cudapic_state_synchronize(self._h))
+
+
+class GpuBatch:
+    """Discharges (GpuSimState objects on one device) stepped in lockstep:
+    every kernel of a step is one launch over all of them
+    (cudapic_batch_*).  The states keep their buffers and API; close the
+    batch before the states."""
+
+    def __init__(self, states):
+        self.states = list(states)
+        arr = (C.c_void_p * len(self.states))(*[st.handle for st in self.states])
+        h = C.c_void_p()
+        check(lib.cudapic_batch_create(arr, len(self.states), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.cudapic_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self):
+        return lib.cudapic_batch_stream(self._h) or 0
+
+    def run_steps(self, n_steps):
+        check(lib.cudapic_batch_run_steps(self._h, int(n_steps)))
+
+    def run_cycles(self, n_cycles):
+        self.run_steps(int(n_cycles) * self.states[0].params.n_t)
+
+    def synchronize(self):
+        check(lib.cudapic_batch_synchronize(self._h))

@@ -439,6 +439,10 @@ int cudapic_state_set_fused(cudapic_state *s, int on);
  * tail (every kernel waits for its predecessor before touching global data).
  * off: plain stream order.  The captured graphs are rebuilt. */
 int cudapic_state_set_overlap(cudapic_state *s, int on);
+/* on (default when N_T is a multiple of N_SUB): run_steps replays captured
+ * CUDA graphs of 2 N_SUB steps.  off: every step is launched from the host,
+ * as the reference's driver does (Rust-CUDA/src/main.rs:1725-1808). */
+int cudapic_state_set_graphs(cudapic_state *s, int on);
 /* Reads the counters (synchronises the state's stream). */
 int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i);
 /* Reads and returns the device error word (synchronises). */
@@ -492,6 +496,29 @@ int cudapic_state_save(cudapic_state *s, const char *path);
  * restores the RNG planes from `path`.rng, or seeds the reference's master
  * streams when there is none (a file written by eduPIC).  Synchronises. */
 int cudapic_state_load(cudapic_state *s, const char *path);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent discharges stepped in lockstep: every kernel of a step
+ * is ONE launch over all discharges of the batch (persistent grids over the
+ * discharges' concatenated particles, per-discharge descriptors, counters
+ * and tickets), 2 N_SUB steps per captured CUDA graph.  The reference runs
+ * one discharge per process and has no counterpart; this serves parameter
+ * sweeps of many small discharges, which alone leave most SMs idle.
+ *
+ * The discharges are existing states (fused mode, one device, equal N_T and
+ * N_SUB and Poisson arithmetic flag, all at the same step, all measuring or
+ * none); they keep their buffers and every state call keeps working between
+ * batch runs.  A batch does not own its states: destroy it before them.
+ * At most 1024 discharges, capacities summing to at most 2^31. */
+typedef struct cudapic_batch cudapic_batch;
+int cudapic_batch_create(cudapic_state *const *states, uint32_t count, cudapic_batch **out);
+int cudapic_batch_destroy(cudapic_batch *b);
+/* Enqueues n_steps of every discharge on the batch's stream, after the
+ * work pending on each state's stream; each state's stream then waits for
+ * the batch.  Asynchronous. */
+int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps);
+int cudapic_batch_synchronize(cudapic_batch *b);
+cudapic_stream_t cudapic_batch_stream(const cudapic_batch *b);
 
 #ifdef __cplusplus
 }

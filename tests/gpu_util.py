@@ -18,6 +18,17 @@ def host(t):
     return a.view(np.uint32) if a.dtype == np.int32 else a
 
 
+def device_array(ptr, n, dtype):
+    """Copies n elements at a device address (a library buffer) to the host;
+    the caller has synchronised the stream that wrote them."""
+    from cuda.bindings import runtime as rt
+    out = np.empty(n, dtype)
+    if n:
+        err = rt.cudaMemcpy(out.ctypes.data, int(ptr), out.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)[0]
+        assert err == rt.cudaError_t.cudaSuccess, err
+    return out
+
+
 def counter(v):
     return dev(np.array([v], np.uint32))
 
