@@ -8,12 +8,16 @@
 // [EEPF] -- for every discharge of the batch in one launch each
 // (kernels_batch.cu), in one captured graph of 2 N_SUB steps.
 //
-// The discharges stay cudapic_state objects: their buffers, counters,
-// tables and measurements are used in place, and every state API call keeps
-// working between batch runs.  The batch records each state's buffer
-// orientation when it builds its descriptors; a run checks that nothing else
-// moved a state since (else it rebuilds them) and afterwards stores the
-// states' new sides, step counts and measurement windows.
+// The discharges stay cudapic_state objects.  While a batch exists their
+// particle planes (both sides of both species and the RNG planes) live in
+// one pool owned by the batch, each discharge at an element offset, so the
+// kernels take the plane bases as launch parameters; the states point into
+// the pool, and every state call keeps working between batch runs.  The
+// pool's side 0 / 1 are the same roles for every discharge; a state moved
+// on its own is brought back to the batch's side by a copy.  Destroying the
+// batch gives every state its own planes back.  Each state's densities,
+// counters, tables and measurements are used in place through a
+// per-discharge descriptor, rebuilt when a state's density roles moved.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,17 +40,22 @@ struct cudapic_batch {
     cudaEvent_t done = nullptr;
     BatchDisc *desc = nullptr;
     uint32_t *counts = nullptr;      // [2][D] written by the batched Poisson solve
+    float *pool = nullptr;           // POOL_PLANES x pool_len elements
+    uint64_t pool_len = 0;
+    std::vector<uint32_t> off;       // element offset of each discharge
+    uint32_t pooled = 0;             // states [0, pooled) point into the pool
     uint32_t max_n_g = 0, flags = 0;
     uint64_t cap_sum = 0;
     bool built = false;
-    // orientation of each state at the build: e side, i side, e_cur, i_cur
-    std::vector<std::array<int, 4>> origin;
-    // roles relative to the build (the same for every discharge)
-    int se = 0, si = 0, ecur = 0, icur = 0;
+    // density roles of each state at the build: e_cur, i_cur
+    std::vector<std::array<int, 2>> origin;
+    int se = 0, si = 0;              // pool sides of the electrons and ions (absolute)
+    int ecur = 0, icur = 0;          // density roles relative to the build
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};
 
     uint32_t count() const { return (uint32_t)states.size(); }
+    float *plane(int p) const { return pool + (uint64_t)p * pool_len; }
 };
 
 namespace {
@@ -58,14 +67,83 @@ void destroy_graphs(cudapic_batch *b) {
     }
 }
 
-bool oriented(const cudapic_batch *b, uint32_t k) {
-    const cudapic_state *s = b->states[k];
-    const auto &o = b->origin[k];
-    return s->side[0] == (o[0] ^ b->se) && s->side[1] == (o[1] ^ b->si) && s->e_cur == (o[2] ^ b->ecur) &&
-           s->i_cur == (o[3] ^ b->icur);
+// Points a state's particle planes at planes[0..23] (pool order: its range
+// of the pool, or its own buffers again).
+void point_state(cudapic_state *s, float *const *planes) {
+    for (int sp = 0; sp < 2; ++sp) {
+        for (int side = 0; side < 2; ++side) {
+            s->x[sp][side] = planes[pool_plane(sp, side, 0)];
+            s->vx[sp][side] = planes[pool_plane(sp, side, 1)];
+            s->vy[sp][side] = planes[pool_plane(sp, side, 2)];
+            s->vz[sp][side] = planes[pool_plane(sp, side, 3)];
+        }
+        for (int k = 0; k < 4; ++k) s->rng[sp][k] = reinterpret_cast<uint32_t *>(planes[pool_rng_plane(sp, k)]);
+    }
+    state_drop_graphs(s);
 }
 
-// Descriptors of the states as they are oriented now; roles back to zero.
+// The state's 24 planes in pool order (pool side j = the state's side
+// side[sp] ^ j, so the live side lands on pool side 0).
+void state_planes(const cudapic_state *s, float *out[POOL_PLANES]) {
+    for (int sp = 0; sp < 2; ++sp) {
+        for (int j = 0; j < 2; ++j) {
+            const int a = s->side[sp] ^ j;
+            out[pool_plane(sp, j, 0)] = s->x[sp][a];
+            out[pool_plane(sp, j, 1)] = s->vx[sp][a];
+            out[pool_plane(sp, j, 2)] = s->vy[sp][a];
+            out[pool_plane(sp, j, 3)] = s->vz[sp][a];
+        }
+        for (int k = 0; k < 4; ++k) out[pool_rng_plane(sp, k)] = reinterpret_cast<float *>(s->rng[sp][k]);
+    }
+}
+
+// Moves every state's planes into the pool (live side to pool side 0).
+int pool_states(cudapic_batch *b) {
+    for (uint32_t k = 0; k < b->count(); ++k) {
+        cudapic_state *s = b->states[k];
+        const size_t bytes = (size_t)s->params.capacity * sizeof(float);
+        CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "batch: state sync"));
+        float *from[POOL_PLANES], *to[POOL_PLANES];
+        state_planes(s, from);
+        for (int p = 0; p < POOL_PLANES; ++p) {
+            to[p] = b->plane(p) + b->off[k];
+            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(to[p], from[p], bytes, cudaMemcpyDeviceToDevice, b->stream),
+                                     "batch: pool copy"));
+        }
+        CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(b->stream), "batch: pool sync"));
+        for (int p = 0; p < POOL_PLANES; ++p) state_release(s, from[p]);
+        point_state(s, to);
+        s->side[0] = s->side[1] = 0;
+        s->batch = b;
+        b->pooled = k + 1;
+    }
+    return CUDAPIC_OK;
+}
+
+// Gives every pooled state its own planes back (the pool's contents, same sides).
+int unpool_states(cudapic_batch *b) {
+    while (b->pooled > 0) {
+        const uint32_t k = b->pooled - 1;
+        cudapic_state *s = b->states[k];
+        const size_t bytes = (size_t)s->params.capacity * sizeof(float);
+        float *own[POOL_PLANES];
+        for (int p = 0; p < POOL_PLANES; ++p) {
+            void *ptr = nullptr;
+            CUDAPIC_CHECK(state_alloc(s, &ptr, bytes));
+            own[p] = static_cast<float *>(ptr);
+            CUDAPIC_CHECK(check_cuda(cudaMemcpyAsync(own[p], b->plane(p) + b->off[k], bytes,
+                                                     cudaMemcpyDeviceToDevice, b->stream), "batch: unpool copy"));
+        }
+        CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(b->stream), "batch: unpool sync"));
+        point_state(s, own);
+        s->batch = nullptr;
+        b->pooled = k;
+    }
+    return CUDAPIC_OK;
+}
+
+// Descriptors of the states' per-discharge buffers, density roles as they
+// are oriented now (relative roles back to zero).
 int build(cudapic_batch *b) {
     const uint32_t D = b->count();
     std::vector<BatchDisc> host(D);
@@ -75,16 +153,7 @@ int build(cudapic_batch *b) {
         BatchDisc &d = host[k];
         std::memset(&d, 0, sizeof(d));
         d.g = s->grid;
-        for (int sp = 0; sp < 2; ++sp) {
-            for (int side = 0; side < 2; ++side) {
-                const int a = s->side[sp] ^ side;
-                d.x[sp][side] = s->x[sp][a];
-                d.vx[sp][side] = s->vx[sp][a];
-                d.vy[sp][side] = s->vy[sp][a];
-                d.vz[sp][side] = s->vz[sp][a];
-            }
-            for (int p = 0; p < 4; ++p) d.rng[sp][p] = s->rng[sp][p];
-        }
+        d.off = b->off[k];
         for (int r = 0; r < 2; ++r) {
             d.e_dens[r] = s->e_dens[s->e_cur ^ r];
             d.i_dens[r] = s->i_dens[s->i_cur ^ r];
@@ -103,14 +172,48 @@ int build(cudapic_batch *b) {
         d.cumul_i = s->cumul_i;
         d.esum = s->esum;
         d.eepf = s->eepf;
-        b->origin[k] = {s->side[0], s->side[1], s->e_cur, s->i_cur};
+        b->origin[k] = {s->e_cur, s->i_cur};
     }
     CUDAPIC_CHECK(check_cuda(cudaMemcpy(b->desc, host.data(), D * sizeof(BatchDisc), cudaMemcpyHostToDevice),
                              "batch: upload descriptors"));
-    b->se = b->si = b->ecur = b->icur = 0;
+    b->ecur = b->icur = 0;
     destroy_graphs(b);
     b->built = true;
     return CUDAPIC_OK;
+}
+
+StepPlanes step_planes(const cudapic_batch *b, int sp, int src, int ion_side) {
+    StepPlanes pl;
+    pl.sx = b->plane(pool_plane(sp, src, 0));
+    pl.svx = b->plane(pool_plane(sp, src, 1));
+    pl.svy = b->plane(pool_plane(sp, src, 2));
+    pl.svz = b->plane(pool_plane(sp, src, 3));
+    pl.dx = b->plane(pool_plane(sp, src ^ 1, 0));
+    pl.dvx = b->plane(pool_plane(sp, src ^ 1, 1));
+    pl.dvy = b->plane(pool_plane(sp, src ^ 1, 2));
+    pl.dvz = b->plane(pool_plane(sp, src ^ 1, 3));
+    pl.rng0 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 0)));
+    pl.rng1 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 1)));
+    pl.rng2 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 2)));
+    pl.rng3 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 3)));
+    pl.ix = b->plane(pool_plane(1, ion_side, 0));
+    pl.ivx = b->plane(pool_plane(1, ion_side, 1));
+    pl.ivy = b->plane(pool_plane(1, ion_side, 2));
+    pl.ivz = b->plane(pool_plane(1, ion_side, 3));
+    return pl;
+}
+
+SidePlanes side_planes(const cudapic_batch *b, int sp, int side) {
+    SidePlanes s;
+    s.x = b->plane(pool_plane(sp, side, 0));
+    s.vx = b->plane(pool_plane(sp, side, 1));
+    s.vy = b->plane(pool_plane(sp, side, 2));
+    s.vz = b->plane(pool_plane(sp, side, 3));
+    s.rng0 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 0)));
+    s.rng1 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 1)));
+    s.rng2 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 2)));
+    s.rng3 = reinterpret_cast<uint32_t *>(b->plane(pool_rng_plane(sp, 3)));
+    return s;
 }
 
 // One step of every discharge (the order of state.cpp's fused step).
@@ -121,29 +224,23 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure) {
     if (ion_step) b->icur ^= 1;  // the buffer that collected the period's ion deposits becomes current
     CUDAPIC_CHECK(launch_batch_poisson(b->desc, b->counts, D, b->max_n_g, b->flags, b->ecur, b->icur, ion_step ? 1 : 0,
                                        measure ? 1 : 0, st));
+    StepRoles r{};
+    r.dens_i = b->icur ^ 1;
+    r.measure = measure ? 1 : 0;
     if (ion_step) {
-        StepRoles ri{};
-        ri.src = b->si;
-        ri.dst = b->si ^ 1;
-        ri.ion_side = b->si ^ 1;
-        ri.dens = b->icur ^ 1;
-        ri.dens_i = b->icur ^ 1;
-        ri.measure = measure ? 1 : 0;
-        CUDAPIC_CHECK(launch_batch_step(false, b->desc, b->counts + D, D, b->cap_sum, b->max_n_g, ri, st));
+        r.dens = b->icur ^ 1;
+        CUDAPIC_CHECK(launch_batch_step(false, step_planes(b, 1, b->si, b->si ^ 1), b->desc, b->counts + D, D,
+                                        b->cap_sum, b->max_n_g, r, st));
         b->si ^= 1;
     }
-    StepRoles re{};
-    re.src = b->se;
-    re.dst = b->se ^ 1;
-    re.ion_side = b->si;
-    re.dens = b->ecur ^ 1;
-    re.dens_i = b->icur ^ 1;
-    re.measure = measure ? 1 : 0;
-    CUDAPIC_CHECK(launch_batch_step(true, b->desc, b->counts, D, b->cap_sum, b->max_n_g, re, st));
+    r.dens = b->ecur ^ 1;
+    CUDAPIC_CHECK(launch_batch_step(true, step_planes(b, 0, b->se, b->si), b->desc, b->counts, D, b->cap_sum,
+                                    b->max_n_g, r, st));
     b->se ^= 1;
     b->ecur ^= 1;
-    if (ion_step) CUDAPIC_CHECK(launch_batch_collisions_i(b->desc, D, b->cap_sum, b->si, measure ? 1 : 0, st));
-    if (measure) CUDAPIC_CHECK(launch_batch_eepf(b->desc, D, b->cap_sum, b->se, st));
+    if (ion_step)
+        CUDAPIC_CHECK(launch_batch_collisions_i(side_planes(b, 1, b->si), b->desc, D, b->cap_sum, measure ? 1 : 0, st));
+    if (measure) CUDAPIC_CHECK(launch_batch_eepf(side_planes(b, 0, b->se), b->desc, D, b->cap_sum, st));
     return CUDAPIC_OK;
 }
 
@@ -182,32 +279,35 @@ extern "C" int cudapic_batch_create(cudapic_state *const *states, uint32_t count
     CUDAPIC_REQUIRE(count >= 1 && count <= BATCH_MAX_DISCHARGES, "batch_create: count must be in [1, 1024]");
     const cudapic_state *s0 = states[0];
     CUDAPIC_REQUIRE(s0, "batch_create: null state");
-    uint64_t cap_sum = 0;
+    uint64_t cap_sum = 0, pool_len = 0;
     uint32_t max_n_g = 0;
+    std::vector<uint32_t> off(count);
     for (uint32_t k = 0; k < count; ++k) {
         const cudapic_state *s = states[k];
         CUDAPIC_REQUIRE(s, "batch_create: null state");
         for (uint32_t j = 0; j < k; ++j) CUDAPIC_REQUIRE(states[j] != s, "batch_create: a state appears twice");
+        CUDAPIC_REQUIRE(!s->batch, "batch_create: a state already belongs to a batch");
         CUDAPIC_REQUIRE(s->device == s0->device, "batch_create: the states must share one device");
         CUDAPIC_REQUIRE(s->params.n_t == s0->params.n_t && s->params.n_sub == s0->params.n_sub,
                         "batch_create: the states must share N_T and N_SUB");
         CUDAPIC_REQUIRE((s->params.flags & CUDAPIC_FLAG_POISSON_F32_SCAN) ==
                             (s0->params.flags & CUDAPIC_FLAG_POISSON_F32_SCAN),
                         "batch_create: the states must share the Poisson arithmetic flag");
-        CUDAPIC_REQUIRE(s->graphs_enabled, "batch_create: N_T must be a multiple of N_SUB");
-        const void *planes[8] = {s->x[0][0], s->x[0][1], s->vx[0][0], s->vx[0][1],
-                                 s->rng[0][0], s->rng[0][1], s->rng[0][2], s->rng[0][3]};
-        CUDAPIC_REQUIRE(electron_step_eligible(planes, 8, s->grid.capacity), "batch_create: unaligned state buffers");
+        CUDAPIC_REQUIRE(s->graphs_enabled || (s->params.n_t % s->params.n_sub) == 0,
+                        "batch_create: N_T must be a multiple of N_SUB");
+        off[k] = (uint32_t)pool_len;
         cap_sum += s->grid.capacity;
+        pool_len += (s->grid.capacity + 63u) & ~63ull;
         max_n_g = std::max(max_n_g, s->grid.n_g);
+        CUDAPIC_REQUIRE(pool_len <= 0x80000000ull, "batch_create: the capacities must sum to at most 2^31");
     }
-    CUDAPIC_REQUIRE(cap_sum <= 0x80000000ull, "batch_create: the capacities must sum to at most 2^31");
     DeviceGuard dg(s0->device);
     cudapic_batch *b = new (std::nothrow) cudapic_batch();
     if (!b) return fail(CUDAPIC_ERR_ARG, "batch_create: out of host memory");
     b->device = s0->device;
-    b->states.assign(states, states + count);
     b->cap_sum = cap_sum;
+    b->pool_len = pool_len;
+    b->off = off;
     b->max_n_g = max_n_g;
     b->flags = s0->params.flags;
     auto cleanup = [&](int rc) {
@@ -218,12 +318,20 @@ extern "C" int cudapic_batch_create(cudapic_state *const *states, uint32_t count
     if ((rc = check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch: stream")) ||
         (rc = check_cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch: event")) ||
         (rc = check_cuda(cudaMalloc(&b->desc, count * sizeof(BatchDisc)), "batch: descriptors")) ||
-        (rc = check_cuda(cudaMalloc(&b->counts, 2ull * count * sizeof(uint32_t)), "batch: counts")))
+        (rc = check_cuda(cudaMalloc(&b->counts, 2ull * count * sizeof(uint32_t)), "batch: counts")) ||
+        (rc = check_cuda(cudaMalloc(&b->pool, (size_t)POOL_PLANES * pool_len * sizeof(float)), "batch: pool")))
         return cleanup(rc);
     b->ready.assign(count, nullptr);
     for (auto &ev : b->ready)
         if ((rc = check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "batch: event")))
             return cleanup(rc);
+    // the states join only once everything else is in place
+    b->states.assign(states, states + count);
+    if ((rc = pool_states(b))) {
+        // a state moved already points into the pool: give the planes back
+        unpool_states(b);
+        return cleanup(rc);
+    }
     *out = b;
     return CUDAPIC_OK;
 }
@@ -232,15 +340,22 @@ extern "C" int cudapic_batch_destroy(cudapic_batch *b) {
     if (!b) return CUDAPIC_OK;
     DeviceGuard dg(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    const int rc = unpool_states(b);
+    if (rc != CUDAPIC_OK) {
+        // some states still point into the pool: keep it (and the batch's
+        // other buffers) rather than leave them dangling
+        return rc;
+    }
     destroy_graphs(b);
     for (auto ev : b->ready)
         if (ev) cudaEventDestroy(ev);
     if (b->done) cudaEventDestroy(b->done);
     if (b->desc) cudaFree(b->desc);
     if (b->counts) cudaFree(b->counts);
+    if (b->pool) cudaFree(b->pool);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
-    return CUDAPIC_OK;
+    return rc;
 }
 
 extern "C" cudapic_stream_t cudapic_batch_stream(const cudapic_batch *b) {
@@ -266,13 +381,30 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
         CUDAPIC_REQUIRE(s->steps_done == steps0, "batch_run_steps: the states are at different steps");
         CUDAPIC_REQUIRE(s->measure == measure, "batch_run_steps: the states differ in measurement mode");
         CUDAPIC_REQUIRE(s->fused, "batch_run_steps: a state is in unfused (reference sequence) mode");
-        if (b->built && !oriented(b, k)) stale = true;
+        if (b->built && (s->e_cur != (b->origin[k][0] ^ b->ecur) || s->i_cur != (b->origin[k][1] ^ b->icur)))
+            stale = true;
     }
     if (stale) CUDAPIC_CHECK(build(b));
     // after every state's pending work (uploads, seeding, its own steps)
     for (uint32_t k = 0; k < D; ++k) {
         CUDAPIC_CHECK(check_cuda(cudaEventRecord(b->ready[k], b->states[k]->stream), "batch: record"));
         CUDAPIC_CHECK(check_cuda(cudaStreamWaitEvent(b->stream, b->ready[k], 0), "batch: wait"));
+    }
+    // a state stepped on its own lives on the other pool side: copy it back
+    for (uint32_t k = 0; k < D; ++k) {
+        cudapic_state *s = b->states[k];
+        const int want[2] = {b->se, b->si};
+        const size_t bytes = (size_t)s->params.capacity * sizeof(float);
+        for (int sp = 0; sp < 2; ++sp) {
+            if (s->side[sp] == want[sp]) continue;
+            for (int c = 0; c < 4; ++c)
+                CUDAPIC_CHECK(check_cuda(
+                    cudaMemcpyAsync(b->plane(pool_plane(sp, want[sp], c)) + b->off[k],
+                                    b->plane(pool_plane(sp, s->side[sp], c)) + b->off[k], bytes,
+                                    cudaMemcpyDeviceToDevice, b->stream), "batch: side copy"));
+            s->side[sp] = want[sp];
+            state_drop_graphs(s);
+        }
     }
     for (uint32_t k = 0; k < D; ++k)
         if (!b->states[k]->dens_valid) CUDAPIC_CHECK(state_prime_fused(b->states[k], b->stream));
@@ -305,11 +437,10 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
     const uint64_t done_steps = step - steps0;
     for (uint32_t k = 0; k < D; ++k) {
         cudapic_state *s = b->states[k];
-        const auto &o = b->origin[k];
-        s->side[0] = o[0] ^ b->se;
-        s->side[1] = o[1] ^ b->si;
-        s->e_cur = o[2] ^ b->ecur;
-        s->i_cur = o[3] ^ b->icur;
+        s->side[0] = b->se;
+        s->side[1] = b->si;
+        s->e_cur = b->origin[k][0] ^ b->ecur;
+        s->i_cur = b->origin[k][1] ^ b->icur;
         s->steps_done = step;
         if (s->measure) s->measure_steps += done_steps;
     }

@@ -3,9 +3,10 @@
 //
 // A batch steps many independent discharges (cudapic_state objects) in
 // lockstep: one launch per kernel of the step covers every discharge.  The
-// descriptors hold each discharge's buffers as they were oriented when the
-// batch was (re)built; the launches select the side and density roles of
-// the current step by index, the same for every discharge.
+// particle planes of all discharges live in one pool, so the kernels take
+// the plane bases as launch parameters and each discharge's offset from its
+// descriptor; the descriptors hold the other per-discharge buffers, with
+// the density roles as they were oriented when the batch was (re)built.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -20,10 +21,29 @@ namespace cudapic {
 // shared-memory prefix over the discharges' counts).
 constexpr uint32_t BATCH_MAX_DISCHARGES = 1024;
 
+// Pooled particle planes of a batch: one allocation of PLANES x len
+// elements; discharge d owns [off_d, off_d + capacity_d) of every plane
+// (off_d a multiple of 64, so every discharge starts 256-byte aligned).
+// Plane (species, side, component) is (species * 2 + side) * 4 + component
+// with components x, vx, vy, vz; RNG plane (species, k) is 16 + species * 4 + k.
+constexpr int POOL_PLANES = 24;
+constexpr int pool_plane(int species, int side, int comp) { return (species * 2 + side) * 4 + comp; }
+constexpr int pool_rng_plane(int species, int k) { return 16 + species * 4 + k; }
+
+// Particle planes of a step, read as kernel parameters.  Indices into them
+// are `off` + a discharge-local index: off = 0 for a one-discharge launch,
+// the discharge's offset in a batch's pooled planes otherwise, so the bases
+// stay launch constants and only the offset is per discharge.
+struct StepPlanes {
+    const float *sx, *svx, *svy, *svz;        // source side
+    float *dx, *dvx, *dvy, *dvz;              // destination side
+    uint32_t *rng0, *rng1, *rng2, *rng3;      // electrons: RNG planes (by source slot)
+    float *ix, *ivx, *ivy, *ivz;              // electrons: ion side receiving ionization spawns
+};
+
 struct BatchDisc {
     cudapic_grid g;                                        // dev_err, work: the discharge's own words
-    float *x[2][2], *vx[2][2], *vy[2][2], *vz[2][2];       // [species][side]
-    uint32_t *rng[2][4];                                   // [species][plane]
+    uint32_t off;                                          // element offset in the pooled planes
     float *e_dens[2], *i_dens[2];                          // [role]
     uint32_t *counters;                                    // n_e, n_i, alive, step, dev_err, alive_i, ticket
     float *efield, *pot;
@@ -36,13 +56,17 @@ struct BatchDisc {
     uint32_t *eepf;
 };
 
-// Roles of a particle step: sides and density buffers by index.
+// Density roles of a particle step (the same for every discharge).
 struct StepRoles {
-    int src, dst;      // the species' source and destination side
-    int ion_side;      // electrons: side of the ions receiving ionization spawns
     int dens;          // density buffer receiving the survivors
     int dens_i;        // electrons: ion density buffer receiving spawned ions
     int measure;       // count absorbed particles and collisions
+};
+
+// Planes of one species on one side (ion collisions, EEPF).
+struct SidePlanes {
+    float *x, *vx, *vy, *vz;
+    uint32_t *rng0, *rng1, *rng2, *rng3;
 };
 
 // Solves every discharge's field (one CTA each) and writes the clamped
@@ -53,14 +77,18 @@ struct StepRoles {
 int launch_batch_poisson(const BatchDisc *desc, uint32_t *counts, uint32_t D, uint32_t max_n_g, uint32_t flags,
                          int e_read, int i_read, int ion_step, int measure, cudaStream_t stream);
 // The fused electron step (mcc) or the ion push with deposit (!mcc) of every
-// discharge; counts: that species' counts written by launch_batch_poisson.
-int launch_batch_step(bool mcc, const BatchDisc *desc, const uint32_t *counts, uint32_t D, uint64_t cap_sum,
-                      uint32_t max_n_g, const StepRoles &r, cudaStream_t stream);
-// Ion collisions of every discharge (ions on `side`, counts read from the
-// discharges' counters).
-int launch_batch_collisions_i(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, int measure,
-                              cudaStream_t stream);
-// EEPF and centre-energy samples of every discharge (electrons on `side`).
-int launch_batch_eepf(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, cudaStream_t stream);
+// discharge over the pooled planes `pl` (the source, destination and spawn
+// sides chosen by the caller); counts: that species' counts written by
+// launch_batch_poisson.
+int launch_batch_step(bool mcc, const StepPlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
+                      uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream);
+// Ion collisions of every discharge (ions on the pooled side `ions`, counts
+// read from the discharges' counters).
+int launch_batch_collisions_i(const SidePlanes &ions, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,
+                              int measure, cudaStream_t stream);
+// EEPF and centre-energy samples of every discharge (electrons on the pooled
+// side `electrons`).
+int launch_batch_eepf(const SidePlanes &electrons, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,
+                      cudaStream_t stream);
 
 }  // namespace cudapic

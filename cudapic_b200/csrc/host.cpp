@@ -218,7 +218,7 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     v.push_stages >= 2 && v.push_stages <= 6 && v.push_ctas_per_sm >= 1 && v.push_ctas_per_sm <= 8 &&
                     v.mcc_stages >= 2 && v.mcc_stages <= 4 && v.mcc_ctas_per_sm >= 1 && v.mcc_ctas_per_sm <= 8 &&
                     (v.mcc_variant == 1 || v.mcc_variant == 2) && v.step_stages >= 2 && v.step_stages <= 6 &&
-                    v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 && (v.step_rows == 2 || v.step_rows == 4);
+                    v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 && (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4);
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuning = v;

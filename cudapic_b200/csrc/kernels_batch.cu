@@ -8,10 +8,12 @@
 //    count rounded up to a multiple of 4 (so every segment starts 16-byte
 //    aligned); CTA c owns an equal contiguous share of it, which cuts into at
 //    most a few discharges: its segments;
-//  * per segment the CTA loads that discharge's descriptor (buffers, grid
-//    constants, tables) into shared memory and runs the same tile pipeline
-//    as the one-discharge fused step (step.cuh), with the discharge's own
-//    slot counters, density and E-field;
+//  * the particle planes of all discharges live in one pool: the plane bases
+//    are launch parameters, a discharge is an element offset into them;
+//  * per segment the CTA loads that discharge's descriptor (offset, grid
+//    constants, buffers, tables) into shared memory and runs the same tile
+//    pipeline as the one-discharge fused step (step.cuh), with the
+//    discharge's own slot counters, density and E-field;
 //  * each discharge's count is published by the last CTA to finish it (its
 //    own ticket, expecting the CTAs whose shares meet the discharge).
 // The plan (a prefix over the counts) is recomputed by every CTA from the
@@ -27,6 +29,14 @@ namespace cudapic {
 namespace {
 
 __device__ __forceinline__ uint32_t round4(uint32_t n) { return (n + 3u) & ~3u; }
+
+// A shared word read by a volatile load (never kept in a register across code
+// that does not need it).
+__device__ __forceinline__ uint32_t lds_volatile(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)));
+    return v;
+}
 
 // P[d] = sum_{k<d} round4(count(k)) for d in [0, D]; one call by the whole
 // CTA (ES_THREADS threads), which synchronises before returning.
@@ -108,75 +118,86 @@ __device__ __forceinline__ void publish_count_of(uint32_t *ticket, uint32_t *dst
 }  // namespace
 
 // MCC: the fused electron step of every discharge; !MCC: the ion push with
-// the deposit of the next ion density.  MINB: resident CTAs per SM the
-// register allocation is bounded for (cudapic_tuning.step_ctas_per_sm: 3
-// caps it at 80 registers, 2 leaves it free).
-template <int U, bool MCC, int MINB>
+// the deposit of the next ion density.  The plane bases are launch
+// parameters (one pool for all discharges); per segment only the discharge's
+// offset, grid constants and a few buffers differ.  MINB: resident CTAs per
+// SM the register allocation is bounded for (cudapic_tuning.step_ctas_per_sm);
+// MEAS: the electrode and collision counters of a measurement window.
+template <int U, bool MCC, int MINB, bool MEAS>
 __global__ void __launch_bounds__(ES_THREADS, MINB)
-    batch_step_kernel(const BatchDisc *__restrict__ desc, const uint32_t *__restrict__ counts, uint32_t D,
-                      const StepRoles r, uint32_t ef_pad, int stages, int copies, uint32_t epoch) {
+    batch_step_kernel(const __grid_constant__ StepPlanes pl, const BatchDisc *__restrict__ desc,
+                      const uint32_t *__restrict__ counts, uint32_t D, const StepRoles r, uint32_t ef_pad,
+                      int stages, int copies, uint32_t epoch) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t offs[3][StepShape<U, MCC>::NSEG];
     __shared__ uint32_t s_base[3];
     __shared__ uint32_t wsum[ES_WARPS];
-    __shared__ StepIO s_io;
+    __shared__ StepDisc s_dc;
     __shared__ cudapic_grid s_g;
+    __shared__ uint32_t s_d, s_off;
     const StepSmem<U, MCC> sm(smem, stages, copies, ef_pad, offs, s_base);
     uint32_t *P = reinterpret_cast<uint32_t *>(sm.end(stages));  // [D + 1]
     step_smem_init(sm, stages, copies, ef_pad);
     grid_dep_wait();
     plan_prefix([&](uint32_t d) { return counts[d]; }, D, P, wsum);
-    uint32_t chunk, beg, end;
-    cta_share(P[D], chunk, beg, end);
-    const int sp = MCC ? 0 : 1;
     uint32_t it = 0;
     bool ok = true;
-    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
+    uint32_t d;
+    {
+        uint32_t chunk, beg, end;
+        cta_share(P[D], chunk, beg, end);
+        d = first_discharge(P, D, beg);
+    }
+    // Nothing of the plan stays in registers across a segment (the tile
+    // loop needs them all): the share is recomputed from the plan and the
+    // discharge index reloaded from shared memory after each segment.
+    for (;; ++d) {
+        uint32_t chunk, beg, end;
+        cta_share(P[D], chunk, beg, end);
+        if (d >= D || P[d] >= end) break;
         const uint32_t n = counts[d];
         const uint32_t lo = max(beg, P[d]) - P[d];
         const uint32_t hi = min(end, P[d] + n) - P[d];
         if (lo >= hi) continue;
-        const BatchDisc &dd = desc[d];
         if (threadIdx.x == 0) {
+            const BatchDisc &dd = desc[d];
+            s_d = d;
+            s_off = dd.off;
             s_g = dd.g;
-            StepIO io;
-            io.efield = dd.efield;
-            io.sx = dd.x[sp][r.src];
-            io.svx = dd.vx[sp][r.src];
-            io.svy = dd.vy[sp][r.src];
-            io.svz = dd.vz[sp][r.src];
-            io.dx = dd.x[sp][r.dst];
-            io.dvx = dd.vx[sp][r.dst];
-            io.dvy = dd.vy[sp][r.dst];
-            io.dvz = dd.vz[sp][r.dst];
-            io.rng0 = dd.rng[sp][0];
-            io.rng1 = dd.rng[sp][1];
-            io.rng2 = dd.rng[sp][2];
-            io.rng3 = dd.rng[sp][3];
-            io.sigma_tot = MCC ? dd.sigma_tot_e : dd.sigma_tot_i;
-            io.cs = dd.cs;
-            io.sigma_max = dd.sigma_max_e;
-            io.factor = MCC ? dd.g.factor_e : dd.g.factor_i;
-            io.dt = MCC ? dd.g.dt_e : dd.g.dt_i;
-            io.ix = dd.x[1][r.ion_side];
-            io.ivx = dd.vx[1][r.ion_side];
-            io.ivy = dd.vy[1][r.ion_side];
-            io.ivz = dd.vz[1][r.ion_side];
-            io.alive = dd.counters + (MCC ? 2 : 5);
-            io.n_i = dd.counters + 1;
-            io.dens = MCC ? dd.e_dens[r.dens] : dd.i_dens[r.dens];
-            io.dens_i = dd.i_dens[r.dens_i];
-            io.wall = r.measure ? dd.wall + sp : nullptr;
-            io.coll = r.measure && MCC ? dd.mcount : nullptr;
-            s_io = io;
+            StepDisc dc;
+            dc.efield = dd.efield;
+            dc.sigma_tot = MCC ? dd.sigma_tot_e : dd.sigma_tot_i;
+            dc.cs = dd.cs;
+            dc.sigma_max = dd.sigma_max_e;
+            dc.factor = MCC ? dd.g.factor_e : dd.g.factor_i;
+            dc.dt = MCC ? dd.g.dt_e : dd.g.dt_i;
+            dc.alive = dd.counters + (MCC ? 2 : 5);
+            dc.n_i = dd.counters + 1;
+            dc.dens = MCC ? dd.e_dens[r.dens] : dd.i_dens[r.dens];
+            dc.dens_i = dd.i_dens[r.dens_i];
+            dc.wall = MEAS ? dd.wall + (MCC ? 0 : 1) : nullptr;
+            dc.coll = MEAS && MCC ? dd.mcount : nullptr;
+            s_dc = dc;
             if (lo == 0 && dd.g.work) atomicAdd(dd.g.work, (unsigned long long)n);
         }
         __syncthreads();
-        if (ok) ok = step_segment<U, MCC>(s_io, s_g, lo, hi, sm, stages, copies, ef_pad, epoch, it);
-        const uint32_t expected = (P[d] + n - 1) / chunk - P[d] / chunk + 1;
-        publish_count_of(dd.counters + 6, dd.counters + (MCC ? 0 : 1), dd.counters + (MCC ? 2 : 5), s_g.capacity,
-                         expected);
-        __syncthreads();  // s_io and s_g are rewritten for the next segment
+        if (ok) {
+            // the grid constants in registers: the tile loop's shared-memory
+            // stores would otherwise force reloads of s_g at every use
+            const cudapic_grid g = s_g;
+            ok = step_segment<U, MCC, true, MEAS>(pl, s_dc, g, s_g, s_off, lo, hi, sm, stages, copies, ef_pad, epoch,
+                                                  it);
+        }
+        d = lds_volatile(&s_d);
+        {
+            uint32_t chunk2, beg2, end2;
+            cta_share(P[D], chunk2, beg2, end2);
+            const uint32_t n2 = counts[d];
+            const uint32_t expected = (P[d] + n2 - 1) / chunk2 - P[d] / chunk2 + 1;
+            uint32_t *ctr = desc[d].counters;
+            publish_count_of(ctr + 6, ctr + (MCC ? 0 : 1), ctr + (MCC ? 2 : 5), s_g.capacity, expected);
+        }
+        __syncthreads();  // s_dc, s_g, s_d and s_off are rewritten for the next segment
     }
 }
 
@@ -196,7 +217,8 @@ struct IonCollIO {
 };
 
 __global__ void __launch_bounds__(ES_THREADS)
-    batch_collisions_i_kernel(const BatchDisc *__restrict__ desc, uint32_t D, int side, int measure) {
+    batch_collisions_i_kernel(const __grid_constant__ SidePlanes ions, const BatchDisc *__restrict__ desc,
+                              uint32_t D, int measure) {
     extern __shared__ __align__(16) uint32_t bc_smem[];
     uint32_t *P = bc_smem;                                   // [D + 1]
     __shared__ uint32_t queue[ES_WARPS][5][BC_QCAP];
@@ -223,13 +245,13 @@ __global__ void __launch_bounds__(ES_THREADS)
         if (tid == 0) {
             s_g = dd.g;
             IonCollIO io;
-            io.vx = dd.vx[1][side];
-            io.vy = dd.vy[1][side];
-            io.vz = dd.vz[1][side];
-            io.rng0 = dd.rng[1][0];
-            io.rng1 = dd.rng[1][1];
-            io.rng2 = dd.rng[1][2];
-            io.rng3 = dd.rng[1][3];
+            io.vx = ions.vx + dd.off;
+            io.vy = ions.vy + dd.off;
+            io.vz = ions.vz + dd.off;
+            io.rng0 = ions.rng0 + dd.off;
+            io.rng1 = ions.rng1 + dd.off;
+            io.rng2 = ions.rng2 + dd.off;
+            io.rng3 = ions.rng3 + dd.off;
             io.sigma_tot = dd.sigma_tot_i;
             io.cs = dd.cs;
             io.coll = measure ? dd.mcount + 1 : nullptr;
@@ -311,7 +333,7 @@ __global__ void __launch_bounds__(ES_THREADS)
 // accumulate_eepf (Rust-CUDA/src/main.rs:1301-1339) of every discharge with
 // the centre-energy sums of the report; one shared histogram per segment.
 __global__ void __launch_bounds__(ES_THREADS)
-    batch_eepf_kernel(const BatchDisc *__restrict__ desc, uint32_t D, int side) {
+    batch_eepf_kernel(const __grid_constant__ SidePlanes electrons, const BatchDisc *__restrict__ desc, uint32_t D) {
     extern __shared__ __align__(16) uint32_t be_smem[];
     uint32_t *P = be_smem;  // [D + 1]
     __shared__ uint32_t hist[N_EEPF];
@@ -333,7 +355,8 @@ __global__ void __launch_bounds__(ES_THREADS)
         if (lo >= hi) continue;
         const BatchDisc &dd = desc[d];
         const cudapic_grid &g = dd.g;
-        const float *x = dd.x[0][side], *vx = dd.vx[0][side], *vy = dd.vy[0][side], *vz = dd.vz[0][side];
+        const float *x = electrons.x + dd.off, *vx = electrons.vx + dd.off, *vy = electrons.vy + dd.off,
+                    *vz = electrons.vz + dd.off;
         const float *ef = dd.efield;
         const float min_x = g.min_x, max_x = g.max_x, inv_dx = g.inv_dx, kick = g.eepf_half_kick;
         const float half_me = g.half_me_over_e;
@@ -377,9 +400,10 @@ __global__ void __launch_bounds__(ES_THREADS)
 
 namespace {
 
-template <int U, bool MCC, int MINB>
-int launch_batch_step_t(const BatchDisc *desc, const uint32_t *counts, uint32_t D, uint64_t cap_sum,
-                        uint32_t max_n_g, const StepRoles &r, cudaStream_t stream, const cudapic_tuning &t) {
+template <int U, bool MCC, int MINB, bool MEAS>
+int launch_batch_step_t(const StepPlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
+                        uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream,
+                        const cudapic_tuning &t) {
     constexpr int TILE = StepShape<U, MCC>::TILE;
     int stages = std::min(std::max(t.step_stages, 2), ES_MAX_STAGES);
     int copies = std::max(1, std::min(t.density_copies, ES_WARPS));
@@ -391,7 +415,7 @@ int launch_batch_step_t(const BatchDisc *desc, const uint32_t *counts, uint32_t 
     while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "batch step: n_g too large");
     const size_t smem = bytes();
-    auto kern = batch_step_kernel<U, MCC, MINB>;
+    auto kern = batch_step_kernel<U, MCC, MINB, MEAS>;
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                              "cudaFuncSetAttribute(batch step)"));
     int per_sm = 0;
@@ -402,41 +426,55 @@ int launch_batch_step_t(const BatchDisc *desc, const uint32_t *counts, uint32_t 
     const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
     const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
     return launch_kernel(MCC ? "batch_step_electrons" : "batch_push_ions", kern, dim3(grid), dim3(ES_THREADS), smem,
-                         stream, desc, counts, D, r, ef_pad, stages, copies, epoch);
+                         stream, pl, desc, counts, D, r, ef_pad, stages, copies, epoch);
 }
 
 }  // namespace
 
-int launch_batch_step(bool mcc, const BatchDisc *desc, const uint32_t *counts, uint32_t D, uint64_t cap_sum,
-                      uint32_t max_n_g, const StepRoles &r, cudaStream_t stream) {
-    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch step: bad discharge count");
-    const cudapic_tuning t = tuning();
+template <bool MEAS>
+int launch_batch_step_m(bool mcc, const StepPlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
+                        uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream,
+                        const cudapic_tuning &t) {
     const bool three = t.step_ctas_per_sm >= 3;
     if (mcc) {
         if (t.step_rows == 4)
-            return three ? launch_batch_step_t<4, true, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
-                         : launch_batch_step_t<4, true, 2>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
-        return three ? launch_batch_step_t<2, true, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
-                     : launch_batch_step_t<2, true, 2>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
+            return three ? launch_batch_step_t<4, true, 3, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                         : launch_batch_step_t<4, true, 2, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
+        if (t.step_rows == 1)
+            return three ? launch_batch_step_t<1, true, 3, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                         : launch_batch_step_t<1, true, 2, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
+        return three ? launch_batch_step_t<2, true, 3, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t)
+                     : launch_batch_step_t<2, true, 2, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
     }
-    return t.step_rows == 4 ? launch_batch_step_t<4, false, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t)
-                            : launch_batch_step_t<2, false, 3>(desc, counts, D, cap_sum, max_n_g, r, stream, t);
+    return t.step_rows == 4
+               ? launch_batch_step_t<4, false, 3, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t)
+               : launch_batch_step_t<2, false, 3, MEAS>(pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
 }
 
-int launch_batch_collisions_i(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, int measure,
-                              cudaStream_t stream) {
+int launch_batch_step(bool mcc, const StepPlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
+                      uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream) {
+    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch step: bad discharge count");
+    const cudapic_tuning t = tuning();
+    if (r.measure) return launch_batch_step_m<true>(mcc, pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
+    return launch_batch_step_m<false>(mcc, pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
+}
+
+int launch_batch_collisions_i(const SidePlanes &ions, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,
+                              int measure, cudaStream_t stream) {
     if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch collisions: bad discharge count");
     const size_t smem = (size_t)(D + 1) * sizeof(uint32_t);
     const unsigned grid = persistent_grid(4, (cap_sum + ES_THREADS * BC_U - 1) / (ES_THREADS * BC_U));
     return launch_kernel("batch_collisions_i", batch_collisions_i_kernel, dim3(grid), dim3(ES_THREADS), smem, stream,
-                         desc, D, side, measure);
+                         ions, desc, D, measure);
 }
 
-int launch_batch_eepf(const BatchDisc *desc, uint32_t D, uint64_t cap_sum, int side, cudaStream_t stream) {
+int launch_batch_eepf(const SidePlanes &electrons, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,
+                      cudaStream_t stream) {
     if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch eepf: bad discharge count");
     const size_t smem = (size_t)(D + 1) * sizeof(uint32_t);
     const unsigned grid = persistent_grid(2, (cap_sum + ES_THREADS - 1) / ES_THREADS);
-    return launch_kernel("batch_eepf", batch_eepf_kernel, dim3(grid), dim3(ES_THREADS), smem, stream, desc, D, side);
+    return launch_kernel("batch_eepf", batch_eepf_kernel, dim3(grid), dim3(ES_THREADS), smem, stream, electrons, desc,
+                         D);
 }
 
 }  // namespace cudapic

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
                 ev = collide_ion(i, t.idx, vxi, vyi, vzi, t.vxa, t.vya, t.vza, rs, cs, vx, vy, vz, g);
             } else {
                 const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
-                ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
+                ev = collide_electron(0u, i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
                                       alive_i, g, dep_e, dep_i);
             }
             rng0[i] = rs.s0;
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
                 ev = collide_ion(i, t.idx, vxi, vyi, vzi, t.vxa, t.vya, t.vza, rs, cs, vx, vy, vz, g);
             } else {
                 const Test t = test_electron(vxi, vyi, vzi, rs, table, g);
-                ev = collide_electron(i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
+                ev = collide_electron(0u, i, t.idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
                                       alive_i, g, dep_e, dep_i);
             }
             rng0[i] = rs.s0;

@@ -75,37 +75,38 @@ __global__ void __launch_bounds__(ES_THREADS)
     const uint32_t beg = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, beg + chunk);
     if (g.work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(g.work, (unsigned long long)n);
-    StepIO io;
-    io.efield = efield;
-    io.sx = sx;
-    io.svx = svx;
-    io.svy = svy;
-    io.svz = svz;
-    io.dx = dx_;
-    io.dvx = dvx;
-    io.dvy = dvy;
-    io.dvz = dvz;
-    io.rng0 = rng0;
-    io.rng1 = rng1;
-    io.rng2 = rng2;
-    io.rng3 = rng3;
-    io.sigma_tot = sigma_tot_e;
-    io.cs = cs;
-    io.sigma_max = sigma_max;
-    io.factor = g.factor_e;
-    io.dt = g.dt_e;
-    io.ix = ix;
-    io.ivx = ivx;
-    io.ivy = ivy;
-    io.ivz = ivz;
-    io.alive = alive;
-    io.n_i = n_i;
-    io.dens = dens_e;
-    io.dens_i = dens_i;
-    io.wall = wall;
-    io.coll = coll;
+    StepPlanes pl;
+    pl.sx = sx;
+    pl.svx = svx;
+    pl.svy = svy;
+    pl.svz = svz;
+    pl.dx = dx_;
+    pl.dvx = dvx;
+    pl.dvy = dvy;
+    pl.dvz = dvz;
+    pl.rng0 = rng0;
+    pl.rng1 = rng1;
+    pl.rng2 = rng2;
+    pl.rng3 = rng3;
+    pl.ix = ix;
+    pl.ivx = ivx;
+    pl.ivy = ivy;
+    pl.ivz = ivz;
+    StepDisc dc;
+    dc.efield = efield;
+    dc.sigma_tot = sigma_tot_e;
+    dc.cs = cs;
+    dc.sigma_max = sigma_max;
+    dc.factor = g.factor_e;
+    dc.dt = g.dt_e;
+    dc.alive = alive;
+    dc.n_i = n_i;
+    dc.dens = dens_e;
+    dc.dens_i = dens_i;
+    dc.wall = wall;
+    dc.coll = coll;
     uint32_t it = 0;
-    step_segment<U, true>(io, g, beg, end, sm, stages, copies, ef_pad, epoch, it);
+    step_segment<U, true, false, true>(pl, dc, g, g, 0u, beg, end, sm, stages, copies, ef_pad, epoch, it);
     publish_count(link.ticket, link.dst, link.src, link.clear_src, g.capacity);
 }
 
@@ -164,7 +165,9 @@ int launch_electron_step(const float *efield, const float *sx, const float *svx,
     const void *planes[8] = {sx, svx, svy, svz, rng0, rng1, rng2, rng3};
     if (!electron_step_eligible(planes, 8, g.capacity)) return CUDAPIC_ERR_NOT_SUPPORTED;
     const cudapic_tuning t = tuning();
-    auto launch = t.step_rows == 4 ? launch_electron_step_t<4> : launch_electron_step_t<2>;
+    auto launch = t.step_rows == 4   ? launch_electron_step_t<4>
+                  : t.step_rows == 1 ? launch_electron_step_t<1>
+                                     : launch_electron_step_t<2>;
     return launch(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e,
                   ix, ivx, ivy, ivz, alive, n_active, n_i, dens_e, dens_i, g, stream, link, wall, coll, t);
 }

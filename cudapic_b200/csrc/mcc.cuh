@@ -130,8 +130,9 @@ __device__ __forceinline__ void deposit_global(float *dens, float xv, const cuda
 // rs already past the test draw), writes its velocity and any spawns;
 // returns the event (1 elastic, 2 excitation, 3 ionization).  dep_e / dep_i
 // (may be null): next-step densities that also receive the spawned
-// electron / ion.
-static __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
+// electron / ion.  Slots (i and the spawns' claimed slots) are relative to
+// element `off` of the planes (a discharge of a batch's pool; 0 otherwise).
+static __device__ __noinline__ uint32_t collide_electron(uint32_t off, uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
                                                   Xoshiro128p &rs, const float *__restrict__ cs, float *x, float *vx,
                                                   float *vy, float *vz, float *ix, float *ivx, float *ivy,
                                                   float *ivz, uint32_t *alive_e, uint32_t *alive_i,
@@ -179,13 +180,13 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t id
         dm::sincosf_det(eta_new, &se2, &ce2);
         float ngx, ngy, ngz;
         rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
-        const float xi = x[i];
+        const float xi = x[off + i];
         uint32_t slot;
         if (claim_slot(alive_e, g.capacity, slot)) {
-            x[slot] = xi;
-            vx[slot] = wx + g.f2 * ngx;
-            vy[slot] = wy + g.f2 * ngy;
-            vz[slot] = wz + g.f2 * ngz;
+            x[off + slot] = xi;
+            vx[off + slot] = wx + g.f2 * ngx;
+            vy[off + slot] = wy + g.f2 * ngy;
+            vz[off + slot] = wz + g.f2 * ngz;
             if (dep_e) deposit_global(dep_e, xi, g);
         } else {
             set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
@@ -193,10 +194,10 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t id
         float a, b, c;
         rs.three_normal(g.normal_range, a, b, c);
         if (claim_slot(alive_i, g.capacity, slot)) {
-            ix[slot] = xi;
-            ivx[slot] = a;
-            ivy[slot] = b;
-            ivz[slot] = c;
+            ix[off + slot] = xi;
+            ivx[off + slot] = a;
+            ivy[off + slot] = b;
+            ivz[off + slot] = c;
             if (dep_i) deposit_global(dep_i, xi, g);
         } else {
             set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
@@ -207,9 +208,9 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t i, uint32_t id
     dm::sincosf_det(eta, &se, &ce);
     float ngx, ngy, ngz;
     rotate(gm, chi_s, chi_c, se, ce, eu, ngx, ngy, ngz);
-    vx[i] = wx + g.f2 * ngx;
-    vy[i] = wy + g.f2 * ngy;
-    vz[i] = wz + g.f2 * ngz;
+    vx[off + i] = wx + g.f2 * ngx;
+    vy[off + i] = wy + g.f2 * ngy;
+    vz[off + i] = wz + g.f2 * ngz;
     return ev;
 }
 

@@ -31,6 +31,22 @@ __device__ __forceinline__ PushResult push_one(float xi, float vxi, const float 
     return r;
 }
 
+// push_one with the hot constants passed in (registers of the caller); the
+// error word is read from `gm` only for a position out of range.
+__device__ __forceinline__ PushResult push_one_c(float xi, float vxi, const float *ef, float factor, float dt,
+                                                 float inv_dx, uint32_t n_g, float gap, const cudapic_grid &gm) {
+    float pos = xi * inv_dx;
+    if (!(pos >= 0.0f && pos < (float)n_g - 0.5f)) set_dev_err(gm.dev_err, CUDAPIC_DEVERR_POSITION);
+    int p = cell_of(pos, n_g);
+    float c2 = pos - (float)p;
+    float e_x = (1.0f - c2) * ef[p] + c2 * ef[p + 1];
+    PushResult r;
+    r.vx = vxi + factor * e_x;
+    r.x = xi + r.vx * dt;
+    r.keep = r.x >= 0.0f && r.x <= gap;
+    return r;
+}
+
 // Boundary check of C/eduPIC.cc:623-667 for one row of a warp (every lane
 // calls it): particles with a pushed position x < 0 count at the powered
 // electrode, x > L at the grounded one, one atomic per electrode and row;

@@ -55,6 +55,29 @@ bool state_is_ion_step(const cudapic_state *s, uint64_t step) {
     return ((step % s->params.n_t) % s->params.n_sub) == 0;
 }
 
+int state_alloc(cudapic_state *s, void **p, size_t bytes) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess) return check_cuda(e, "cudaMalloc");
+    s->allocations.push_back(ptr);
+    *p = ptr;
+    return CUDAPIC_OK;
+}
+
+void state_release(cudapic_state *s, void *p) {
+    auto it = std::find(s->allocations.begin(), s->allocations.end(), p);
+    if (it == s->allocations.end()) return;
+    s->allocations.erase(it);
+    cudaFree(p);
+}
+
+void state_drop_graphs(cudapic_state *s) {
+    for (auto &g : s->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
 }  // namespace cudapic
 
 namespace {

@@ -49,6 +49,7 @@ struct cudapic_state {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
     bool graphs_enabled = true;
     std::vector<void *> allocations;
+    void *batch = nullptr;  // the batch whose pool holds the particle planes (batch.cpp)
 
     uint32_t *n_e() const { return counters + 0; }
     uint32_t *n_i() const { return counters + 1; }
@@ -81,5 +82,11 @@ struct DeviceGuard {
 int state_prime_fused(cudapic_state *s, cudaStream_t stream);
 // True when step `step` moves the ions (every N_SUB-th step of an RF period).
 bool state_is_ion_step(const cudapic_state *s, uint64_t step);
+// Device memory owned by the state (freed with it).
+int state_alloc(cudapic_state *s, void **p, size_t bytes);
+// Frees a buffer allocated by the state (no-op for memory it does not own).
+void state_release(cudapic_state *s, void *p);
+// Drops the captured CUDA graphs (after the state's buffers moved).
+void state_drop_graphs(cudapic_state *s);
 
 }  // namespace cudapic

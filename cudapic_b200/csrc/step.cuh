@@ -12,6 +12,7 @@
 // (check_collisions_e / collision_e, :971-1165) with the RNG stream of each
 // particle's source slot; without (ions) it is the ion push of the driver.
 #pragma once
+#include "batch_internal.h"
 #include "common.cuh"
 #include "mcc.cuh"
 #include "push.cuh"
@@ -45,16 +46,27 @@ __host__ __device__ constexpr size_t step_smem_bytes(int stages, int copies, uin
            (size_t)ES_WARPS * S::QCAP * 4 + (size_t)stages * sizeof(uint64_t);
 }
 
-// Buffers of one segment.
-struct StepIO {
+// A per-discharge pointer of a segment's StepDisc that the tile loop uses
+// rarely.  SH: the StepDisc is in shared memory (the batched kernels) and
+// the pointer is reloaded where it is used, so that no register holds it
+// across the loop; otherwise it is read as is (kernel parameters).
+template <bool SH, typename T>
+__device__ __forceinline__ T *dcp(T *const &field) {
+    if constexpr (SH) {
+        uint64_t v;
+        asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(smem_addr(&field)));
+        return reinterpret_cast<T *>(v);
+    } else {
+        return field;
+    }
+}
+
+// Per-discharge buffers and constants of a segment.
+struct StepDisc {
     const float *efield;
-    const float *sx, *svx, *svy, *svz;        // source side
-    float *dx, *dvx, *dvy, *dvz;              // destination side
-    uint32_t *rng0, *rng1, *rng2, *rng3;      // MCC: RNG planes (by source slot)
     const float *sigma_tot, *cs;              // MCC: total and per-process cross sections
     float sigma_max;                          // MCC: largest entry of sigma_tot
     float factor, dt;                         // push constants of the species
-    float *ix, *ivx, *ivy, *ivz;              // MCC: ion side receiving ionization spawns
     uint32_t *alive;                          // destination slot counter
     uint32_t *n_i;                            // MCC: ion count (spawn slots)
     float *dens;                              // next density of the species (survivors)
@@ -121,15 +133,22 @@ __device__ __forceinline__ void step_smem_init(const StepSmem<U, MCC> &sm, int s
     for (uint32_t k = threadIdx.x; k < ef_pad; k += ES_THREADS) sm.acc[k] = 0ull;
 }
 
-// Processes the particles [beg, end) of one species of one discharge.  On
-// entry the histograms and the accumulator are zero; on return they are
-// zero again (drained, the accumulator flushed into io.dens and cleared).
-// `it` counts the tiles this CTA has run through the stage ring (it selects
-// the stage and its mbarrier phase) and is advanced by the segment's tiles.
-// Returns false when a stage wait timed out (CUDAPIC_DEVERR_TIMEOUT set);
-// the survivors held so far are still written and the deposits flushed.
-template <int U, bool MCC>
-__device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_grid &g, uint32_t beg, uint32_t end,
+// Processes the particles [beg, end) (discharge-local) of one species of
+// one discharge whose planes start at element `off`.  On entry the
+// histograms and the accumulator are zero; on return they are zero again
+// (drained, the accumulator flushed into dc.dens and cleared).  `it` counts
+// the tiles this CTA has run through the stage ring (it selects the stage
+// and its mbarrier phase) and is advanced by the segment's tiles.  Returns
+// false when a stage wait timed out (CUDAPIC_DEVERR_TIMEOUT set); the
+// survivors held so far are still written and the deposits flushed.
+// g: the grid constants as the tile loop reads them (a register copy in the
+// batched kernels); gm: the same constants in memory, for the out-of-line
+// scattering routine.
+// SH: dc lives in shared memory; WALL: compile the electrode counters in
+// (dc.wall may still be null at run time).
+template <int U, bool MCC, bool SH, bool WALL>
+__device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDisc &dc, const cudapic_grid &g,
+                                             const cudapic_grid &gm, uint32_t off, uint32_t beg, uint32_t end,
                                              const StepSmem<U, MCC> &sm, int stages, int copies, uint32_t ef_pad,
                                              uint32_t epoch, uint32_t &it) {
     using S = StepShape<U, MCC>;
@@ -141,6 +160,11 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const unsigned lt = lanemask_lt();
+    // the push and test constants, read once (io may live in shared memory,
+    // which the tile loop writes)
+    const float factor = dc.factor, dt = dc.dt, sigma_max = dc.sigma_max;
+    const float inv_dx = g.inv_dx, gap = g.gap;
+    const uint32_t n_g = g.n_g;
     const uint32_t it0 = it;
     const uint32_t ntiles = (end - beg + TILE - 1) / TILE;  // this segment's tiles
 
@@ -149,19 +173,19 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
         const uint32_t cnt = min((uint32_t)TILE, end - t0);
         const uint32_t bytes = ((cnt + 3u) & ~3u) * 4u;  // beg is a multiple of 4; so is the capacity
         mbar_arrive_expect_tx(&sm.bar[stage], PLANES * bytes);
-        bulk_load(sm.in + (stage * PLANES + 0) * TILE, io.sx + t0, bytes, &sm.bar[stage]);
-        bulk_load(sm.in + (stage * PLANES + 1) * TILE, io.svx + t0, bytes, &sm.bar[stage]);
-        bulk_load(sm.in + (stage * PLANES + 2) * TILE, io.svy + t0, bytes, &sm.bar[stage]);
-        bulk_load(sm.in + (stage * PLANES + 3) * TILE, io.svz + t0, bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 0) * TILE, pl.sx + (off + t0), bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 1) * TILE, pl.svx + (off + t0), bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 2) * TILE, pl.svy + (off + t0), bytes, &sm.bar[stage]);
+        bulk_load(sm.in + (stage * PLANES + 3) * TILE, pl.svz + (off + t0), bytes, &sm.bar[stage]);
         if (MCC) {
-            bulk_load(sm.in + (stage * PLANES + 4) * TILE, io.rng0 + t0, bytes, &sm.bar[stage]);
-            bulk_load(sm.in + (stage * PLANES + 5) * TILE, io.rng1 + t0, bytes, &sm.bar[stage]);
-            bulk_load(sm.in + (stage * PLANES + 6) * TILE, io.rng2 + t0, bytes, &sm.bar[stage]);
-            bulk_load(sm.in + (stage * PLANES + 7) * TILE, io.rng3 + t0, bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 4) * TILE, pl.rng0 + (off + t0), bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 5) * TILE, pl.rng1 + (off + t0), bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 6) * TILE, pl.rng2 + (off + t0), bytes, &sm.bar[stage]);
+            bulk_load(sm.in + (stage * PLANES + 7) * TILE, pl.rng3 + (off + t0), bytes, &sm.bar[stage]);
         }
     };
 
-    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.ef[k] = io.efield[k];
+    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.ef[k] = dcp<SH>(dc.efield)[k];
     uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
     uint32_t *wq = sm.queue + warp * QCAP;
     __syncthreads();
@@ -172,25 +196,29 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
 
     // Scatters wq[first, first + count), one collider per lane.
     auto drain = [&](uint32_t first, uint32_t count) {
-        if (io.coll && lane == 0) atomicAdd(io.coll, (unsigned long long)count);  // collision events (measurement)
+        unsigned long long *ncoll = dcp<SH>(dc.coll);
+        if (ncoll && lane == 0) atomicAdd(ncoll, (unsigned long long)count);  // collision events (measurement)
         if ((uint32_t)lane < count) {
-            const uint32_t i = wq[first + lane];
-            const PushResult pr = push_one(io.sx[i], io.svx[i], sm.ef, io.factor, io.dt, g);
-            const float vy = io.svy[i], vz = io.svz[i];
-            Xoshiro128p rs{io.rng0[i], io.rng1[i], io.rng2[i], io.rng3[i]};
-            const Test t = test_electron(pr.vx, vy, vz, rs, GlobalTable{io.sigma_tot}, g);  // collides, as before
+            const uint32_t i = off + wq[first + lane];
+            const PushResult pr = push_one_c(pl.sx[i], pl.svx[i], sm.ef, factor, dt, inv_dx, n_g, gap, gm);
+            const float vy = pl.svy[i], vz = pl.svz[i];
+            Xoshiro128p rs{pl.rng0[i], pl.rng1[i], pl.rng2[i], pl.rng3[i]};
+            // collides, as before
+            const Test t = test_electron(pr.vx, vy, vz, rs, GlobalTable{dcp<SH>(dc.sigma_tot)}, gm);
             uint32_t slot;
-            if (claim_slot(io.alive, g.capacity, slot)) {
-                io.dx[slot] = pr.x;
-                collide_electron(slot, t.idx, pr.vx, vy, vz, rs, io.cs, io.dx, io.dvx, io.dvy, io.dvz, io.ix, io.ivx,
-                                 io.ivy, io.ivz, io.alive, io.n_i, g, io.dens, io.dens_i);
+            uint32_t *alive = dcp<SH>(dc.alive);
+            if (claim_slot(alive, g.capacity, slot)) {
+                pl.dx[off + slot] = pr.x;
+                collide_electron(off, slot, t.idx, pr.vx, vy, vz, rs, dcp<SH>(dc.cs), pl.dx, pl.dvx, pl.dvy, pl.dvz,
+                                 pl.ix, pl.ivx, pl.ivy, pl.ivz, alive, dcp<SH>(dc.n_i), gm, dcp<SH>(dc.dens),
+                                 dcp<SH>(dc.dens_i));
             } else {
-                set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_E);
+                set_dev_err(gm.dev_err, CUDAPIC_DEVERR_SPAWN_E);
             }
-            io.rng0[i] = rs.s0;
-            io.rng1[i] = rs.s1;
-            io.rng2[i] = rs.s2;
-            io.rng3[i] = rs.s3;
+            pl.rng0[i] = rs.s0;
+            pl.rng1[i] = rs.s1;
+            pl.rng2[i] = rs.s2;
+            pl.rng3[i] = rs.s3;
         }
         __syncwarp();
     };
@@ -213,7 +241,7 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
         const uint32_t r3 = k % 3u, p3 = (k + 2u) % 3u;  // buffers of this tile and of the previous one
         // every thread waits for the stage's bulk copies itself (bounded)
         ok = mbar_wait_bounded(&sm.bar[s], parity);
-        if (!ok) set_dev_err(g.dev_err, CUDAPIC_DEVERR_TIMEOUT);
+        if (!ok) set_dev_err(gm.dev_err, CUDAPIC_DEVERR_TIMEOUT);
 
         const uint32_t t0 = beg + tile * TILE;
         const uint32_t cnt = ok ? min((uint32_t)TILE, end - t0) : 0u;
@@ -230,18 +258,22 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
         for (int u = 0; u < U; ++u) {
             const uint32_t j = (uint32_t)u * ES_THREADS + tid;
             const bool valid = j < cnt;
-            const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * g.gap;
+            const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * gap;
             const float v0 = valid ? __uint_as_float(b[TILE + j]) : 0.0f;
-            const PushResult pr = push_one(x0, v0, sm.ef, io.factor, io.dt, g);
+            const PushResult pr = push_one_c(x0, v0, sm.ef, factor, dt, inv_dx, n_g, gap, gm);
             if (valid && pr.keep) keep |= 1u << u;
             cur.x[u] = pr.x;
             cur.vx[u] = pr.vx;
             if (!MCC) {
                 cur.vy[u] = __uint_as_float(b[2 * TILE + j]);
                 cur.vz[u] = __uint_as_float(b[3 * TILE + j]);
-                if (io.wall) count_wall(io.wall, true, valid && !pr.keep, pr.x, pr.vx, cur.vy[u], cur.vz[u], g.gap);
-            } else if (io.wall) {
-                count_wall(io.wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, g.gap);
+                if (WALL) {
+                    cudapic_wall_counters *wall = dcp<SH>(dc.wall);
+                    if (wall) count_wall(wall, true, valid && !pr.keep, pr.x, pr.vx, cur.vy[u], cur.vz[u], gap);
+                }
+            } else if (WALL) {
+                cudapic_wall_counters *wall = dcp<SH>(dc.wall);
+                if (wall) count_wall(wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, gap);
             }
         }
         if (MCC) {
@@ -256,7 +288,7 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
                 const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
                 const float velocity = sqrtf(v2);
                 const float rnd = rs.uniform();
-                if ((keep >> u & 1u) && may_collide(rnd, velocity, io.sigma_max, io.dt)) may |= 1u << u;
+                if ((keep >> u & 1u) && may_collide(rnd, velocity, sigma_max, dt)) may |= 1u << u;
                 st[u][0] = rs.s0;
                 st[u][1] = rs.s1;
                 st[u][2] = rs.s2;
@@ -272,8 +304,8 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
                         const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
                         const float velocity = sqrtf(v2);
                         const float rnd = rs.uniform();
-                        const uint32_t idx = energy_index(g.half_me_over_e * v2);
-                        if (collision_draw(rnd, __ldg(io.sigma_tot + idx) * velocity * io.dt)) coll |= 1u << u;
+                        const uint32_t idx = energy_index(gm.half_me_over_e * v2);
+                        if (collision_draw(rnd, __ldg(dcp<SH>(dc.sigma_tot) + idx) * velocity * dt)) coll |= 1u << u;
                     }
                 }
             }
@@ -288,11 +320,11 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
             const bool stay = kept && !collide;
             if (kept) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
             if (MCC && stay) {
-                const uint32_t i = t0 + j;
-                io.rng0[i] = st[u][0];
-                io.rng1[i] = st[u][1];
-                io.rng2[i] = st[u][2];
-                io.rng3[i] = st[u][3];
+                const uint32_t i = off + t0 + j;
+                pl.rng0[i] = st[u][0];
+                pl.rng1[i] = st[u][1];
+                pl.rng2[i] = st[u][2];
+                pl.rng3[i] = st[u][3];
             }
             const unsigned m = __ballot_sync(0xffffffffu, stay);
             cur.lane_off[u] = __popc(m & lt);
@@ -323,12 +355,12 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
                 if (prev.keep & (1u << u)) {
                     const uint32_t slot = base + sm.offs[p3][u * ES_WARPS + warp] + prev.lane_off[u];
                     if (slot < g.capacity) {
-                        io.dx[slot] = prev.x[u];
-                        io.dvx[slot] = prev.vx[u];
-                        io.dvy[slot] = prev.vy[u];
-                        io.dvz[slot] = prev.vz[u];
+                        pl.dx[off + slot] = prev.x[u];
+                        pl.dvx[off + slot] = prev.vx[u];
+                        pl.dvy[off + slot] = prev.vy[u];
+                        pl.dvz[off + slot] = prev.vz[u];
                     } else {
-                        set_dev_err(g.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
+                        set_dev_err(gm.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
                     }
                 }
             }
@@ -342,7 +374,7 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
                 if (lane >= o) incl += t;
             }
             if (lane < NSEG) sm.offs[r3][lane] = incl - v;
-            if (lane == 31) pending_base = incl ? atomicAdd(io.alive, incl) : 0u;
+            if (lane == 31) pending_base = incl ? atomicAdd(dcp<SH>(dc.alive), incl) : 0u;
         }
         prev = cur;
         have_prev = true;
@@ -353,22 +385,22 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
             }
         }
     }
-    const uint32_t pl = (it0 + tile + 2u) % 3u;  // buffers of the last tile with survivors held in registers
-    if (have_prev && warp == 0 && lane == 31) sm.s_base[pl] = pending_base;
+    const uint32_t lb = (it0 + tile + 2u) % 3u;  // buffers of the last tile with survivors held in registers
+    if (have_prev && warp == 0 && lane == 31) sm.s_base[lb] = pending_base;
     __syncthreads();
     if (have_prev) {
-        const uint32_t base = sm.s_base[pl];
+        const uint32_t base = sm.s_base[lb];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (prev.keep & (1u << u)) {
-                const uint32_t slot = base + sm.offs[pl][u * ES_WARPS + warp] + prev.lane_off[u];
+                const uint32_t slot = base + sm.offs[lb][u * ES_WARPS + warp] + prev.lane_off[u];
                 if (slot < g.capacity) {
-                    io.dx[slot] = prev.x[u];
-                    io.dvx[slot] = prev.vx[u];
-                    io.dvy[slot] = prev.vy[u];
-                    io.dvz[slot] = prev.vz[u];
+                    pl.dx[off + slot] = prev.x[u];
+                    pl.dvx[off + slot] = prev.vx[u];
+                    pl.dvy[off + slot] = prev.vy[u];
+                    pl.dvz[off + slot] = prev.vz[u];
                 } else {
-                    set_dev_err(g.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
+                    set_dev_err(gm.dev_err, MCC ? CUDAPIC_DEVERR_SPAWN_E : CUDAPIC_DEVERR_SPAWN_I);
                 }
             }
         }
@@ -377,7 +409,7 @@ __device__ __forceinline__ bool step_segment(const StepIO &io, const cudapic_gri
     __syncthreads();
     dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
     __syncthreads();
-    dep_flush(sm.acc, io.dens, g);
+    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);
     // the thread that flushed a node clears it (same node ownership as dep_flush)
     for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.acc[k] = 0ull;
     it = it0 + tile;

@@ -142,7 +142,7 @@ typedef struct cudapic_tuning {
                                  2: bulk-copy staged tiles (16-byte aligned pointers)    */
     int step_stages;          /* fused electron step bulk-copy pipeline depth: 2..6      */
     int step_ctas_per_sm;
-    int step_rows;            /* fused electron step particles per thread and tile: 2, 4 */
+    int step_rows;            /* fused electron step particles per thread and tile: 1, 2, 4 */
 } cudapic_tuning;
 
 int cudapic_get_tuning(cudapic_tuning *out);
@@ -507,8 +507,11 @@ int cudapic_state_load(cudapic_state *s, const char *path);
  *
  * The discharges are existing states (fused mode, one device, equal N_T and
  * N_SUB and Poisson arithmetic flag, all at the same step, all measuring or
- * none); they keep their buffers and every state call keeps working between
- * batch runs.  A batch does not own its states: destroy it before them.
+ * none, none in another batch).  While the batch exists their particle and
+ * RNG planes live in one pool it owns (pointers from cudapic_state_buffers
+ * taken before cudapic_batch_create are stale); every state call keeps
+ * working between batch runs, and cudapic_batch_destroy gives each state its
+ * own planes back.  A batch does not own its states: destroy it before them.
  * At most 1024 discharges, capacities summing to at most 2^31. */
 typedef struct cudapic_batch cudapic_batch;
 int cudapic_batch_create(cudapic_state *const *states, uint32_t count, cudapic_batch **out);
