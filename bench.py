@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--workload", choices=["c1", "c2"], default="c1",
                     help="c1: one 4M+4M discharge (plain path); c2: the 256-discharge sweep (batched path)")
     ap.add_argument("--discharges", type=int, default=256)
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="c2: skip the autotuning of the batched kernels' launch shapes")
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="c2: discharges also timed one at a time for the plain comparisons (0: all of them)")
     a = ap.parse_args()
@@ -486,6 +488,14 @@ def run_batched(args):
     batch = Batch(mine, device=local)
     batch.run_steps(STEP * args.warmup)
     batch.synchronize()
+    # launch shapes of the batched kernels for this mix of discharges
+    # (untimed; every rank tunes on its own shard)
+    import cudapic_b200 as cp
+    from cudapic_b200.autotune import tune_batch
+    defaults = cp.get_tuning()
+    tuned, _ = tune_batch(batch) if args.tune else (None, None)
+    batch.run_steps(STEP)
+    batch.synchronize()
     barrier(world)
     with ClockSampler(local) as clk:
         elapsed, work = batch.timed_steps(STEP * args.steps)
@@ -544,6 +554,7 @@ def run_batched(args):
             ev1.synchronize()
             return ev0.elapsed_time(ev1) * 1e-3, st.work() - w0
 
+        cp.set_tuning(**defaults)  # the one-discharge kernels' own shapes
         sums = {"plain": [0.0, 0.0], "fused": [0.0, 0.0]}
         for k in order:
             st = batch.states[k]
@@ -583,6 +594,7 @@ def run_batched(args):
                                "steps; 1 step = %d PIC steps" % (len(specs), STEP),
                    "precision": "f32 particles and push, 2^-20 fixed-point deposits summed exactly in 64-bit "
                                 "integers, FP64 Poisson scans and time averages",
+                   "launch_shapes": tuned or "library defaults",
                    "discharges": len(specs), "particles_total": int(sum(s.particles for s in specs)),
                    "l2": "inputs larger than L2 in aggregate, no flush",
                    "parallelism": "discharges sharded over %d rank(s), no collective" % world},

@@ -9,6 +9,9 @@ fused electron step; each candidate is timed with CUDA events (median of
 
     python -m cudapic_b200.autotune [--particles N] [--n-g 400] [--out tuning.json]
 
+tune_batch() does the same for the batched kernels on a live batch of
+discharges (their shapes depend on the mix of grids and particle counts).
+
 The built-in defaults of libcudapic (host.cpp kDefaultTuning) are the
 values this tool picks on B200 for the 4 M + 4 M steady-state population.
 """
@@ -129,6 +132,37 @@ def tune(st, reps=5, verbose=True):
             print("%-20s best %s  %.2f us (worst %.2f us)" % (name, cfg, us, max(r[1] for r in results[name])))
     cp.set_tuning(**best)
     return best, results
+
+
+# Launch shapes of the batched particle kernels (kernels_batch.cu): rows per
+# thread and tile, bulk-copy stages, resident CTAs per SM and deposit
+# histogram copies.
+BATCH_CANDIDATES = [dict(step_rows=r, step_stages=st_, step_ctas_per_sm=c, density_copies=k)
+                    for r, st_, c, k in itertools.product((1, 2, 4), (2, 4), (2, 3), (4, 8))]
+
+
+def tune_batch(batch, candidates=None, rounds=2, verbose=False):
+    """Times every candidate shape of the batched particle kernels on a live
+    ``cudapic_b200.batch.Batch`` (one captured period of 2 N_SUB steps each,
+    after an untimed period that captures the graph with the new shapes),
+    `rounds` interleaved passes; keeps and returns the shape with the best
+    median particle-steps/s: (best dict, {shape: [rates]})."""
+    import cudapic_b200 as cp
+    cands = list(candidates or BATCH_CANDIDATES)
+    period = 2 * batch.states[0].params.n_sub
+    rates = {}
+    for _ in range(rounds):
+        for cand in cands:
+            cp.set_tuning(**cand)
+            batch.run_steps(period)
+            t, w = batch.timed_steps(period)
+            key = tuple(sorted(cand.items()))
+            rates.setdefault(key, []).append(w / t)
+            if verbose:
+                print("  batch %s %.2f G particle-steps/s" % (cand, w / t / 1e9), flush=True)
+    best = max(rates, key=lambda k: statistics.median(rates[k]))
+    cp.set_tuning(**dict(best))
+    return dict(best), {str(dict(k)): v for k, v in rates.items()}
 
 
 def main():

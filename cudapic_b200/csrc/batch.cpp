@@ -53,6 +53,7 @@ struct cudapic_batch {
     int ecur = 0, icur = 0;          // density roles relative to the build
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};
+    uint64_t graph_gen[2] = {0, 0};                  // tuning generation at capture
 
     uint32_t count() const { return (uint32_t)states.size(); }
     float *plane(int p) const { return pool + (uint64_t)p * pool_len; }
@@ -268,6 +269,7 @@ int build_graph(cudapic_batch *b, uint64_t first_step, bool measure) {
     CUDAPIC_CHECK(check_cuda(e, "end capture"));
     e = cudaGraphInstantiate(&b->graph[m], graph, 0);
     cudaGraphDestroy(graph);
+    b->graph_gen[m] = tuning_generation();
     return check_cuda(e, "cudaGraphInstantiate");
 }
 
@@ -415,7 +417,8 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
         if ((step % period) == 0 && n_steps >= period) {
             const int m = measure ? 1 : 0;
             const int key[4] = {b->se, b->si, b->ecur, b->icur};
-            if (b->graph[m] && std::memcmp(key, b->graph_key[m], sizeof(key)) != 0) {
+            if (b->graph[m] && (std::memcmp(key, b->graph_key[m], sizeof(key)) != 0 ||
+                                b->graph_gen[m] != tuning_generation())) {
                 cudaGraphExecDestroy(b->graph[m]);
                 b->graph[m] = nullptr;
             }

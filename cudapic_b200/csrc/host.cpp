@@ -73,6 +73,7 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
+uint64_t g_tuning_gen = 0;  // advanced by every cudapic_set_tuning
 }  // namespace
 
 namespace {
@@ -86,6 +87,11 @@ PdlScope::~PdlScope() { t_pdl = prev; }
 cudapic_tuning tuning() {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     return g_tuning;
+}
+
+uint64_t tuning_generation() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return g_tuning_gen;
 }
 
 unsigned persistent_grid(int per_sm, uint64_t units) {
@@ -218,10 +224,12 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     v.push_stages >= 2 && v.push_stages <= 6 && v.push_ctas_per_sm >= 1 && v.push_ctas_per_sm <= 8 &&
                     v.mcc_stages >= 2 && v.mcc_stages <= 4 && v.mcc_ctas_per_sm >= 1 && v.mcc_ctas_per_sm <= 8 &&
                     (v.mcc_variant == 1 || v.mcc_variant == 2) && v.step_stages >= 2 && v.step_stages <= 6 &&
-                    v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 && (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4);
+                    v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 &&
+                    (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4);
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuning = v;
+    ++g_tuning_gen;
     return CUDAPIC_OK;
 }
 

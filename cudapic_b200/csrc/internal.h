@@ -31,6 +31,9 @@ int validate_grid(const cudapic_grid *g);
 
 // Current launch shapes (defaults filled in for zero fields).
 cudapic_tuning tuning();
+// Advanced by every cudapic_set_tuning: captured graphs baked the shapes of
+// the generation they were captured in.
+uint64_t tuning_generation();
 
 // Programmatic dependent launch (PDL).  Inside a PdlScope the kernel
 // launches of the calling thread carry cudaLaunchAttributeProgrammatic-

@@ -273,6 +273,7 @@ int build_graph(cudapic_state *s) {
     CUDAPIC_CHECK(check_cuda(e, "end capture"));
     e = cudaGraphInstantiate(&s->graph[m], graph, 0);
     cudaGraphDestroy(graph);
+    s->graph_gen[m] = tuning_generation();
     return check_cuda(e, "cudaGraphInstantiate");
 }
 
@@ -623,8 +624,9 @@ extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
         if (s->graphs_enabled && primed && (s->steps_done % period) == 0 && n_steps >= period) {
             const int m = s->measure ? 1 : 0;
             const int key[4] = {s->side[0], s->side[1], s->e_cur, s->i_cur};
-            if (s->graph[m] && std::memcmp(key, s->graph_key[m], sizeof(key)) != 0) {
-                cudaGraphExecDestroy(s->graph[m]);  // buffer roles differ from the captured ones
+            if (s->graph[m] && (std::memcmp(key, s->graph_key[m], sizeof(key)) != 0 ||
+                                s->graph_gen[m] != tuning_generation())) {
+                cudaGraphExecDestroy(s->graph[m]);  // buffer roles or launch shapes differ from the captured ones
                 s->graph[m] = nullptr;
             }
             int rc = build_graph(s);

@@ -47,6 +47,7 @@ struct cudapic_state {
     bool measure = false;
     uint64_t steps_done = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
+    uint64_t graph_gen[2] = {0, 0};                  // tuning generation at capture
     bool graphs_enabled = true;
     std::vector<void *> allocations;
     void *batch = nullptr;  // the batch whose pool holds the particle planes (batch.cpp)
