@@ -104,7 +104,7 @@ class Report(C.Structure):
         "density_center", "plasma_freq", "mean_energy_center", "debye_length", "e_coll_freq", "i_coll_freq",
         "wp_dt_e", "dx_over_debye", "max_e_coll_dt_e", "max_i_coll_dt_i")] + [("conditions_ok", C.c_int)] + [
         (n, C.c_double) for n in ("cfl_max_energy", "ion_flux_pow", "ion_flux_gnd", "mean_ion_energy_pow",
-                                  "mean_ion_energy_gnd", "e_flux_pow", "e_flux_gnd")]
+                                  "mean_ion_energy_gnd", "e_flux_pow", "e_flux_gnd", "power_e", "power_i")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -183,6 +183,9 @@ SIGNATURES = {
     "cudapic_state_steps_done": [_VP, C.POINTER(C.c_uint64)],
     "cudapic_state_synchronize": [_VP],
     "cudapic_state_download_measurements": [_VP, _VP, _VP, _VP],
+    "cudapic_state_xt_shape": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
+    "cudapic_state_download_xt": [_VP, C.c_int, _VP],
+    "cudapic_state_write_xt": [_VP, C.c_char_p],
     "cudapic_batch_create": [C.POINTER(_VP), _U32, C.POINTER(_VP)],
     "cudapic_batch_destroy": [_VP],
     "cudapic_batch_run_steps": [_VP, C.c_uint64],

@@ -47,8 +47,9 @@ struct cudapic_batch {
     uint32_t max_n_g = 0, flags = 0;
     uint64_t cap_sum = 0;
     bool built = false;
-    // density roles of each state at the build: e_cur, i_cur
+    // density roles of each state at the build: e_cur, i_cur; its XT buffer
     std::vector<std::array<int, 2>> origin;
+    std::vector<double *> xt_at_build;
     int se = 0, si = 0;              // pool sides of the electrons and ions (absolute)
     int ecur = 0, icur = 0;          // density roles relative to the build
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [measure]
@@ -149,6 +150,7 @@ int build(cudapic_batch *b) {
     const uint32_t D = b->count();
     std::vector<BatchDisc> host(D);
     b->origin.resize(D);
+    b->xt_at_build.resize(D);
     for (uint32_t k = 0; k < D; ++k) {
         cudapic_state *s = b->states[k];
         BatchDisc &d = host[k];
@@ -173,6 +175,9 @@ int build(cudapic_batch *b) {
         d.cumul_i = s->cumul_i;
         d.esum = s->esum;
         d.eepf = s->eepf;
+        d.xt = s->xt;
+        d.n_xt = s->n_xt;
+        b->xt_at_build[k] = s->xt;
         b->origin[k] = {s->e_cur, s->i_cur};
     }
     CUDAPIC_CHECK(check_cuda(cudaMemcpy(b->desc, host.data(), D * sizeof(BatchDisc), cudaMemcpyHostToDevice),
@@ -225,6 +230,13 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure) {
     if (ion_step) b->icur ^= 1;  // the buffer that collected the period's ion deposits becomes current
     CUDAPIC_CHECK(launch_batch_poisson(b->desc, b->counts, D, b->max_n_g, b->flags, b->ecur, b->icur, ion_step ? 1 : 0,
                                        measure ? 1 : 0, st));
+    if (measure) {  // XT diagnostics: the particles before their push
+        CUDAPIC_CHECK(launch_batch_xt_particles(false, side_planes(b, 0, b->se), b->desc, D, b->max_n_g, b->cap_sum,
+                                                st));
+        if (ion_step)
+            CUDAPIC_CHECK(launch_batch_xt_particles(true, side_planes(b, 1, b->si), b->desc, D, b->max_n_g,
+                                                    b->cap_sum, st));
+    }
     StepRoles r{};
     r.dens_i = b->icur ^ 1;
     r.measure = measure ? 1 : 0;
@@ -383,7 +395,8 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
         CUDAPIC_REQUIRE(s->steps_done == steps0, "batch_run_steps: the states are at different steps");
         CUDAPIC_REQUIRE(s->measure == measure, "batch_run_steps: the states differ in measurement mode");
         CUDAPIC_REQUIRE(s->fused, "batch_run_steps: a state is in unfused (reference sequence) mode");
-        if (b->built && (s->e_cur != (b->origin[k][0] ^ b->ecur) || s->i_cur != (b->origin[k][1] ^ b->icur)))
+        if (b->built && (s->e_cur != (b->origin[k][0] ^ b->ecur) || s->i_cur != (b->origin[k][1] ^ b->icur) ||
+                         s->xt != b->xt_at_build[k]))
             stale = true;
     }
     if (stale) CUDAPIC_CHECK(build(b));

@@ -54,6 +54,8 @@ struct BatchDisc {
     unsigned long long *mcount;                            // [3]: e / i collisions, EEPF samples
     double *cumul_e, *cumul_i, *esum;
     uint32_t *eepf;
+    double *xt;                                            // XT accumulators (may be null), n_xt columns
+    uint32_t n_xt;
 };
 
 // Density roles of a particle step (the same for every discharge).
@@ -90,5 +92,8 @@ int launch_batch_collisions_i(const SidePlanes &ions, const BatchDisc *desc, uin
 // side `electrons`).
 int launch_batch_eepf(const SidePlanes &electrons, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,
                       cudaStream_t stream);
+// XT accumulation of one species of every discharge (before its push).
+int launch_batch_xt_particles(bool ions, const SidePlanes &sp, const BatchDisc *desc, uint32_t D, uint32_t max_n_g,
+                              uint64_t cap_sum, cudaStream_t stream);
 
 }  // namespace cudapic

@@ -126,6 +126,25 @@ int launch_eepf(const float *x, const float *vx, const float *vy, const float *v
                 const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream,
                 double *esum = nullptr, unsigned long long *ecount = nullptr);
 
+// XT diagnostics (kernels_xt.cu): steps per column (eduPIC's N_BIN) and the
+// raw accumulators, each [n_g][n_xt] doubles, n_xt = N_T / XT_BIN.
+constexpr uint32_t XT_BIN = 20;
+enum XtRaw : int {
+    XT_COUNT_E = 0, XT_UE, XT_MEANEE, XT_IONIZ,  // electron weights and weighted sums
+    XT_COUNT_I, XT_UI, XT_MEANEI,                // ion weights and weighted sums
+    XT_POT, XT_EFIELD, XT_NE, XT_NI,             // grid quantities
+    XT_RAW
+};
+// Adds one species' particles (before the push) to the XT column of the step
+// the Poisson kernel just solved.
+int launch_xt_particles(bool ions, const float *x, const float *vx, const float *vy, const float *vz,
+                        const uint32_t *n_active, const float *efield, const float *cs, const uint32_t *step_counter,
+                        const cudapic_grid &g, uint32_t n_xt, double *xt, cudaStream_t stream);
+// Adds the potential, field and densities of that step.
+int launch_xt_grid(const float *pot, const float *efield, const float *e_density, const float *i_density,
+                   const uint32_t *step_counter, const cudapic_grid &g, uint32_t n_xt, double *xt,
+                   cudaStream_t stream);
+
 // Largest electron / ion collision frequencies of the total tables [1/s]
 // (C/eduPIC.cc:252-276) and the CFL energy limit [eV] (report.cpp).
 void table_coll_freqs(const float *sigma_tot_e, const float *sigma_tot_i, double *max_e, double *max_i);

@@ -307,7 +307,8 @@ int launch_poisson(const float *e_density, const float *i_density, float *pot, f
 // above, with the discharge's own step counter and RF table), writes its
 // clamped particle counts for the batched particle kernels and, when
 // measuring, adds the densities it read to the time averages
-// (accumulate_density, Rust-CUDA/src/main.rs:1294-1299).
+// (accumulate_density, Rust-CUDA/src/main.rs:1294-1299) and, with XT
+// diagnostics, the step's grid quantities to their XT column.
 template <typename T, int PT>
 __global__ void __launch_bounds__(POIS_MAX_THREADS)
     batch_poisson_kernel(const BatchDisc *__restrict__ desc, uint32_t *__restrict__ counts, uint32_t D, int e_read,
@@ -332,6 +333,19 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
     }
     poisson_body<T, PT>(e_dens, i_dens, dd.pot, dd.efield, 0.0f, dd.pot0_table, ctr + 3, s_g, dd.e_dens[e_read ^ 1],
                         ion_step ? dd.i_dens[i_read ^ 1] : nullptr);
+    if (measure && dd.xt) {  // XT grid quantities of the step (C/eduPIC.cc:705-715)
+        __syncthreads();
+        const uint32_t t = (*(volatile const uint32_t *)(ctr + 3) + s_g.n_t - 1u) % s_g.n_t;
+        const uint32_t col = t / XT_BIN;
+        const size_t plane = (size_t)s_g.n_g * dd.n_xt;
+        for (uint32_t k = threadIdx.x; k < s_g.n_g; k += blockDim.x) {
+            const size_t at = (size_t)k * dd.n_xt + col;
+            dd.xt[XT_POT * plane + at] += (double)dd.pot[k];
+            dd.xt[XT_EFIELD * plane + at] += (double)dd.efield[k];
+            dd.xt[XT_NE * plane + at] += (double)e_dens[k];
+            dd.xt[XT_NI * plane + at] += (double)i_dens[k];
+        }
+    }
 }
 
 template <typename T, int PT>

@@ -193,6 +193,16 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
     if (s->measure) {
         CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density(), s->cumul_e, &g, (cudapic_stream_t)st));
         if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density(), s->cumul_i, &g, (cudapic_stream_t)st));
+        if (s->xt) {  // XT diagnostics: the grid of this step and the particles before their push
+            CUDAPIC_CHECK(launch_xt_grid(s->pot, s->efield, s->e_density(), s->i_density(), s->step_counter(), g,
+                                         s->n_xt, s->xt, st));
+            CUDAPIC_CHECK(launch_xt_particles(false, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->n_e(),
+                                              s->efield, s->cs, s->step_counter(), g, s->n_xt, s->xt, st));
+            if (ion_step)
+                CUDAPIC_CHECK(launch_xt_particles(true, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
+                                                  s->n_i(), s->efield, s->cs, s->step_counter(), g, s->n_xt, s->xt,
+                                                  st));
+        }
     }
     if (fused) {
         const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc);
@@ -604,6 +614,17 @@ extern "C" int cudapic_state_set_measure(cudapic_state *s, int on) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_measure: null state");
     DeviceGuard dg(s->device);
     const size_t n_g = s->params.n_g;
+    if (on && !s->xt && s->params.n_t % XT_BIN == 0) {
+        const uint32_t n_xt = s->params.n_t / XT_BIN;
+        void *p = nullptr;
+        CUDAPIC_CHECK(state_alloc(s, &p, (size_t)XT_RAW * n_g * n_xt * sizeof(double)));
+        s->xt = static_cast<double *>(p);
+        s->n_xt = n_xt;
+        destroy_graphs(s);
+    }
+    if (s->xt)
+        CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->xt, 0, (size_t)XT_RAW * n_g * s->n_xt * sizeof(double), s->stream),
+                                 "zero xt"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_e, 0, n_g * sizeof(double), s->stream), "zero cumul_e"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->cumul_i, 0, n_g * sizeof(double), s->stream), "zero cumul_i"));
     CUDAPIC_CHECK(check_cuda(cudaMemsetAsync(s->eepf, 0, 2000 * sizeof(uint32_t), s->stream), "zero eepf"));
@@ -749,6 +770,7 @@ extern "C" int cudapic_state_report(cudapic_state *s, cudapic_report *out) {
     }
     r.mean_ion_energy_pow = hp > 0.0 ? mp / hp : NAN;
     r.mean_ion_energy_gnd = hg > 0.0 ? mg / hg : NAN;
+    CUDAPIC_CHECK(xt_power(s, &r.power_e, &r.power_i));  // C/eduPIC.cc:1011-1026
     *out = r;
     return CUDAPIC_OK;
 }
@@ -803,6 +825,13 @@ extern "C" int cudapic_state_write_info(cudapic_state *s, const char *path) {
         std::fprintf(f, "Electron flux at powered electrode    = %12.3e [m^{-2} s^{-1}]\n", r.e_flux_pow);
         std::fprintf(f, "Electron flux at grounded electrode   = %12.3e [m^{-2} s^{-1}]\n", r.e_flux_gnd);
         std::fprintf(f, "%s", rule);
+        if (!std::isnan(r.power_e)) {  // :1011-1026
+            std::fprintf(f, "Absorbed power calculated as <j*E>:\n");
+            std::fprintf(f, "Electron power density (average)      = %12.3e [W m^{-3}]\n", r.power_e);
+            std::fprintf(f, "Ion power density (average)           = %12.3e [W m^{-3}]\n", r.power_i);
+            std::fprintf(f, "Total power density(average)          = %12.3e [W m^{-3}]\n", r.power_e + r.power_i);
+            std::fprintf(f, "%s", rule);
+        }
     }
     const bool ok = std::fclose(f) == 0;
     return ok ? CUDAPIC_OK : fail(CUDAPIC_ERR_ARG, std::string("state_write_info: write failed: ") + path);

@@ -43,6 +43,8 @@ struct cudapic_state {
     uint64_t measure_steps = 0;
     double max_e_coll_freq = 0.0, max_i_coll_freq = 0.0;  // of the tables [1/s]
     uint32_t *eepf = nullptr;
+    double *xt = nullptr;   // XT accumulators [XT_RAW][n_g][n_xt] (allocated when measuring starts)
+    uint32_t n_xt = 0;      // XT columns (0: N_T is not a multiple of XT_BIN)
 
     bool measure = false;
     uint64_t steps_done = 0;
@@ -89,5 +91,8 @@ int state_alloc(cudapic_state *s, void **p, size_t bytes);
 void state_release(cudapic_state *s, void *p);
 // Drops the captured CUDA graphs (after the state's buffers moved).
 void state_drop_graphs(cudapic_state *s);
+// Space- and time-averaged <j E> power of the electrons and ions from the
+// XT diagnostics [W m^-3] (NaN without them), xt.cpp.
+int xt_power(cudapic_state *s, double *power_e, double *power_i);
 
 }  // namespace cudapic

@@ -165,6 +165,25 @@ class GpuSimState:
         """The report as eduPIC's info.txt."""
         check(lib.cudapic_state_write_info(self._h, str(path).encode()))
 
+    def xt_shape(self):
+        """(n_g, n_xt) of the XT diagnostics; n_xt = 0 without them."""
+        n_g, n_xt = C.c_uint32(), C.c_uint32()
+        check(lib.cudapic_state_xt_shape(self._h, C.byref(n_g), C.byref(n_xt)))
+        return n_g.value, n_xt.value
+
+    def download_xt(self, quantity):
+        """One normalised XT quantity of the measurement window (name of
+        XT_NAMES or its index) as an [n_g, n_xt] array (eduPIC's *_xt.dat)."""
+        q = XT_NAMES.index(quantity) if isinstance(quantity, str) else int(quantity)
+        n_g, n_xt = self.xt_shape()
+        out = np.zeros((n_g, n_xt), np.float64)
+        check(lib.cudapic_state_download_xt(self._h, q, out.ctypes.data))
+        return out
+
+    def write_xt(self, directory):
+        """eduPIC's eleven *_xt.dat files in `directory`."""
+        check(lib.cudapic_state_write_xt(self._h, str(directory).encode()))
+
     def wall_counters(self):
         """Electrode counters of the measurement window:
         {"e": {...}, "i": {...}} with abs_pow, abs_gnd, ifed_pow, ifed_gnd."""
@@ -213,6 +232,10 @@ class GpuSimState:
 
     def synchronize(self):
         check(lib.cudapic_state_synchronize(self._h))
+
+
+# XT quantities in the order of eduPIC's save_all_xt files (CUDAPIC_XT_*)
+XT_NAMES = ("pot", "efield", "ne", "ni", "je", "ji", "powere", "poweri", "meanee", "meanei", "ioniz")
 
 
 class GpuBatch:

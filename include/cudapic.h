@@ -483,10 +483,40 @@ typedef struct cudapic_report {
     double ion_flux_pow, ion_flux_gnd;   /* m^-2 s^-1                         */
     double mean_ion_energy_pow, mean_ion_energy_gnd;   /* eV                  */
     double e_flux_pow, e_flux_gnd;       /* m^-2 s^-1                         */
+    double power_e, power_i;      /* <j E> of the XT diagnostics, W m^-3 (NaN
+                                     without them), C/eduPIC.cc:1011-1026   */
 } cudapic_report;
 int cudapic_state_report(cudapic_state *s, cudapic_report *out);
 /* Writes the report as eduPIC's info.txt (same lines and number formats). */
 int cudapic_state_write_info(cudapic_state *s, const char *path);
+/* Spatio-temporal (XT) diagnostics of the measurement window (eduPIC's
+ * measurement mode, C/eduPIC.cc:557-614 and :705-715, normalised as
+ * norm_all_xt, :864-903): [N_G][N_XT] doubles, N_XT = N_T / CUDAPIC_XT_BIN
+ * columns of CUDAPIC_XT_BIN steps of the RF period each.  Collected while
+ * measuring when N_T is a multiple of CUDAPIC_XT_BIN (else n_xt = 0).
+ * Quantities in the order of eduPIC's save_all_xt files. */
+#define CUDAPIC_XT_BIN 20
+enum {
+    CUDAPIC_XT_POT = 0,     /* potential [V]                       pot_xt.dat     */
+    CUDAPIC_XT_EFIELD,      /* electric field [V/m]                efield_xt.dat  */
+    CUDAPIC_XT_NE,          /* electron density [m^-3]             ne_xt.dat      */
+    CUDAPIC_XT_NI,          /* ion density [m^-3]                  ni_xt.dat      */
+    CUDAPIC_XT_JE,          /* electron current density [A m^-2]   je_xt.dat      */
+    CUDAPIC_XT_JI,          /* ion current density [A m^-2]        ji_xt.dat      */
+    CUDAPIC_XT_POWERE,      /* electron power absorption [W m^-3]  powere_xt.dat  */
+    CUDAPIC_XT_POWERI,      /* ion power absorption [W m^-3]       poweri_xt.dat  */
+    CUDAPIC_XT_MEANEE,      /* mean electron energy [eV]           meanee_xt.dat  */
+    CUDAPIC_XT_MEANEI,      /* mean ion energy [eV]                meanei_xt.dat  */
+    CUDAPIC_XT_IONIZ,       /* ionization rate [m^-3 s^-1]         ioniz_xt.dat   */
+    CUDAPIC_XT_QUANTITIES
+};
+int cudapic_state_xt_shape(const cudapic_state *s, uint32_t *n_g, uint32_t *n_xt);
+/* One normalised quantity, out[node * n_xt + column].  Synchronises. */
+int cudapic_state_download_xt(cudapic_state *s, int quantity, double *out);
+/* eduPIC's eleven *_xt.dat files (one row per node, "%e  " per column) in
+ * `directory`.  Synchronises. */
+int cudapic_state_write_xt(cudapic_state *s, const char *directory);
+
 /* Checkpoint: the particles of both species in eduPIC's picdata.bin format
  * at `path` (Time = steps done x DT_E, cycles_done = whole RF periods), and
  * the RNG planes of every slot in `path`.rng.  Synchronises. */

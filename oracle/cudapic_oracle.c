@@ -665,3 +665,34 @@ void orc_accumulate_eepf(const float *x, const float *vx, const float *vy, const
         if (binf < (float)ORC_N_EEPF) eepf[(uint32_t)binf] += 1;
     }
 }
+
+/* XT diagnostics, C/eduPIC.cc:557-576 (electrons) and :599-614 (ions). */
+void orc_xt_accumulate(const float *efield, const float *x, const float *vx, const float *vy, const float *vz,
+                       uint32_t n, int ions, const float *cs_ion, const orc_phys *ph, double *out) {
+    const uint32_t n_g = ph->n_g;
+    const float factor = ions ? ph->factor_i : ph->factor_e;
+    const float half_m = ions ? HALF_MI_OVER_E : ph->half_me_over_e;
+    const float rate_scale = (float)((double)ph->dt_e * ph->gas_density);
+    for (uint32_t i = 0; i < n; ++i) {
+        float pos = x[i] * ph->inv_dx;
+        int p = cell_of(pos, n_g);
+        float c2 = pos - (float)p;
+        float c1 = 1.0f - c2;
+        float e_x = c1 * efield[p] + c2 * efield[p + 1];
+        float v = vx[i] + 0.5f * factor * e_x;
+        float v2 = v * v + vy[i] * vy[i] + vz[i] * vz[i];
+        float energy = half_m * v2;
+        out[p] += c1;
+        out[p + 1] += c2;
+        out[n_g + p] += c1 * v;
+        out[n_g + p + 1] += c2 * v;
+        out[2 * n_g + p] += c1 * energy;
+        out[2 * n_g + p + 1] += c2 * energy;
+        if (!ions) {
+            float t = fminf(energy / 0.001f + 0.5f, (float)(ORC_CS_RANGES - 1));
+            float rate = cs_ion[(uint32_t)t] * sqrtf(v2) * rate_scale;
+            out[3 * n_g + p] += c1 * rate;
+            out[3 * n_g + p + 1] += c2 * rate;
+        }
+    }
+}

@@ -164,6 +164,15 @@ void orc_accumulate_eepf(const float *x, const float *vx, const float *vy, const
                          const float *efield, uint32_t n_active, uint32_t *eepf,
                          const orc_phys *ph);
 
+/* ---- XT diagnostics (C/eduPIC.cc:557-576, :599-614) ---- */
+/* One step of eduPIC's measurement branch for one species, before the push,
+ * in the f32 arithmetic of the GPU kernel: with c1 = 1 - c2 and c2 the CIC
+ * weights of node p and p + 1, v = vx + 1/2 factor e_x and E = 1/2 m |v|^2 / e,
+ * out[q * n_g + node] += c (q 0), c v (q 1), c E (q 2) and, for electrons,
+ * c sigma_ion(E) |v| DT_E n_gas (q 3, cs_ion: eduPIC's sigma[E_ION] table). */
+void orc_xt_accumulate(const float *efield, const float *x, const float *vx, const float *vy, const float *vz,
+                       uint32_t n, int ions, const float *cs_ion, const orc_phys *ph, double *out);
+
 
 #ifdef __cplusplus
 }

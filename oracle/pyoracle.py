@@ -23,7 +23,7 @@ __all__ = [
     "cross_sections", "get_density_f32", "get_density_f64", "poisson_thomas_f64",
     "poisson_scan_f32", "poisson_dps_flexible_f64", "move_and_compact",
     "check_collisions_e", "check_collisions_i", "p_coll_e_exact",
-    "accumulate_density", "accumulate_eepf", "REF_DIR", "CS_RANGES", "N_EEPF",
+    "accumulate_density", "accumulate_eepf", "xt_accumulate", "xt_normalise", "REF_DIR", "CS_RANGES", "N_EEPF",
     "MATH_FN",
 ]
 
@@ -113,6 +113,7 @@ def _declare(L):
     L.orc_p_coll_e_exact.restype = C.c_double
     L.orc_accumulate_density.argtypes = [_f32p, _f64p, C.c_uint32]
     L.orc_accumulate_eepf.argtypes = [_f32p] * 5 + [C.c_uint32, _u32p, P(OrcPhys)]
+    L.orc_xt_accumulate.argtypes = [_f32p] * 5 + [C.c_uint32, C.c_int, _f32p, P(OrcPhys), _f64p]
 
 
 def default_params(**overrides):
@@ -265,3 +266,39 @@ def accumulate_density(density, cumul):
 def accumulate_eepf(x, vx, vy, vz, efield, n_active, eepf, ph):
     lib().orc_accumulate_eepf(_f32(x), _f32(vx), _f32(vy), _f32(vz), _f32(efield), n_active, eepf,
                               C.byref(ph))
+
+
+def xt_accumulate(efield, x, vx, vy, vz, ions, cs_ion, ph):
+    """One step of eduPIC's XT measurement branch for one species: an array
+    [3 or 4, n_g] of the weight, velocity, energy (and ionization-rate) sums."""
+    n_g = ph.n_g
+    out = np.zeros(4 * n_g, np.float64)  # the ions leave the rate row untouched
+    cs = _f32(cs_ion if cs_ion is not None else np.zeros(1, np.float32))
+    lib().orc_xt_accumulate(_f32(efield), _f32(x), _f32(vx), _f32(vy), _f32(vz), len(x), 1 if ions else 0, cs,
+                            C.byref(ph), out)
+    return out.reshape(4, n_g)[:3 if ions else 4]
+
+
+def xt_normalise(raw, n_t, n_xt, measure_steps, gap, n_g, frequency, weight, electrode_area):
+    """norm_all_xt, C/eduPIC.cc:864-903: the eleven quantities (pot, efield,
+    ne, ni, je, ji, powere, poweri, meanee, meanei, ioniz) from the raw sums
+    raw[name] ([n_g, n_xt] each: count_e, ue, meanee, ioniz, count_i, ui,
+    meanei, pot, efield, ne, ni)."""
+    e_charge = 1.60217662e-19
+    cycles = measure_steps / n_t
+    dx = gap / (n_g - 1)
+    f1 = n_xt / (cycles * n_t)
+    f2 = weight / (electrode_area * dx) / (cycles * ((1.0 / frequency) / n_xt))
+    out = {k: raw[k] * f1 for k in ("pot", "efield", "ne", "ni")}
+    ce, ci = raw["count_e"], raw["count_i"]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ue = np.where(ce > 0, raw["ue"] / ce, 0.0)
+        ui = np.where(ci > 0, raw["ui"] / ci, 0.0)
+        out["je"] = np.where(ce > 0, -ue * out["ne"] * e_charge, 0.0)
+        out["meanee"] = np.where(ce > 0, raw["meanee"] / ce, 0.0)
+        out["ioniz"] = np.where(ce > 0, raw["ioniz"] * f2, 0.0)
+        out["ji"] = np.where(ci > 0, ui * out["ni"] * e_charge, 0.0)
+        out["meanei"] = np.where(ci > 0, raw["meanei"] / ci, 0.0)
+    out["powere"] = out["je"] * out["efield"]
+    out["poweri"] = out["ji"] * out["efield"]
+    return out
