@@ -13,6 +13,13 @@ timed on the device with events on the batch's stream.
 ``shard`` spreads discharges over the ranks of a multi-GPU job (no
 collective during the run: the discharges are independent); ``gather``
 collects per-rank results on every rank through ``torch.distributed``.
+
+    python -m cudapic_b200.batch [--discharges 256 | --one-discharge N] [--steps 40]
+                                 [--tune | --rows R --ctas C --stages S --copies K]
+
+times a batch (the C2 sweep, or one argon CCP of N particles per species at
+the reference parameters) and prints one JSON line: the target of the
+committed ncu captures of the batched kernels.
 """
 import math
 from dataclasses import asdict, dataclass
@@ -185,3 +192,47 @@ class Batch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--discharges", type=int, default=256)
+    ap.add_argument("--one-discharge", type=int, default=0,
+                    help="one discharge of N particles per species at the reference parameters instead of the sweep")
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=40)
+    ap.add_argument("--tune", action="store_true", help="autotune the batched kernels' launch shapes first")
+    ap.add_argument("--rows", type=int)
+    ap.add_argument("--ctas", type=int)
+    ap.add_argument("--stages", type=int)
+    ap.add_argument("--copies", type=int)
+    a = ap.parse_args(argv)
+    import cudapic_b200 as cp
+    if a.one_discharge:
+        specs = [DischargeSpec(voltage=250.0, pressure=10.0, gap=0.025, n_g=400, particles=a.one_discharge, seed=17)]
+    else:
+        specs = c2_specs(n=a.discharges)
+    shape = {k: v for k, v in (("step_rows", a.rows), ("step_ctas_per_sm", a.ctas), ("step_stages", a.stages),
+                               ("density_copies", a.copies)) if v}
+    if shape:
+        cp.set_tuning(**shape)
+    with Batch(specs) as b:
+        b.run_steps(a.warmup)
+        b.synchronize()
+        if a.tune:
+            from cudapic_b200.autotune import tune_batch
+            tune_batch(b)
+            b.run_steps(a.warmup)
+        t, w = b.timed_steps(a.steps)
+        tu = cp.get_tuning()
+        print(json.dumps({"discharges": len(specs), "steps": a.steps, "particle_steps_per_s": w / t,
+                          "ms_per_step": 1e3 * t / a.steps, "device_errors": sum(1 for e in b.device_errors() if e),
+                          "shape": {k: tu[k] for k in ("step_rows", "step_ctas_per_sm", "step_stages",
+                                                       "density_copies")}}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
