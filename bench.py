@@ -115,6 +115,9 @@ def measured_peaks():
 # ---------------------------------------------------------------- clocks
 
 class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 20 ms; only the samples
+    taken between __enter__ (which returns once the sampler is running) and
+    __exit__ -- the timed region -- are summarised."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
@@ -122,25 +125,43 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
+        self.lines = []
+        self.out = ""
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.perf_counter(), line))
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        deadline = time.perf_counter() + 5.0
+        while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.t0 = time.perf_counter()
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out, _ = self.proc.communicate()
+        if self.proc is None:
+            return
+        t1 = time.perf_counter() + 0.025  # the sample in flight at the end of the region
+        time.sleep(0.03)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            self.proc.wait()
+        self.reader.join(timeout=5)
+        self.out = "".join(line for t, line in self.lines if self.t0 <= t <= t1)
 
     def summary(self):
         sm, mx, reasons = [], [], set()
