@@ -16,6 +16,10 @@ It writes:
   edupic_ref_eepf.txt    -- its EEPF (Figure12_eepf.dat).
   edupic_ref_conv_tail.txt -- last 100 cycles of its particle counts
       (Figure9_conv.dat).
+  edupic_ref_xt_means.txt -- its XT maps (Figure11*_xt.dat) averaged over
+      the RF period: one row per node, columns pot, efield, je, ji, heate,
+      heati, meanee, meanei, ioniz.
+  edupic_ref_ifed.txt    -- its IFEDs at both electrodes (Figure13_ifed.dat).
   edupic_c0_conv.txt     -- cycle, N_e, N_i of the reference CPU program
       (eduPIC 1.0 built from C/eduPIC.cc by oracle/Makefile, Mersenne
       Twister seed 5489) for the init cycle plus 10 cycles from 1000 + 1000
@@ -45,6 +49,17 @@ def main():
     raw = os.path.join(REF, "C", "ReferenceCase_RawData")
     shutil.copyfile(os.path.join(raw, "Figure10_density.dat"), os.path.join(HERE, "edupic_ref_density.txt"))
     shutil.copyfile(os.path.join(raw, "Figure12_eepf.dat"), os.path.join(HERE, "edupic_ref_eepf.txt"))
+    shutil.copyfile(os.path.join(raw, "Figure13_ifed.dat"), os.path.join(HERE, "edupic_ref_ifed.txt"))
+    cols = []
+    for name in ("c)_pot", "d)_efield", "e)_je", "f)_ji", "g)_heate", "h)_heati", "i)_meanee", "j)_meanei",
+                 "k)_ioniz"):
+        with open(os.path.join(raw, "Figure11%s_xt.dat" % name)) as f:
+            rows = [[float(v) for v in ln.split()] for ln in f if ln.strip()]
+        cols.append([sum(r) / len(r) for r in rows])
+    with open(os.path.join(HERE, "edupic_ref_xt_means.txt"), "w") as f:
+        f.write("# pot efield je ji heate heati meanee meanei ioniz (RF-period averages per node)\n")
+        for k in range(len(cols[0])):
+            f.write("  ".join("%.6e" % c[k] for c in cols) + "\n")
     with open(os.path.join(raw, "Figure9_conv.dat")) as f:
         lines = [ln for ln in f if ln.strip()]
     with open(os.path.join(HERE, "edupic_ref_conv_tail.txt"), "w") as f:
