@@ -1,0 +1,192 @@
+"""Runs against eduPIC's reference case and reports the end-to-end error.
+
+eduPIC (C/eduPIC.cc, FP64) ships a converged reference case
+(C/ReferenceCase_RawData: argon, 25 mm, 250 V, 13.56 MHz, 10 Pa, ~107 k
+electrons after ~7900 RF cycles).  This module starts discharges near that
+steady state -- electrons and ions sampled from the reference's
+time-averaged density profiles with 3 eV / 0.03 eV Maxwellians -- lets them
+relax, measures a window, and compares with eduPIC's outputs normalised as
+eduPIC normalises them:
+
+  * n_e, n_i: cycle-averaged densities (save_density, C/eduPIC.cc:787-798);
+  * potential: the XT potential map averaged over the RF period (Fig. 11c);
+  * EEPF: save_eepf (:804-818), compared below 15 eV;
+  * <j E> electron power density (:1011-1026, the mean of Fig. 11g);
+  * the electron count (the mean of the last 100 cycles of Fig. 9).
+
+Errors are relative L2 norms (relative differences for the scalars); each
+mode runs two seeds side by side, and their difference is the statistical
+noise floor.  Arithmetic modes:
+
+  * ``mixed``: the fused driver -- f32 particles, 2^-20 fixed-point deposits
+    summed exactly in 64-bit integers, FP64 Poisson scans and FP64 time
+    averages (the default path);
+  * ``f32_poisson``: the same with the reference's f32 Poisson scans;
+  * ``reference_f32``: the reference's launch sequence with f32 atomic
+    deposits and f32 Poisson scans (the arithmetic of the reference's GPU path).
+
+    python -m cudapic_b200.refcase --reference DIR [--modes mixed,f32_poisson,reference_f32]
+                                   [--relax 300] [--measure 100]
+
+DIR holds eduPIC's reference outputs under the names of tests/golden
+(edupic_ref_density.txt, edupic_ref_eepf.txt, edupic_ref_xt_means.txt,
+edupic_ref_conv_tail.txt).
+"""
+import json
+import os
+
+import numpy as np
+
+E_MASS = 9.10938356e-31
+AR_MASS = 6.63352090e-26
+E_CHARGE = 1.60217662e-19
+DE_EEPF = 0.05
+EEPF_BAND_EV = 15.0
+
+MODES = ("mixed", "f32_poisson", "reference_f32")
+
+
+def load_reference(directory):
+    """eduPIC's reference-case outputs: density [N_G, 3] (x, n_e, n_i), EEPF
+    [2000, 2], RF-period means of the XT maps [N_G, 9] (pot, efield, je, ji,
+    heate, heati, meanee, meanei, ioniz), the last 100 cycles of the counts."""
+    def f(name):
+        return np.loadtxt(os.path.join(directory, name))
+    return {"density": f("edupic_ref_density.txt"), "eepf": f("edupic_ref_eepf.txt"),
+            "xt_means": f("edupic_ref_xt_means.txt"), "conv_tail": f("edupic_ref_conv_tail.txt")}
+
+
+def sample_profile(dens, dx, weight, area, mass, t_ev, rng):
+    """Superparticles distributed like a nodal density profile (each cell at
+    the mean of its nodes, uniform inside), Maxwellian velocities at t_ev."""
+    cell = 0.5 * (dens[:-1] + dens[1:])
+    n = int(round(cell.sum() * dx * area / weight))
+    k = rng.choice(len(cell), size=n, p=cell / cell.sum())
+    x = ((k + rng.random(n)) * dx).astype(np.float32)
+    s = np.sqrt(t_ev * E_CHARGE / mass)
+    v = rng.normal(0.0, s, (3, n)).astype(np.float32)
+    return x, v[0], v[1], v[2]
+
+
+def start_states(ref, mode, seeds=(1, 2), capacity=400_000):
+    """One state per seed at the reference parameters, particles from the
+    reference profiles, in the arithmetic of `mode`."""
+    import cudapic_b200 as cp
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    flags = 0
+    if mode in ("f32_poisson", "reference_f32"):
+        flags |= cp.FLAG_POISSON_F32_SCAN
+    if mode == "reference_f32":
+        flags |= cp.FLAG_DEPOSIT_F32
+    states = []
+    try:
+        for seed in seeds:
+            p = cp.default_params(capacity=capacity, flags=flags)
+            st = GpuSimState(p)
+            states.append(st)
+            if mode == "reference_f32":
+                st.set_fused(False)
+            dx = p.gap / (p.n_g - 1)
+            rng = np.random.default_rng(seed)
+            d = ref["density"]
+            st.upload_electrons(ParticlesSoA(*sample_profile(d[:, 1], dx, p.weight, p.electrode_area, E_MASS, 3.0,
+                                                             rng)))
+            st.upload_ions(ParticlesSoA(*sample_profile(d[:, 2], dx, p.weight, p.electrode_area, AR_MASS, 0.03,
+                                                        rng)))
+            st.seed(e_master=(0x12345678 + seed, 0x11112222, 0x22223333, 0x33334444),
+                    i_master=(0x44445555 + seed, 0x55556666, 0x66667777, 0x77778888))
+    except Exception:
+        for st in states:
+            st.close()
+        raise
+    return states
+
+
+def run(states, relax, measure):
+    """relax cycles, then a measurement window of `measure` cycles; fused
+    states step together in one batch, others one after another."""
+    from cudapic_b200.sim import GpuBatch
+    if all(st.fused for st in states):
+        with GpuBatch(states) as b:
+            b.run_cycles(relax)
+            b.synchronize()
+            for st in states:
+                st.set_measure(True)
+            b.run_cycles(measure)
+            b.synchronize()
+    else:
+        for st in states:
+            st.run_cycles(relax)
+            st.set_measure(True)
+            st.run_cycles(measure)
+            st.synchronize()
+
+
+def outputs(st, measure):
+    """A state's measurement window normalised as eduPIC's outputs."""
+    steps = measure * st.params.n_t
+    ce, ci, eepf = st.download_measurements()
+    # the ion density is summed on ion steps only (Rust-CUDA/src/main.rs:1752,
+    # averaged over them at :1586); eduPIC sums the held density every step
+    ion_steps = steps // st.params.n_sub
+    counts = eepf.astype(np.float64)
+    energy = (np.arange(len(counts)) + 0.5) * DE_EEPF
+    r = st.report()
+    return {"ne": ce / steps, "ni": ci / ion_steps, "pot": st.download_xt("pot").mean(axis=1),
+            "eepf": counts / (counts.sum() * DE_EEPF) / np.sqrt(energy), "power_e": r["power_e"],
+            "count_e": float(st.counts()[0]), "device_error": st.device_error()}
+
+
+def compare(got, ref):
+    """(errors, seed-to-seed spread) of the outputs of two or more seeds
+    against the reference: the largest error over the seeds, the spread
+    between the first two."""
+    band = (np.arange(len(ref["eepf"])) + 0.5) * DE_EEPF < EEPF_BAND_EV
+    want = {"ne": ref["density"][:, 1], "ni": ref["density"][:, 2], "pot": ref["xt_means"][:, 0],
+            "eepf": ref["eepf"][:, 1], "power_e": float(ref["xt_means"][:, 4].mean()),
+            "count_e": float(ref["conv_tail"][:, 1].mean())}
+
+    def rel_l2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    errors, spread = {}, {}
+    for key in ("ne", "ni", "pot", "eepf", "power_e", "count_e"):
+        if key in ("power_e", "count_e"):
+            errors[key] = max(abs(g[key] / want[key] - 1.0) for g in got)
+            spread[key] = abs(got[0][key] / got[1][key] - 1.0)
+        else:
+            sel = band if key == "eepf" else slice(None)
+            errors[key] = max(rel_l2(g[key][sel], want[key][sel]) for g in got)
+            spread[key] = rel_l2(got[0][key][sel], got[1][key][sel])
+    return errors, spread
+
+
+def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
+    states = start_states(ref, mode, seeds)
+    try:
+        run(states, relax, measure)
+        got = [outputs(st, measure) for st in states]
+    finally:
+        for st in states:
+            st.close()
+    errors, spread = compare(got, ref)
+    return {"mode": mode, "relax_cycles": relax, "measured_cycles": measure, "seeds": list(seeds),
+            "errors": errors, "seed_spread": spread, "device_errors": [g["device_error"] for g in got]}
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, help="directory of eduPIC's reference-case outputs")
+    ap.add_argument("--modes", default=",".join(MODES))
+    ap.add_argument("--relax", type=int, default=300)
+    ap.add_argument("--measure", type=int, default=100)
+    a = ap.parse_args(argv)
+    ref = load_reference(a.reference)
+    for mode in a.modes.split(","):
+        print(json.dumps(study(ref, mode, a.relax, a.measure)), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

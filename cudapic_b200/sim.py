@@ -53,6 +53,7 @@ class GpuSimState:
         self.grid = _lib.Grid()
         check(lib.cudapic_state_grid(self._h, C.byref(self.grid)))
         self.capacity = self.grid.capacity
+        self.fused = True
 
     # -- lifetime -----------------------------------------------------
     @classmethod
@@ -138,6 +139,7 @@ class GpuSimState:
         the next density in one launch (default on); off: the reference's
         launch sequence."""
         check(lib.cudapic_state_set_fused(self._h, 1 if on else 0))
+        self.fused = bool(on)
 
     def set_graphs(self, on=True):
         """Replay captured CUDA graphs (default) or launch every step from the host."""

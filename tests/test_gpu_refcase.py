@@ -1,116 +1,37 @@
 """End-to-end physics against eduPIC: the reference case of
 C/ReferenceCase_RawData (eduPIC in FP64, converged over ~7900 RF cycles:
-argon, 25 mm, 250 V, 13.56 MHz, 10 Pa) against this library's driver.
-
-Converging from 1000 particles takes thousands of cycles, so the run starts
-near the steady state: electrons and ions are sampled from the reference's
-time-averaged density profiles (3 eV / 0.03 eV Maxwellians), relax for
-RELAX cycles, then a measurement window of MEASURE cycles is compared with
-the reference's cycle-averaged n_e, n_i (Figure 10), potential (Figure 11c
-averaged over the period), EEPF (Figure 12) and <j E> electron power
-(Figure 11g).  Two seeds run side by side in one batch; their difference
-is the statistical noise floor, printed with the errors.  The tolerances
-are the stated end-to-end error of the f32 path against the FP64 oracle.
+argon, 25 mm, 250 V, 13.56 MHz, 10 Pa) against this library's fused driver
+(cudapic_b200.refcase: two seeds started from the reference's density
+profiles, RELAX cycles of relaxation, MEASURE cycles measured).  Compared:
+cycle-averaged n_e, n_i (Figure 10), the period-averaged potential (Figure
+11c), the EEPF below 15 eV (Figure 12), the <j E> electron power (Figure
+11g) and the electron count (Figure 9).  The tolerances are the stated
+end-to-end error of the f32 path against the FP64 oracle; the two seeds'
+difference (printed) is the statistical noise floor.
 """
 import os
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-E_MASS = 9.10938356e-31
-AR_MASS = 6.63352090e-26
-E_CHARGE = 1.60217662e-19
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 RELAX, MEASURE = 300, 100
-# stated end-to-end error (relative L2) against the FP64 reference case
-# (measured: n_e 0.054, EEPF 0.042, power 0.014, N_e 0.051, potential 0.002 at a
-# seed-to-seed spread of 0.002-0.011; the few per cent of n_e and N_e follow
-# the GPU reference's model differences from eduPIC, e.g. electrons spawned
-# in a step do not collide in the same step)
+# Measured: n_e 0.054, EEPF 0.042, power 0.014, N_e 0.051, potential 0.002
+# at a seed-to-seed spread of 0.002-0.011; the few per cent of n_e and N_e
+# follow the GPU reference's model differences from eduPIC (for example,
+# electrons spawned in a step do not collide in the same step).
 TOL = {"ne": 0.08, "ni": 0.08, "pot": 0.02, "eepf": 0.08, "power_e": 0.05, "count_e": 0.08}
 
 
-def _rel_l2(a, b):
-    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
-
-
-def _sample(dens, dx, weight, area, mass, t_ev, rng):
-    """Particles distributed like the nodal density profile (piecewise
-    constant per cell at the cell mean), Maxwellian velocities."""
-    cell = 0.5 * (dens[:-1] + dens[1:])
-    n = int(round(cell.sum() * dx * area / weight))
-    k = rng.choice(len(cell), size=n, p=cell / cell.sum())
-    x = ((k + rng.random(n)) * dx).astype(np.float32)
-    s = np.sqrt(t_ev * E_CHARGE / mass)
-    v = rng.normal(0.0, s, (3, n)).astype(np.float32)
-    return x, v[0], v[1], v[2]
-
-
-def _eepf(counts):
-    """eduPIC's normalisation (C/eduPIC.cc:804-818): f(E) = count / (sum dE) / sqrt(E)."""
-    de = 0.05
-    e = (np.arange(len(counts)) + 0.5) * de
-    return e, counts / (counts.sum() * de) / np.sqrt(e)
-
-
 def test_reference_case_profiles_against_edupic(cudapic, cuda_device):
-    import cudapic_b200 as cp
-    from cudapic_b200.sim import GpuBatch, GpuSimState, ParticlesSoA
-    ref_d = np.loadtxt(os.path.join(GOLDEN, "edupic_ref_density.txt"))
-    ref_eepf = np.loadtxt(os.path.join(GOLDEN, "edupic_ref_eepf.txt"))
-    ref_xt = np.loadtxt(os.path.join(GOLDEN, "edupic_ref_xt_means.txt"))
-    ref_conv = np.loadtxt(os.path.join(GOLDEN, "edupic_ref_conv_tail.txt"))
-    states = []
-    try:
-        for seed in (1, 2):
-            p = cp.default_params(capacity=400_000)
-            st = GpuSimState(p)
-            dx = p.gap / (p.n_g - 1)
-            rng = np.random.default_rng(seed)
-            st.upload_electrons(ParticlesSoA(*_sample(ref_d[:, 1], dx, p.weight, p.electrode_area, E_MASS, 3.0, rng)))
-            st.upload_ions(ParticlesSoA(*_sample(ref_d[:, 2], dx, p.weight, p.electrode_area, AR_MASS, 0.03, rng)))
-            st.seed(e_master=(0x12345678 + seed, 0x11112222, 0x22223333, 0x33334444),
-                    i_master=(0x44445555 + seed, 0x55556666, 0x66667777, 0x77778888))
-            states.append(st)
-        with GpuBatch(states) as b:
-            b.run_cycles(RELAX)
-            b.synchronize()
-            for st in states:
-                st.set_measure(True)
-            b.run_cycles(MEASURE)
-            b.synchronize()
-        got = []
-        for st in states:
-            assert st.device_error() == 0
-            steps = MEASURE * st.params.n_t
-            ce, ci, eepf = st.download_measurements()
-            r = st.report()
-            # the ion density is summed on ion steps only (Rust-CUDA/src/main.rs:1752,
-            # averaged over them at :1586); eduPIC sums the held density every step
-            ion_steps = steps // st.params.n_sub
-            got.append({"ne": ce / steps, "ni": ci / ion_steps, "pot": st.download_xt("pot").mean(axis=1),
-                        "eepf": _eepf(eepf.astype(np.float64))[1], "power_e": r["power_e"],
-                        "count_e": float(st.counts()[0])})
-        e_ref = _eepf(np.ones(2000))[0]
-        band = e_ref < 15.0                      # the populated part of the EEPF
-        want = {"ne": ref_d[:, 1], "ni": ref_d[:, 2], "pot": ref_xt[:, 0], "eepf": ref_eepf[:, 1],
-                "power_e": float(ref_xt[:, 4].mean()), "count_e": float(ref_conv[:, 1].mean())}
-        errors, spread = {}, {}
-        for key in TOL:
-            if key in ("power_e", "count_e"):
-                errors[key] = max(abs(g[key] / want[key] - 1.0) for g in got)
-                spread[key] = abs(got[0][key] / got[1][key] - 1.0)
-            else:
-                sel = band if key == "eepf" else slice(None)
-                errors[key] = max(_rel_l2(g[key][sel], want[key][sel]) for g in got)
-                spread[key] = _rel_l2(got[0][key][sel], got[1][key][sel])
-        print("\nreference case, %d relaxation + %d measured cycles, 2 seeds" % (RELAX, MEASURE))
-        for key in TOL:
-            print("  %-8s error %.4f  seed-to-seed %.4f  tolerance %.2f" % (key, errors[key], spread[key], TOL[key]))
-        for key in TOL:
-            assert errors[key] <= TOL[key], (key, errors[key], spread[key])
-    finally:
-        for st in states:
-            st.close()
+    from cudapic_b200 import refcase
+    ref = refcase.load_reference(GOLDEN)
+    r = refcase.study(ref, "mixed", RELAX, MEASURE)
+    print("\nreference case, %d relaxation + %d measured cycles, 2 seeds" % (RELAX, MEASURE))
+    for key in TOL:
+        print("  %-8s error %.4f  seed-to-seed %.4f  tolerance %.2f"
+              % (key, r["errors"][key], r["seed_spread"][key], TOL[key]))
+    assert r["device_errors"] == [0, 0]
+    for key in TOL:
+        assert r["errors"][key] <= TOL[key], (key, r["errors"][key], r["seed_spread"][key])
