@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(ES_THREADS, MINB)
     __shared__ StepDisc s_dc;
     __shared__ cudapic_grid s_g;
     __shared__ uint32_t s_d, s_off;
-    const StepSmem<U, MCC> sm(smem, stages, copies, ef_pad, offs, s_base);
+    __shared__ uint32_t ccnt[3][StepShape<U, MCC>::NSEG];
+    const StepSmem<U, MCC> sm(smem, stages, copies, ef_pad, offs, s_base, ccnt);
     uint32_t *P = reinterpret_cast<uint32_t *>(sm.end(stages));  // [D + 1]
     step_smem_init(sm, stages, copies, ef_pad);
     grid_dep_wait();

@@ -64,7 +64,8 @@ __global__ void __launch_bounds__(ES_THREADS)
     // may still be storing the tile before the previous one.
     __shared__ uint32_t offs[3][StepShape<U, true>::NSEG];
     __shared__ uint32_t s_base[3];
-    const StepSmem<U, true> sm(smem, stages, copies, ef_pad, offs, s_base);
+    __shared__ uint32_t ccnt[3][StepShape<U, true>::NSEG];
+    const StepSmem<U, true> sm(smem, stages, copies, ef_pad, offs, s_base, ccnt);
     step_smem_init(sm, stages, copies, ef_pad);
     grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);

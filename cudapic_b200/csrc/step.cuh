@@ -24,14 +24,17 @@ constexpr int ES_THREADS = 256;
 constexpr int ES_WARPS = ES_THREADS / 32;
 constexpr int ES_MAX_STAGES = 6;  // pipeline depth: cudapic_tuning.step_stages
 
-// U (cudapic_tuning.step_rows, 2 or 4): particles per thread and tile, so a
-// tile holds 256 U particles; a warp's collider queue holds 31 + 32 U
-// entries at most.  Planes: x, vx, vy, vz (+ rng0..3 with MCC).
+// U (cudapic_tuning.step_rows, 1, 2 or 4): particles per thread and tile,
+// so a tile holds 256 U particles.  Planes: x, vx, vy, vz (+ rng0..3 with
+// MCC).  Colliders wait in one CTA-wide queue until DRAIN_AT are pending
+// (or the segment ends); the queue then never holds more than
+// DRAIN_AT - 1 + TILE entries.
 template <int U, bool MCC>
 struct StepShape {
     static constexpr int TILE = ES_THREADS * U;
     static constexpr int PLANES = MCC ? 8 : 4;
-    static constexpr int QCAP = MCC ? 32 + 32 * U : 0;
+    static constexpr int DRAIN_AT = 2 * ES_THREADS;
+    static constexpr int QCAP = MCC ? DRAIN_AT + TILE : 0;
     static constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
     static_assert(U * ES_WARPS <= 32, "one warp scans the (row, warp) counts");
 };
@@ -43,7 +46,7 @@ template <int U, bool MCC>
 __host__ __device__ constexpr size_t step_smem_bytes(int stages, int copies, uint32_t ef_pad) {
     using S = StepShape<U, MCC>;
     return (size_t)stages * S::PLANES * S::TILE * 4 + (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 +
-           (size_t)ES_WARPS * S::QCAP * 4 + (size_t)stages * sizeof(uint64_t);
+           (size_t)S::QCAP * 4 + (size_t)stages * sizeof(uint64_t);
 }
 
 // A per-discharge pointer of a segment's StepDisc that the tile loop uses
@@ -85,18 +88,21 @@ struct StepSmem {
     uint64_t *bar;
     uint32_t (*offs)[StepShape<U, MCC>::NSEG];  // [3][NSEG]
     uint32_t *s_base;                            // [3]
+    uint32_t (*ccnt)[StepShape<U, MCC>::NSEG];   // [3][NSEG] colliders per (row, warp) (MCC)
 
     __device__ __forceinline__ StepSmem(unsigned char *smem, int stages, int copies, uint32_t ef_pad,
-                                        uint32_t (*offs_)[StepShape<U, MCC>::NSEG], uint32_t *s_base_) {
+                                        uint32_t (*offs_)[StepShape<U, MCC>::NSEG], uint32_t *s_base_,
+                                        uint32_t (*ccnt_)[StepShape<U, MCC>::NSEG]) {
         using S = StepShape<U, MCC>;
         in = reinterpret_cast<uint32_t *>(smem);
         ef = reinterpret_cast<float *>(in + stages * S::PLANES * S::TILE);
         acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);
         hist = reinterpret_cast<uint32_t *>(acc + ef_pad);
         queue = hist + (uint32_t)copies * ef_pad;
-        bar = reinterpret_cast<uint64_t *>(queue + ES_WARPS * S::QCAP);
+        bar = reinterpret_cast<uint64_t *>(queue + S::QCAP);
         offs = offs_;
         s_base = s_base_;
+        ccnt = ccnt_;
     }
     // end of the carved region (the batched kernels put their plan there)
     __device__ __forceinline__ unsigned char *end(int stages) const {
@@ -187,19 +193,20 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
 
     for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.ef[k] = dcp<SH>(dc.efield)[k];
     uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
-    uint32_t *wq = sm.queue + warp * QCAP;
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < stages; ++s)
             if ((uint32_t)s < ntiles) issue((uint32_t)s, (int)((it0 + (uint32_t)s) % (uint32_t)stages));
     }
 
-    // Scatters wq[first, first + count), one collider per lane.
-    auto drain = [&](uint32_t first, uint32_t count) {
+    // Scatters the queued colliders sm.queue[0, count), one per thread and
+    // round: all the CTA's threads work the independent collision chains
+    // together.  The caller has synchronised since the last queue write.
+    auto drain = [&](uint32_t count) {
         unsigned long long *ncoll = dcp<SH>(dc.coll);
-        if (ncoll && lane == 0) atomicAdd(ncoll, (unsigned long long)count);  // collision events (measurement)
-        if ((uint32_t)lane < count) {
-            const uint32_t i = off + wq[first + lane];
+        if (ncoll && tid == 0) atomicAdd(ncoll, (unsigned long long)count);  // collision events (measurement)
+        for (uint32_t q = tid; q < count; q += ES_THREADS) {
+            const uint32_t i = off + sm.queue[q];
             const PushResult pr = push_one_c(pl.sx[i], pl.svx[i], sm.ef, factor, dt, inv_dx, n_g, gap, gm);
             const float vy = pl.svy[i], vz = pl.svz[i];
             Xoshiro128p rs{pl.rng0[i], pl.rng1[i], pl.rng2[i], pl.rng3[i]};
@@ -220,14 +227,13 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
             pl.rng2[i] = rs.s2;
             pl.rng3[i] = rs.s3;
         }
-        __syncwarp();
     };
 
     StepOut<U> prev;
     bool have_prev = false;
     bool ok = true;
     uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
-    uint32_t qn = 0;            // this warp's queued colliders (warp-uniform)
+    uint32_t qn = 0;            // queued colliders of the CTA (uniform: every thread counts the same)
     uint32_t tile = 0;
     for (; tile < ntiles; ++tile) {
         const uint32_t k = it0 + tile;  // position in the stage ring
@@ -332,8 +338,7 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
             if (lane == 0) sm.offs[r3][u * ES_WARPS + warp] = __popc(m);
             if (MCC) {
                 const unsigned cm = __ballot_sync(0xffffffffu, collide);
-                if (collide) wq[qn + __popc(cm & lt)] = t0 + j;
-                qn += __popc(cm);
+                if (lane == 0) sm.ccnt[r3][u * ES_WARPS + warp] = __popc(cm);
             }
         }
         // publish the previous tile's base (its atomic had this iteration to return)
@@ -379,9 +384,30 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
         prev = cur;
         have_prev = true;
         if (MCC) {
-            while (qn >= 32) {  // full-warp drains from the top of the queue
-                qn -= 32;
-                drain(qn, 32);
+            // queue this tile's colliders behind the earlier ones: every warp
+            // scans the (row, warp) counts, which the tile barrier made visible
+            // and which stay until the tile after next
+            const uint32_t c = lane < NSEG ? sm.ccnt[r3][lane] : 0u;
+            uint32_t cincl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, cincl, o);
+                if (lane >= o) cincl += t;
+            }
+            const uint32_t total = __shfl_sync(0xffffffffu, cincl, 31);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const bool collide = coll >> u & 1u;
+                const unsigned cm = __ballot_sync(0xffffffffu, collide);
+                const uint32_t seg = (uint32_t)(u * ES_WARPS + warp);
+                const uint32_t before = __shfl_sync(0xffffffffu, cincl - c, (int)seg);
+                if (collide) sm.queue[qn + before + __popc(cm & lt)] = t0 + (uint32_t)u * ES_THREADS + tid;
+            }
+            qn += total;
+            if (qn >= (uint32_t)S::DRAIN_AT) {  // uniform: every thread holds the same qn
+                __syncthreads();
+                drain(qn);
+                qn = 0;
             }
         }
     }
@@ -405,7 +431,10 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
             }
         }
     }
-    if (MCC && qn) drain(0, qn);
+    if (MCC && qn) {
+        __syncthreads();
+        drain(qn);
+    }
     __syncthreads();
     dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
     __syncthreads();
