@@ -33,7 +33,7 @@ template <int U, bool MCC>
 struct StepShape {
     static constexpr int TILE = ES_THREADS * U;
     static constexpr int PLANES = MCC ? 8 : 4;
-    static constexpr int DRAIN_AT = 2 * ES_THREADS;
+    static constexpr int DRAIN_AT = 4 * ES_THREADS;
     static constexpr int QCAP = MCC ? DRAIN_AT + TILE : 0;
     static constexpr int NSEG = U * ES_WARPS;  // (row, warp) segments of a tile
     static_assert(U * ES_WARPS <= 32, "one warp scans the (row, warp) counts");
