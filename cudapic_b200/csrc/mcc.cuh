@@ -37,6 +37,39 @@ __device__ __forceinline__ Euler euler_angles(float gx, float gy, float gz) {
     return e;
 }
 
+// The same angles' sines and cosines from their exact algebraic forms,
+// without the angles: sin theta = r / |g|, cos theta = gx / |g| with
+// r = sqrt(gy^2 + gz^2), and sin phi = gz / r, cos phi = gy / r (the special
+// cases gx = 0 and gy = 0 as above, with cos(+-pi/2) = 0 exactly).  Equal to
+// euler_angles up to the rounding of the transcendentals it skips.
+__device__ __forceinline__ Euler euler_angles_alg(float gx, float gy, float gz) {
+    Euler e;
+    const float r2 = gy * gy + gz * gz;
+    const float r = sqrtf(r2);
+    if (gx == 0.0f) {
+        e.st = 1.0f;
+        e.ct = 0.0f;
+    } else {
+        const float gn = sqrtf(gx * gx + r2);
+        e.st = r / gn;
+        e.ct = gx / gn;
+    }
+    if (gy == 0.0f) {
+        e.sp = (gz > 0.0f) ? 1.0f : -1.0f;
+        e.cp = 0.0f;
+    } else {
+        e.sp = gz / r;
+        e.cp = gy / r;
+    }
+    return e;
+}
+
+// sin and cos of acos(c), c in [-1, 1]: sqrt((1 - c)(1 + c)) and c.
+__device__ __forceinline__ void sincos_of_acos(float c, float *s, float *co) {
+    *s = sqrtf(fmaxf(0.0f, (1.0f - c) * (1.0f + c)));
+    *co = c;
+}
+
 // Scattered relative velocity, Rust-CUDA/src/main.rs:1152-1158.
 __device__ __forceinline__ void rotate(float g, float sc, float cc, float se, float ce, const Euler &a, float &gx,
                                        float &gy, float &gz) {
@@ -132,11 +165,18 @@ __device__ __forceinline__ void deposit_global(float *dens, float xv, const cuda
 // (may be null): next-step densities that also receive the spawned
 // electron / ion.  Slots (i and the spawns' claimed slots) are relative to
 // element `off` of the planes (a discharge of a batch's pool; 0 otherwise).
-static __device__ __noinline__ uint32_t collide_electron(uint32_t off, uint32_t i, uint32_t idx, float vxi, float vyi, float vzi,
-                                                  Xoshiro128p &rs, const float *__restrict__ cs, float *x, float *vx,
-                                                  float *vy, float *vz, float *ix, float *ivx, float *ivy,
-                                                  float *ivz, uint32_t *alive_e, uint32_t *alive_i,
-                                                  const cudapic_grid &g, float *dep_e, float *dep_i) {
+// ALG: the sines and cosines of the Euler angles, of the scattering angles
+// chi = acos(c) and of eta + pi from their algebraic forms (euler_angles_alg,
+// sincos_of_acos, sin(eta + pi) = -sin eta) instead of evaluating the
+// angles: the same draws and events, velocities equal up to the rounding of
+// the skipped transcendentals, a fraction of the arithmetic.
+template <bool ALG>
+static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_t i, uint32_t idx, float vxi,
+                                                    float vyi, float vzi, Xoshiro128p &rs,
+                                                    const float *__restrict__ cs, float *x, float *vx, float *vy,
+                                                    float *vz, float *ix, float *ivx, float *ivy, float *ivz,
+                                                    uint32_t *alive_e, uint32_t *alive_i, const cudapic_grid &g,
+                                                    float *dep_e, float *dep_i) {
     const float exc_j = 11.5f * E_CHARGE_F;
     const float ion_j = 15.8f * E_CHARGE_F;
     float gx = vxi, gy = vyi, gz = vzi;
@@ -145,23 +185,25 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t off, uint32_t 
     const float t0 = __ldg(cs + idx);
     const float t1 = t0 + __ldg(cs + CS_RANGES + idx);
     const float t2 = t1 + __ldg(cs + 2 * CS_RANGES + idx);
-    const Euler eu = euler_angles(gx, gy, gz);
-    float chi_s, chi_c, eta;
+    const Euler eu = ALG ? euler_angles_alg(gx, gy, gz) : euler_angles(gx, gy, gz);
+    float chi_s, chi_c, eta, se, ce;
     uint32_t ev;
     const float rnd = rs.uniform();
     if (rnd < t0 / t2) {
         ev = 1;  // elastic
-        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        const float c = 1.0f - 2.0f * rs.uniform();
         eta = TWO_PI_F * rs.uniform();
-        dm::sincosf_det(chi, &chi_s, &chi_c);
+        if (ALG) sincos_of_acos(c, &chi_s, &chi_c);
+        else dm::sincosf_det(dm::acosf_det(c), &chi_s, &chi_c);
     } else if (rnd < t1 / t2) {
         ev = 2;  // excitation
         float en = 0.5f * E_MASS_F * gm * gm;
         en = fabsf(en - exc_j);
         gm = sqrtf(2.0f * en / E_MASS_F);
-        const float chi = dm::acosf_det(1.0f - 2.0f * rs.uniform());
+        const float c = 1.0f - 2.0f * rs.uniform();
         eta = TWO_PI_F * rs.uniform();
-        dm::sincosf_det(chi, &chi_s, &chi_c);
+        if (ALG) sincos_of_acos(c, &chi_s, &chi_c);
+        else dm::sincosf_det(dm::acosf_det(c), &chi_s, &chi_c);
     } else {
         ev = 3;  // ionization
         float en = 0.5f * E_MASS_F * gm * gm;
@@ -171,13 +213,17 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t off, uint32_t 
         const float e_orig = fabsf(en - e_new);
         gm = sqrtf(2.0f * e_orig / E_MASS_F);
         const float g_new = sqrtf(2.0f * e_new / E_MASS_F);
-        const float chi = dm::acosf_det(sqrtf(e_orig / en));
-        const float chi_new = dm::acosf_det(sqrtf(e_new / en));
         eta = TWO_PI_F * rs.uniform();
-        const float eta_new = eta + PI_F;
         float sc2, cc2, se2, ce2;
-        dm::sincosf_det(chi_new, &sc2, &cc2);
-        dm::sincosf_det(eta_new, &se2, &ce2);
+        if (ALG) {  // eta_new = eta + pi
+            sincos_of_acos(sqrtf(e_new / en), &sc2, &cc2);
+            dm::sincosf_det(eta, &se, &ce);
+            se2 = -se;
+            ce2 = -ce;
+        } else {
+            dm::sincosf_det(dm::acosf_det(sqrtf(e_new / en)), &sc2, &cc2);
+            dm::sincosf_det(eta + PI_F, &se2, &ce2);
+        }
         float ngx, ngy, ngz;
         rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
         const float xi = x[off + i];
@@ -202,16 +248,27 @@ static __device__ __noinline__ uint32_t collide_electron(uint32_t off, uint32_t 
         } else {
             set_dev_err(g.dev_err, CUDAPIC_DEVERR_SPAWN_I);
         }
-        dm::sincosf_det(chi, &chi_s, &chi_c);
+        if (ALG) sincos_of_acos(sqrtf(e_orig / en), &chi_s, &chi_c);
+        else dm::sincosf_det(dm::acosf_det(sqrtf(e_orig / en)), &chi_s, &chi_c);
     }
-    float se, ce;
-    dm::sincosf_det(eta, &se, &ce);
+    if (!ALG || ev != 3) dm::sincosf_det(eta, &se, &ce);
     float ngx, ngy, ngz;
     rotate(gm, chi_s, chi_c, se, ce, eu, ngx, ngy, ngz);
     vx[off + i] = wx + g.f2 * ngx;
     vy[off + i] = wy + g.f2 * ngy;
     vz[off + i] = wz + g.f2 * ngz;
     return ev;
+}
+
+// The reference formulation (the drop-in collision kernels).
+static __device__ __forceinline__ uint32_t collide_electron(uint32_t off, uint32_t i, uint32_t idx, float vxi,
+                                                            float vyi, float vzi, Xoshiro128p &rs,
+                                                            const float *__restrict__ cs, float *x, float *vx,
+                                                            float *vy, float *vz, float *ix, float *ivx, float *ivy,
+                                                            float *ivz, uint32_t *alive_e, uint32_t *alive_i,
+                                                            const cudapic_grid &g, float *dep_e, float *dep_i) {
+    return collide_electron_t<false>(off, i, idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz, alive_e,
+                                     alive_i, g, dep_e, dep_i);
 }
 
 struct IonTest {

@@ -216,9 +216,9 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
             uint32_t *alive = dcp<SH>(dc.alive);
             if (claim_slot(alive, g.capacity, slot)) {
                 pl.dx[off + slot] = pr.x;
-                collide_electron(off, slot, t.idx, pr.vx, vy, vz, rs, dcp<SH>(dc.cs), pl.dx, pl.dvx, pl.dvy, pl.dvz,
-                                 pl.ix, pl.ivx, pl.ivy, pl.ivz, alive, dcp<SH>(dc.n_i), gm, dcp<SH>(dc.dens),
-                                 dcp<SH>(dc.dens_i));
+                collide_electron_t<true>(off, slot, t.idx, pr.vx, vy, vz, rs, dcp<SH>(dc.cs), pl.dx, pl.dvx, pl.dvy,
+                                         pl.dvz, pl.ix, pl.ivx, pl.ivy, pl.ivz, alive, dcp<SH>(dc.n_i), gm,
+                                         dcp<SH>(dc.dens), dcp<SH>(dc.dens_i));
             } else {
                 set_dev_err(gm.dev_err, CUDAPIC_DEVERR_SPAWN_E);
             }

@@ -471,6 +471,36 @@ static inline void euler_angles(float gx, float gy, float gz, float *st, float *
     *cp = orc_cosf(phi);
 }
 
+/* The same sines and cosines from their algebraic forms (the fused step's
+ * scattering, cudapic_b200/csrc/mcc.cuh euler_angles_alg): sin theta = r/|g|,
+ * cos theta = gx/|g|, sin phi = gz/r, cos phi = gy/r, r = sqrt(gy^2 + gz^2),
+ * with the special cases of euler_angles and cos(+-pi/2) = 0 exactly. */
+static inline void euler_angles_alg(float gx, float gy, float gz, float *st, float *ct, float *sp, float *cp) {
+    const float r2 = gy * gy + gz * gz;
+    const float r = sqrtf(r2);
+    if (gx == 0.0f) {
+        *st = 1.0f;
+        *ct = 0.0f;
+    } else {
+        const float gn = sqrtf(gx * gx + r2);
+        *st = r / gn;
+        *ct = gx / gn;
+    }
+    if (gy == 0.0f) {
+        *sp = (gz > 0.0f) ? 1.0f : -1.0f;
+        *cp = 0.0f;
+    } else {
+        *sp = gz / r;
+        *cp = gy / r;
+    }
+}
+
+/* sin and cos of acos(c): sqrt((1 - c)(1 + c)) and c. */
+static inline void sincos_of_acos(float c, float *s, float *co) {
+    *s = sqrtf(fmaxf(0.0f, (1.0f - c) * (1.0f + c)));
+    *co = c;
+}
+
 /* Rotation of a relative velocity of magnitude g by (chi, eta) in the frame
  * given by the Euler angles, Rust-CUDA/src/main.rs:1152-1158. */
 static inline void rotate(float g, float chi_s, float chi_c, float eta_s, float eta_c,
@@ -490,13 +520,15 @@ double orc_p_coll_e_exact(const float *sigma_tot_e, float vx, float vy, float vz
     return 1.0 - exp(-nu * (double)ph->dt_e);
 }
 
-/* check_collisions_e + collision_e, Rust-CUDA/src/main.rs:971-1165. */
-void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t n_active,
-                            float *x, float *vx, float *vy, float *vz,
-                            uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,
-                            float *ix, float *ivx, float *ivy, float *ivz,
-                            uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
-                            uint8_t *events, uint32_t *dropped) {
+/* check_collisions_e + collision_e, Rust-CUDA/src/main.rs:971-1165; alg:
+ * the sines and cosines of the Euler angles, of chi = acos(c) and of
+ * eta + pi from their algebraic forms (the fused step's scattering). */
+static void check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t n_active,
+                               float *x, float *vx, float *vy, float *vz,
+                               uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,
+                               float *ix, float *ivx, float *ivy, float *ivz,
+                               uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
+                               uint8_t *events, uint32_t *dropped, int alg) {
     const uint32_t R = ORC_CS_RANGES;
     const float me = (float)ORC_E_MASS;
     const float qe = (float)ORC_E_CHARGE;
@@ -521,22 +553,33 @@ void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t 
             float t1 = t0 + cs[1 * R + idx];
             float t2 = t1 + cs[2 * R + idx];
             float st, ct, sp, cp;
-            euler_angles(gx, gy, gz, &st, &ct, &sp, &cp);
+            if (alg) euler_angles_alg(gx, gy, gz, &st, &ct, &sp, &cp);
+            else euler_angles(gx, gy, gz, &st, &ct, &sp, &cp);
             float chi_s, chi_c, eta;
             float rnd = draw(&rs);
             if (rnd < t0 / t2) {
                 ev = 1;
-                float chi = orc_acosf(1.0f - 2.0f * draw(&rs));
+                float c = 1.0f - 2.0f * draw(&rs);
                 eta = F_TWO_PI * draw(&rs);
-                chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                if (alg) {
+                    sincos_of_acos(c, &chi_s, &chi_c);
+                } else {
+                    float chi = orc_acosf(c);
+                    chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                }
             } else if (rnd < t1 / t2) {
                 ev = 2;
                 float en = 0.5f * me * g * g;
                 en = fabsf(en - exc_j);
                 g = sqrtf(2.0f * en / me);
-                float chi = orc_acosf(1.0f - 2.0f * draw(&rs));
+                float c = 1.0f - 2.0f * draw(&rs);
                 eta = F_TWO_PI * draw(&rs);
-                chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                if (alg) {
+                    sincos_of_acos(c, &chi_s, &chi_c);
+                } else {
+                    float chi = orc_acosf(c);
+                    chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                }
             } else {
                 ev = 3;
                 float en = 0.5f * me * g * g;
@@ -545,13 +588,20 @@ void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t 
                 float e_orig = fabsf(en - e_new);
                 g = sqrtf(2.0f * e_orig / me);
                 float g_new = sqrtf(2.0f * e_new / me);
-                float chi = orc_acosf(sqrtf(e_orig / en));
-                float chi_new = orc_acosf(sqrtf(e_new / en));
                 eta = F_TWO_PI * draw(&rs);
-                float eta_new = eta + F_PI;
+                float sc2, cc2, se2, ce2;
+                if (alg) {
+                    sincos_of_acos(sqrtf(e_new / en), &sc2, &cc2);
+                    se2 = -orc_sinf(eta);
+                    ce2 = -orc_cosf(eta);
+                } else {
+                    float chi_new = orc_acosf(sqrtf(e_new / en));
+                    float eta_new = eta + F_PI;
+                    sc2 = orc_sinf(chi_new); cc2 = orc_cosf(chi_new);
+                    se2 = orc_sinf(eta_new); ce2 = orc_cosf(eta_new);
+                }
                 float ngx, ngy, ngz;
-                rotate(g_new, orc_sinf(chi_new), orc_cosf(chi_new), orc_sinf(eta_new), orc_cosf(eta_new),
-                       st, ct, sp, cp, &ngx, &ngy, &ngz);
+                rotate(g_new, sc2, cc2, se2, ce2, st, ct, sp, cp, &ngx, &ngy, &ngz);
                 float a, b, c;
                 uint32_t e_slot = *n_e;
                 int e_ok = e_slot < ph->capacity;
@@ -575,7 +625,12 @@ void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t 
                 } else if (dropped) {
                     ++*dropped;
                 }
-                chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                if (alg) {
+                    sincos_of_acos(sqrtf(e_orig / en), &chi_s, &chi_c);
+                } else {
+                    float chi = orc_acosf(sqrtf(e_orig / en));
+                    chi_s = orc_sinf(chi); chi_c = orc_cosf(chi);
+                }
             }
             float ngx, ngy, ngz;
             rotate(g, chi_s, chi_c, orc_sinf(eta), orc_cosf(eta), st, ct, sp, cp, &ngx, &ngy, &ngz);
@@ -586,6 +641,26 @@ void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t 
         r0[i] = rs.s[0]; r1[i] = rs.s[1]; r2[i] = rs.s[2]; r3[i] = rs.s[3];
         if (events) events[i] = ev;
     }
+}
+
+void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t n_active,
+                            float *x, float *vx, float *vy, float *vz,
+                            uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,
+                            float *ix, float *ivx, float *ivy, float *ivz,
+                            uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
+                            uint8_t *events, uint32_t *dropped) {
+    check_collisions_e(sigma_tot_e, cs, n_active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz, n_e, n_i, ph,
+                       events, dropped, 0);
+}
+
+void orc_check_collisions_e_alg(const float *sigma_tot_e, const float *cs, uint32_t n_active,
+                                float *x, float *vx, float *vy, float *vz,
+                                uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,
+                                float *ix, float *ivx, float *ivy, float *ivz,
+                                uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
+                                uint8_t *events, uint32_t *dropped) {
+    check_collisions_e(sigma_tot_e, cs, n_active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz, n_e, n_i, ph,
+                       events, dropped, 1);
 }
 
 /* check_collisions_i + collision_i, Rust-CUDA/src/main.rs:1167-1292. */

@@ -150,6 +150,16 @@ void orc_check_collisions_e(const float *sigma_tot_e, const float *cs, uint32_t 
                             float *ix, float *ivx, float *ivy, float *ivz,
                             uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
                             uint8_t *events, uint32_t *dropped);
+/* The same with the fused step's scattering arithmetic: the sines and
+ * cosines of the Euler angles, of chi = acos(c) and of eta + pi from their
+ * algebraic forms instead of evaluating the angles (same draws and events;
+ * velocities within the rounding of the skipped transcendentals). */
+void orc_check_collisions_e_alg(const float *sigma_tot_e, const float *cs, uint32_t n_active,
+                                float *x, float *vx, float *vy, float *vz,
+                                uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,
+                                float *ix, float *ivx, float *ivy, float *ivz,
+                                uint32_t *n_e, uint32_t *n_i, const orc_phys *ph,
+                                uint8_t *events, uint32_t *dropped);
 void orc_check_collisions_i(const float *sigma_tot_i, const float *cs, uint32_t n_active,
                             float *vx, float *vy, float *vz,
                             uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3,

@@ -107,6 +107,7 @@ def _declare(L):
     L.orc_check_collisions_e.argtypes = ([_f32p, _f32p, C.c_uint32] + [_f32p] * 4 + [_u32p] * 4 +
                                          [_f32p] * 4 + [P(C.c_uint32), P(C.c_uint32), P(OrcPhys),
                                                         _u8p, P(C.c_uint32)])
+    L.orc_check_collisions_e_alg.argtypes = L.orc_check_collisions_e.argtypes
     L.orc_check_collisions_i.argtypes = ([_f32p, _f32p, C.c_uint32] + [_f32p] * 3 + [_u32p] * 4 +
                                          [P(OrcPhys), _u8p])
     L.orc_p_coll_e_exact.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, P(OrcPhys)]
@@ -236,16 +237,17 @@ def wall_count(efield, x, vx, vy, vz, factor, dt, ph, ions):
     return counts, ifed_pow, ifed_gnd
 
 
-def check_collisions_e(sigma_tot_e, cs, n_active, e, rng, ions, n_e, n_i, ph):
+def check_collisions_e(sigma_tot_e, cs, n_active, e, rng, ions, n_e, n_i, ph, algebraic=False):
     """In-place MCC of electrons.  e = [x, vx, vy, vz] (capacity-sized float32
     arrays), rng = 4 uint32 planes, ions = [x, vx, vy, vz] of the ions.
-    Returns (events, n_e, n_i, dropped)."""
+    algebraic: the fused step's scattering arithmetic.  Returns (events,
+    n_e, n_i, dropped)."""
     ne = C.c_uint32(n_e)
     ni = C.c_uint32(n_i)
     dropped = C.c_uint32(0)
     events = np.zeros(max(n_active, 1), np.uint8)
-    lib().orc_check_collisions_e(sigma_tot_e, cs, n_active, *e, *rng, *ions,
-                                 C.byref(ne), C.byref(ni), C.byref(ph), events, C.byref(dropped))
+    fn = lib().orc_check_collisions_e_alg if algebraic else lib().orc_check_collisions_e
+    fn(sigma_tot_e, cs, n_active, *e, *rng, *ions, C.byref(ne), C.byref(ni), C.byref(ph), events, C.byref(dropped))
     return events[:n_active], ne.value, ni.value, dropped.value
 
 

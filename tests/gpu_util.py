@@ -53,7 +53,8 @@ def sorted_rows(*cols):
 def check_step_electrons(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, cap, seed=(3, 1, 4, 1), n_i0=1000):
     """Runs the fused electron step through the C ABI and checks it against
     the oracle's move_and_compact followed by its check_collisions_e over the
-    survivors, each survivor drawing from the RNG stream of its source slot.
+    survivors (with the fused step's algebraic scattering arithmetic), each
+    survivor drawing from the RNG stream of its source slot.
     RNG planes (every slot), electron and ion sets bit-exact; densities within
     the deposit tolerance.  Returns (survivors, electrons after, ions after)."""
     cs, se, _ = tables
@@ -66,7 +67,7 @@ def check_step_electrons(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef
     e_h = [pad(a) for a in (rx, rvx, rvy, rvz)]
     r_sub = [pad(p[src], np.uint32) for p in rng]
     i_h = [pad(np.full(n_i0, 0.0125, np.float32)) for _ in range(4)]
-    _, ne_ref, ni_ref, dropped = oracle.check_collisions_e(se, cs, m, e_h, r_sub, i_h, m, n_i0, ph)
+    _, ne_ref, ni_ref, dropped = oracle.check_collisions_e(se, cs, m, e_h, r_sub, i_h, m, n_i0, ph, algebraic=True)
     assert dropped == 0
     r_ref = [p.copy() for p in rng]
     for k in range(4):

@@ -237,3 +237,45 @@ def test_wall_count_known_answers(oracle):
     c, _, _ = oracle.wall_count(ef, xs, vxs, vys, vzs, -3.2e4, 1.8e-11, ph, False)
     kept = oracle.move_and_compact(ef, xs, vxs, vys, vzs, -3.2e4, 1.8e-11, ph)[0].size
     assert int(c.sum()) == 20000 - kept and c.min() > 0
+
+
+def test_algebraic_scattering_matches_angle_form(oracle, tables):
+    """The fused step's scattering arithmetic (sines and cosines of the Euler
+    angles, of acos(c) and of eta + pi from their algebraic forms) makes the
+    same decisions, draws and spawns as the reference's angle form, and
+    velocities within a few f32 ulps of the scattered speed."""
+    cs, se, si = tables
+    n = 100_000
+    ph = oracle.phys_from_params(capacity=2 * n)
+    from cudapic_b200.workloads import steady_state
+    x, vx, vy, vz = steady_state(n, 9.10938356e-31, 12.0, dt=ph.dt_e, seed=5)
+    # exact zeros take the special cases gx = 0 and gy = 0
+    vx[:50] = 0.0
+    vy[50:100] = 0.0
+    vx[100:120] = 0.0
+    vy[100:120] = 0.0
+    out = []
+    for alg in (False, True):
+        rng = [np.asarray(p) for p in oracle.seed_streams([7, 8, 9, 10], 2 * n)]
+        e = [np.zeros(2 * n, np.float32) for _ in range(4)]
+        for a, b in zip(e, (x, vx, vy, vz)):
+            a[:n] = b
+        ions = [np.zeros(2 * n, np.float32) for _ in range(4)]
+        r = oracle.check_collisions_e(se, cs, n, e, rng, ions, n, 0, ph, algebraic=alg)
+        out.append((r, e, rng, ions))
+    (ra, ea, ga, ia), (rb, eb, gb, ib) = out
+    np.testing.assert_array_equal(ra[0], rb[0])
+    assert ra[1:] == rb[1:]
+    assert np.sum(ra[0] == 1) > 100 and np.sum(ra[0] == 3) > 10
+    for p, q in zip(ga, gb):
+        np.testing.assert_array_equal(p, q)
+    ne = ra[1]
+    np.testing.assert_array_equal(ea[0][:ne], eb[0][:ne])
+    np.testing.assert_array_equal(ia[0][:ra[2]], ib[0][:ra[2]])
+    for planes_a, planes_b, count in ((ea, eb, ne), (ia, ib, ra[2])):
+        va = np.stack([p[:count].astype(np.float64) for p in planes_a[1:]])
+        vb = np.stack([p[:count].astype(np.float64) for p in planes_b[1:]])
+        speed = np.maximum(np.linalg.norm(va, axis=0), 1.0)
+        assert np.max(np.abs(va - vb) / speed) < 8 * 2.0 ** -23
+    scattered = np.flatnonzero(ra[0])
+    assert np.count_nonzero(ea[1][scattered] != eb[1][scattered]) > 0  # the forms differ in rounding
