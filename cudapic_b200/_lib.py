@@ -23,6 +23,7 @@ DEVERR_SPAWN_I = 0x2
 DEVERR_POSITION = 0x4
 DEVERR_ACTIVE = 0x8
 DEVERR_TIMEOUT = 0x10
+DEVERR_RECORDS = 0x20
 
 FLAG_POISSON_F32_SCAN = 0x1
 FLAG_DEPOSIT_FIXED_POINT = 0x2
@@ -190,6 +191,12 @@ SIGNATURES = {
     "cudapic_batch_destroy": [_VP],
     "cudapic_batch_run_steps": [_VP, C.c_uint64],
     "cudapic_batch_synchronize": [_VP],
+    "cudapic_sens_create": [_VP, _U32, _U32, _U32, C.POINTER(_VP)],
+    "cudapic_sens_forward": [_VP, C.c_double, C.POINTER(C.c_double)],
+    "cudapic_sens_backward": [_VP, C.POINTER(C.c_double)],
+    "cudapic_sens_info": [_VP, C.POINTER(_U32), C.POINTER(_U32), C.POINTER(C.c_uint64)],
+    "cudapic_sens_download": [_VP, C.c_int, _VP, _VP, _VP, _VP, _VP, _U32],
+    "cudapic_sens_destroy": [_VP],
 }
 OTHER = {
     "cudapic_params_default": (None, [C.POINTER(Params)]),

@@ -91,6 +91,11 @@ struct StepLink {
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g, cudaStream_t stream,
                    float *zero_a = nullptr, float *zero_b = nullptr);
+// Adjoint of launch_poisson's solve and field in FP64 (kernels_poisson.cu):
+// eb (field adjoint, cleared) -> neb, nib_acc (density adjoints, the ion one
+// accumulated unless reset_acc) and vbar += cosv * (pot0 adjoint).
+int launch_poisson_adjoint(double *eb, double *neb, double *nib_acc, int reset_acc, double cosv, double *vbar,
+                           const cudapic_grid &g, cudaStream_t stream);
 // dens_out (may be null): also deposit the survivors' new positions there;
 // wall (may be null): count the absorbed particles (with IFEDs for ions).
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,

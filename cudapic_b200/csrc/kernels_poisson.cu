@@ -293,6 +293,120 @@ int launch_poisson_pt(const float *e_density, const float *i_density, float *pot
     }
 }
 
+// Adjoint of the solve and field (the sensitivity path, FP64 sums): from the
+// field adjoint eb, the potential adjoint pb (the transposed differences),
+// lam = T^-1 pb with the same two-scan closed form (T = tridiag(1, -2, 1) is
+// symmetric), the density adjoints neb = -e rho_bar and
+// nib_acc = (reset_acc ? 0 : nib_acc) + e rho_bar (rho_bar = alpha lam inside,
+// the one-sided corrections at the electrodes), and
+// vbar += cosv (pb_0 - lam_1), pot0 = V cosv entering f_1 with a minus sign.
+// One CTA; eb is cleared for the next step.
+template <int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    poisson_adjoint_kernel(double *__restrict__ eb, double *__restrict__ neb, double *__restrict__ nib_acc,
+                           int reset_acc, double cosv, double *__restrict__ vbar, const cudapic_grid g) {
+    extern __shared__ unsigned char smem_raw[];
+    double *eb_s = reinterpret_cast<double *>(smem_raw);  // n
+    __shared__ double wsum[32];
+    __shared__ double r_total_s, lam1_s;
+    const int n = (int)g.n_g;
+    const int tid = threadIdx.x;
+    for (int k = tid; k < n; k += blockDim.x) {
+        eb_s[k] = eb[k];
+        eb[k] = 0.0;
+    }
+    __syncthreads();
+    const double inv_dx = 1.0 / g.dx, half_inv_dx = 0.5 / g.dx;
+    const double hdx_eps = g.dx / (2.0 * 8.85418781e-12);
+    const double alpha = -g.dx * g.dx / 8.85418781e-12;
+    const double e_charge = 1.60217662e-19;
+    const int first = tid * PT;
+    double G[PT], r[PT], R[PT];
+    double local = 0.0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        double gi = 0.0;
+        if (i >= 1 && i <= n - 2) {
+            double p = 0.0;
+            if (i == 1) p -= eb_s[0] * inv_dx;
+            if (i == n - 2) p += eb_s[n - 1] * inv_dx;
+            if (i + 1 <= n - 2) p += eb_s[i + 1] * half_inv_dx;
+            if (i - 1 >= 1) p -= eb_s[i - 1] * half_inv_dx;
+            gi = (double)i * p;
+        }
+        local += gi;
+        G[j] = local;
+    }
+    double tot;
+    double off = block_excl_scan<double>(local, wsum, tot);
+    local = 0.0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        double ri = 0.0;
+        if (i >= 1 && i <= n - 2) ri = (-(G[j] + off) / ((double)i + 1.0)) / (double)i;
+        r[j] = ri;
+        local += ri;
+        R[j] = local;
+    }
+    off = block_excl_scan<double>(local, wsum, tot);
+#pragma unroll
+    for (int j = 0; j < PT; ++j)
+        if (first + j == n - 2) r_total_s = R[j] + off;
+    __syncthreads();
+    const double r_total = r_total_s;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        if (i >= n) continue;
+        double rb;
+        if (i == 0) {
+            rb = -eb_s[0] * hdx_eps;
+        } else if (i == n - 1) {
+            rb = eb_s[n - 1] * hdx_eps;
+        } else {
+            const double lam = (double)i * (r_total - (R[j] + off) + r[j]);
+            if (i == 1) lam1_s = lam;
+            rb = alpha * lam;
+        }
+        neb[i] = -e_charge * rb;
+        nib_acc[i] = (reset_acc ? 0.0 : nib_acc[i]) + e_charge * rb;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const double pb0 = eb_s[0] * inv_dx + (n > 2 ? eb_s[1] * half_inv_dx : 0.0);
+        *vbar += cosv * (pb0 - lam1_s);
+    }
+}
+
+template <int PT>
+int launch_poisson_adjoint_t(double *eb, double *neb, double *nib_acc, int reset_acc, double cosv, double *vbar,
+                             const cudapic_grid &g, int threads, cudaStream_t stream) {
+    const size_t smem = (size_t)g.n_g * sizeof(double);
+    auto kern = poisson_adjoint_kernel<PT>;
+    if (smem > 48 * 1024)
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                 "cudaFuncSetAttribute(poisson_adjoint)"));
+    return launch_kernel("poisson_adjoint", kern, dim3(1), dim3(threads), smem, stream, eb, neb, nib_acc, reset_acc,
+                         cosv, vbar, g);
+}
+
+int launch_poisson_adjoint(double *eb, double *neb, double *nib_acc, int reset_acc, double cosv, double *vbar,
+                           const cudapic_grid &g, cudaStream_t stream) {
+    if (g.n_g < 3 || g.n_g > (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD))
+        return fail(CUDAPIC_ERR_ARG, "poisson_adjoint: n_g outside 3..16384");
+    int threads, pt;
+    poisson_shape(g.n_g, threads, pt);
+    switch (pt) {
+    case 1: return launch_poisson_adjoint_t<1>(eb, neb, nib_acc, reset_acc, cosv, vbar, g, threads, stream);
+    case 2: return launch_poisson_adjoint_t<2>(eb, neb, nib_acc, reset_acc, cosv, vbar, g, threads, stream);
+    case 4: return launch_poisson_adjoint_t<4>(eb, neb, nib_acc, reset_acc, cosv, vbar, g, threads, stream);
+    case 8: return launch_poisson_adjoint_t<8>(eb, neb, nib_acc, reset_acc, cosv, vbar, g, threads, stream);
+    default: return launch_poisson_adjoint_t<16>(eb, neb, nib_acc, reset_acc, cosv, vbar, g, threads, stream);
+    }
+}
+
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
                    cudaStream_t stream, float *zero_a, float *zero_b) {

@@ -57,6 +57,7 @@ typedef enum cudapic_status {
 #define CUDAPIC_DEVERR_POSITION 0x4u  /* gather/deposit met x outside [0,L] or NaN  */
 #define CUDAPIC_DEVERR_ACTIVE   0x8u  /* a count exceeded capacity and was clamped  */
 #define CUDAPIC_DEVERR_TIMEOUT  0x10u /* a bounded wait on an async copy gave up    */
+#define CUDAPIC_DEVERR_RECORDS  0x20u /* sensitivity tape: collision records full    */
 
 /* Discharge and run parameters: the reference's compile-time constants
  * (Rust-CUDA/src/main.rs:40-50, :79) as runtime values. */
@@ -552,6 +553,55 @@ int cudapic_batch_destroy(cudapic_batch *b);
 int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps);
 int cudapic_batch_synchronize(cudapic_batch *b);
 cudapic_stream_t cudapic_batch_stream(const cudapic_batch *b);
+
+/* ------------------------------------------------------- sensitivities
+ * d(observable)/d(voltage) of one discharge by a pathwise adjoint with
+ * collision events and random draws frozen.  The reference has no
+ * differentiation; this differentiates its step loop
+ * (Rust-CUDA/src/main.rs:1725-1808) in slot form: the same kernels in the
+ * same order, but absorbed particles are marked dead (x = -1) instead of
+ * compacted and the spawns of a step take the next free slots in the order
+ * of their parents, so every particle keeps its RNG stream and a run is a
+ * deterministic function of (initial state, voltage).  Deposits are exact
+ * integer sums, the Poisson sums FP64 (a state with
+ * CUDAPIC_FLAG_POISSON_F32_SCAN is refused), scattering uses algebraic sines
+ * and cosines.
+ *
+ * Observables, averaged over a window of K steps from RF phase zero:
+ *   obs[0] = J_P  <j E> electron power averaged over the gap [W m^-3]
+ *                 (C/eduPIC.cc:593-614, 1011-1026, summed per particle);
+ *   obs[1] = J_G  ion flux to the grounded electrode [m^-2 s^-1], the CIC
+ *                 flux density n v at node N_G-1 (C/eduPIC.cc:651-658 counts
+ *                 the same flux).
+ * The forward run saves a checkpoint every `checkpoint_every` steps; the
+ * backward pass recomputes each interval from its checkpoint with a tape
+ * and sweeps it in reverse.  horizon (a multiple of checkpoint_every, 0 =
+ * the whole window): the adjoint restarts from zero at every multiple of
+ * `horizon` steps (the sensitivity with the influence of the voltage
+ * truncated to that horizon; chaotic particle dynamics make the full-window
+ * pathwise derivative grow without bound over long windows). */
+typedef struct cudapic_sens cudapic_sens;
+#define CUDAPIC_SENS_POWER_E     0
+#define CUDAPIC_SENS_ION_FLUX_GND 1
+/* Snapshot of the state's particles and RNG planes (its current contents;
+ * the state is not changed and may be stepped further); window_steps and
+ * checkpoint_every are whole ion cycles (N_SUB), window_steps a multiple of
+ * checkpoint_every; n_g <= 4096. */
+int cudapic_sens_create(cudapic_state *st, uint32_t window_steps, uint32_t checkpoint_every, uint32_t horizon,
+                        cudapic_sens **out);
+/* Runs the window from the snapshot at RF amplitude `voltage` (the same
+ * snapshot and RNG streams every call: common random numbers). */
+int cudapic_sens_forward(cudapic_sens *s, double voltage, double obs[2]);
+/* d obs / d voltage at the voltage of the last forward run. */
+int cudapic_sens_backward(cudapic_sens *s, double grad[2]);
+/* Slot counts and device error word after the last run; device memory held. */
+int cudapic_sens_info(cudapic_sens *s, uint32_t counts[2], uint32_t *dev_err, uint64_t *device_bytes);
+/* Particles of one species after the last run (all `capacity` >= the
+ * state's capacity slots; dead slots have x = -1); rng (may be NULL): the
+ * four planes one after another. */
+int cudapic_sens_download(cudapic_sens *s, int species, float *x, float *vx, float *vy, float *vz, uint32_t *rng,
+                          uint32_t capacity);
+int cudapic_sens_destroy(cudapic_sens *s);
 
 #ifdef __cplusplus
 }

@@ -184,6 +184,28 @@ void orc_xt_accumulate(const float *efield, const float *x, const float *vx, con
                        uint32_t n, int ions, const float *cs_ion, const orc_phys *ph, double *out);
 
 
+/* ---- voltage sensitivity (cudapic_oracle_sens.c) ---- */
+/* Particles of both species in their slots ([0] electrons, [1] ions):
+ * positions (dead slots x = -1), velocities, the four RNG planes, the slot
+ * counts n and the common capacity; dev_err receives 0x1 / 0x2 when an
+ * electron / ion spawn found no slot. */
+typedef struct orc_sens_io {
+    float *x[2], *vx[2], *vy[2], *vz[2];
+    uint32_t *rng[2][4];
+    uint32_t n[2];
+    uint32_t capacity;
+    uint32_t dev_err;
+} orc_sens_io;
+/* Runs `steps` steps of the slot-form model from step 0 of the RF period at
+ * amplitude `voltage`, in place; obs = (J_P [W m^-3], J_G [m^-2 s^-1]).
+ * f64 = 0: the f32 arithmetic of the CUDA path; 1: the same model in double.
+ * grad (may be NULL): d obs / d voltage by the pathwise adjoint; horizon
+ * (a multiple of N_SUB, 0 = the whole window): the adjoint restarts from
+ * zero every `horizon` steps.  Returns -1 on bad arguments. */
+int orc_sens_run(const orc_phys *ph, const float *sigma_tot_e, const float *sigma_tot_i, const float *cs,
+                 double voltage, uint32_t steps, uint32_t horizon, int f64, orc_sens_io *io, double obs[2],
+                 double grad[2]);
+
 #ifdef __cplusplus
 }
 #endif

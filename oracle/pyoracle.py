@@ -24,7 +24,7 @@ __all__ = [
     "poisson_scan_f32", "poisson_dps_flexible_f64", "move_and_compact",
     "check_collisions_e", "check_collisions_i", "p_coll_e_exact",
     "accumulate_density", "accumulate_eepf", "xt_accumulate", "xt_normalise", "REF_DIR", "CS_RANGES", "N_EEPF",
-    "MATH_FN",
+    "MATH_FN", "SensState", "sens_run",
 ]
 
 MATH_FN = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "tan": 4, "atan": 5, "acos": 6, "atan2": 7}
@@ -51,6 +51,14 @@ class OrcPhys(C.Structure):
         ("dx", C.c_double), ("weight_factor_d", C.c_double), ("gas_density", C.c_double),
         ("dt_e_d", C.c_double), ("dt_i_d", C.c_double), ("voltage", C.c_double), ("omega", C.c_double),
         ("n_t", C.c_uint32), ("n_sub", C.c_uint32),
+    ]
+
+
+class OrcSensIo(C.Structure):
+    _fields_ = [
+        ("x", C.c_void_p * 2), ("vx", C.c_void_p * 2), ("vy", C.c_void_p * 2), ("vz", C.c_void_p * 2),
+        ("rng", (C.c_void_p * 4) * 2), ("n", C.c_uint32 * 2), ("capacity", C.c_uint32),
+        ("dev_err", C.c_uint32),
     ]
 
 
@@ -115,6 +123,9 @@ def _declare(L):
     L.orc_accumulate_density.argtypes = [_f32p, _f64p, C.c_uint32]
     L.orc_accumulate_eepf.argtypes = [_f32p] * 5 + [C.c_uint32, _u32p, P(OrcPhys)]
     L.orc_xt_accumulate.argtypes = [_f32p] * 5 + [C.c_uint32, C.c_int, _f32p, P(OrcPhys), _f64p]
+    L.orc_sens_run.argtypes = [P(OrcPhys), _f32p, _f32p, _f32p, C.c_double, C.c_uint32, C.c_uint32, C.c_int,
+                               P(OrcSensIo),
+                               C.POINTER(C.c_double), C.POINTER(C.c_double)]
 
 
 def default_params(**overrides):
@@ -304,3 +315,55 @@ def xt_normalise(raw, n_t, n_xt, measure_steps, gap, n_g, frequency, weight, ele
     out["powere"] = out["je"] * out["efield"]
     out["poweri"] = out["ji"] * out["efield"]
     return out
+
+
+class SensState:
+    """Both species in their slots for the sensitivity model: planes
+    [x, vx, vy, vz] (float32, capacity), RNG planes (4 uint32 per species),
+    slot counts n = [n_e, n_i]."""
+
+    def __init__(self, capacity, electrons, ions, rng_e, rng_i):
+        self.capacity = capacity
+        self.p = []
+        for parts in (electrons, ions):
+            planes = [np.zeros(capacity, np.float32) for _ in range(4)]
+            for a, b in zip(planes, parts):
+                a[:len(b)] = b
+            self.p.append(planes)
+        self.rng = [[np.ascontiguousarray(np.asarray(r, np.uint32)[:capacity]).copy() for r in rr]
+                    for rr in (rng_e, rng_i)]
+        self.n = [len(electrons[0]), len(ions[0])]
+        self.dev_err = 0
+
+    def copy(self):
+        c = SensState.__new__(SensState)
+        c.capacity = self.capacity
+        c.p = [[a.copy() for a in planes] for planes in self.p]
+        c.rng = [[r.copy() for r in rr] for rr in self.rng]
+        c.n = list(self.n)
+        c.dev_err = self.dev_err
+        return c
+
+
+def sens_run(ph, tables, voltage, steps, state, f64=False, grad=True, horizon=0):
+    """Runs the slot-form model in place on `state` (a SensState); returns
+    (obs, grad): obs = [J_P W/m^3, J_G 1/(m^2 s)], grad = d obs / d voltage
+    by the pathwise adjoint (None without grad), restarted every `horizon`
+    steps (0: over the whole window)."""
+    cs, sig_e, sig_i = tables
+    io = OrcSensIo()
+    for k in range(2):
+        io.x[k], io.vx[k], io.vy[k], io.vz[k] = [a.ctypes.data for a in state.p[k]]
+        for c in range(4):
+            io.rng[k][c] = state.rng[k][c].ctypes.data
+        io.n[k] = state.n[k]
+    io.capacity = state.capacity
+    obs = (C.c_double * 2)()
+    g = (C.c_double * 2)()
+    rc = lib().orc_sens_run(C.byref(ph), _f32(sig_e), _f32(sig_i), _f32(cs), float(voltage), int(steps),
+                            int(horizon), 1 if f64 else 0, C.byref(io), obs, g if grad else None)
+    if rc != 0:
+        raise ValueError("orc_sens_run: bad arguments")
+    state.n = [io.n[0], io.n[1]]
+    state.dev_err = io.dev_err
+    return list(obs), (list(g) if grad else None)
