@@ -197,6 +197,11 @@ SIGNATURES = {
     "cudapic_sens_info": [_VP, C.POINTER(_U32), C.POINTER(_U32), C.POINTER(C.c_uint64)],
     "cudapic_sens_download": [_VP, C.c_int, _VP, _VP, _VP, _VP, _VP, _U32],
     "cudapic_sens_destroy": [_VP],
+    "cudapic_fp64_create": [_VP, C.POINTER(_VP)],
+    "cudapic_fp64_set_measure": [_VP, C.c_int],
+    "cudapic_fp64_run_steps": [_VP, C.c_uint64],
+    "cudapic_fp64_measurements": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
+    "cudapic_fp64_destroy": [_VP],
 }
 OTHER = {
     "cudapic_params_default": (None, [C.POINTER(Params)]),

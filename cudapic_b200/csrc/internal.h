@@ -96,6 +96,12 @@ int launch_poisson(const float *e_density, const float *i_density, float *pot, f
 // accumulated unless reset_acc) and vbar += cosv * (pot0 adjoint).
 int launch_poisson_adjoint(double *eb, double *neb, double *nib_acc, int reset_acc, double cosv, double *vbar,
                            const cudapic_grid &g, cudaStream_t stream);
+// FP64 solve and field from FP64 node sums (kernels_poisson.cu, the all-FP64
+// twin): pot0 from pot0_table[*step % n_t], *step advanced; measurement sums
+// may be null.
+int launch_poisson_f64(const double *dens_e, const double *dens_i, double *pot, double *efield,
+                       const double *pot0_table, uint32_t *step, int ion_step, double *cumul_e, double *cumul_i,
+                       double *pot_sum, const cudapic_grid &g, cudaStream_t stream);
 // dens_out (may be null): also deposit the survivors' new positions there;
 // wall (may be null): count the absorbed particles (with IFEDs for ions).
 int launch_move_and_compact(const float *efield, const float *sx, const float *svx, const float *svy,

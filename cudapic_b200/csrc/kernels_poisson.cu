@@ -407,6 +407,119 @@ int launch_poisson_adjoint(double *eb, double *neb, double *nib_acc, int reset_a
     }
 }
 
+// The solve and field in FP64 in and out (the all-FP64 twin, fp64.cu):
+// dens_e / dens_i are the CIC node sums before the boundary doubling;
+// pot0 = pot0_table[*step % n_t], *step advanced.  With measurement
+// (non-null sums): cumul_e += n_e, cumul_i += n_i (ion steps), pot_sum += pot.
+template <int PT>
+__global__ void __launch_bounds__(POIS_MAX_THREADS)
+    poisson_f64_kernel(const double *__restrict__ dens_e, const double *__restrict__ dens_i, double *__restrict__ pot_out,
+                       double *__restrict__ efield_out, const double *__restrict__ pot0_table,
+                       uint32_t *__restrict__ step, int ion_step, double *__restrict__ cumul_e,
+                       double *__restrict__ cumul_i, double *__restrict__ pot_sum, const cudapic_grid g) {
+    extern __shared__ unsigned char smem_raw[];
+    double *pot_s = reinterpret_cast<double *>(smem_raw);  // n
+    __shared__ double wsum[32];
+    __shared__ double r_total_s, pot0_s;
+    const int n = (int)g.n_g;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        const uint32_t t = *step;
+        pot0_s = pot0_table[t % g.n_t];
+        *step = t + 1;
+    }
+    __syncthreads();
+    const double pot0 = pot0_s;
+    const double e_charge = 1.60217662e-19;
+    const double alpha = -g.dx * g.dx / 8.85418781e-12;
+    const int first = tid * PT;
+    double rho[PT], G[PT], r[PT], R[PT];
+    double local = 0.0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        double rh = 0.0, gi = 0.0;
+        if (i < n) {
+            const double b = (i == 0 || i == n - 1) ? 2.0 : 1.0;
+            const double ne = dens_e[i] * b, ni = dens_i[i] * b;
+            if (cumul_e) cumul_e[i] += ne;
+            if (cumul_i && ion_step) cumul_i[i] += ni;
+            rh = e_charge * (ni - ne);
+            if (i != 0) gi = (double)i * (alpha * rh - (i == 1 ? pot0 : 0.0));
+        }
+        rho[j] = rh;
+        local += gi;
+        G[j] = local;
+    }
+    double tot;
+    double off = block_excl_scan<double>(local, wsum, tot);
+    local = 0.0;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        double ri = 0.0;
+        if (i != 0 && i < n - 1) ri = (-(G[j] + off) / ((double)i + 1.0)) / (double)i;
+        r[j] = ri;
+        local += ri;
+        R[j] = local;
+    }
+    off = block_excl_scan<double>(local, wsum, tot);
+#pragma unroll
+    for (int j = 0; j < PT; ++j)
+        if (first + j == n - 2) r_total_s = R[j] + off;
+    __syncthreads();
+    const double r_total = r_total_s;
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        if (i < n) pot_s[i] = i == 0 ? pot0 : (i < n - 1 ? (double)i * (r_total - (R[j] + off) + r[j]) : 0.0);
+    }
+    __syncthreads();
+    const double inv_dx = 1.0 / g.dx, half_inv_dx = 0.5 / g.dx, hdx_eps = g.dx / (2.0 * 8.85418781e-12);
+#pragma unroll
+    for (int j = 0; j < PT; ++j) {
+        const int i = first + j;
+        if (i >= n) continue;
+        const double pk = pot_s[i];
+        double e;
+        if (i == 0) e = (pk - pot_s[1]) * inv_dx - rho[j] * hdx_eps;
+        else if (i == n - 1) e = (pot_s[n - 2] - pk) * inv_dx + rho[j] * hdx_eps;
+        else e = (pot_s[i - 1] - pot_s[i + 1]) * half_inv_dx;
+        pot_out[i] = pk;
+        efield_out[i] = e;
+        if (pot_sum) pot_sum[i] += pk;
+    }
+}
+
+template <int PT>
+int launch_poisson_f64_t(const double *dens_e, const double *dens_i, double *pot, double *efield,
+                         const double *pot0_table, uint32_t *step, int ion_step, double *cumul_e, double *cumul_i,
+                         double *pot_sum, const cudapic_grid &g, int threads, cudaStream_t stream) {
+    const size_t smem = (size_t)g.n_g * sizeof(double);
+    auto kern = poisson_f64_kernel<PT>;
+    if (smem > 48 * 1024)
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                 "cudaFuncSetAttribute(poisson_f64)"));
+    return launch_kernel("poisson_f64", kern, dim3(1), dim3(threads), smem, stream, dens_e, dens_i, pot, efield,
+                         pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g);
+}
+
+int launch_poisson_f64(const double *dens_e, const double *dens_i, double *pot, double *efield,
+                       const double *pot0_table, uint32_t *step, int ion_step, double *cumul_e, double *cumul_i,
+                       double *pot_sum, const cudapic_grid &g, cudaStream_t stream) {
+    if (g.n_g < 3 || g.n_g > (uint32_t)(POIS_MAX_THREADS * POIS_MAX_PER_THREAD))
+        return fail(CUDAPIC_ERR_ARG, "poisson_f64: n_g outside 3..16384");
+    int threads, pt;
+    poisson_shape(g.n_g, threads, pt);
+    switch (pt) {
+    case 1: return launch_poisson_f64_t<1>(dens_e, dens_i, pot, efield, pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g, threads, stream);
+    case 2: return launch_poisson_f64_t<2>(dens_e, dens_i, pot, efield, pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g, threads, stream);
+    case 4: return launch_poisson_f64_t<4>(dens_e, dens_i, pot, efield, pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g, threads, stream);
+    case 8: return launch_poisson_f64_t<8>(dens_e, dens_i, pot, efield, pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g, threads, stream);
+    default: return launch_poisson_f64_t<16>(dens_e, dens_i, pot, efield, pot0_table, step, ion_step, cumul_e, cumul_i, pot_sum, g, threads, stream);
+    }
+}
+
 int launch_poisson(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                    const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
                    cudaStream_t stream, float *zero_a, float *zero_b) {

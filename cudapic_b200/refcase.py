@@ -23,9 +23,11 @@ noise floor.  Arithmetic modes:
     averages (the default path);
   * ``f32_poisson``: the same with the reference's f32 Poisson scans;
   * ``reference_f32``: the reference's launch sequence with f32 atomic
-    deposits and f32 Poisson scans (the arithmetic of the reference's GPU path).
+    deposits and f32 Poisson scans (the arithmetic of the reference's GPU path);
+  * ``fp64``: the all-FP64 GPU twin (cudapic_b200.fp64): the reference's
+    launch sequence with particles, fields, densities and collisions in double.
 
-    python -m cudapic_b200.refcase --reference DIR [--modes mixed,f32_poisson,reference_f32]
+    python -m cudapic_b200.refcase --reference DIR [--modes mixed,f32_poisson,reference_f32,fp64]
                                    [--relax 300] [--measure 100]
 
 DIR holds eduPIC's reference outputs under the names of tests/golden
@@ -43,7 +45,7 @@ E_CHARGE = 1.60217662e-19
 DE_EEPF = 0.05
 EEPF_BAND_EV = 15.0
 
-MODES = ("mixed", "f32_poisson", "reference_f32")
+MODES = ("mixed", "f32_poisson", "reference_f32", "fp64")
 
 
 def load_reference(directory):
@@ -161,12 +163,41 @@ def compare(got, ref):
     return errors, spread
 
 
+def run_fp64(twins, relax, measure):
+    """relax, then measure, cycles of all-FP64 twins (each on its state's
+    stream, side by side)."""
+    for tw in twins:
+        tw.run_cycles(relax)
+    for tw in twins:
+        tw.set_measure(True)
+        tw.run_cycles(measure)
+
+
+def outputs_fp64(tw):
+    """A twin's measurement window normalised as eduPIC's outputs."""
+    m = tw.measurements()
+    counts = m["eepf"].astype(np.float64)
+    energy = (np.arange(len(counts)) + 0.5) * DE_EEPF
+    return {"ne": m["ne"], "ni": m["ni"], "pot": m["pot"],
+            "eepf": counts / (counts.sum() * DE_EEPF) / np.sqrt(energy), "power_e": m["power_e"],
+            "count_e": float(m["counts"][0]), "device_error": m["device_error"]}
+
+
 def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
+    from .fp64 import Fp64Discharge
     states = start_states(ref, mode, seeds)
+    twins = []
     try:
-        run(states, relax, measure)
-        got = [outputs(st, measure) for st in states]
+        if mode == "fp64":
+            twins = [Fp64Discharge(st) for st in states]
+            run_fp64(twins, relax, measure)
+            got = [outputs_fp64(tw) for tw in twins]
+        else:
+            run(states, relax, measure)
+            got = [outputs(st, measure) for st in states]
     finally:
+        for tw in twins:
+            tw.close()
         for st in states:
             st.close()
     errors, spread = compare(got, ref)

@@ -603,6 +603,32 @@ int cudapic_sens_download(cudapic_sens *s, int species, float *x, float *vx, flo
                           uint32_t capacity);
 int cudapic_sens_destroy(cudapic_sens *s);
 
+/* ------------------------------------------------------------ all-FP64
+ * An all-FP64 twin of a discharge for the precision study: the reference's
+ * launch sequence (Rust-CUDA/src/main.rs:1725-1808) with particles, fields,
+ * densities, collision tests and scattering in double (CUDA's double
+ * transcendentals; the reference's RNG draws and f32 cross-section tables
+ * widened to double).  The reference computes in f32 and has no
+ * counterpart.  Created from a state at the start of an ion cycle (its
+ * particles widened, its RNG planes copied, its RF phase continued); the
+ * state is not changed.  n_g <= 4096. */
+typedef struct cudapic_fp64 cudapic_fp64;
+int cudapic_fp64_create(cudapic_state *st, cudapic_fp64 **out);
+/* Starts (on) or stops a measurement window; both clear the window sums. */
+int cudapic_fp64_set_measure(cudapic_fp64 *d, int on);
+int cudapic_fp64_run_steps(cudapic_fp64 *d, uint64_t n_steps);
+/* Window sums (each may be NULL): node densities summed every step
+ * (electrons) or every ion step (ions), boundary nodes doubled [m^-3 x
+ * steps]; potential summed every step [V x steps]; EEPF counts (2000 bins of
+ * 0.05 eV, central 10 % of the gap, after each step); power_sum: the sum
+ * over steps and electrons of (v + f E/2) E at the push [V s^-1], so that
+ * -e (W/A) / L x power_sum / steps is the <j E> power [W m^-3]; steps[0]
+ * measured steps, steps[1] measured ion steps; counts: n_e, n_i now;
+ * dev_err: CUDAPIC_DEVERR_* bits. */
+int cudapic_fp64_measurements(cudapic_fp64 *d, double *cumul_e, double *cumul_i, double *pot_sum, uint32_t *eepf,
+                              double *power_sum, uint64_t steps[2], uint32_t counts[2], uint32_t *dev_err);
+int cudapic_fp64_destroy(cudapic_fp64 *d);
+
 #ifdef __cplusplus
 }
 #endif
