@@ -28,7 +28,11 @@ noise floor.  Arithmetic modes:
     launch sequence with particles, fields, densities and collisions in double.
 
     python -m cudapic_b200.refcase --reference DIR [--modes mixed,f32_poisson,reference_f32,fp64]
-                                   [--relax 300] [--measure 100]
+                                   [--relax 300] [--measure 100] [--cross mixed,fp64]
+
+``--cross a,b`` compares two modes with each other (same model, same starts)
+instead of with eduPIC: mixed against fp64 is the f32 path's error against
+an FP64 computation of the same model.
 
 DIR holds eduPIC's reference outputs under the names of tests/golden
 (edupic_ref_density.txt, edupic_ref_eepf.txt, edupic_ref_xt_means.txt,
@@ -183,7 +187,8 @@ def outputs_fp64(tw):
             "count_e": float(m["counts"][0]), "device_error": m["device_error"]}
 
 
-def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
+def mode_outputs(ref, mode, relax=300, measure=100, seeds=(1, 2)):
+    """Per seed, the outputs of one arithmetic mode (normalised as eduPIC's)."""
     from .fp64 import Fp64Discharge
     states = start_states(ref, mode, seeds)
     twins = []
@@ -200,9 +205,38 @@ def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
             tw.close()
         for st in states:
             st.close()
+    return got
+
+
+def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
+    got = mode_outputs(ref, mode, relax, measure, seeds)
     errors, spread = compare(got, ref)
     return {"mode": mode, "relax_cycles": relax, "measured_cycles": measure, "seeds": list(seeds),
             "errors": errors, "seed_spread": spread, "device_errors": [g["device_error"] for g in got]}
+
+
+def cross(ref, a="mixed", b="fp64", relax=300, measure=100, seeds=(1, 2)):
+    """Mode a against mode b of the same model from the same starts: the
+    relative L2 (relative difference for the scalars) of the seed means, and
+    each mode's seed-to-seed spread (the noise floor of the comparison)."""
+    ga = mode_outputs(ref, a, relax, measure, seeds)
+    gb = mode_outputs(ref, b, relax, measure, seeds)
+    band = (np.arange(len(ref["eepf"])) + 0.5) * DE_EEPF < EEPF_BAND_EV
+    diff, spread = {}, {}
+    for key in ("ne", "ni", "pot", "eepf", "power_e", "count_e"):
+        ma = np.mean([g[key] for g in ga], axis=0)
+        mb = np.mean([g[key] for g in gb], axis=0)
+        if key in ("power_e", "count_e"):
+            diff[key] = abs(ma / mb - 1.0)
+            spread[key] = [abs(g[0][key] / g[1][key] - 1.0) for g in (ga, gb)]
+        else:
+            sel = band if key == "eepf" else slice(None)
+            diff[key] = float(np.linalg.norm(ma[sel] - mb[sel]) / np.linalg.norm(mb[sel]))
+            spread[key] = [float(np.linalg.norm(g[0][key][sel] - g[1][key][sel]) / np.linalg.norm(g[1][key][sel]))
+                           for g in (ga, gb)]
+    return {"modes": [a, b], "relax_cycles": relax, "measured_cycles": measure, "seeds": list(seeds),
+            "difference": diff, "seed_spread": spread,
+            "device_errors": [g["device_error"] for g in ga + gb]}
 
 
 def main(argv=None):
@@ -212,8 +246,13 @@ def main(argv=None):
     ap.add_argument("--modes", default=",".join(MODES))
     ap.add_argument("--relax", type=int, default=300)
     ap.add_argument("--measure", type=int, default=100)
+    ap.add_argument("--cross", help="two modes a,b compared with each other instead of with eduPIC")
     a = ap.parse_args(argv)
     ref = load_reference(a.reference)
+    if a.cross:
+        ma, mb = a.cross.split(",")
+        print(json.dumps(cross(ref, ma, mb, a.relax, a.measure)), flush=True)
+        return 0
     for mode in a.modes.split(","):
         print(json.dumps(study(ref, mode, a.relax, a.measure)), flush=True)
     return 0
