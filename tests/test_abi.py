@@ -89,6 +89,16 @@ def test_argument_validation_without_device(cudapic):
     big.capacity = 0x80000004
     assert lib.cudapic_step_electrons_noalloc(*ptrs, C.c_float(1.0), *tail, C.byref(big), None) == _lib.ERR_ARG
     assert b"CUDAPIC_NOALLOC_MAX_CAPACITY" in lib.cudapic_last_error()
+    # sensitivity and FP64-twin objects: null handles are refused, destroy(NULL) is a no-op
+    h = C.c_void_p()
+    assert lib.cudapic_sens_create(None, 8000, 200, 0, C.byref(h)) == _lib.ERR_ARG
+    out2 = (C.c_double * 2)()
+    assert lib.cudapic_sens_forward(None, C.c_double(250.0), out2) == _lib.ERR_ARG
+    assert lib.cudapic_sens_backward(None, out2) == _lib.ERR_ARG
+    assert lib.cudapic_sens_destroy(None) == _lib.OK
+    assert lib.cudapic_fp64_create(None, C.byref(h)) == _lib.ERR_ARG
+    assert lib.cudapic_fp64_run_steps(None, 1) == _lib.ERR_ARG
+    assert lib.cudapic_fp64_destroy(None) == _lib.OK
 
 
 def test_state_create_reports_missing_device(cudapic):
