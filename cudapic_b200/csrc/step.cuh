@@ -118,13 +118,22 @@ struct StepOut {
     uint32_t keep;  // bit u: the particle of row u is written by the tile
 };
 
-// True unless u certainly exceeds the collision probability at speed
-// `velocity` (same operation order as test_electron): the exact test
-// decides "no collision" whenever u >= fl(a + 5e-7), a = fl(fl(sigma(E) |v|)
-// dt); rounding is monotone, so with sigma_max the largest table entry
-// u >= fl(fl(fl(sigma_max |v|) dt) + 5e-7) implies it.
-__device__ __forceinline__ bool may_collide(float u, float velocity, float sigma_max, float dt) {
-    return u < sigma_max * velocity * dt + 5e-7f;
+// True unless u certainly exceeds the collision probability of an electron
+// with v.v = v2.  The exact test decides "no collision" whenever
+// u >= B = fl(fl(fl(sigma(E) |v|) dt) + 5e-7), |v| = fl(sqrt(v2)); rounding
+// is monotone, so with sigma_max the largest table entry
+// u >= fl(fl(fl(sigma_max |v|) dt) + 5e-7) implies it.  The same bound
+// without the square root: with k2 = fl(fl(sigma_max dt)^2 * 1.0001) and
+// y = fl(u - 5.001e-7) >= 0, fl(y y) >= fl(k2 v2) gives
+// y >= sigma_max dt sqrt(v2) (1 + 4.8e-5) (each rounding is within 2^-24
+// relative), hence u - 5.001e-7 >= A (1 + 4.6e-5) with
+// A = fl(fl(sigma_max |v|) dt) <= sigma_max dt sqrt(v2) (1 + 2e-7), and
+// u >= A + 5e-7 + 1e-10 + 4.6e-5 A > fl(A + 5e-7): the decision is the
+// exact test's, bit for bit; only u within 1e-4 relative of the bound
+// takes the exact test in addition.
+__device__ __forceinline__ bool may_collide(float u, float v2, float k2) {
+    const float y = u - 5.001e-7f;
+    return !(y >= 0.0f && y * y >= k2 * v2);
 }
 
 // Initialises the stage mbarriers (thread 0) and clears the deposit
@@ -169,6 +178,7 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
     // the push and test constants, read once (io may live in shared memory,
     // which the tile loop writes)
     const float factor = dc.factor, dt = dc.dt, sigma_max = dc.sigma_max;
+    const float rej_k2 = sigma_max * dt * (sigma_max * dt) * 1.0001f;  // may_collide's bound
     const float inv_dx = g.inv_dx, gap = g.gap;
     const uint32_t n_g = g.n_g;
     const uint32_t it0 = it;
@@ -292,9 +302,8 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
                 cur.vz[u] = __uint_as_float(b[3 * TILE + j]);
                 Xoshiro128p rs{b[4 * TILE + j], b[5 * TILE + j], b[6 * TILE + j], b[7 * TILE + j]};
                 const float v2 = cur.vx[u] * cur.vx[u] + cur.vy[u] * cur.vy[u] + cur.vz[u] * cur.vz[u];
-                const float velocity = sqrtf(v2);
                 const float rnd = rs.uniform();
-                if ((keep >> u & 1u) && may_collide(rnd, velocity, sigma_max, dt)) may |= 1u << u;
+                if ((keep >> u & 1u) && may_collide(rnd, v2, rej_k2)) may |= 1u << u;
                 st[u][0] = rs.s0;
                 st[u][1] = rs.s1;
                 st[u][2] = rs.s2;
