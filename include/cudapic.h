@@ -586,7 +586,8 @@ typedef struct cudapic_sens cudapic_sens;
 /* Snapshot of the state's particles and RNG planes (its current contents;
  * the state is not changed and may be stepped further); window_steps and
  * checkpoint_every are whole ion cycles (N_SUB), window_steps a multiple of
- * checkpoint_every; n_g <= 4096. */
+ * checkpoint_every; n_g <= 4096.  The object runs on the state's stream
+ * and reads the state's cross-section tables: destroy it before the state. */
 int cudapic_sens_create(cudapic_state *st, uint32_t window_steps, uint32_t checkpoint_every, uint32_t horizon,
                         cudapic_sens **out);
 /* Runs the window from the snapshot at RF amplitude `voltage` (the same
@@ -611,7 +612,8 @@ int cudapic_sens_destroy(cudapic_sens *s);
  * widened to double).  The reference computes in f32 and has no
  * counterpart.  Created from a state at the start of an ion cycle (its
  * particles widened, its RNG planes copied, its RF phase continued); the
- * state is not changed.  n_g <= 4096. */
+ * state is not changed.  n_g <= 4096.  The twin runs on the state's stream
+ * and reads the state's cross-section tables: destroy it before the state. */
 typedef struct cudapic_fp64 cudapic_fp64;
 int cudapic_fp64_create(cudapic_state *st, cudapic_fp64 **out);
 /* Starts (on) or stops a measurement window; both clear the window sums. */
