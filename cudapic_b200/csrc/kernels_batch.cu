@@ -415,13 +415,21 @@ int launch_batch_step_t(const StepPlanes &pl, const BatchDisc *desc, const uint3
     while (bytes() > budget && stages > 2) --stages;
     while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "batch step: n_g too large");
-    const size_t smem = bytes();
     auto kern = batch_step_kernel<U, MCC, MINB, MEAS>;
-    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                             "cudaFuncSetAttribute(batch step)"));
     int per_sm = 0;
-    CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ES_THREADS, smem),
-                             "occupancy(batch step)"));
+    auto occupancy = [&]() {
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes()),
+                                 "cudaFuncSetAttribute(batch step)"));
+        return check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ES_THREADS, bytes()),
+                          "occupancy(batch step)");
+    };
+    CUDAPIC_CHECK(occupancy());
+    // large grids: fewer histogram copies rather than fewer CTAs per SM
+    while (per_sm < t.step_ctas_per_sm && copies > 1) {
+        copies = (copies + 1) / 2;
+        CUDAPIC_CHECK(occupancy());
+    }
+    const size_t smem = bytes();
     per_sm = std::min(std::max(per_sm, 1), t.step_ctas_per_sm);
     const unsigned grid = persistent_grid(per_sm, (cap_sum + TILE - 1) / TILE);
     const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;

@@ -306,11 +306,20 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         while (smem > (size_t)max_smem_optin() && copies > 1) smem = bytes(copies = (copies + 1) / 2);
         if (smem > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_ARG, "move_and_compact: n_g too large");
         auto kern = dep ? move_and_compact_tma_kernel<true> : move_and_compact_tma_kernel<false>;
-        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                                 "cudaFuncSetAttribute(move_and_compact)"));
         int per_sm = 0;
-        CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_THREADS, smem),
-                                 "occupancy(move_and_compact)"));
+        auto occupancy = [&]() {
+            CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                     "cudaFuncSetAttribute(move_and_compact)"));
+            return check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_THREADS, smem),
+                              "occupancy(move_and_compact)");
+        };
+        CUDAPIC_CHECK(occupancy());
+        // large grids: fewer histogram copies rather than fewer CTAs per SM
+        while (dep && per_sm < t.push_ctas_per_sm && copies > 1) {
+            copies = (copies + 1) / 2;
+            smem = bytes(stages);
+            CUDAPIC_CHECK(occupancy());
+        }
         per_sm = std::min(std::max(per_sm, 1), t.push_ctas_per_sm);
         const uint64_t tiles_max = ((uint64_t)g.capacity + MC_TILE - 1) / MC_TILE;
         const unsigned grid = persistent_grid(per_sm, tiles_max);

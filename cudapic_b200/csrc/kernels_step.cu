@@ -137,13 +137,22 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     while (bytes() > budget && stages > 2) --stages;
     while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "step_electrons: n_g too large");
-    const size_t smem = bytes();
     auto kern = electron_step_kernel<U>;
-    CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                             "cudaFuncSetAttribute(step_electrons)"));
     int per_sm = 0;
-    CUDAPIC_CHECK(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ES_THREADS, smem),
-                             "occupancy(step_electrons)"));
+    auto occupancy = [&]() {
+        CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes()),
+                                 "cudaFuncSetAttribute(step_electrons)"));
+        return check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ES_THREADS, bytes()),
+                          "occupancy(step_electrons)");
+    };
+    CUDAPIC_CHECK(occupancy());
+    // large grids: fewer histogram copies rather than fewer CTAs per SM (the
+    // copies only spread atomic conflicts, which a large grid spreads by itself)
+    while (per_sm < t.step_ctas_per_sm && copies > 1) {
+        copies = (copies + 1) / 2;
+        CUDAPIC_CHECK(occupancy());
+    }
+    const size_t smem = bytes();
     per_sm = std::min(std::max(per_sm, 1), t.step_ctas_per_sm);
     const uint64_t tiles_max = ((uint64_t)g.capacity + ES_TILE - 1) / ES_TILE;
     const unsigned grid = persistent_grid(per_sm, tiles_max);
