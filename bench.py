@@ -212,8 +212,10 @@ def barrier(world):
 
 # ---------------------------------------------------------------- CPU (reference program)
 
-def cpu_reference_run(args, n_marks_warm, n_marks_timed, per_share_cap=None):
-    """eduPIC on all host cores; returns (value, cores, sample description)."""
+def cpu_reference_run(args, n_marks_warm, n_marks_timed, per_share_cap=None, single=False):
+    """eduPIC on all host cores; returns (value, cores, sample description,
+    per-step figures, total), with single: also (last) the throughput of one
+    process alone on one core with one share."""
     from oracle import edupic_runner as R
     cores = R.host_cores()
     e, i = population(args)
@@ -226,7 +228,12 @@ def cpu_reference_run(args, n_marks_warm, n_marks_timed, per_share_cap=None):
               "(weight x%.1f, same density), %d x %d PIC steps timed after %d warm-up" %
               (cores, n_e_share, len(shares[0][1][0]), args.particles / n_e_share, n_marks_timed, STEP,
                n_marks_warm))
-    return value, cores, sample, per_step, total
+    if not single:
+        return value, cores, sample, per_step, total
+    one = R.run(shares[:1], weight, n_marks_warm + n_marks_timed, n_g=args.n_g)
+    value_1 = R.window_throughput(one, n_marks_warm, n_marks_warm + n_marks_timed)[0]
+    sample += "; the same share alone on one core: single_core_value"
+    return value, cores, sample, per_step, total, value_1
 
 
 def run_reference(args):
@@ -237,13 +244,14 @@ def run_reference(args):
     if not R.available(args.n_g):
         print(json.dumps({"impl": "reference", "unavailable": "eduPIC reference build missing (oracle/_ref)"}))
         return 0
-    value, cores, sample, per_step, _ = cpu_reference_run(args, args.warmup, args.steps)
+    value, cores, sample, per_step, _, value_1 = cpu_reference_run(args, args.warmup, args.steps, single=True)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(per_step), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args), "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                         "single_core_value": value_1},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -454,8 +462,9 @@ def run_ours(args):
         try:
             from oracle import edupic_runner as R
             if R.available(args.n_g):
-                v, cores, sample, _, _ = cpu_reference_run(args, 1, 3, per_share_cap=1 << 17)
-                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+                v, cores, sample, _, _, v1 = cpu_reference_run(args, 1, 3, per_share_cap=1 << 17, single=True)
+                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                       "single_core_value": v1}
         except Exception as ex:  # the baseline is reported, never the measured product
             cpu = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
 
