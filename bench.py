@@ -37,7 +37,6 @@ population; N > 1 ranks other than 0 exit without work.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
