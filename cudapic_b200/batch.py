@@ -16,9 +16,11 @@ collects per-rank results on every rank through ``torch.distributed``.
 
     python -m cudapic_b200.batch [--discharges 256 | --one-discharge N] [--steps 40]
                                  [--tune | --rows R --ctas C --stages S --copies K]
+                                 [--pressure P] [--voltage V]
 
-times a batch (the C2 sweep, or one argon CCP of N particles per species at
-the reference parameters) and prints one JSON line: the target of the
+times a batch (the C2 sweep, optionally with every discharge at one
+pressure or voltage, or one argon CCP of N particles per species at the
+reference parameters) and prints one JSON line: the target of the
 committed ncu captures of the batched kernels.
 """
 import math
@@ -204,6 +206,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=40)
     ap.add_argument("--tune", action="store_true", help="autotune the batched kernels' launch shapes first")
+    ap.add_argument("--pressure", type=float, help="every discharge of the sweep at this pressure [Pa]")
+    ap.add_argument("--voltage", type=float, help="every discharge of the sweep at this RF amplitude [V]")
     ap.add_argument("--rows", type=int)
     ap.add_argument("--ctas", type=int)
     ap.add_argument("--stages", type=int)
@@ -214,6 +218,11 @@ def main(argv=None):
         specs = [DischargeSpec(voltage=250.0, pressure=10.0, gap=0.025, n_g=400, particles=a.one_discharge, seed=17)]
     else:
         specs = c2_specs(n=a.discharges)
+        for s in specs:
+            if a.pressure:
+                s.pressure = a.pressure
+            if a.voltage:
+                s.voltage = a.voltage
     shape = {k: v for k, v in (("step_rows", a.rows), ("step_ctas_per_sm", a.ctas), ("step_stages", a.stages),
                                ("density_copies", a.copies)) if v}
     if shape:
