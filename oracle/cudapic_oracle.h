@@ -202,6 +202,10 @@ typedef struct orc_sens_io {
  * grad (may be NULL): d obs / d voltage by the pathwise adjoint; horizon
  * (a multiple of N_SUB, 0 = the whole window): the adjoint restarts from
  * zero every `horizon` steps.  Returns -1 on bad arguments. */
+/* Adjoint of the Poisson solve and field (the closed form of the CUDA solve,
+ * C/eduPIC.cc:461-494): from the field adjoint eb [n_g], the adjoints of
+ * the electron and ion densities; returns the adjoint of pot0. */
+double orc_sens_poisson_adjoint(const double *eb, const orc_phys *ph, double *neb, double *nib);
 int orc_sens_run(const orc_phys *ph, const float *sigma_tot_e, const float *sigma_tot_i, const float *cs,
                  double voltage, uint32_t steps, uint32_t horizon, int f64, orc_sens_io *io, double obs[2],
                  double grad[2]);

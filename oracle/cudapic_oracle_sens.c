@@ -177,6 +177,10 @@ static double poisson_adjoint(const double *eb, const orc_phys *ph, double *neb,
     return pot0b;
 }
 
+double orc_sens_poisson_adjoint(const double *eb, const orc_phys *ph, double *neb, double *nib) {
+    return poisson_adjoint(eb, ph, neb, nib);
+}
+
 /* x adjoint of a CIC deposit at x: d/dx sum_k db[k] dens_k(x). */
 static inline double deposit_gather(double x, const double *db, const orc_phys *ph) {
     const uint32_t n_g = ph->n_g;

@@ -24,7 +24,7 @@ __all__ = [
     "poisson_scan_f32", "poisson_dps_flexible_f64", "move_and_compact",
     "check_collisions_e", "check_collisions_i", "p_coll_e_exact",
     "accumulate_density", "accumulate_eepf", "xt_accumulate", "xt_normalise", "REF_DIR", "CS_RANGES", "N_EEPF",
-    "MATH_FN", "SensState", "sens_run",
+    "MATH_FN", "SensState", "sens_run", "sens_poisson_adjoint",
 ]
 
 MATH_FN = {"exp": 0, "log": 1, "sin": 2, "cos": 3, "tan": 4, "atan": 5, "acos": 6, "atan2": 7}
@@ -123,6 +123,8 @@ def _declare(L):
     L.orc_accumulate_density.argtypes = [_f32p, _f64p, C.c_uint32]
     L.orc_accumulate_eepf.argtypes = [_f32p] * 5 + [C.c_uint32, _u32p, P(OrcPhys)]
     L.orc_xt_accumulate.argtypes = [_f32p] * 5 + [C.c_uint32, C.c_int, _f32p, P(OrcPhys), _f64p]
+    L.orc_sens_poisson_adjoint.argtypes = [_f64p, P(OrcPhys), _f64p, _f64p]
+    L.orc_sens_poisson_adjoint.restype = C.c_double
     L.orc_sens_run.argtypes = [P(OrcPhys), _f32p, _f32p, _f32p, C.c_double, C.c_uint32, C.c_uint32, C.c_int,
                                P(OrcSensIo),
                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -367,3 +369,13 @@ def sens_run(ph, tables, voltage, steps, state, f64=False, grad=True, horizon=0)
     state.n = [io.n[0], io.n[1]]
     state.dev_err = io.dev_err
     return list(obs), (list(g) if grad else None)
+
+
+def sens_poisson_adjoint(eb, ph):
+    """(neb, nib, pot0b): adjoints of the electron and ion densities and of
+    pot0 for the field adjoint eb (the oracle's Poisson adjoint)."""
+    eb = np.ascontiguousarray(eb, np.float64)
+    neb = np.zeros(ph.n_g, np.float64)
+    nib = np.zeros(ph.n_g, np.float64)
+    p0 = lib().orc_sens_poisson_adjoint(eb, C.byref(ph), neb, nib)
+    return neb, nib, p0

@@ -74,3 +74,21 @@ def test_slot_form_keeps_slots_and_appends_spawns(oracle, tables):
         assert dead.sum() > 0             # and some particles reached the electrodes
     assert s.n[0] - st0.n[0] == s.n[1] - st0.n[1]
     assert s.dev_err == 0
+
+
+@pytest.mark.parametrize("n_g", [3, 4, 57, 400, 4096])
+def test_poisson_adjoint_is_the_transpose(oracle, n_g):
+    """<eb, E(dn_e, dn_i, dpot0)> = <neb, dn_e> + <nib, dn_i> + pot0b dpot0
+    for the FP64 solve (linear with zero base), random vectors."""
+    ph = oracle.phys_from_params(n_g=n_g)
+    rng = np.random.default_rng(n_g)
+    eb = rng.normal(size=n_g)
+    neb, nib, p0b = oracle.sens_poisson_adjoint(eb, ph)
+    for _ in range(3):
+        dne = rng.normal(size=n_g).astype(np.float32) * np.float32(1e15)
+        dni = rng.normal(size=n_g).astype(np.float32) * np.float32(1e15)
+        dp0 = float(rng.normal() * 100.0)
+        ef = oracle.poisson_thomas_f64(dne, dni, dp0, ph)[1]
+        lhs = float(np.dot(eb, ef))
+        rhs = float(np.dot(neb, dne.astype(np.float64)) + np.dot(nib, dni.astype(np.float64)) + p0b * dp0)
+        assert lhs == pytest.approx(rhs, rel=1e-9, abs=1e-9 * np.abs(eb).sum() * np.abs(ef).max())
