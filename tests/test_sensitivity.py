@@ -92,3 +92,19 @@ def test_poisson_adjoint_is_the_transpose(oracle, n_g):
         lhs = float(np.dot(eb, ef))
         rhs = float(np.dot(neb, dne.astype(np.float64)) + np.dot(nib, dni.astype(np.float64)) + p0b * dp0)
         assert lhs == pytest.approx(rhs, rel=1e-9, abs=1e-9 * np.abs(eb).sum() * np.abs(ef).max())
+
+
+def test_spawns_beyond_capacity_are_dropped_and_flagged(oracle, tables):
+    """A capacity just above the initial counts: the spawns that find no slot
+    are dropped, both counts stop at the capacity, both error bits are set."""
+    from cudapic_b200.workloads import steady_state
+    n = 2000
+    cap = n + 8
+    ph = oracle.phys_from_params(capacity=cap, weight=7e4 * 120000 / n)
+    e = steady_state(n, E_MASS, 12.0, dt=ph.dt_e, seed=4)
+    i = steady_state(n, AR_MASS, 0.03, dt=ph.dt_i, seed=5)
+    st = oracle.SensState(cap, e, i, oracle.seed_streams([1, 2, 3, 4], cap), oracle.seed_streams([5, 6, 7, 8], cap))
+    obs, grad = oracle.sens_run(ph, tables, 250.0, 200, st)
+    assert st.n == [cap, cap]
+    assert st.dev_err == 0x3
+    assert np.isfinite(obs).all() and np.isfinite(grad).all()
