@@ -25,6 +25,7 @@ collision events and random draws frozen:
 
     python -m cudapic_b200.sensitivity [--particles 1000000] [--window 8000]
         [--checkpoint 200] [--horizons 0,200,1000] [--dv 0.5] [--relax-cycles 10]
+        [--seeds 1,2,3,4]
 """
 import ctypes as C
 import json
@@ -131,14 +132,13 @@ def steady_state(particles=1_000_000, relax_cycles=10, seed=1, reference=None):
     return st
 
 
-def study(particles=1_000_000, window=8000, checkpoint=200, horizons=(0, 200, 1000), dv=0.5, voltage=250.0,
-          relax_cycles=10, seed=1):
+def one_start(particles=1_000_000, window=8000, checkpoint=200, horizons=(0, 200, 1000), dv=0.5, voltage=250.0,
+              relax_cycles=10, seed=1):
     """Adjoint sensitivities for each horizon against central differences
-    with common random numbers, with timings."""
+    with common random numbers, from one relaxed start, with timings."""
     import torch
     st = steady_state(particles, relax_cycles, seed)
-    out = {"particles": particles, "window_steps": window, "checkpoint_every": checkpoint, "dv": dv,
-           "voltage": voltage, "counts": st.counts(), "horizons": []}
+    out = {"seed": seed, "counts": st.counts(), "horizons": []}
     try:
         with VoltageSensitivity(st, window, checkpoint, 0) as s:
             torch.cuda.synchronize()
@@ -161,6 +161,30 @@ def study(particles=1_000_000, window=8000, checkpoint=200, horizons=(0, 200, 10
     return out
 
 
+def mean_and_error(values):
+    """(mean, standard error of the mean) of per-start values."""
+    a = np.asarray(values, np.float64)
+    if a.size < 2:
+        return float(a.mean()), float("nan")
+    return float(a.mean()), float(a.std(ddof=1) / np.sqrt(a.size))
+
+
+def study(particles=1_000_000, window=8000, checkpoint=200, horizons=(0, 200, 1000), dv=0.5, voltage=250.0,
+          relax_cycles=10, seeds=(1,)):
+    """one_start for every seed, and over the starts the mean and standard
+    error of the central differences and of each horizon's adjoint (the
+    difference of one start is noise-dominated over long windows)."""
+    starts = [one_start(particles, window, checkpoint, horizons, dv, voltage, relax_cycles, sd) for sd in seeds]
+    out = {"particles": particles, "window_steps": window, "checkpoint_every": checkpoint, "dv": dv,
+           "voltage": voltage, "relax_cycles": relax_cycles, "starts": starts, "summary": {}}
+    for k in OBSERVABLES:
+        sm = {"central_difference": mean_and_error([r["central_difference"][k] for r in starts])}
+        for j, h in enumerate(horizons):
+            sm["adjoint_h%d" % h] = mean_and_error([r["horizons"][j]["adjoint"][k] for r in starts])
+        out["summary"][k] = sm
+    return out
+
+
 def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser()
@@ -171,9 +195,10 @@ def main(argv=None):
     ap.add_argument("--dv", type=float, default=0.5)
     ap.add_argument("--voltage", type=float, default=250.0)
     ap.add_argument("--relax-cycles", type=int, default=10)
+    ap.add_argument("--seeds", default="1", help="relaxed starts, e.g. 1,2,3,4: mean and standard error over them")
     a = ap.parse_args(argv)
     r = study(a.particles, a.window, a.checkpoint, [int(h) for h in a.horizons.split(",")], a.dv, a.voltage,
-              a.relax_cycles)
+              a.relax_cycles, [int(x) for x in a.seeds.split(",")])
     print(json.dumps(r), flush=True)
     return 0
 

@@ -108,3 +108,12 @@ def test_spawns_beyond_capacity_are_dropped_and_flagged(oracle, tables):
     assert st.n == [cap, cap]
     assert st.dev_err == 0x3
     assert np.isfinite(obs).all() and np.isfinite(grad).all()
+
+
+def test_study_summary_statistics(cudapic):
+    """The study's per-start aggregation: mean and standard error."""
+    from cudapic_b200.sensitivity import mean_and_error
+    m, e = mean_and_error([1.0, 2.0, 3.0, 6.0])
+    assert m == 3.0 and e == pytest.approx(np.std([1.0, 2.0, 3.0, 6.0], ddof=1) / 2.0)
+    m, e = mean_and_error([4.0])
+    assert m == 4.0 and e != e  # NaN: no spread from one start
