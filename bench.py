@@ -1,41 +1,56 @@
 """Benchmark of the cudaPIC per-timestep PIC/MCC cycle on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n-g 400|4096]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c0]
 
-Workload (single-GPU microbenchmark configuration of the reference's
-headline metric): 4 194 304 electrons (Maxwellian 3 eV) + 4 194 304 Ar+ ions
-(Maxwellian 0.03 eV), positions uniform in [0, L], ~0.1 % within one step of
-an electrode moving outward; argon CCP L = 25 mm, N_G = 400, 13.56 MHz,
-250 V, 10 Pa, 350 K, N_T = 4000, N_SUB = 20.  The superparticle weight is
-scaled to 7e4 * 120 000 / 4 194 304 so that the plasma density equals the
-reference case's steady state.  Seeded synthetic data.
+Metric: particle-steps/s (one electron advanced by one electron step, or one
+ion by one ion step, counts 1), counted on the device.
 
-One benchmark step = 40 PIC time steps (two ion subcycles) of the
-reference's loop, Rust-CUDA/src/main.rs:1728-1807: per time step
-get_density(e) -> solve_poisson_scan_f32 -> move_and_compact(e) ->
-check_collisions_e, plus get_density(i), move_and_compact(i),
-check_collisions_i on every 20th step.  Metric: particle-steps/s (one
-electron advanced by one electron step, or one ion by one ion step, counts
-1), counted on the device.
+--workload c2 (default): the configuration the metric "batched+mixed vs
+plain GPU path" is quoted on.  256 independent argon CCP discharges,
+seeded: V ~ U(100, 500) V, p ~ logU(5, 50) Pa, L ~ U(15, 40) mm,
+N_G in {200, 400, 800}, 1e4..1e6 particles per species (Maxwellian 3 eV
+electrons, 0.03 eV ions, x ~ U[0, L]); seeded synthetic data.  Every kernel
+of a step is one launch over all discharges of a rank (libcudapic's batch
+driver), 2 N_SUB steps per captured CUDA graph; discharges are sharded over
+the ranks of an N-GPU job with no collective.  One benchmark step = 40 PIC
+time steps of every discharge (the reference loop
+Rust-CUDA/src/main.rs:1725-1808).  Phases:
+  1. untimed: warm-up, autotuning of the batched kernels' launch shapes;
+  2. every discharge reset to its initial population (RNG re-seeded), W
+     warm-up steps, K steps timed with CUDA events on the batch's stream
+     (inputs resident in HBM; ~3.7 GB of electron planes per PIC step, far above
+     the 126 MB L2, so no flush);
+  3. e2e: every discharge re-uploaded from pinned host memory, K steps, every
+     discharge's counts read back, all inside a wall-clock region;
+  4. per-kernel device times of 40 uncaptured batched steps (roofline);
+  5. the same discharges one at a time, each reset first, W + K steps
+     (K timed): (a) the plain path -- the reference's launch sequence,
+     every kernel launched from the host each step -- and (b) the
+     one-discharge fused driver.  speedup_vs_plain = batched / plain.
+A discharge whose device error word is set in any phase (spawns beyond its
+capacity) is excluded from every sum and counted in the line.
 
-Each timed step touches > 190 MB (electron SoA source + destination + RNG
-planes), more than the 126 MB L2, so no L2 flush is needed between steps.
+--workload c1: the fused one-discharge driver on one 4 194 304 + 4 194 304
+steady-state discharge (argon CCP, 25 mm, N_G = 400, 250 V, 10 Pa).
 
---workload c2 runs the batched path instead: the 256-discharge sweep of the
-reference's batched configuration (V ~ U(100, 500) V, p ~ logU(5, 50) Pa,
-L ~ U(15, 40) mm, N_G in {200, 400, 800}, 1e4..1e6 particles per species,
-seeded), every kernel of a step one launch over all discharges of a rank
-(libcudapic's batch driver), discharges sharded over the ranks of an N-GPU
-job; the line also reports the same discharges run one at a time through
-the reference's launch sequence (the plain path) and through the
-one-discharge fused driver.
+--workload c0: the plain eduPIC case, 1000 + 1000 particles at rest, one
+initialising RF cycle then 10 RF cycles timed: the fused graph driver, the
+reference launch sequence and eduPIC on one core.
 
 --impl reference times the reference's own CPU implementation of the path,
 eduPIC 1.0 (C/eduPIC.cc, built from the reference tree into oracle/_ref/),
-on all host cores, each core running an independent share of the same
-population; N > 1 ranks other than 0 exit without work.
+on the selected workload: c2 a sample of the sweep's discharges stratified
+by particle count, one full-size discharge per host core; c1 equal shares of
+the 4 M + 4 M population, one per core; c0 the case itself on one core (the
+program is single-threaded).  Processes start together behind a barrier;
+one reference step is --cpu-step-s seconds of all-core work, the value the
+particle-steps all cores did inside the K-step window divided by it.  The
+GPU arm's cpu_baseline runs the same function with the same window.  For
+N > 1 ranks other than 0 exit without work.
 """
 import argparse
+import importlib.util
 import json
 import os
 import statistics
@@ -56,6 +71,7 @@ N_PARTICLES = 1 << 22
 E_MASS = 9.10938356e-31
 AR_MASS = 6.63352090e-26
 FALLBACK_HBM_GBS = 6650.0
+C0_CYCLES = 10
 
 
 def parse():
@@ -64,41 +80,42 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n-g", type=int, default=400)
-    ap.add_argument("--particles", type=int, default=N_PARTICLES)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-breakdown", action="store_true")
-    ap.add_argument("--workload", choices=["c1", "c2"], default="c1",
-                    help="c1: one 4M+4M discharge (plain path); c2: the 256-discharge sweep (batched path)")
-    ap.add_argument("--discharges", type=int, default=256)
+    ap.add_argument("--workload", choices=["c2", "c1", "c0"], default="c2",
+                    help="c2: the 256-discharge sweep (batched path, default); c1: one 4M+4M discharge "
+                         "(fused one-discharge driver); c0: the plain eduPIC case")
+    ap.add_argument("--n-g", type=int, default=400, help="c1: grid points")
+    ap.add_argument("--particles", type=int, default=N_PARTICLES, help="c1: particles per species")
+    ap.add_argument("--discharges", type=int, default=256, help="c2: discharges of the sweep")
+    ap.add_argument("--capacity-factor", type=float, default=3.0, help="c2: slots per initial particle")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="c2: skip the autotuning of the batched kernels' launch shapes")
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="c2: discharges also timed one at a time for the plain comparisons (0: all of them)")
+    ap.add_argument("--cpu-step-s", type=float, default=1.0,
+                    help="seconds of all-core eduPIC work per reference step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-breakdown", action="store_true")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
 
 
-def workload_config(args):
-    return {
-        "workload": "plain GPU path: %d e + %d Ar+ steady state, argon CCP L=25mm, N_G=%d, 250V, 10Pa, "
-                    "13.56MHz, N_T=4000, N_SUB=20; 1 step = %d PIC steps" % (args.particles, args.particles,
-                                                                          args.n_g, STEP),
-        "particles_per_species": args.particles,
-        "n_g": args.n_g,
-        "pic_steps_per_step": STEP,
-        "weight": 7.0e4 * 120000 / args.particles,
-        "l2": "inputs larger than L2 (>190 MB touched per PIC step), no flush",
-        "parallelism": "replicas (one independent discharge per GPU)",
-    }
+def load_workloads():
+    """cudapic_b200/workloads.py loaded by path: plain numpy, so that the CPU
+    reference arm never maps the CUDA library."""
+    spec = importlib.util.spec_from_file_location("cudapic_workloads", os.path.join(ROOT, "cudapic_b200",
+                                                                                     "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def population(args, rank=0):
-    from cudapic_b200.workloads import steady_state
+    """c1: the 4M + 4M steady-state population."""
+    W = load_workloads()
     dt_e = 1.0 / 13.56e6 / 4000
-    e = steady_state(args.particles, E_MASS, 3.0, dt=dt_e, seed=11 + 2 * rank)
-    i = steady_state(args.particles, AR_MASS, 0.03, dt=20 * dt_e, seed=12 + 2 * rank)
+    e = W.steady_state(args.particles, E_MASS, 3.0, dt=dt_e, seed=11 + 2 * rank)
+    i = W.steady_state(args.particles, AR_MASS, 0.03, dt=20 * dt_e, seed=12 + 2 * rank)
     return e, i
 
 
@@ -109,6 +126,27 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_config(args):
+    if args.workload == "c2":
+        return {"workload": "C2 batched sweep: %d argon CCP discharges (V ~ U(100,500) V, p ~ logU(5,50) Pa, "
+                            "L ~ U(15,40) mm, N_G in {200,400,800}, 1e4..1e6 particles per species, seeded); "
+                            "1 step = %d PIC steps of every discharge" % (args.discharges, STEP),
+                "discharges": args.discharges, "pic_steps_per_step": STEP,
+                "l2": "inputs larger than L2 (~3.7 GB of electron planes read and written per PIC step), no flush"}
+    if args.workload == "c1":
+        return {"workload": "C1 fused one-discharge driver: %d e + %d Ar+ steady state, argon CCP L=25mm, N_G=%d, "
+                            "250V, 10Pa, 13.56MHz, N_T=4000, N_SUB=20; 1 step = %d PIC steps"
+                            % (args.particles, args.particles, args.n_g, STEP),
+                "particles_per_species": args.particles, "n_g": args.n_g, "pic_steps_per_step": STEP,
+                "weight": 7.0e4 * 120000 / args.particles,
+                "l2": "inputs larger than L2 (>190 MB touched per PIC step), no flush",
+                "parallelism": "replicas (one independent discharge per GPU)"}
+    return {"workload": "C0 plain eduPIC case: 1000 e + 1000 Ar+ at rest, argon CCP L=25mm, N_G=400, 250V, 10Pa; "
+                        "one initialising RF cycle, then %d RF cycles timed (1 step = 1 RF cycle)" % C0_CYCLES,
+            "rf_cycles": C0_CYCLES, "l2": "population fits in L2 (launch-bound case)",
+            "parallelism": "one discharge"}
 
 
 # ---------------------------------------------------------------- clocks
@@ -211,28 +249,80 @@ def barrier(world):
 
 # ---------------------------------------------------------------- CPU (reference program)
 
-def cpu_reference_run(args, n_marks_warm, n_marks_timed, per_share_cap=None, single=False):
-    """eduPIC on all host cores; returns (value, cores, sample description,
-    per-step figures, total), with single: also (last) the throughput of one
-    process alone on one core with one share."""
+def cpu_jobs(args, cores):
+    """The eduPIC processes of the selected workload, and a description."""
+    W = load_workloads()
+    if args.workload == "c2":
+        specs = W.c2_specs(n=args.discharges)
+        order = sorted(range(len(specs)), key=lambda k: specs[k].particles)
+        n = min(cores, len(specs))
+        pick = [order[int((j + 0.5) * len(order) / n)] for j in range(n)]
+        jobs = []
+        for k in pick:
+            s = specs[k]
+            e, i = W.initial_population(s)
+            jobs.append({"electrons": e, "ions": i, "weight": s.weight, "n_g": s.n_g,
+                         "env": {"EDUPIC_VOLTAGE": repr(s.voltage), "EDUPIC_L": repr(s.gap),
+                                 "EDUPIC_PRESSURE": repr(s.pressure)}})
+        parts = sorted(specs[k].particles for k in pick)
+        what = ("%d of the %d sweep discharges (stratified by particle count: %d..%d per species, median %d), "
+                "each at full size in its own process" % (n, len(specs), parts[0], parts[-1], parts[len(parts) // 2]))
+        return jobs, what
+    if args.workload == "c1":
+        e, i = population(args)
+        jobs = []
+        for k in range(cores):
+            ek = tuple(np.asarray(a[k::cores]) for a in e)
+            ik = tuple(np.asarray(a[k::cores]) for a in i)
+            jobs.append({"electrons": ek, "ions": ik, "weight": 7.0e4 * 120000 / len(ek[0]), "n_g": args.n_g})
+        what = ("the %d + %d population dealt into %d equal shares (%d e + %d Ar+ each, weight scaled to the same "
+                "density), one per process" % (args.particles, args.particles, cores, len(jobs[0]["electrons"][0]),
+                                                len(jobs[0]["ions"][0])))
+        return jobs, what
+    raise ValueError(args.workload)
+
+
+def cpu_reference(args):
+    """eduPIC on all host cores over the common window of the selected
+    workload (c2, c1), plus one of its processes alone on one core."""
     from oracle import edupic_runner as R
     cores = R.host_cores()
-    e, i = population(args)
-    shares = R.split_population(e, i, cores, per_share_cap=per_share_cap)
-    n_e_share = len(shares[0][0][0])
-    weight = 7.0e4 * 120000 / args.particles * (args.particles / n_e_share)
-    marks = R.run(shares, weight, n_marks_warm + n_marks_timed, n_g=args.n_g)
-    value, total, wall, per_step = R.window_throughput(marks, n_marks_warm, n_marks_warm + n_marks_timed)
-    sample = ("eduPIC 1.0 (C/eduPIC.cc, g++ -O3) x %d processes, %d e + %d Ar+ per process "
-              "(weight x%.1f, same density), %d x %d PIC steps timed after %d warm-up" %
-              (cores, n_e_share, len(shares[0][1][0]), args.particles / n_e_share, n_marks_timed, STEP,
-               n_marks_warm))
-    if not single:
-        return value, cores, sample, per_step, total
-    one = R.run(shares[:1], weight, n_marks_warm + n_marks_timed, n_g=args.n_g)
-    value_1 = R.window_throughput(one, n_marks_warm, n_marks_warm + n_marks_timed)[0]
-    sample += "; the same share alone on one core: single_core_value"
-    return value, cores, sample, per_step, total, value_1
+    jobs, what = cpu_jobs(args, cores)
+    warm_s, window_s = args.warmup * args.cpu_step_s, args.steps * args.cpu_step_s
+    value, rates, window, per_job = R.run_window(jobs, warm_s, window_s)
+    mid = sorted(range(len(jobs)), key=lambda k: len(jobs[k]["electrons"][0]))[len(jobs) // 2]
+    one = R.run_window([jobs[mid]], warm_s, min(window_s, 10.0))[0]
+    sample = ("eduPIC 1.0 (C/eduPIC.cc, g++ -O3) x %d processes on %d host cores: %s; all started together, "
+              "%.0f s warm-up, particle-steps inside a %.0f s window (%d steps of %.1f s); "
+              "single_core_value: the median process alone on one core"
+              % (len(jobs), cores, what, warm_s, window, args.steps, args.cpu_step_s))
+    return {"value": value, "unit": UNIT, "cores": len(jobs), "kind": "reference", "sample": sample,
+            "single_core_value": one, "window_s": window}
+
+
+def edupic_c0():
+    """configs[0] on the reference CPU program: the initialising cycle
+    (eduPIC 0), then C0_CYCLES RF cycles (eduPIC 10) timed from its marks (set-up excluded)."""
+    import shutil
+    import tempfile
+    from oracle import edupic_runner as R
+    exe = os.path.join(R.REF_DIR, "eduPIC")
+    d = tempfile.mkdtemp(prefix="edupic_c0_")
+    try:
+        subprocess.run([exe, "0"], cwd=d, check=True, capture_output=True)
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, str(C0_CYCLES)], cwd=d, check=True, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        marks = [(int(a), int(b), int(c)) for a, b, c in R._MARK.findall(r.stderr)]
+        work = marks[-1][1] - marks[0][1]
+        secs = (marks[-1][2] - marks[0][2]) * 1e-9
+        return {"value": work / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "eduPIC 1.0 on one core: the init cycle from 1000 + 1000 particles at rest, then %d RF "
+                          "cycles timed (%d particle-steps, %.2f s; %.2f s with set-up)" % (C0_CYCLES, work, secs,
+                                                                                         wall),
+                "work": work, "seconds": secs}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def run_reference(args):
@@ -240,24 +330,42 @@ def run_reference(args):
     if rank != 0:
         return 0
     from oracle import edupic_runner as R
-    if not R.available(args.n_g):
+    if not all(R.available(g) for g in (200, 400, 800)) or (args.workload == "c1" and not R.available(args.n_g)):
         print(json.dumps({"impl": "reference", "unavailable": "eduPIC reference build missing (oracle/_ref)"}))
         return 0
-    value, cores, sample, per_step, _, value_1 = cpu_reference_run(args, args.warmup, args.steps, single=True)
+    if args.workload == "c0":
+        cpu = edupic_c0()
+        ms = 1e3 * cpu["seconds"] / C0_CYCLES
+        steps, warm = C0_CYCLES, 1
+    else:
+        cpu = cpu_reference(args)
+        ms = 1e3 * cpu["window_s"] / args.steps
+        steps, warm = args.steps, args.warmup
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(per_step), "higher_is_better": True,
+        "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args), "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
-                         "single_core_value": value_1},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": workload_config(args), "impl": "reference", "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
-# ---------------------------------------------------------------- GPU arm
+def cpu_baseline(args, rank, world):
+    """The reference arm's measurement, on rank 0 of a 1-GPU run only."""
+    if rank != 0 or world != 1 or args.no_cpu_baseline:
+        return None
+    try:
+        from oracle import edupic_runner as R
+        if not all(R.available(g) for g in (200, 400, 800)):
+            return None
+        return edupic_c0() if args.workload == "c0" else cpu_reference(args)
+    except Exception as ex:  # the baseline is reported, never the measured product
+        return {"value": None, "unit": UNIT, "error": str(ex)[:200]}
+
+
+# ---------------------------------------------------------------- GPU arm: one discharge (c1)
 
 ALGO_BYTES = {  # algorithmic bytes per particle per launch
     "get_density": 4,            # read x
@@ -352,7 +460,7 @@ def kernel_breakdown(st, K, reps, flush):
     return res
 
 
-def run_ours(args):
+def run_one_discharge(args):
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
@@ -456,17 +564,7 @@ def run_ours(args):
                     "frac": d["gbs"] / peak, "traffic": traffic, "peak_source": peak_kind,
                     "algo_bytes_per_particle": d["bytes_per_particle"]}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            from oracle import edupic_runner as R
-            if R.available(args.n_g):
-                v, cores, sample, _, _, v1 = cpu_reference_run(args, 1, 3, per_share_cap=1 << 17, single=True)
-                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
-                       "single_core_value": v1}
-        except Exception as ex:  # the baseline is reported, never the measured product
-            cpu = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
-
+    cpu = cpu_baseline(args, rank, world)
     st.close()
     if world > 1:
         import torch.distributed as dist
@@ -509,67 +607,91 @@ STATED_ERROR = {"kernels": "RNG, push/compaction, collisions bit-exact with the 
                               "N_e 0.053; f32 and FP64 arithmetic modes agree within the seed spread (<= 0.012)"}
 
 
+# ---------------------------------------------------------------- GPU arm: the batched sweep (c2)
+
 def run_batched(args):
-    """The C2 sweep through cudapic_b200.batch (see the module docstring)."""
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
-    from cudapic_b200.batch import Batch, c2_specs, gather, shard
-    specs = c2_specs(n=args.discharges)
-    mine = [specs[k] for k in shard(specs, world)[rank]]
-    batch = Batch(mine, device=local)
-    batch.run_steps(STEP * args.warmup)
-    batch.synchronize()
-    # launch shapes of the batched kernels for this mix of discharges
-    # (untimed; every rank tunes on its own shard)
     import cudapic_b200 as cp
     from cudapic_b200.autotune import tune_batch
+    from cudapic_b200.batch import Batch, c2_specs, gather, initial_population, shard
+    specs = c2_specs(n=args.discharges)
+    mine = [specs[k] for k in shard(specs, world)[rank]]
+    batch = Batch(mine, device=local, capacity_factor=args.capacity_factor)
+    flagged = set()
+
+    def note_errors():
+        for k, e in enumerate(batch.device_errors()):
+            if e:
+                flagged.add(k)
+
+    # 1. untimed: warm-up and the launch shapes of the batched kernels for this
+    #    mix of discharges (every rank tunes on its own shard)
+    batch.run_steps(STEP * args.warmup)
+    batch.synchronize()
     defaults = cp.get_tuning()
     tuned, _ = tune_batch(batch) if args.tune else (None, None)
-    batch.run_steps(STEP)
+
+    # 2. device-timed: from the initial populations, W warm-up steps, K timed
+    batch.reset()
+    batch.run_steps(STEP * args.warmup)
     batch.synchronize()
     barrier(world)
+    works0 = batch.works()
     with ClockSampler(local) as clk:
-        elapsed, work = batch.timed_steps(STEP * args.steps)
+        elapsed, _ = batch.timed_steps(STEP * args.steps)
     barrier(world)
-    elapsed_max, work_sum = reduce_max_sum(world, elapsed, work)
-    value = work_sum / elapsed_max
-    errors = batch.device_errors()
-    flagged = [k for k, pc in enumerate(batch.prechecks()) if not pc["conditions_ok"]]
+    works_timed = [b - a for a, b in zip(works0, batch.works())]
+    note_errors()
 
-    # end to end through the public API: every discharge re-uploaded from
-    # pinned host memory, the steps, every discharge's counts read back
-    from cudapic_b200.batch import initial_population
+    # 3. end to end through the public API: every discharge re-uploaded from
+    #    pinned host memory, the steps, every discharge's counts read back
     pinned = []
     for st, spec in zip(batch.states, mine):
         e, i = initial_population(spec, st.grid.dt_e, st.grid.dt_i)
         pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*e, *i)])
-    lib = __import__("cudapic_b200").lib
+    h2d = 16 * sum(2 * p[0].numel() for p in pinned)
     barrier(world)
     batch.synchronize()
-    w0 = batch.work()
+    w0 = batch.works()
     t0 = time.perf_counter()
-    h2d = d2h = 0
-    for st, arrs in zip(batch.states, pinned):
-        n = arrs[0].numel()
-        for sp in (0, 1):
-            __import__("cudapic_b200").check(lib.cudapic_state_upload(
-                st.handle, sp, *(t.data_ptr() for t in arrs[4 * sp:4 * sp + 4]), n))
-            h2d += 16 * n
+    batch.reset(pinned=pinned, reseed=False)
     batch.run_steps(STEP * args.steps)
-    for st in batch.states:
-        st.counts()
-        d2h += 8
+    batch.counts()
     e2e_wall = time.perf_counter() - t0
-    e2e_work = batch.work() - w0
-    e2e_max, e2e_sum = reduce_max_sum(world, e2e_wall, e2e_work)
+    works_e2e = [b - a for a, b in zip(w0, batch.works())]
+    d2h = 8 * len(batch.states)
+    note_errors()
 
-    # the single-simulation comparisons, rank 0's discharges one at a time
-    # (the same states, continuing from where the batch left them):
-    #  * plain: the reference's launch sequence, every step launched from the
-    #    host (no fusion, no graph, no programmatic dependent launch);
-    #  * fused: this library's one-discharge driver (fused step, graphs, PDL).
+    # 4. per-kernel device times of 40 uncaptured steps (roofline)
+    breakdown = None
+    if not args.no_breakdown:
+        c_before = np.array(batch.counts(), np.float64).sum(axis=0)
+        prof = batch.profile_steps(STEP)
+        c_after = np.array(batch.counts(), np.float64).sum(axis=0)
+        n_e_mean, n_i_mean = 0.5 * (c_before + c_after)
+        breakdown = {}
+        for k, (ms, n) in prof.items():
+            if not n:
+                continue
+            us = 1e3 * ms / n
+            d = {"us": us, "launches": int(n), "share": None}
+            per = {"electron_step": (64, n_e_mean), "ion_push": (32, n_i_mean), "ion_collisions": (44, n_i_mean)}
+            if k in per:
+                b, cnt = per[k]
+                d.update({"bytes_per_particle": b, "n": cnt, "algo_bytes": b * cnt, "gbs": b * cnt / (us * 1e3)})
+            breakdown[k] = d
+        tot = sum(v["us"] * v["launches"] for v in breakdown.values())
+        for v in breakdown.values():
+            v["share"] = v["us"] * v["launches"] / tot
+        note_errors()
+
+    # 5. the single-simulation comparisons, rank 0's discharges one at a time,
+    #    each from its initial population
     plain = fused = None
+    sums = {"plain": [0.0, []], "fused": [0.0, []]}
+    order = []
     if rank == 0:
         order = sorted(range(len(mine)), key=lambda k: mine[k].particles)
         if 0 < args.plain_sample < len(order):
@@ -587,11 +709,11 @@ def run_batched(args):
             return ev0.elapsed_time(ev1) * 1e-3, st.work() - w0
 
         cp.set_tuning(**defaults)  # the one-discharge kernels' own shapes
-        sums = {"plain": [0.0, 0.0], "fused": [0.0, 0.0]}
         for k in order:
             st = batch.states[k]
             for mode in ("plain", "fused"):
                 on = mode == "fused"
+                batch.reset_one(k)
                 st.set_fused(on)
                 st.set_graphs(on)
                 st.set_overlap(on)
@@ -599,17 +721,33 @@ def run_batched(args):
                 st.synchronize()
                 t, w = alone(st, STEP * args.steps)
                 sums[mode][0] += t
-                sums[mode][1] += w
-        what = "%d of the %d discharges, each alone in turn, %d PIC steps each" % (len(order), len(specs),
-                                                                                 STEP * args.steps)
-        plain = {"value": sums["plain"][1] / sums["plain"][0], "unit": UNIT,
+                sums[mode][1].append((k, w))
+                if st.device_error():
+                    flagged.add(k)
+
+    # every sum leaves out the discharges flagged in any phase
+    flagged_all = set().union(*gather(sorted(flagged), world)) if world > 1 else flagged
+    per_rank_flagged = gather(len(flagged), world)
+    work_timed = sum(w for k, w in enumerate(works_timed) if k not in flagged)
+    work_e2e = sum(w for k, w in enumerate(works_e2e) if k not in flagged)
+    elapsed_max, work_sum = reduce_max_sum(world, elapsed, work_timed)
+    e2e_max, e2e_sum = reduce_max_sum(world, e2e_wall, work_e2e)
+    value = work_sum / elapsed_max
+    if rank == 0:
+        what = "%d of the %d discharges, each alone in turn from its initial population, %d warm-up + %d timed " \
+               "PIC steps each" % (len(order), len(specs), STEP * args.warmup, STEP * args.steps)
+        for mode in ("plain", "fused"):
+            w = sum(x for k, x in sums[mode][1] if k not in flagged)
+            sums[mode].append(w / sums[mode][0] if sums[mode][0] else None)
+        plain = {"value": sums["plain"][2], "unit": UNIT,
                  "path": "reference launch sequence (get_density, Poisson, move_and_compact, check_collisions), "
                          "every step launched from the host", "sample": what}
-        fused = {"value": sums["fused"][1] / sums["fused"][0], "unit": UNIT,
+        fused = {"value": sums["fused"][2], "unit": UNIT,
                  "path": "one-discharge fused driver (fused electron step, CUDA graph of 2 N_SUB steps, PDL)",
                  "sample": what}
-    per_rank = gather({"discharges": len(mine), "errors": sum(1 for e in errors if e)}, world)
+    n_clean = sum(1 for k in range(len(mine)) if k not in flagged)
     batch.close()
+    cpu = cpu_baseline(args, rank, world)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -617,34 +755,114 @@ def run_batched(args):
         return 0
     peak, peak_kind = measured_peaks()
     ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
+    roofline = None
+    if breakdown and "electron_step" in breakdown:
+        d = breakdown["electron_step"]
+        roofline = {"bound": "hbm", "kernel": "batch_step_kernel<MCC> (fused electron step of all discharges)",
+                    "achieved": d["gbs"], "peak": peak, "unit": "GB/s", "frac": d["gbs"] / peak,
+                    "traffic": ncu_traffic("batch_electron_step", d["n"]), "peak_source": peak_kind,
+                    "algo_bytes_per_particle": 64,
+                    "aggregate_gbs": 64.0 * work_sum / elapsed_max / 1e9}
+    cfg = workload_config(args)
+    cfg.update({"precision": "f32 particles and push, 2^-20 fixed-point deposits summed exactly in 64-bit integers, "
+                             "FP64 Poisson scans and time averages",
+                "launch_shapes": tuned or "library defaults",
+                "particles_total": int(sum(s.particles for s in specs)),
+                "capacity_factor": args.capacity_factor,
+                "parallelism": "discharges sharded over %d rank(s), no collective" % world})
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batched path: %d discharges of the C2 sweep (V, p, L, N_G, 1e4..1e6 particles per "
-                               "species sampled, seeded), one launch per kernel for all discharges, graph of 2 N_SUB "
-                               "steps; 1 step = %d PIC steps" % (len(specs), STEP),
-                   "precision": "f32 particles and push, 2^-20 fixed-point deposits summed exactly in 64-bit "
-                                "integers, FP64 Poisson scans and time averages",
-                   "launch_shapes": tuned or "library defaults",
-                   "discharges": len(specs), "particles_total": int(sum(s.particles for s in specs)),
-                   "l2": "inputs larger than L2 in aggregate, no flush",
-                   "parallelism": "discharges sharded over %d rank(s), no collective" % world},
+        "config": cfg,
         "plain_sequential": plain,
         "fused_sequential": fused,
-        "speedup_vs_plain": value / plain["value"] if plain else None,
-        "speedup_vs_fused_single": value / fused["value"] if fused else None,
+        "speedup_vs_plain": value / plain["value"] if plain and plain["value"] else None,
+        "speedup_vs_fused_single": value / fused["value"] if fused and fused["value"] else None,
         "e2e": {"value": e2e_sum / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_max},
-        "roofline": {"bound": "hbm", "kernel": "all (batch aggregate, 64 B per particle-step)",
-                     "achieved": 64.0 * work_sum / elapsed_max / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": 64.0 * work_sum / elapsed_max / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+        "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu,
         "stated_error": STATED_ERROR, "clocks": clk.summary(),
         "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2),
-        "discharges_with_device_errors": sum(r["errors"] for r in per_rank),
-        "precheck_flagged": len(flagged),
+        "discharges_counted": n_clean if world == 1 else None,
+        "discharges_excluded": len(flagged_all),
+        "excluded_why": "device error word set in some phase (spawns beyond the capacity of %.1fx the initial "
+                        "population); their particle-steps are not counted, their time is" % args.capacity_factor,
+        "excluded_per_rank": per_rank_flagged,
     }
     print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm: the plain eduPIC case (c0)
+
+def run_c0(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    import cudapic_b200 as cp
+    from cudapic_b200.sim import GpuSimState, ParticlesSoA
+    W = load_workloads()
+    e0 = W.edupic_initial(1000, seed=0)
+    i0 = W.edupic_initial(1000, seed=1)
+    res = {}
+    for mode in ("fused", "plain"):
+        st = GpuSimState(capacity=40_000, device=local)
+        on = mode == "fused"
+        st.set_fused(on)
+        st.set_graphs(on)
+        st.set_overlap(on)
+        st.upload_electrons(ParticlesSoA(*e0))
+        st.upload_ions(ParticlesSoA(*i0))
+        st.seed()
+        st.run_cycles(1)          # the initialising cycle (eduPIC 0), graphs captured
+        st.synchronize()
+        s = torch.cuda.ExternalStream(st.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = st.work()
+        if on:
+            clk = ClockSampler(local)
+            clk.__enter__()
+        ev0.record(s)
+        st.run_cycles(C0_CYCLES)
+        ev1.record(s)
+        ev1.synchronize()
+        if on:
+            clk.__exit__(None, None, None)
+        t = ev0.elapsed_time(ev1) * 1e-3
+        res[mode] = {"seconds": t, "work": st.work() - w0, "counts": st.counts(), "dev_err": st.device_error()}
+        if on:
+            # end to end: upload from pinned memory, the init cycle and 10 cycles, counts read back per cycle
+            pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*e0, *i0)]
+            st.seed()
+            torch.cuda.synchronize()
+            w1 = st.work()
+            t0 = time.perf_counter()
+            for sp in (0, 1):
+                cp.check(cp.lib.cudapic_state_upload(st.handle, sp, *(p.data_ptr() for p in pin[4 * sp:4 * sp + 4]),
+                                                     1000))
+            for _ in range(C0_CYCLES + 1):
+                st.run_cycles(1)
+                st.counts()
+            e2e_t = time.perf_counter() - t0
+            res["e2e"] = {"value": (st.work() - w1) / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * 1000,
+                          "d2h_bytes_per_step": 8, "wall_s": e2e_t}
+        st.close()
+    cpu = cpu_baseline(args, rank, world)
+    f, p = res["fused"], res["plain"]
+    line = {
+        "metric": METRIC, "value": f["work"] / f["seconds"], "unit": UNIT, "n_gpus": 1, "steps": C0_CYCLES,
+        "warmup": 1, "ms_per_step": 1e3 * f["seconds"] / C0_CYCLES, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
+        "plain_path": {"value": p["work"] / p["seconds"], "unit": UNIT, "seconds": p["seconds"],
+                       "path": "reference launch sequence, every kernel launched from the host"},
+        "fused_seconds": f["seconds"], "particle_steps": f["work"], "counts_end": f["counts"],
+        "e2e": res["e2e"], "cpu_baseline": cpu, "clocks": clk.summary(), "roofline": None,
+        "gpu_launches": C0_CYCLES * 4000 * 2 + C0_CYCLES * 200 * 2,
+        "device_error_bits": [f["dev_err"], p["dev_err"]],
+    }
+    if rank == 0:
+        print(json.dumps(line))
     return 0
 
 
@@ -656,4 +874,4 @@ if __name__ == "__main__":
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if a.impl == "reference":
         sys.exit(run_reference(a))
-    sys.exit(run_batched(a) if a.workload == "c2" else run_ours(a))
+    sys.exit({"c2": run_batched, "c1": run_one_discharge, "c0": run_c0}[a.workload](a))

@@ -180,6 +180,8 @@ SIGNATURES = {
     "cudapic_state_run_steps": [_VP, C.c_uint64],
     "cudapic_state_counts": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_device_error": [_VP, C.POINTER(_U32)],
+    "cudapic_state_debug_wait_timeout": [_VP, C.c_longlong],
+    "cudapic_state_clear_device_error": [_VP],
     "cudapic_state_work": [_VP, C.POINTER(C.c_ulonglong)],
     "cudapic_state_steps_done": [_VP, C.POINTER(C.c_uint64)],
     "cudapic_state_synchronize": [_VP],
@@ -191,6 +193,7 @@ SIGNATURES = {
     "cudapic_batch_destroy": [_VP],
     "cudapic_batch_run_steps": [_VP, C.c_uint64],
     "cudapic_batch_synchronize": [_VP],
+    "cudapic_batch_profile_steps": [_VP, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_uint64)],
     "cudapic_sens_create": [_VP, _U32, _U32, _U32, C.POINTER(_VP)],
     "cudapic_sens_forward": [_VP, C.c_double, C.POINTER(C.c_double)],
     "cudapic_sens_backward": [_VP, C.POINTER(C.c_double)],

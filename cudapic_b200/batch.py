@@ -23,47 +23,9 @@ pressure or voltage, or one argon CCP of N particles per species at the
 reference parameters) and prints one JSON line: the target of the
 committed ncu captures of the batched kernels.
 """
-import math
-from dataclasses import asdict, dataclass
+from dataclasses import asdict
 
-import numpy as np
-
-E_MASS = 9.10938356e-31
-AR_MASS = 6.63352090e-26
-
-
-@dataclass
-class DischargeSpec:
-    """One discharge of a sweep (argon CCP, eduPIC physics)."""
-    voltage: float      # RF amplitude [V]
-    pressure: float     # [Pa]
-    gap: float          # electrode gap [m]
-    n_g: int            # grid points
-    particles: int      # initial electrons (and ions)
-    seed: int
-
-    def params(self, capacity_factor=2.0):
-        import cudapic_b200 as cp
-        cap = int(math.ceil(self.particles * capacity_factor / 4.0)) * 4
-        # superparticle weight of the reference steady state scaled to the particle count
-        return cp.default_params(voltage=self.voltage, pressure=self.pressure, gap=self.gap, n_g=self.n_g,
-                                 capacity=cap, weight=7.0e4 * 120000 / self.particles)
-
-
-def c2_specs(n=256, seed=0x5EED):
-    """The C2 sweep: V ~ U(100, 500) V, p ~ logU(5, 50) Pa, L ~ U(15, 40) mm,
-    N_G in {200, 400, 800}, particles per species ~ logU(1e4, 1e6)."""
-    rng = np.random.default_rng(seed)
-    specs = []
-    for k in range(n):
-        specs.append(DischargeSpec(
-            voltage=float(rng.uniform(100.0, 500.0)),
-            pressure=float(math.exp(rng.uniform(math.log(5.0), math.log(50.0)))),
-            gap=float(rng.uniform(0.015, 0.040)),
-            n_g=int(rng.choice([200, 400, 800])),
-            particles=int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6))))),
-            seed=int(seed) * 1000 + k))
-    return specs
+from .workloads import DischargeSpec, c2_specs, initial_population  # noqa: F401  (the sweep's definitions)
 
 
 def shard(specs, world):
@@ -104,14 +66,6 @@ def reduce_max_sum(world, elapsed, work):
     return t.item(), w.item()
 
 
-def initial_population(spec, dt_e, dt_i):
-    """Maxwellian electrons (3 eV) and ions (0.03 eV) uniform in the gap."""
-    from cudapic_b200.workloads import steady_state
-    e = steady_state(spec.particles, E_MASS, 3.0, gap=spec.gap, dt=dt_e, seed=spec.seed)
-    i = steady_state(spec.particles, AR_MASS, 0.03, gap=spec.gap, dt=dt_i, seed=spec.seed + 1)
-    return e, i
-
-
 class Batch:
     """Every discharge of ``specs`` as a GpuSimState, stepped by one GpuBatch."""
 
@@ -128,8 +82,7 @@ class Batch:
                 e, i = initial_population(spec, g.dt_e, g.dt_i)
                 st.upload_electrons(ParticlesSoA(*e))
                 st.upload_ions(ParticlesSoA(*i))
-                st.seed(e_master=(0x12345678 ^ spec.seed, 0x11112222, 0x22223333, 0x33334444),
-                        i_master=(0x44445555 ^ spec.seed, 0x55556666, 0x66667777, 0x77778888))
+                self._seed(st, spec)
             self.batch = GpuBatch(self.states)
         except Exception:
             self.close()
@@ -167,6 +120,44 @@ class Batch:
         end.record(s)
         end.synchronize()
         return start.elapsed_time(end) * 1e-3, self.work() - w0
+
+    def profile_steps(self, n_steps):
+        """Per-kernel device time of n_steps uncaptured batched steps."""
+        return self.batch.profile_steps(n_steps)
+
+    def reset(self, pinned=None, reseed=True):
+        """Every discharge back to its initial population (from `pinned`
+        host tensors when given: per discharge e x, vx, vy, vz, i x, vx, vy,
+        vz), RNG streams re-seeded unless reseed is False, device error words
+        cleared; enqueued on each state's stream."""
+        for k in range(len(self.states)):
+            self.reset_one(k, None if pinned is None else pinned[k], reseed)
+
+    def reset_one(self, k, pinned=None, reseed=True):
+        import cudapic_b200 as cp
+        from cudapic_b200.sim import ParticlesSoA
+        st, spec = self.states[k], self.specs[k]
+        if pinned is None:
+            e, i = initial_population(spec, st.grid.dt_e, st.grid.dt_i)
+            st.upload_electrons(ParticlesSoA(*e))
+            st.upload_ions(ParticlesSoA(*i))
+        else:
+            n = pinned[0].numel()
+            for sp in (0, 1):
+                cp.check(cp.lib.cudapic_state_upload(st.handle, sp, *(t.data_ptr() for t in pinned[4 * sp:4 * sp + 4]),
+                                                     n))
+        if reseed:
+            self._seed(st, spec)
+        st.clear_device_error()
+
+    @staticmethod
+    def _seed(st, spec):
+        st.seed(e_master=(0x12345678 ^ spec.seed, 0x11112222, 0x22223333, 0x33334444),
+                i_master=(0x44445555 ^ spec.seed, 0x55556666, 0x66667777, 0x77778888))
+
+    def works(self):
+        """Particle-steps counted so far, per discharge."""
+        return [st.work() for st in self.states]
 
     def counts(self):
         return [st.counts() for st in self.states]

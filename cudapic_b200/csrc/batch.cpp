@@ -222,14 +222,35 @@ SidePlanes side_planes(const cudapic_batch *b, int sp, int side) {
     return s;
 }
 
+// Per-kernel timing of uncaptured steps (cudapic_batch_profile_steps): an
+// event before and after every kernel group of a step.
+struct BatchProfile {
+    std::vector<cudaEvent_t> ev;   // pairs, in the order of `kind`
+    std::vector<int> kind;         // CUDAPIC_BATCH_K_*
+    int mark(int k, cudaStream_t st, bool end) {
+        cudaEvent_t e = nullptr;
+        CUDAPIC_CHECK(check_cuda(cudaEventCreate(&e), "batch profile: event"));
+        ev.push_back(e);
+        if (!end) kind.push_back(k);
+        return check_cuda(cudaEventRecord(e, st), "batch profile: record");
+    }
+    ~BatchProfile() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
 // One step of every discharge (the order of state.cpp's fused step).
-int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure) {
-    PdlScope pdl(true);
+int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, BatchProfile *prof = nullptr) {
+    PdlScope pdl(prof == nullptr);  // the profiler's events sit between the kernels
     const uint32_t D = b->count();
     cudaStream_t st = b->stream;
+    auto begin = [&](int k) { return prof ? prof->mark(k, st, false) : CUDAPIC_OK; };
+    auto finish = [&](int k) { return prof ? prof->mark(k, st, true) : CUDAPIC_OK; };
     if (ion_step) b->icur ^= 1;  // the buffer that collected the period's ion deposits becomes current
+    CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_POISSON));
     CUDAPIC_CHECK(launch_batch_poisson(b->desc, b->counts, D, b->max_n_g, b->flags, b->ecur, b->icur, ion_step ? 1 : 0,
                                        measure ? 1 : 0, st));
+    CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_POISSON));
     if (measure) {  // XT diagnostics: the particles before their push
         CUDAPIC_CHECK(launch_batch_xt_particles(false, side_planes(b, 0, b->se), b->desc, D, b->max_n_g, b->cap_sum,
                                                 st));
@@ -242,17 +263,24 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure) {
     r.measure = measure ? 1 : 0;
     if (ion_step) {
         r.dens = b->icur ^ 1;
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ION_PUSH));
         CUDAPIC_CHECK(launch_batch_step(false, step_planes(b, 1, b->si, b->si ^ 1), b->desc, b->counts + D, D,
                                         b->cap_sum, b->max_n_g, r, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ION_PUSH));
         b->si ^= 1;
     }
     r.dens = b->ecur ^ 1;
+    CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_STEP));
     CUDAPIC_CHECK(launch_batch_step(true, step_planes(b, 0, b->se, b->si), b->desc, b->counts, D, b->cap_sum,
                                     b->max_n_g, r, st));
+    CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_STEP));
     b->se ^= 1;
     b->ecur ^= 1;
-    if (ion_step)
+    if (ion_step) {
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ION_COLLISIONS));
         CUDAPIC_CHECK(launch_batch_collisions_i(side_planes(b, 1, b->si), b->desc, D, b->cap_sum, measure ? 1 : 0, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ION_COLLISIONS));
+    }
     if (measure) CUDAPIC_CHECK(launch_batch_eepf(side_planes(b, 0, b->se), b->desc, D, b->cap_sum, st));
     return CUDAPIC_OK;
 }
@@ -382,9 +410,12 @@ extern "C" int cudapic_batch_synchronize(cudapic_batch *b) {
     return check_cuda(cudaStreamSynchronize(b->stream), "batch_synchronize");
 }
 
-extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
-    if (!b) return fail(CUDAPIC_ERR_ARG, "batch_run_steps: null batch");
-    DeviceGuard dg(b->device);
+namespace {
+
+// Checks the states and brings them to where the batch's kernels expect
+// them: descriptors current, after each state's pending work, live sides on
+// the batch's sides, fused densities primed.
+int prepare_run(cudapic_batch *b) {
     const uint32_t D = b->count();
     cudapic_state *s0 = b->states[0];
     const uint64_t steps0 = s0->steps_done;
@@ -423,6 +454,38 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
     }
     for (uint32_t k = 0; k < D; ++k)
         if (!b->states[k]->dens_valid) CUDAPIC_CHECK(state_prime_fused(b->states[k], b->stream));
+    return CUDAPIC_OK;
+}
+
+// The states' bookkeeping after steps [steps0, step) were enqueued; every
+// state's own stream continues after the batch's work.
+int finish_run(cudapic_batch *b, uint64_t steps0, uint64_t step) {
+    const uint32_t D = b->count();
+    const uint64_t done_steps = step - steps0;
+    for (uint32_t k = 0; k < D; ++k) {
+        cudapic_state *s = b->states[k];
+        s->side[0] = b->se;
+        s->side[1] = b->si;
+        s->e_cur = b->origin[k][0] ^ b->ecur;
+        s->i_cur = b->origin[k][1] ^ b->icur;
+        s->steps_done = step;
+        if (s->measure) s->measure_steps += done_steps;
+    }
+    CUDAPIC_CHECK(check_cuda(cudaEventRecord(b->done, b->stream), "batch: record"));
+    for (uint32_t k = 0; k < D; ++k)
+        CUDAPIC_CHECK(check_cuda(cudaStreamWaitEvent(b->states[k]->stream, b->done, 0), "batch: wait"));
+    return CUDAPIC_OK;
+}
+
+}  // namespace
+
+extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
+    if (!b) return fail(CUDAPIC_ERR_ARG, "batch_run_steps: null batch");
+    DeviceGuard dg(b->device);
+    CUDAPIC_CHECK(prepare_run(b));
+    cudapic_state *s0 = b->states[0];
+    const uint64_t steps0 = s0->steps_done;
+    const bool measure = s0->measure;
     const uint64_t period = 2ull * s0->params.n_sub;
     uint64_t step = steps0;
     int rc = CUDAPIC_OK;
@@ -450,19 +513,39 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
         }
     }
     // the states' bookkeeping follows what was enqueued
-    const uint64_t done_steps = step - steps0;
-    for (uint32_t k = 0; k < D; ++k) {
-        cudapic_state *s = b->states[k];
-        s->side[0] = b->se;
-        s->side[1] = b->si;
-        s->e_cur = b->origin[k][0] ^ b->ecur;
-        s->i_cur = b->origin[k][1] ^ b->icur;
-        s->steps_done = step;
-        if (s->measure) s->measure_steps += done_steps;
-    }
-    // every state's own stream continues after the batch's work
-    const int rc2 = check_cuda(cudaEventRecord(b->done, b->stream), "batch: record");
-    for (uint32_t k = 0; k < D && rc2 == CUDAPIC_OK; ++k)
-        CUDAPIC_CHECK(check_cuda(cudaStreamWaitEvent(b->states[k]->stream, b->done, 0), "batch: wait"));
+    const int rc2 = finish_run(b, steps0, step);
     return rc != CUDAPIC_OK ? rc : rc2;
+}
+
+extern "C" int cudapic_batch_profile_steps(cudapic_batch *b, uint64_t n_steps, double ms[CUDAPIC_BATCH_KERNELS],
+                                           uint64_t launches[CUDAPIC_BATCH_KERNELS]) {
+    if (!b) return fail(CUDAPIC_ERR_ARG, "batch_profile_steps: null batch");
+    CUDAPIC_REQUIRE(ms && launches, "batch_profile_steps: null pointer");
+    CUDAPIC_REQUIRE(n_steps <= 4096, "batch_profile_steps: at most 4096 steps per call");
+    DeviceGuard dg(b->device);
+    CUDAPIC_CHECK(prepare_run(b));
+    cudapic_state *s0 = b->states[0];
+    const uint64_t steps0 = s0->steps_done;
+    const bool measure = s0->measure;
+    uint64_t step = steps0;
+    BatchProfile prof;
+    int rc = CUDAPIC_OK;
+    for (; step < steps0 + n_steps && rc == CUDAPIC_OK; ++step)
+        rc = enqueue_batch_step(b, state_is_ion_step(s0, step), measure, &prof);
+    if (rc != CUDAPIC_OK) --step;  // the failed step was not (completely) enqueued
+    const int rc2 = finish_run(b, steps0, step);
+    CUDAPIC_CHECK(rc);
+    CUDAPIC_CHECK(rc2);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(b->stream), "batch profile: sync"));
+    for (int k = 0; k < CUDAPIC_BATCH_KERNELS; ++k) {
+        ms[k] = 0.0;
+        launches[k] = 0;
+    }
+    for (size_t j = 0; j < prof.kind.size(); ++j) {
+        float t = 0.0f;
+        CUDAPIC_CHECK(check_cuda(cudaEventElapsedTime(&t, prof.ev[2 * j], prof.ev[2 * j + 1]), "batch profile: time"));
+        ms[prof.kind[j]] += t;
+        launches[prof.kind[j]] += 1;
+    }
+    return CUDAPIC_OK;
 }

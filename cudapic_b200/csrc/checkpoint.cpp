@@ -89,8 +89,11 @@ extern "C" int cudapic_picdata_read_header(const char *path, double *time, uint3
     if (std::fseek(file.f, (long)(4ull * ne * sizeof(double)), SEEK_CUR) != 0)
         return fail(CUDAPIC_ERR_ARG, "picdata: truncated file");
     CUDAPIC_CHECK(read_count(file.f, &ni));
+    // eduPIC truncates the stored cycle count with int() (C/eduPIC.cc:767);
+    // a value that is no count at all (negative, NaN, 2^32 or more) is a malformed file
+    if (!(head[1] >= 0.0 && head[1] < 4294967296.0)) return fail(CUDAPIC_ERR_ARG, "picdata: bad cycle count");
     if (time) *time = head[0];
-    if (cycles_done) *cycles_done = head[1] >= 0.0 ? (uint32_t)head[1] : 0u;
+    if (cycles_done) *cycles_done = (uint32_t)head[1];
     if (n_e) *n_e = ne;
     if (n_i) *n_i = ni;
     return CUDAPIC_OK;

@@ -167,6 +167,10 @@ double cfl_max_energy(const cudapic_params &p);
 int rng_sidecar_write(const char *path, uint32_t capacity, const std::vector<uint32_t> planes[2][4]);
 int rng_sidecar_read(const char *path, uint32_t capacity, std::vector<uint32_t> planes[2][4]);
 
+// One CTA whose bounded mbarrier wait runs out after `limit` SM clocks and
+// sets CUDAPIC_DEVERR_TIMEOUT in dev_err (kernels_misc.cu).
+int launch_wait_timeout_probe(uint32_t *dev_err, long long limit, cudaStream_t stream);
+
 }  // namespace cudapic
 
 #define CUDAPIC_CHECK(expr)                                   \

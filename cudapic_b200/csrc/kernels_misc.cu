@@ -15,6 +15,7 @@
 #include "detmath.cuh"
 #include "internal.h"
 #include "rng.cuh"
+#include "tma.cuh"
 
 #include "generated/jump_tables.inc"
 
@@ -107,6 +108,30 @@ __global__ void math_eval_kernel(int fn, const float *__restrict__ in, const flo
     default: r = dm::atan2f_det(v, in2[i]); break;
     }
     out[i] = r;
+}
+
+// Self-test of the bounded waits: thread 0 arms an mbarrier for 16 bytes of
+// transfer that no copy will deliver, and every thread waits on it with a
+// limit of `limit` SM clocks.  The wait runs out and the CTA reports
+// CUDAPIC_DEVERR_TIMEOUT into dev_err, the route a stage wait of the
+// streaming kernels takes when a bulk copy does not complete.  No copy is
+// issued, so nothing is in flight when the kernel returns.
+__global__ void wait_timeout_probe_kernel(uint32_t *dev_err, long long limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16u);
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) set_dev_err(dev_err, CUDAPIC_DEVERR_TIMEOUT);
+}
+
+int launch_wait_timeout_probe(uint32_t *dev_err, long long limit, cudaStream_t stream) {
+    wait_timeout_probe_kernel<<<1, 64, 0, stream>>>(dev_err, limit);
+    return check_launch("wait_timeout_probe");
 }
 
 }  // namespace cudapic

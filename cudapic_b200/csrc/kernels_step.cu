@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(ES_THREADS)
                          uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                          const float *__restrict__ sigma_tot_e, const float *__restrict__ cs, float sigma_max,
                          float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive,
-                         const uint32_t *__restrict__ n_active, uint32_t *n_i, float *dens_e, float *dens_i,
+                         const uint32_t *n_active, uint32_t *n_i, float *dens_e, float *dens_i,
                          const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int stages, int copies,
                          uint32_t epoch, const StepLink link, cudapic_wall_counters *wall,
                          unsigned long long *coll) {
@@ -68,6 +68,8 @@ __global__ void __launch_bounds__(ES_THREADS)
     const StepSmem<U, true> sm(smem, stages, copies, ef_pad, offs, s_base, ccnt);
     step_smem_init(sm, stages, copies, ef_pad);
     grid_dep_wait();
+    // n_active may be link.dst (the no-alloc entry publishes the new count in
+    // place): it is read here, before this CTA takes its ticket, and never again
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
     // Balanced partition: CTA c owns the particles [beg, end), an equal share
     // (a multiple of 4, so every tile start stays 16-byte aligned) cut into

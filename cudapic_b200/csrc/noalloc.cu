@@ -14,13 +14,12 @@
 //
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds its 256 bytes until the process exits.  Host code cannot use
-// the array's name as a device address; the first call on each device looks
-// the address up with cudaGetSymbolAddress (with that device current) and
-// caches it.  Calls share the array, so two calls whose kernels overlap on
-// one GPU race on its counters.
+// the array's name as a device address; every call looks the address up with
+// cudaGetSymbolAddress in the calling thread's current context (a cheap
+// host-side lookup), so a context of the caller's own, or the module that a
+// cudaDeviceReset reloads, gets its own array's address.  Calls share the
+// array, so two calls whose kernels overlap on one GPU race on its counters.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "internal.h"
 
@@ -30,23 +29,12 @@ static __device__ __align__(256) uint32_t g_step_scratch[CUDAPIC_NOALLOC_SCRATCH
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-uint32_t *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_step_scratch on the current device (looked up once).
+// Device address of g_step_scratch in the current context.
 int scratch_address(uint32_t **out) {
-    int dev = -1;
-    CUDAPIC_CHECK(cudapic::check_cuda(cudaGetDevice(&dev), "step_electrons_noalloc: cudaGetDevice"));
-    if (dev < 0 || dev >= kMaxDevices) return cudapic::fail(CUDAPIC_ERR_NOT_SUPPORTED, "step_electrons_noalloc: device index");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        CUDAPIC_CHECK(cudapic::check_cuda(cudaGetSymbolAddress(&p, g_step_scratch),
-                                          "step_electrons_noalloc: cudaGetSymbolAddress"));
-        g_scratch_ptr[dev] = static_cast<uint32_t *>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void *p = nullptr;
+    CUDAPIC_CHECK(cudapic::check_cuda(cudaGetSymbolAddress(&p, g_step_scratch),
+                                      "step_electrons_noalloc: cudaGetSymbolAddress"));
+    *out = static_cast<uint32_t *>(p);
     return CUDAPIC_OK;
 }
 

@@ -28,6 +28,10 @@
 #include "internal.h"
 #include "state_impl.h"
 
+namespace {
+constexpr long long MBAR_PROBE_MAX_CYCLES = 1ll << 31;  // the streaming kernels' own limit
+}
+
 using namespace cudapic;
 
 namespace cudapic {
@@ -690,6 +694,20 @@ extern "C" int cudapic_state_device_error(cudapic_state *s, uint32_t *bits) {
         return fail(CUDAPIC_ERR_CAPACITY, "device reported a capacity overflow");
     if (*bits & CUDAPIC_DEVERR_TIMEOUT) return fail(CUDAPIC_ERR_TIMEOUT, "device reported a wait timeout");
     return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_clear_device_error(cudapic_state *s) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_clear_device_error: null state");
+    DeviceGuard dg(s->device);
+    return check_cuda(cudaMemsetAsync(s->dev_err(), 0, sizeof(uint32_t), s->stream), "clear device error word");
+}
+
+extern "C" int cudapic_state_debug_wait_timeout(cudapic_state *s, long long limit_cycles) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_debug_wait_timeout: null state");
+    CUDAPIC_REQUIRE(limit_cycles > 0 && limit_cycles <= MBAR_PROBE_MAX_CYCLES,
+                    "state_debug_wait_timeout: limit_cycles must be in [1, 2^31]");
+    DeviceGuard dg(s->device);
+    return launch_wait_timeout_probe(s->dev_err(), limit_cycles, s->stream);
 }
 
 extern "C" int cudapic_state_work(cudapic_state *s, unsigned long long *particle_steps) {

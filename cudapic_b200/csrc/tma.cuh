@@ -52,12 +52,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Bounded wait for phase `parity` of `bar`; false once `limit` SM clocks
+// have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  long long limit = MBAR_TIMEOUT_CYCLES) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > MBAR_TIMEOUT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
 }

@@ -74,9 +74,23 @@ def sample_profile(dens, dx, weight, area, mass, t_ev, rng):
     return x, v[0], v[1], v[2]
 
 
-def start_states(ref, mode, seeds=(1, 2), capacity=400_000):
+def start_particles(ref, seed, weight=7.0e4, gap=0.025, n_g=400, area=1.0e-4):
+    """The start of one seed: electrons, then ions, each (x, vx, vy, vz) f32,
+    sampled from the reference profiles with numpy's default_rng(seed).  The
+    same arrays start the GPU runs (start_states) and the eduPIC runs of
+    tests/golden/make_samestart.py."""
+    dx = gap / (n_g - 1)
+    rng = np.random.default_rng(seed)
+    d = ref["density"]
+    e = sample_profile(d[:, 1], dx, weight, area, E_MASS, 3.0, rng)
+    i = sample_profile(d[:, 2], dx, weight, area, AR_MASS, 0.03, rng)
+    return e, i
+
+
+def start_states(ref, mode, seeds=(1, 2), capacity=400_000, weight=7.0e4, options=None):
     """One state per seed at the reference parameters, particles from the
-    reference profiles, in the arithmetic of `mode`."""
+    reference profiles, in the arithmetic of `mode`.  options: driver
+    switches applied to every state (e.g. {"spawn_collide": True})."""
     import cudapic_b200 as cp
     from cudapic_b200.sim import GpuSimState, ParticlesSoA
     flags = 0
@@ -87,18 +101,16 @@ def start_states(ref, mode, seeds=(1, 2), capacity=400_000):
     states = []
     try:
         for seed in seeds:
-            p = cp.default_params(capacity=capacity, flags=flags)
+            p = cp.default_params(capacity=capacity, flags=flags, weight=weight)
             st = GpuSimState(p)
             states.append(st)
             if mode == "reference_f32":
                 st.set_fused(False)
-            dx = p.gap / (p.n_g - 1)
-            rng = np.random.default_rng(seed)
-            d = ref["density"]
-            st.upload_electrons(ParticlesSoA(*sample_profile(d[:, 1], dx, p.weight, p.electrode_area, E_MASS, 3.0,
-                                                             rng)))
-            st.upload_ions(ParticlesSoA(*sample_profile(d[:, 2], dx, p.weight, p.electrode_area, AR_MASS, 0.03,
-                                                        rng)))
+            for name, on in (options or {}).items():
+                getattr(st, "set_" + name)(on)
+            e, i = start_particles(ref, seed, p.weight, p.gap, p.n_g, p.electrode_area)
+            st.upload_electrons(ParticlesSoA(*e))
+            st.upload_ions(ParticlesSoA(*i))
             st.seed(e_master=(0x12345678 + seed, 0x11112222, 0x22223333, 0x33334444),
                     i_master=(0x44445555 + seed, 0x55556666, 0x66667777, 0x77778888))
     except Exception:

@@ -222,6 +222,9 @@ class GpuSimState:
             check(rc)
         return bits.value
 
+    def clear_device_error(self):
+        check(lib.cudapic_state_clear_device_error(self._h))
+
     def work(self):
         w = C.c_ulonglong()
         check(lib.cudapic_state_work(self._h, C.byref(w)))
@@ -276,6 +279,16 @@ class GpuBatch:
 
     def run_steps(self, n_steps):
         check(lib.cudapic_batch_run_steps(self._h, int(n_steps)))
+
+    BATCH_KERNELS = ("poisson", "ion_push", "electron_step", "ion_collisions")
+
+    def profile_steps(self, n_steps):
+        """Runs n_steps uncaptured with CUDA events around every kernel
+        (cudapic_batch_profile_steps); returns {kernel: (ms summed, launches)}."""
+        ms = (C.c_double * 4)()
+        n = (C.c_uint64 * 4)()
+        check(lib.cudapic_batch_profile_steps(self._h, int(n_steps), ms, n))
+        return {k: (ms[j], n[j]) for j, k in enumerate(self.BATCH_KERNELS)}
 
     def run_cycles(self, n_cycles):
         self.run_steps(int(n_cycles) * self.states[0].params.n_t)

@@ -11,10 +11,19 @@
 * ``sweep_params``    -- 256 seeded discharge parameter sets (voltage
   U(100, 500) V, pressure logU(5, 50) Pa, gap U(15, 40) mm, N_G in
   {200, 400, 800}, particles per species logU(1e4, 1e6)).
+* ``c2_specs`` / ``DischargeSpec`` / ``initial_population`` -- the batched
+  sweep's discharges and their seeded starting populations.
+
+Plain numpy: nothing here loads the CUDA library, so CPU-side tools (the
+eduPIC baseline runner, fixture scripts) can load this file on its own.
 """
 import math
+from dataclasses import dataclass
 
 import numpy as np
+
+DT_E_REFERENCE = 1.0 / 13.56e6 / 4000   # electron time step of the 13.56 MHz, N_T = 4000 discharges
+N_SUB = 20
 
 E_CHARGE = 1.60217662e-19
 E_MASS = 9.10938356e-31
@@ -66,3 +75,49 @@ def sweep_params(n_discharges=256, seed=0x5EED):
             "particles": int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6))))),
         })
     return out
+
+
+@dataclass
+class DischargeSpec:
+    """One discharge of a sweep (argon CCP, eduPIC physics)."""
+    voltage: float      # RF amplitude [V]
+    pressure: float     # [Pa]
+    gap: float          # electrode gap [m]
+    n_g: int            # grid points
+    particles: int      # initial electrons (and ions)
+    seed: int
+
+    @property
+    def weight(self):
+        """Superparticle weight of the reference steady state (7e4 at ~1.2e5
+        particles) scaled to the particle count."""
+        return 7.0e4 * 120000 / self.particles
+
+    def params(self, capacity_factor=2.0):
+        import cudapic_b200 as cp
+        cap = int(math.ceil(self.particles * capacity_factor / 4.0)) * 4
+        return cp.default_params(voltage=self.voltage, pressure=self.pressure, gap=self.gap, n_g=self.n_g,
+                                 capacity=cap, weight=self.weight)
+
+
+def c2_specs(n=256, seed=0x5EED):
+    """The C2 sweep: V ~ U(100, 500) V, p ~ logU(5, 50) Pa, L ~ U(15, 40) mm,
+    N_G in {200, 400, 800}, particles per species ~ logU(1e4, 1e6)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(n):
+        specs.append(DischargeSpec(
+            voltage=float(rng.uniform(100.0, 500.0)),
+            pressure=float(math.exp(rng.uniform(math.log(5.0), math.log(50.0)))),
+            gap=float(rng.uniform(0.015, 0.040)),
+            n_g=int(rng.choice([200, 400, 800])),
+            particles=int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6))))),
+            seed=int(seed) * 1000 + k))
+    return specs
+
+
+def initial_population(spec, dt_e=DT_E_REFERENCE, dt_i=N_SUB * DT_E_REFERENCE):
+    """Maxwellian electrons (3 eV) and ions (0.03 eV) uniform in the gap."""
+    e = steady_state(spec.particles, E_MASS, 3.0, gap=spec.gap, dt=dt_e, seed=spec.seed)
+    i = steady_state(spec.particles, AR_MASS, 0.03, gap=spec.gap, dt=dt_i, seed=spec.seed + 1)
+    return e, i

@@ -250,8 +250,11 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
  * CUDAPIC_NOALLOC_SCRATCH_BYTES (held by every GPU that loads the library
  * until exit), and the new electron count is written into *n_e in place.
  * The call allocates nothing; it clears the two counters on `stream` before
- * the launch.  The first call on a device looks up the array's address with
- * that device current; make it before any stream capture.  Every call shares
+ * the launch.  Every call looks up the array's address in the calling
+ * thread's current context (so a non-primary context, or the module that a
+ * cudaDeviceReset reloads, gets its own array); the first call on a device
+ * may load the library's module, so make it before any stream capture.
+ * Every call shares
  * the array: calls whose kernels overlap on one GPU race.  Rejects (with
  * CUDAPIC_ERR_ARG) a capacity above CUDAPIC_NOALLOC_MAX_CAPACITY, where the
  * shared 32-bit slot counter could wrap, besides the checks of
@@ -448,6 +451,17 @@ int cudapic_state_set_graphs(cudapic_state *s, int on);
 int cudapic_state_counts(cudapic_state *s, uint32_t *n_e, uint32_t *n_i);
 /* Reads and returns the device error word (synchronises). */
 int cudapic_state_device_error(cudapic_state *s, uint32_t *bits);
+/* Clears the state's device error word (on its stream), e.g. after a
+ * capacity overflow was handled by re-uploading the particles. */
+int cudapic_state_clear_device_error(cudapic_state *s);
+/* Self-test of the bounded device waits (no reference counterpart; the
+ * reference has no device-side error reporting): enqueues on the state's
+ * stream one CTA that arms an mbarrier for a transfer no copy delivers and
+ * waits on it for at most limit_cycles SM clocks (1 .. 2^31), so the wait
+ * runs out and CUDAPIC_DEVERR_TIMEOUT is set in the state's device error
+ * word; cudapic_state_device_error then returns CUDAPIC_ERR_TIMEOUT.  The
+ * context stays usable; the state's error word keeps the bit. */
+int cudapic_state_debug_wait_timeout(cudapic_state *s, long long limit_cycles);
 /* Particle-steps processed so far (electrons each step, ions each N_SUB). */
 int cudapic_state_work(cudapic_state *s, unsigned long long *particle_steps);
 int cudapic_state_steps_done(const cudapic_state *s, uint64_t *steps);
@@ -552,6 +566,18 @@ int cudapic_batch_destroy(cudapic_batch *b);
  * the batch.  Asynchronous. */
 int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps);
 int cudapic_batch_synchronize(cudapic_batch *b);
+/* Per-kernel device time of the batched step (no reference counterpart: a
+ * measurement aid).  Runs n_steps (<= 4096) like cudapic_batch_run_steps but
+ * uncaptured, with CUDA events around every kernel launch of a step, waits,
+ * and returns per kernel kind the summed milliseconds and launch counts.
+ * Programmatic dependent launch is off between the kernels of these steps. */
+#define CUDAPIC_BATCH_K_POISSON 0         /* batched Poisson (+ XT grid columns) */
+#define CUDAPIC_BATCH_K_ION_PUSH 1        /* ion push + compaction + deposit     */
+#define CUDAPIC_BATCH_K_ELECTRON_STEP 2   /* fused electron step                 */
+#define CUDAPIC_BATCH_K_ION_COLLISIONS 3  /* ion MCC                             */
+#define CUDAPIC_BATCH_KERNELS 4
+int cudapic_batch_profile_steps(cudapic_batch *b, uint64_t n_steps, double ms[CUDAPIC_BATCH_KERNELS],
+                                uint64_t launches[CUDAPIC_BATCH_KERNELS]);
 cudapic_stream_t cudapic_batch_stream(const cudapic_batch *b);
 
 /* ------------------------------------------------------- sensitivities

@@ -14,8 +14,9 @@
 #include <ctime>
 
 // Grid and time resolution size static arrays: compile-time.  Voltage, gap,
-// pressure and superparticle weight are read from the environment
-// (EDUPIC_VOLTAGE, EDUPIC_L, EDUPIC_PRESSURE, EDUPIC_WEIGHT) when set.
+// pressure, superparticle weight and the random seed are read from the
+// environment (EDUPIC_VOLTAGE, EDUPIC_L, EDUPIC_PRESSURE, EDUPIC_WEIGHT,
+// EDUPIC_SEED) when set.
 static inline double edupic_env(const char *name, double def) {
     const char *v = getenv(name);
     return v ? atof(v) : def;
@@ -45,8 +46,10 @@ static inline double edupic_env(const char *name, double def) {
 #ifndef EDUPIC_MAX_N_P
 #define EDUPIC_MAX_N_P 8388608
 #endif
+// Mersenne-Twister seed of the run (C/eduPIC.cc:165 seeds from
+// std::random_device): EDUPIC_SEED from the environment, default 5489.
 #ifndef EDUPIC_SEED
-#define EDUPIC_SEED 5489u
+#define EDUPIC_SEED ((unsigned)edupic_env("EDUPIC_SEED", 5489.0))
 #endif
 #ifndef EDUPIC_STEPS_PER_CYCLE
 #define EDUPIC_STEPS_PER_CYCLE N_T
@@ -64,7 +67,29 @@ static inline unsigned long long edupic_now_ns() {
     return (unsigned long long)ts.tv_sec * 1000000000ull + (unsigned long long)ts.tv_nsec;
 }
 
+// Start barrier of a group of processes timed together: with
+// EDUPIC_READY_FILE and EDUPIC_START_FILE set, the first time step (after the
+// cross sections are set up and picdata.bin is read) creates the ready file
+// and waits until the start file exists (at most ten minutes).
+static inline void edupic_start_barrier() {
+    const char *ready = getenv("EDUPIC_READY_FILE");
+    const char *start = getenv("EDUPIC_START_FILE");
+    if (!ready || !start) return;
+    if (FILE *f = fopen(ready, "w")) fclose(f);
+    const unsigned long long t0 = edupic_now_ns();
+    for (;;) {
+        if (FILE *f = fopen(start, "r")) {
+            fclose(f);
+            return;
+        }
+        if (edupic_now_ns() - t0 > 600ull * 1000000000ull) return;
+        struct timespec ts = {0, 200000};
+        nanosleep(&ts, nullptr);
+    }
+}
+
 static inline void edupic_hook_step(int t, int n_e, int n_i, int n_sub) {
+    if (edupic_steps_done == 0) edupic_start_barrier();
     if (edupic_steps_done % EDUPIC_MARK_EVERY == 0)
         fprintf(stderr, "EDUPIC_MARK %llu %llu %llu\n", edupic_steps_done, edupic_particle_steps,
                 edupic_now_ns());

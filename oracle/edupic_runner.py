@@ -4,21 +4,27 @@ oracle/_ref/ by oracle/Makefile) as the timed CPU baseline.
 Test and baseline infrastructure only: used by bench.py's CPU-baseline leg
 and its reference arm, never by the product.
 
-The workload is split into one independent eduPIC process per host core.
-Each process resumes from a picdata.bin holding its share of the particles
-(eduPIC's own checkpoint format, C/eduPIC.cc:726-781) with the
-superparticle weight scaled by the number of shares, so every process
-simulates the same discharge density as the whole population.  The
-benchmark builds count particle-steps with the GPU metric (every electron
-each step, every ion on steps t % N_SUB == 0) and print a timestamped mark
-every 40 steps; the aggregate throughput over a window of marks is
-sum(particle-steps) / (last end - first start) across processes.
+A workload is a list of jobs, one independent eduPIC process per host core.
+Each process resumes from a picdata.bin holding its particles (eduPIC's own
+checkpoint format, C/eduPIC.cc:726-781) with its own voltage, gap, pressure,
+superparticle weight and grid size.  The benchmark builds count
+particle-steps with the GPU metric (every electron each step, every ion on
+steps t % N_SUB == 0) and print a timestamped mark every 40 steps.
+
+run_window() times all processes over one common wall-clock window: every
+process sets itself up (cross sections, picdata.bin), reports ready and
+waits at a start barrier; once all are ready they start together, run
+through a warm-up and the window, and are stopped after it.  Each process's
+particle-steps inside the window are read from its marks (linear between
+two marks), so the aggregate is the work all cores did while all of them
+were busy, divided by the window.
 """
 import os
 import re
 import shutil
 import subprocess
 import tempfile
+import time
 
 import numpy as np
 
@@ -62,68 +68,83 @@ def write_picdata(path, electrons, ions, time=0.0, cycles_done=1):
             np.asarray(a, np.float64).tofile(f)
 
 
-def run(shares, weight, n_marks, n_g=400, env=None, timeout=900):
-    """Starts one eduPIC process per share and waits for all.
+def _work_at(marks, t_ns):
+    """Particle-steps a process had done at time t_ns (linear between marks)."""
+    for (s0, w0, a), (s1, w1, b) in zip(marks, marks[1:]):
+        if a <= t_ns <= b:
+            return w0 + (w1 - w0) * (t_ns - a) / max(1, b - a)
+    raise RuntimeError("eduPIC marks do not cover the timing window")
 
-    shares: list of (electrons, ions), each a tuple of 4 arrays (x, vx, vy, vz).
-    n_marks: number of 40-step benchmark steps each process runs.
-    Returns one list of marks (steps, particle_steps, t_ns) per process.
+
+def run_window(jobs, warm_s, window_s, timeout=900):
+    """Times `jobs` as concurrent eduPIC processes over a common window.
+
+    jobs: list of dicts with "electrons", "ions" (tuples of x, vx, vy, vz),
+    "weight", "n_g" and optional "env" (EDUPIC_VOLTAGE, EDUPIC_L,
+    EDUPIC_PRESSURE, ...) and "marks" (40-step marks the process may run;
+    it is stopped once the window has passed).
+    Returns (aggregate particle-steps/s, per-job particle-steps/s, window
+    seconds, per-job particle-steps in the window).
     """
-    exe = binary(n_g)
-    base_env = dict(os.environ)
-    base_env["EDUPIC_WEIGHT"] = repr(float(weight))
-    if env:
-        base_env.update({k: str(v) for k, v in env.items()})
     tmp = tempfile.mkdtemp(prefix="edupic_")
+    start_file = os.path.join(tmp, "start")
     procs = []
     try:
-        for k, (e, i) in enumerate(shares):
+        for k, job in enumerate(jobs):
             d = os.path.join(tmp, "p%d" % k)
             os.makedirs(d)
-            write_picdata(os.path.join(d, "picdata.bin"), e, i)
+            write_picdata(os.path.join(d, "picdata.bin"), job["electrons"], job["ions"])
+            env = dict(os.environ)
+            env.update({kk: str(v) for kk, v in (job.get("env") or {}).items()})
+            env["EDUPIC_WEIGHT"] = repr(float(job["weight"]))
+            env["EDUPIC_READY_FILE"] = os.path.join(d, "ready")
+            env["EDUPIC_START_FILE"] = start_file
             err = open(os.path.join(d, "stderr.txt"), "w")
-            p = subprocess.Popen([exe, str(n_marks)], cwd=d, env=base_env, stdout=subprocess.DEVNULL, stderr=err)
+            p = subprocess.Popen([binary(job["n_g"]), str(int(job.get("marks", 100000)))], cwd=d, env=env,
+                                 stdout=subprocess.DEVNULL, stderr=err)
             procs.append((p, err, d))
-        marks = []
+        deadline = time.monotonic() + timeout
+        while not all(os.path.exists(os.path.join(d, "ready")) for _, _, d in procs):
+            if time.monotonic() > deadline or any(p.poll() is not None for p, _, _ in procs):
+                raise RuntimeError("eduPIC processes did not reach the start barrier")
+            time.sleep(0.01)
+        t_start = time.monotonic_ns()   # CLOCK_MONOTONIC, the clock of the marks
+        with open(start_file, "w"):
+            pass
+        a = t_start + int(warm_s * 1e9)
+        b = a + int(window_s * 1e9)
+        # stop once every process has printed a mark after the window
+        while True:
+            time.sleep(0.05)
+            if time.monotonic_ns() > b + int(1e9 * max(5.0, 0.5 * window_s)):
+                break
+            done = True
+            for p, _, d in procs:
+                text = open(os.path.join(d, "stderr.txt")).read()
+                m = _MARK.findall(text)
+                if p.poll() is None and (not m or int(m[-1][2]) < b):
+                    done = False
+                    break
+            if done:
+                break
+        for p, _, _ in procs:
+            if p.poll() is None:
+                p.kill()
+        per_job, rates = [], []
         for p, err, d in procs:
-            rc = p.wait(timeout=timeout)
+            p.wait(timeout=30)
             err.close()
-            if rc != 0:
-                raise RuntimeError("eduPIC exited with %d" % rc)
             text = open(os.path.join(d, "stderr.txt")).read()
-            marks.append([(int(a), int(b), int(c)) for a, b, c in _MARK.findall(text)])
-        return marks
+            marks = [(int(x), int(y), int(z)) for x, y, z in _MARK.findall(text)]
+            w = _work_at(marks, b) - _work_at(marks, a)
+            per_job.append(w)
+            rates.append(w / window_s)
+        return sum(per_job) / window_s, rates, window_s, per_job
     finally:
         for p, err, _ in procs:
             if p.poll() is None:
                 p.kill()
+                p.wait()
+            if not err.closed:
+                err.close()
         shutil.rmtree(tmp, ignore_errors=True)
-
-
-def window_throughput(marks, first, last):
-    """Aggregate particle-steps/s between marks `first` and `last` (indices of
-    40-step marks) over all processes, and the per-mark wall times (s)."""
-    total = 0
-    t0 = min(m[first][2] for m in marks)
-    t1 = max(m[last][2] for m in marks)
-    for m in marks:
-        total += m[last][1] - m[first][1]
-    per_step = []
-    for k in range(first, last):
-        a = min(m[k][2] for m in marks)
-        b = max(m[k + 1][2] for m in marks)
-        per_step.append((b - a) * 1e-9)
-    return total / ((t1 - t0) * 1e-9), total, (t1 - t0) * 1e-9, per_step
-
-
-def split_population(electrons, ions, shares, per_share_cap=None, seed=0):
-    """Deals particles round-robin into `shares` parts (optionally capped)."""
-    out = []
-    for k in range(shares):
-        e = tuple(np.asarray(a[k::shares]) for a in electrons)
-        i = tuple(np.asarray(a[k::shares]) for a in ions)
-        if per_share_cap:
-            e = tuple(a[:per_share_cap] for a in e)
-            i = tuple(a[:per_share_cap] for a in i)
-        out.append((e, i))
-    return out

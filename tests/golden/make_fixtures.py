@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures of tests/golden/ from the reference tree.
 
-Run in a container that has the reference checkout (default /root/reference,
-override with CUDAPIC_REFERENCE):
+Run where the reference checkout is present (CUDAPIC_REFERENCE, default a
+sibling of this repository named "reference"):
 
     python tests/golden/make_fixtures.py
 
@@ -35,7 +35,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 ORACLE = os.path.join(ROOT, "oracle")
-REF = os.environ.get("CUDAPIC_REFERENCE", "/root/reference")
+REF = os.environ.get("CUDAPIC_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def main():

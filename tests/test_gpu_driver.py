@@ -290,3 +290,36 @@ def test_c1_population_steps_without_device_errors(cudapic, cuda_device):
     assert 0.9 * n < ne <= n * 1.01 and 0.95 * n < ni <= n * 1.01
     assert st.device_error() == 0
     st.close()
+
+
+def test_bounded_wait_timeout_reaches_host(cudapic, cuda_device):
+    """A bounded mbarrier wait that runs out (a transfer that no copy ever
+    delivers, limit 4000 SM clocks) reports CUDAPIC_DEVERR_TIMEOUT in the
+    state's device error word, which the host reads as CUDAPIC_ERR_TIMEOUT;
+    the context and the state stay usable."""
+    import ctypes as C
+    st = _c0_state(cudapic)
+    st.run_steps(3)
+    assert st.device_error() == 0
+    cudapic.check(cudapic.lib.cudapic_state_debug_wait_timeout(st.handle, C.c_longlong(4000)))
+    bits = C.c_uint32()
+    rc = cudapic.lib.cudapic_state_device_error(st.handle, C.byref(bits))
+    assert rc == cudapic._lib.ERR_TIMEOUT
+    assert bits.value & cudapic.DEVERR_TIMEOUT
+    with pytest.raises(cudapic.CudapicError) as ex:
+        st.device_error(raise_on_error=True)
+    assert ex.value.status == cudapic._lib.ERR_TIMEOUT
+    n0 = st.steps_done()
+    st.run_steps(5)  # the stream still runs
+    assert st.steps_done() == n0 + 5
+    assert st.counts()[0] > 0
+    st.close()
+
+
+def test_bounded_wait_limit_is_checked(cudapic, cuda_device):
+    import ctypes as C
+    st = _c0_state(cudapic)
+    for bad in (0, -1, (1 << 31) + 1):
+        assert cudapic.lib.cudapic_state_debug_wait_timeout(st.handle, C.c_longlong(bad)) == cudapic._lib.ERR_ARG
+    assert st.device_error() == 0
+    st.close()

@@ -5,8 +5,9 @@ buffers), so the kernel's slot counter and completion ticket live in a
 static device array of the library and the new count is written into n_e.
 
 Two calls in a row, each against cudapic_step_electrons on the same inputs:
-the second call finds the static array as the first one left it, so it also
-shows that the counters are cleared between calls.  The file name makes
+the second call runs on the static array as the first one left it (the
+kernel's last CTA resets both counters itself, and the entry point also
+clears them on the stream before every launch).  The file name makes
 pytest collect it last, so a run that stops at the first failure has run
 every other test before it."""
 import numpy as np
