@@ -93,6 +93,8 @@ def parse():
                     help="c2: discharges also timed one at a time for the plain comparisons (0: all of them)")
     ap.add_argument("--cpu-step-s", type=float, default=1.0,
                     help="seconds of all-core eduPIC work per reference step")
+    ap.add_argument("--no-inplace", dest="inplace", action="store_false",
+                    help="c1/c2: every electron step compacts (no in-place steps between)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-breakdown", action="store_true")
     a = ap.parse_args()
@@ -373,6 +375,7 @@ ALGO_BYTES = {  # algorithmic bytes per particle per launch
     "check_collisions_e": 44,    # read v (12) + RNG (16), write RNG (16); colliders' v writes not counted
     "check_collisions_i": 44,
     "step_electrons": 64,        # read x, v, RNG (32); write x, v, RNG of survivors (32)
+    "step_electrons_inplace": 56,  # read x, v, RNG (32); write x, vx, RNG in place (24)
 }
 
 
@@ -455,6 +458,22 @@ def kernel_breakdown(st, K, reps, flush):
         n_i_c.fill_(n_i)
         dens.zero_()
     timed("step_electrons", step_e, n_e, 64, pre=reset_step)
+    # the in-place step's two passes (on the live planes: each launch advances them by one step)
+    lst = torch.zeros(g.capacity, dtype=torch.int32, device="cuda")
+    cnt, ticket = dev_u32(0), dev_u32(0)
+
+    def stream_pass():
+        K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e,
+                                 b.sigma_max_e, ne_c, lst, cnt, dens, g, stream=stream.cuda_stream)
+
+    def scatter_pass():
+        K.scatter_colliders_e(b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.cs, lst, cnt, ticket, b.x[1], b.vx[1],
+                              b.vy[1], b.vz[1], ne_c, n_i_c, dens, dens_i, g, stream=stream.cuda_stream)
+    timed("step_electrons_inplace", stream_pass, n_e, 56, pre=lambda: (cnt.zero_(), dens.zero_()))
+    n_coll = int(cnt.item())
+    timed("scatter_colliders_e", scatter_pass, n_coll, 0,
+          pre=lambda: (cnt.zero_(), ne_c.fill_(n_e), n_i_c.fill_(n_i), stream_pass()))
+    res["scatter_colliders_e"]["colliders_per_step"] = n_coll
     timed("check_collisions_i", lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                              *b.rng[1], g, stream=stream.cuda_stream), n_i, 44)
     return res
@@ -470,6 +489,7 @@ def run_one_discharge(args):
     n = args.particles
     params = cp.default_params(n_g=args.n_g, capacity=2 * n, weight=7.0e4 * 120000 / n)
     st = GpuSimState(params, device=local)
+    st.set_inplace(args.inplace)
     stream = torch.cuda.Stream()
     st.set_stream(stream)
     (e, i) = population(args, rank)
@@ -499,8 +519,10 @@ def run_one_discharge(args):
     elapsed_max, work_sum = reduce_max_sum(world, elapsed, work)
     value = work_sum / elapsed_max
     ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
-    # fused driver: Poisson and the fused electron step every step; ion push and MCC on ion steps
-    launches = args.steps * (STEP * 2 + ion_steps * 2)
+    # fused driver: Poisson every step; the electron step (in place: stream + scatter pass, two launches;
+    # compacting: one) every step; ion push and MCC on ion steps
+    compacting = STEP // 20 if args.inplace else STEP
+    launches = args.steps * (STEP + compacting + 2 * (STEP - compacting) + ion_steps * 2)
 
     # ---------------- end to end through the C ABI with host buffers
     pinned = {}
@@ -552,8 +574,12 @@ def run_one_discharge(args):
         breakdown = kernel_breakdown(st, cp.kernels, reps=7, flush=L2Flusher())
         # launches of each kernel in one bench step of the fused driver (the plain
         # get_density / move_and_compact / check_collisions_e lines are for comparison)
-        share_w = {"solve_poisson": STEP, "step_electrons": STEP, "move_and_compact_deposit_i": ion_steps,
+        # the driver's schedule: in place except the step before every N_SUB-th one
+        compacting = STEP // 20 if args.inplace else STEP
+        share_w = {"solve_poisson": STEP, "step_electrons": compacting, "move_and_compact_deposit_i": ion_steps,
                    "check_collisions_i": ion_steps}
+        if args.inplace:
+            share_w.update({"step_electrons_inplace": STEP - compacting, "scatter_colliders_e": STEP - compacting})
         tot = sum(breakdown[k]["us"] * w for k, w in share_w.items())
         for k in breakdown:
             breakdown[k]["share"] = breakdown[k]["us"] * share_w.get(k, 0) / tot
@@ -619,6 +645,8 @@ def run_batched(args):
     specs = c2_specs(n=args.discharges)
     mine = [specs[k] for k in shard(specs, world)[rank]]
     batch = Batch(mine, device=local, capacity_factor=args.capacity_factor)
+    for st in batch.states:
+        st.set_inplace(args.inplace)
     flagged = set()
 
     def note_errors():
@@ -633,8 +661,15 @@ def run_batched(args):
     defaults = cp.get_tuning()
     tuned, _ = tune_batch(batch) if args.tune else (None, None)
 
+    # the initial populations in pinned host memory: every reset below and the
+    # end-to-end phase upload them from there
+    pinned = []
+    for st, spec in zip(batch.states, mine):
+        e, i = initial_population(spec, st.grid.dt_e, st.grid.dt_i)
+        pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*e, *i)])
+
     # 2. device-timed: from the initial populations, W warm-up steps, K timed
-    batch.reset()
+    batch.reset(pinned=pinned)
     batch.run_steps(STEP * args.warmup)
     batch.synchronize()
     barrier(world)
@@ -647,10 +682,6 @@ def run_batched(args):
 
     # 3. end to end through the public API: every discharge re-uploaded from
     #    pinned host memory, the steps, every discharge's counts read back
-    pinned = []
-    for st, spec in zip(batch.states, mine):
-        e, i = initial_population(spec, st.grid.dt_e, st.grid.dt_i)
-        pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*e, *i)])
     h2d = 16 * sum(2 * p[0].numel() for p in pinned)
     barrier(world)
     batch.synchronize()
@@ -677,7 +708,8 @@ def run_batched(args):
                 continue
             us = 1e3 * ms / n
             d = {"us": us, "launches": int(n), "share": None}
-            per = {"electron_step": (64, n_e_mean), "ion_push": (32, n_i_mean), "ion_collisions": (44, n_i_mean)}
+            per = {"electron_step": (64, n_e_mean), "electron_inplace": (56, n_e_mean), "ion_push": (32, n_i_mean),
+                   "ion_collisions": (44, n_i_mean)}
             if k in per:
                 b, cnt = per[k]
                 d.update({"bytes_per_particle": b, "n": cnt, "algo_bytes": b * cnt, "gbs": b * cnt / (us * 1e3)})
@@ -713,7 +745,7 @@ def run_batched(args):
             st = batch.states[k]
             for mode in ("plain", "fused"):
                 on = mode == "fused"
-                batch.reset_one(k)
+                batch.reset_one(k, pinned[k])
                 st.set_fused(on)
                 st.set_graphs(on)
                 st.set_overlap(on)
@@ -756,13 +788,18 @@ def run_batched(args):
     peak, peak_kind = measured_peaks()
     ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
     roofline = None
-    if breakdown and "electron_step" in breakdown:
-        d = breakdown["electron_step"]
-        roofline = {"bound": "hbm", "kernel": "batch_step_kernel<MCC> (fused electron step of all discharges)",
-                    "achieved": d["gbs"], "peak": peak, "unit": "GB/s", "frac": d["gbs"] / peak,
-                    "traffic": ncu_traffic("batch_electron_step", d["n"]), "peak_source": peak_kind,
-                    "algo_bytes_per_particle": 64,
-                    "aggregate_gbs": 64.0 * work_sum / elapsed_max / 1e9}
+    if breakdown:
+        dom = max((k for k in breakdown if "gbs" in breakdown[k]), key=lambda k: breakdown[k]["share"])
+        d = breakdown[dom]
+        names = {"electron_inplace": ("batch_inplace_kernel (in-place electron step of all discharges, stream pass)",
+                                      "batch_electron_inplace"),
+                 "electron_step": ("batch_step_kernel<MCC> (compacting fused electron step of all discharges)",
+                                   "batch_electron_step")}
+        label, key = names.get(dom, (dom, dom))
+        roofline = {"bound": "hbm", "kernel": label, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
+                    "frac": d["gbs"] / peak, "traffic": ncu_traffic(key, d["n"]), "peak_source": peak_kind,
+                    "algo_bytes_per_particle": d["bytes_per_particle"],
+                    "aggregate_gbs_64B": 64.0 * work_sum / elapsed_max / 1e9}
     cfg = workload_config(args)
     cfg.update({"precision": "f32 particles and push, 2^-20 fixed-point deposits summed exactly in 64-bit integers, "
                              "FP64 Poisson scans and time averages",
@@ -783,7 +820,8 @@ def run_batched(args):
                 "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_max},
         "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu,
         "stated_error": STATED_ERROR, "clocks": clk.summary(),
-        "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2),
+        "gpu_launches": args.steps * (STEP + (STEP // 20) + 2 * (STEP - STEP // 20) + ion_steps * 2
+                                      if args.inplace else STEP * 2 + ion_steps * 2),
         "discharges_counted": n_clean if world == 1 else None,
         "discharges_excluded": len(flagged_all),
         "excluded_why": "device error word set in some phase (spawns beyond the capacity of %.1fx the initial "

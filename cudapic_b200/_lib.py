@@ -69,7 +69,7 @@ class Tuning(C.Structure):
     _fields_ = [(name, C.c_int) for name in (
         "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
         "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant", "step_stages",
-        "step_ctas_per_sm", "step_rows")]
+        "step_ctas_per_sm", "step_rows", "inplace_ctas_per_sm", "inplace_copies")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -154,6 +154,8 @@ SIGNATURES = {
     "cudapic_state_load": [_VP, C.c_char_p],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],
+    "cudapic_step_electrons_inplace": [_VP] * 10 + [_F] + [_VP] * 4 + [_GP, _VP],
+    "cudapic_scatter_colliders_e": [_VP] * 20 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
     "cudapic_accumulate_density": [_VP, _VP, _GP, _VP],
     "cudapic_accumulate_eepf": [_VP] * 7 + [_GP, _VP],
@@ -175,6 +177,8 @@ SIGNATURES = {
     "cudapic_state_seed": [_VP, C.POINTER(_U32), C.POINTER(_U32)],
     "cudapic_state_set_measure": [_VP, C.c_int],
     "cudapic_state_set_fused": [_VP, C.c_int],
+    "cudapic_state_set_inplace": [_VP, C.c_int],
+    "cudapic_state_set_spawn_collide": [_VP, C.c_int],
     "cudapic_state_set_overlap": [_VP, C.c_int],
     "cudapic_state_set_graphs": [_VP, C.c_int],
     "cudapic_state_run_steps": [_VP, C.c_uint64],

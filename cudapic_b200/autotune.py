@@ -134,11 +134,16 @@ def tune(st, reps=5, verbose=True):
     return best, results
 
 
-# Launch shapes of the batched particle kernels (kernels_batch.cu): rows per
-# thread and tile, bulk-copy stages, resident CTAs per SM and deposit
-# histogram copies.
-BATCH_CANDIDATES = [dict(step_rows=r, step_stages=st_, step_ctas_per_sm=c, density_copies=k)
-                    for r, st_, c, k in itertools.product((1, 2, 4), (2, 4), (2, 3), (4, 8))]
+# Launch shapes of the batched particle kernels (kernels_batch.cu): the
+# in-place electron step's resident CTAs per SM and histogram copies (it runs
+# all but one step in N_SUB), and the compacting step's rows per thread and
+# resident CTAs per SM.
+BATCH_CANDIDATES = [dict(inplace_ctas_per_sm=ic, inplace_copies=ik, step_rows=r, step_stages=2, step_ctas_per_sm=c,
+                         density_copies=4)
+                    for ic, ik, (r, c) in itertools.product((3, 4), (4, 8), ((4, 2), (2, 3)))]
+# the same sweep with every electron step compacting (no in-place steps)
+BATCH_CANDIDATES_COMPACTING = [dict(step_rows=r, step_stages=st_, step_ctas_per_sm=c, density_copies=k)
+                               for r, st_, c, k in itertools.product((1, 2, 4), (2, 4), (2, 3), (4, 8))]
 
 
 def tune_batch(batch, candidates=None, rounds=2, verbose=False):
@@ -148,7 +153,9 @@ def tune_batch(batch, candidates=None, rounds=2, verbose=False):
     `rounds` interleaved passes; keeps and returns the shape with the best
     median particle-steps/s: (best dict, {shape: [rates]})."""
     import cudapic_b200 as cp
-    cands = list(candidates or BATCH_CANDIDATES)
+    if candidates is None:
+        candidates = BATCH_CANDIDATES if batch.batch.inplace else BATCH_CANDIDATES_COMPACTING
+    cands = list(candidates)
     period = 2 * batch.states[0].params.n_sub
     rates = {}
     for _ in range(rounds):

@@ -25,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I", ROOT, "-Xcompiler", "-fPIC,-ff
           "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "--expt-relaxed-constexpr"]
 
 SOURCES = ["host.cpp", "state.cpp", "batch.cpp", "checkpoint.cpp", "report.cpp", "kernels_density.cu",
-           "kernels_poisson.cu", "kernels_push.cu", "kernels_mcc.cu", "kernels_step.cu", "kernels_batch.cu",
+           "kernels_poisson.cu", "kernels_push.cu", "kernels_mcc.cu", "kernels_step.cu", "kernels_inplace.cu", "kernels_batch.cu",
            "kernels_misc.cu", "kernels_xt.cu", "xt.cpp", "noalloc.cu", "sensitivity.cu", "fp64.cu"]
 
 

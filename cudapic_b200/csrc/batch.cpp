@@ -39,7 +39,8 @@ struct cudapic_batch {
     std::vector<cudaEvent_t> ready;  // per state: its stream's work before a run
     cudaEvent_t done = nullptr;
     BatchDisc *desc = nullptr;
-    uint32_t *counts = nullptr;      // [2][D] written by the batched Poisson solve
+    uint32_t *counts = nullptr;      // [2][D] written by the batched Poisson solve; [2D]: scatter ticket
+    bool inplace = true;             // in-place electron steps between compacting ones (all states in-place)
     float *pool = nullptr;           // POOL_PLANES x pool_len elements
     uint64_t pool_len = 0;
     std::vector<uint32_t> off;       // element offset of each discharge
@@ -239,8 +240,12 @@ struct BatchProfile {
     }
 };
 
+// As in the one-discharge driver: the electron step before every N_SUB-th
+// step compacts (and the last step of every run), the others run in place.
+bool batch_compact_step(const cudapic_state *s0, uint64_t step) { return ((step + 1) % s0->params.n_sub) == 0; }
+
 // One step of every discharge (the order of state.cpp's fused step).
-int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, BatchProfile *prof = nullptr) {
+int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, bool compact, BatchProfile *prof = nullptr) {
     PdlScope pdl(prof == nullptr);  // the profiler's events sit between the kernels
     const uint32_t D = b->count();
     cudaStream_t st = b->stream;
@@ -270,11 +275,26 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, BatchProfi
         b->si ^= 1;
     }
     r.dens = b->ecur ^ 1;
-    CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_STEP));
-    CUDAPIC_CHECK(launch_batch_step(true, step_planes(b, 0, b->se, b->si), b->desc, b->counts, D, b->cap_sum,
-                                    b->max_n_g, r, st));
-    CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_STEP));
-    b->se ^= 1;
+    if (b->inplace && !compact) {
+        // in place: the electrons stay on their side, colliders are listed
+        // in the other side's x plane, the scatter pass follows
+        const SidePlanes es = side_planes(b, 0, b->se);
+        const InplacePlanes pl{es.x, es.vx, es.vy, es.vz, es.rng0, es.rng1, es.rng2, es.rng3};
+        uint32_t *list = reinterpret_cast<uint32_t *>(b->plane(pool_plane(0, b->se ^ 1, 0)));
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_INPLACE));
+        CUDAPIC_CHECK(launch_batch_inplace(pl, list, b->desc, b->counts, D, b->cap_sum, b->max_n_g, r, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_INPLACE));
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_SCATTER));
+        CUDAPIC_CHECK(launch_batch_scatter(pl, list, side_planes(b, 1, b->si), b->desc, D, b->cap_sum, r,
+                                           b->counts + 2 * D, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_SCATTER));
+    } else {
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_STEP));
+        CUDAPIC_CHECK(launch_batch_step(true, step_planes(b, 0, b->se, b->si), b->desc, b->counts, D, b->cap_sum,
+                                        b->max_n_g, r, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_STEP));
+        b->se ^= 1;
+    }
     b->ecur ^= 1;
     if (ion_step) {
         CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ION_COLLISIONS));
@@ -294,7 +314,8 @@ int build_graph(cudapic_batch *b, uint64_t first_step, bool measure) {
     CUDAPIC_CHECK(check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
     int rc = CUDAPIC_OK;
     for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k)
-        rc = enqueue_batch_step(b, state_is_ion_step(s0, first_step + k), measure);
+        rc = enqueue_batch_step(b, state_is_ion_step(s0, first_step + k), measure,
+                                batch_compact_step(s0, first_step + k) || k + 1 == period);
     cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
     // 2 N_SUB steps return every role to its start
     b->se = roles0[0];
@@ -360,7 +381,8 @@ extern "C" int cudapic_batch_create(cudapic_state *const *states, uint32_t count
     if ((rc = check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch: stream")) ||
         (rc = check_cuda(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch: event")) ||
         (rc = check_cuda(cudaMalloc(&b->desc, count * sizeof(BatchDisc)), "batch: descriptors")) ||
-        (rc = check_cuda(cudaMalloc(&b->counts, 2ull * count * sizeof(uint32_t)), "batch: counts")) ||
+        (rc = check_cuda(cudaMalloc(&b->counts, (2ull * count + 8) * sizeof(uint32_t)), "batch: counts")) ||
+        (rc = check_cuda(cudaMemset(b->counts, 0, (2ull * count + 8) * sizeof(uint32_t)), "batch: counts")) ||
         (rc = check_cuda(cudaMalloc(&b->pool, (size_t)POOL_PLANES * pool_len * sizeof(float)), "batch: pool")))
         return cleanup(rc);
     b->ready.assign(count, nullptr);
@@ -421,14 +443,20 @@ int prepare_run(cudapic_batch *b) {
     const uint64_t steps0 = s0->steps_done;
     const bool measure = s0->measure;
     bool stale = !b->built;
+    bool inplace = true;
     for (uint32_t k = 0; k < D; ++k) {
         const cudapic_state *s = b->states[k];
+        inplace = inplace && s->inplace;
         CUDAPIC_REQUIRE(s->steps_done == steps0, "batch_run_steps: the states are at different steps");
         CUDAPIC_REQUIRE(s->measure == measure, "batch_run_steps: the states differ in measurement mode");
         CUDAPIC_REQUIRE(s->fused, "batch_run_steps: a state is in unfused (reference sequence) mode");
         if (b->built && (s->e_cur != (b->origin[k][0] ^ b->ecur) || s->i_cur != (b->origin[k][1] ^ b->icur) ||
                          s->xt != b->xt_at_build[k]))
             stale = true;
+    }
+    if (inplace != b->inplace) {
+        b->inplace = inplace;
+        destroy_graphs(b);
     }
     if (stale) CUDAPIC_CHECK(build(b));
     // after every state's pending work (uploads, seeding, its own steps)
@@ -506,7 +534,8 @@ extern "C" int cudapic_batch_run_steps(cudapic_batch *b, uint64_t n_steps) {
             }
             continue;
         }
-        rc = enqueue_batch_step(b, state_is_ion_step(s0, step), measure);
+        rc = enqueue_batch_step(b, state_is_ion_step(s0, step), measure,
+                                batch_compact_step(s0, step) || n_steps == 1);
         if (rc == CUDAPIC_OK) {
             step += 1;
             n_steps -= 1;
@@ -531,7 +560,8 @@ extern "C" int cudapic_batch_profile_steps(cudapic_batch *b, uint64_t n_steps, d
     BatchProfile prof;
     int rc = CUDAPIC_OK;
     for (; step < steps0 + n_steps && rc == CUDAPIC_OK; ++step)
-        rc = enqueue_batch_step(b, state_is_ion_step(s0, step), measure, &prof);
+        rc = enqueue_batch_step(b, state_is_ion_step(s0, step), measure,
+                                batch_compact_step(s0, step) || step + 1 == steps0 + n_steps, &prof);
     if (rc != CUDAPIC_OK) --step;  // the failed step was not (completely) enqueued
     const int rc2 = finish_run(b, steps0, step);
     CUDAPIC_CHECK(rc);

@@ -49,6 +49,11 @@ __device__ __forceinline__ int cell_of(float pos, uint32_t n_g) {
     return p;
 }
 
+// A slot that an in-place electron step emptied (inplace.cuh): its electron
+// left through an electrode and x holds a negative marker.  Live positions
+// are in [0, L]; kernels that read electron slots skip dead ones.
+__device__ __forceinline__ bool slot_dead(float x) { return x < 0.0f; }
+
 __device__ __forceinline__ bool pos_in_range(float pos, uint32_t n_g) {
     return pos >= 0.0f && pos <= (float)(n_g - 1);
 }

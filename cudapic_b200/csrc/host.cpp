@@ -70,7 +70,8 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*density_threads*/ 512, /*density_ctas_per_sm*/ 4, /*density_copies*/ 4, /*density_cluster*/ 4,
     /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1,
-    /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2};
+    /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2,
+    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
 uint64_t g_tuning_gen = 0;  // advanced by every cudapic_set_tuning
@@ -216,6 +217,8 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
     if (!v.step_stages) v.step_stages = d.step_stages;
     if (!v.step_ctas_per_sm) v.step_ctas_per_sm = d.step_ctas_per_sm;
     if (!v.step_rows) v.step_rows = d.step_rows;
+    if (!v.inplace_ctas_per_sm) v.inplace_ctas_per_sm = d.inplace_ctas_per_sm;
+    if (!v.inplace_copies) v.inplace_copies = d.inplace_copies;
     const bool ok = (v.density_threads == 256 || v.density_threads == 512 || v.density_threads == 1024) &&
                     v.density_ctas_per_sm >= 1 && v.density_ctas_per_sm <= 8 && v.density_copies >= 1 &&
                     v.density_copies <= 32 &&
@@ -225,7 +228,8 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     v.mcc_stages >= 2 && v.mcc_stages <= 4 && v.mcc_ctas_per_sm >= 1 && v.mcc_ctas_per_sm <= 8 &&
                     (v.mcc_variant == 1 || v.mcc_variant == 2) && v.step_stages >= 2 && v.step_stages <= 6 &&
                     v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 &&
-                    (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4);
+                    (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4) && v.inplace_ctas_per_sm >= 1 &&
+                    v.inplace_ctas_per_sm <= 8 && v.inplace_copies >= 1 && v.inplace_copies <= 8;
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuning = v;

@@ -1,0 +1,243 @@
+// inplace.cuh -- the in-place electron step, shared by the one-discharge
+// kernels (kernels_inplace.cu) and the batched ones (kernels_batch.cu).
+//
+// The compacting fused step (step.cuh) writes every survivor into the other
+// side, so each tile needs a block-wide scan and barrier before its stores.
+// The in-place step keeps every electron in its slot instead:
+//  * stream pass (inplace_segment): four consecutive slots per thread and
+//    round, read with 16-byte loads from the eight SoA planes (x, vx, vy, vz,
+//    rng0..3); push (Rust-CUDA/src/main.rs:596-620), electrode absorption,
+//    collision test (:992-1012, the certain-rejection bound of step.cuh
+//    first), CIC deposit of the new position into the next density
+//    (push.cuh, 2^-20 fixed point); x, vx and the RNG state go back to the
+//    same slots (vy, vz do not change in the push: 24 B written per electron
+//    against 32 B read).  An absorbed electron leaves its slot with
+//    x = DEAD_X; later passes skip it.  Colliders are appended, by slot, to
+//    a collider list (per-warp queues in shared memory, one atomicAdd per
+//    32 entries);
+//  * scatter pass (inplace_scatter): every listed collider continues its
+//    RNG stream past the test draw and is scattered in place
+//    (collision_e, :1035-1165); spawned electrons are appended after the
+//    live slots, spawned ions to the ion side.
+// No block barrier orders the stores, and the only per-tile cost of the
+// compaction is gone.  The holes are closed by the compacting step, which
+// the drivers run every N_SUB steps and as the last step of every run, so
+// the particle planes are compact whenever a caller can see them.
+// Every electron draws from the RNG stream of the slot it occupies, in the
+// reference's order (test draw, then the scattering draws), as in the
+// compacting fused step.
+#pragma once
+#include "step.cuh"
+
+namespace cudapic {
+
+constexpr float DEAD_X = -1.0f;     // x of a slot whose electron left through an electrode
+constexpr int IP_THREADS = 256;
+constexpr int IP_WARPS = IP_THREADS / 32;
+constexpr int IP_ROW = 4;           // slots per thread and round (one 16-byte load per plane)
+constexpr int IP_ROUND = IP_THREADS * IP_ROW;
+constexpr int IP_QCAP = 32 + 32 * IP_ROW;  // per-warp collider queue: < 32 left over + one round
+
+
+// Dynamic shared memory of the stream pass: E[ef_pad] f32, the 64-bit
+// deposit accumulator [ef_pad], [copies][ef_pad] fixed-point histograms,
+// [IP_WARPS][IP_QCAP] collider queues.
+__host__ __device__ constexpr size_t inplace_smem_bytes(int copies, uint32_t ef_pad) {
+    return (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 + (size_t)IP_WARPS * IP_QCAP * 4;
+}
+
+struct InplaceSmem {
+    float *ef;
+    unsigned long long *acc;
+    uint32_t *hist;
+    uint32_t *queue;
+    __device__ __forceinline__ InplaceSmem(unsigned char *smem, int copies, uint32_t ef_pad) {
+        ef = reinterpret_cast<float *>(smem);
+        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);
+        hist = reinterpret_cast<uint32_t *>(acc + ef_pad);
+        queue = hist + (uint32_t)copies * ef_pad;
+    }
+    __device__ __forceinline__ unsigned char *end() const {
+        return reinterpret_cast<unsigned char *>(queue + IP_WARPS * IP_QCAP);
+    }
+};
+
+__device__ __forceinline__ void inplace_smem_init(const InplaceSmem &sm, int copies, uint32_t ef_pad) {
+    for (uint32_t k = threadIdx.x; k < (uint32_t)copies * ef_pad; k += IP_THREADS) sm.hist[k] = 0u;
+    for (uint32_t k = threadIdx.x; k < ef_pad; k += IP_THREADS) sm.acc[k] = 0ull;
+}
+
+// Moves whole groups of 32 queued colliders of the calling warp to the
+// list (one atomicAdd per call), or all of them with `all`; the rest move
+// to the front of the queue.  Every lane calls it with the same qn.
+__device__ __forceinline__ void flush_colliders(uint32_t *q, uint32_t &qn, bool all, uint32_t *list,
+                                                uint32_t *count, uint32_t capacity, uint32_t *dev_err) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = all ? qn : (qn & ~31u);
+    if (n == 0) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t k = lane; k < n; k += 32) {
+        // the list has one entry per slot: it cannot hold more than `capacity`
+        if (base + k < capacity) list[base + k] = q[k];
+        else set_dev_err(dev_err, CUDAPIC_DEVERR_SPAWN_E);
+    }
+    __syncwarp();
+    const uint32_t rest = qn - n;
+    const uint32_t v = lane < (int)rest ? q[n + lane] : 0u;
+    __syncwarp();
+    if (lane < (int)rest) q[lane] = v;
+    __syncwarp();
+    qn = rest;
+}
+
+// The stream pass over slots [beg, end) (discharge-local, beg a multiple of
+// 4) of one discharge whose planes start at element `off`.  Every thread of
+// the CTA calls it with the same arguments; on entry the histograms and the
+// accumulator are zero and the queues empty, and so they are on return (the
+// deposits flushed into dc.dens, the colliders into `list` / `count`).  The
+// live electrons processed are added to `live` (per thread).
+// SH: dc lives in shared memory; WALL: compile the electrode counters in.
+template <bool SH, bool WALL>
+__device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const StepDisc &dc, const cudapic_grid &g,
+                                                const cudapic_grid &gm, uint32_t off, uint32_t beg, uint32_t end,
+                                                const InplaceSmem &sm, int copies, uint32_t ef_pad, uint32_t epoch,
+                                                uint32_t *list, uint32_t *count, uint32_t &live) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const unsigned lt = lanemask_lt();
+    const float factor = dc.factor, dt = dc.dt, sigma_max = dc.sigma_max;
+    const float rej_k2 = sigma_max * dt * (sigma_max * dt) * 1.0001f;  // may_collide's bound
+    const float inv_dx = g.inv_dx, gap = g.gap;
+    const uint32_t n_g = g.n_g;
+    for (uint32_t k = tid; k < n_g; k += IP_THREADS) sm.ef[k] = dcp<SH>(dc.efield)[k];
+    uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
+    uint32_t *q = sm.queue + warp * IP_QCAP;
+    uint32_t qn = 0;
+    __syncthreads();
+    const uint32_t rounds = (end - beg + IP_ROUND - 1) / IP_ROUND;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        if (r != 0 && r % epoch == 0) {  // drain the deposit copies before they can overflow
+            __syncthreads();
+            dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
+            __syncthreads();
+        }
+        const uint32_t s0 = beg + (r * IP_THREADS + (uint32_t)tid) * IP_ROW;  // first slot of this thread
+        const bool any = s0 < end;
+        const uint32_t i0 = off + s0;
+        float4 X = make_float4(0.f, 0.f, 0.f, 0.f), VX = X, VY = X, VZ = X;
+        uint4 R0 = make_uint4(0u, 0u, 0u, 0u), R1 = R0, R2 = R0, R3 = R0;
+        if (any) {
+            X = *reinterpret_cast<const float4 *>(pl.x + i0);
+            VX = *reinterpret_cast<const float4 *>(pl.vx + i0);
+            VY = *reinterpret_cast<const float4 *>(pl.vy + i0);
+            VZ = *reinterpret_cast<const float4 *>(pl.vz + i0);
+            R0 = *reinterpret_cast<const uint4 *>(pl.rng0 + i0);
+            R1 = *reinterpret_cast<const uint4 *>(pl.rng1 + i0);
+            R2 = *reinterpret_cast<const uint4 *>(pl.rng2 + i0);
+            R3 = *reinterpret_cast<const uint4 *>(pl.rng3 + i0);
+        }
+        float x[IP_ROW] = {X.x, X.y, X.z, X.w};
+        float vx[IP_ROW] = {VX.x, VX.y, VX.z, VX.w};
+        const float vy[IP_ROW] = {VY.x, VY.y, VY.z, VY.w};
+        const float vz[IP_ROW] = {VZ.x, VZ.y, VZ.z, VZ.w};
+        uint32_t s[4][IP_ROW] = {{R0.x, R0.y, R0.z, R0.w}, {R1.x, R1.y, R1.z, R1.w}, {R2.x, R2.y, R2.z, R2.w},
+                                 {R3.x, R3.y, R3.z, R3.w}};
+        uint32_t kept = 0, may = 0, coll = 0;  // bit u: slot s0 + u survives / may collide / collides
+        // (1) push; dead and past-the-end slots push a harmless stand-in and are masked
+#pragma unroll
+        for (int u = 0; u < IP_ROW; ++u) {
+            const bool valid = s0 + (uint32_t)u < end && !slot_dead(x[u]);
+            const PushResult pr = push_one_c(valid ? x[u] : 0.5f * gap, valid ? vx[u] : 0.0f, sm.ef, factor, dt,
+                                             inv_dx, n_g, gap, gm);
+            if (WALL) {
+                cudapic_wall_counters *wall = dcp<SH>(dc.wall);
+                if (wall) count_wall(wall, false, valid && !pr.keep, pr.x, 0.0f, 0.0f, 0.0f, gap);
+            }
+            if (valid) {
+                ++live;
+                if (pr.keep) {
+                    kept |= 1u << u;
+                    x[u] = pr.x;
+                    vx[u] = pr.vx;
+                } else {
+                    x[u] = DEAD_X;
+                }
+            }
+        }
+        // (2) the collision test's draw and the certain rejection, which needs no table
+#pragma unroll
+        for (int u = 0; u < IP_ROW; ++u) {
+            if (kept >> u & 1u) {
+                Xoshiro128p rs{s[0][u], s[1][u], s[2][u], s[3][u]};
+                const float v2 = vx[u] * vx[u] + vy[u] * vy[u] + vz[u] * vz[u];
+                const float rnd = rs.uniform();
+                if (may_collide(rnd, v2, rej_k2)) {
+                    // (3) the exact test where the bound cannot decide (a few per cent)
+                    const float velocity = sqrtf(v2);
+                    const uint32_t idx = energy_index(gm.half_me_over_e * v2);
+                    if (collision_draw(rnd, __ldg(dcp<SH>(dc.sigma_tot) + idx) * velocity * dt)) coll |= 1u << u;
+                    may |= 1u << u;
+                }
+                s[0][u] = rs.s0;
+                s[1][u] = rs.s1;
+                s[2][u] = rs.s2;
+                s[3][u] = rs.s3;
+                dep_add(h, x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            }
+        }
+        if (any) {
+            *reinterpret_cast<float4 *>(pl.x + i0) = make_float4(x[0], x[1], x[2], x[3]);
+            *reinterpret_cast<float4 *>(pl.vx + i0) = make_float4(vx[0], vx[1], vx[2], vx[3]);
+            *reinterpret_cast<uint4 *>(pl.rng0 + i0) = make_uint4(s[0][0], s[0][1], s[0][2], s[0][3]);
+            *reinterpret_cast<uint4 *>(pl.rng1 + i0) = make_uint4(s[1][0], s[1][1], s[1][2], s[1][3]);
+            *reinterpret_cast<uint4 *>(pl.rng2 + i0) = make_uint4(s[2][0], s[2][1], s[2][2], s[2][3]);
+            *reinterpret_cast<uint4 *>(pl.rng3 + i0) = make_uint4(s[3][0], s[3][1], s[3][2], s[3][3]);
+        }
+        // (4) queue this round's colliders (warp-synchronous)
+        const unsigned wc = __ballot_sync(0xffffffffu, coll != 0);
+        if (wc) {
+#pragma unroll
+            for (int u = 0; u < IP_ROW; ++u) {
+                const bool c = coll >> u & 1u;
+                const unsigned cm = __ballot_sync(0xffffffffu, c);
+                if (c) q[qn + __popc(cm & lt)] = s0 + (uint32_t)u;
+                qn += __popc(cm);
+            }
+            __syncwarp();
+            if (qn >= 32) flush_colliders(q, qn, false, list, count, g.capacity, gm.dev_err);
+        }
+        (void)may;
+    }
+    flush_colliders(q, qn, true, list, count, g.capacity, gm.dev_err);
+    __syncthreads();
+    dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
+    __syncthreads();
+    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);
+    for (uint32_t k = tid; k < n_g; k += IP_THREADS) sm.acc[k] = 0ull;
+}
+
+// The scatter pass for one listed collider at discharge-local slot i: its
+// RNG stream continues past the test draw (collision_e,
+// Rust-CUDA/src/main.rs:1035-1165, with the fused step's algebraic sines
+// and cosines); velocity and RNG state go back in place, a spawned electron
+// takes the next slot of n_e, a spawned ion the next slot of n_i.
+__device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, float *ix, float *ivx, float *ivy, float *ivz,
+                                                uint32_t off, uint32_t i, const float *cs, uint32_t *n_e,
+                                                uint32_t *n_i, const cudapic_grid &g, float *dens_e, float *dens_i) {
+    const uint32_t k = off + i;
+    const float vxi = pl.vx[k], vyi = pl.vy[k], vzi = pl.vz[k];
+    Xoshiro128p rs{pl.rng0[k], pl.rng1[k], pl.rng2[k], pl.rng3[k]};
+    const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
+    const uint32_t idx = energy_index(g.half_me_over_e * v2);
+    collide_electron_t<true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, ix, ivx, ivy, ivz, n_e,
+                             n_i, g, dens_e, dens_i);
+    pl.rng0[k] = rs.s0;
+    pl.rng1[k] = rs.s1;
+    pl.rng2[k] = rs.s2;
+    pl.rng3[k] = rs.s3;
+}
+
+}  // namespace cudapic

@@ -77,7 +77,6 @@ __global__ void __launch_bounds__(ES_THREADS)
     const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 3u) & ~3u;
     const uint32_t beg = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, beg + chunk);
-    if (g.work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(g.work, (unsigned long long)n);
     StepPlanes pl;
     pl.sx = sx;
     pl.svx = svx;
@@ -108,8 +107,9 @@ __global__ void __launch_bounds__(ES_THREADS)
     dc.dens_i = dens_i;
     dc.wall = wall;
     dc.coll = coll;
-    uint32_t it = 0;
-    step_segment<U, true, false, true>(pl, dc, g, g, 0u, beg, end, sm, stages, copies, ef_pad, epoch, it);
+    uint32_t it = 0, live = 0;
+    step_segment<U, true, false, true>(pl, dc, g, g, 0u, beg, end, sm, stages, copies, ef_pad, epoch, it, live);
+    add_work(g.work, live);
     publish_count(link.ticket, link.dst, link.src, link.clear_src, g.capacity);
 }
 

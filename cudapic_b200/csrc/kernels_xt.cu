@@ -49,6 +49,7 @@ __device__ __forceinline__ void xt_accumulate(const float *__restrict__ x, const
     const float half_m = ION ? HALF_MI_OVER_E : g.half_me_over_e;
     const float rate_scale = (float)((double)g.dt_e * g.gas_density);
     for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        if (slot_dead(x[i])) continue;  // emptied by an in-place electron step
         const float pos = x[i] * g.inv_dx;
         const int p = cell_of(pos, n_g);
         const float c2 = pos - (float)p;

@@ -25,6 +25,7 @@
 #include <new>
 #include <vector>
 
+#include "batch_internal.h"
 #include "internal.h"
 #include "state_impl.h"
 
@@ -104,13 +105,18 @@ void destroy_graphs(cudapic_state *s) {
     }
 }
 
-// Particle part of a fused-mode step: [ion push] -> fused electron step ->
+// Particle part of a fused-mode step: [ion push] -> electron step ->
 // [ion collisions] -> [measurement]; the kernels publish the particle counts
 // themselves (StepLink), so the step holds no copy or memset node.  The
-// electrons draw from the RNG stream of their source slot (kernels_step.cu).
-// Returns CUDAPIC_ERR_NOT_SUPPORTED, having enqueued nothing, when the
-// electron planes are not aligned for the fused kernel.
-int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, float *i_acc) {
+// electron step is the compacting fused kernel (kernels_step.cu) when
+// `compact` or when the in-place step is off, else the in-place stream and
+// scatter passes (kernels_inplace.cu: electrons stay in their slots,
+// absorbed ones are marked dead, colliders listed in the other side's x
+// plane).  Either way an electron draws from the RNG stream of the slot it
+// occupies when the step starts.  Returns CUDAPIC_ERR_NOT_SUPPORTED, having
+// enqueued nothing, when the electron planes are not aligned for the fused
+// kernels.
+int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, float *i_acc, bool compact) {
     const cudapic_grid &g = s->grid;
     cudaStream_t st = s->stream;
     const int E = 0, I = 1;
@@ -131,19 +137,35 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
         si ^= 1;
         s->side[I] = si;
     }
-    StepLink le;
-    le.ticket = s->ticket();
-    le.dst = s->n_e();
-    le.src = s->alive();
-    le.clear_src = 1;
-    CUDAPIC_CHECK(launch_electron_step(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
-                                       s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
-                                       s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3], s->sigma_tot_e, s->cs,
-                                       s->sigma_max_e, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
-                                       s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le,
-                                       s->measure ? s->wall : nullptr, s->measure ? s->mcount : nullptr));
-    se ^= 1;
-    s->side[E] = se;
+    if (s->inplace && !compact) {
+        const InplacePlanes pl{s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
+                               s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3]};
+        uint32_t *list = reinterpret_cast<uint32_t *>(s->x[E][se ^ 1]);  // the other side is free until compaction
+        CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->sigma_max_e, s->n_e(), list,
+                                              s->counters + CTR_COLL_COUNT, e_next, g, st,
+                                              s->measure ? s->wall : nullptr, s->counters + CTR_SPAWN_FROM));
+        CUDAPIC_CHECK(launch_electron_scatter(pl, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si], s->cs, list,
+                                              s->counters + CTR_COLL_COUNT, s->counters + CTR_COLL_TICKET, s->n_e(),
+                                              s->n_i(), g, st, e_next, i_acc, s->measure ? s->mcount : nullptr));
+        if (s->spawn_collide)
+            CUDAPIC_CHECK(launch_spawn_collide(pl, s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si],
+                                               s->sigma_tot_e, s->cs, s->counters + CTR_SPAWN_FROM, s->n_e(), s->n_i(),
+                                               g, st, e_next, i_acc, s->measure ? s->mcount : nullptr));
+    } else {
+        StepLink le;
+        le.ticket = s->ticket();
+        le.dst = s->n_e();
+        le.src = s->alive();
+        le.clear_src = 1;
+        CUDAPIC_CHECK(launch_electron_step(s->efield, s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
+                                           s->x[E][se ^ 1], s->vx[E][se ^ 1], s->vy[E][se ^ 1], s->vz[E][se ^ 1],
+                                           s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3], s->sigma_tot_e,
+                                           s->cs, s->sigma_max_e, s->x[I][si], s->vx[I][si], s->vy[I][si],
+                                           s->vz[I][si], s->alive(), s->n_e(), s->n_i(), e_next, i_acc, g, st, le,
+                                           s->measure ? s->wall : nullptr, s->measure ? s->mcount : nullptr));
+        se ^= 1;
+        s->side[E] = se;
+    }
     s->e_cur ^= 1;
     if (ion_step) {
         CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
@@ -157,8 +179,9 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
     return CUDAPIC_OK;
 }
 
-// One reference time step (Rust-CUDA/src/main.rs:1728-1807).
-int enqueue_step(cudapic_state *s, bool ion_step) {
+// One reference time step (Rust-CUDA/src/main.rs:1728-1807).  compact: a
+// fused-mode step that closes the holes of earlier in-place steps.
+int enqueue_step(cudapic_state *s, bool ion_step, bool compact) {
     PdlScope pdl(s->overlap);
     const cudapic_grid &g = s->grid;
     cudaStream_t st = s->stream;
@@ -209,7 +232,7 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
         }
     }
     if (fused) {
-        const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc);
+        const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc, compact);
         if (rc != CUDAPIC_ERR_NOT_SUPPORTED) return rc;  // else: buffers not aligned for the fused kernel
     }
     // electrons: push + compact into the other side
@@ -256,6 +279,11 @@ int enqueue_step(cudapic_state *s, bool ion_step) {
 
 bool is_ion_step(const cudapic_state *s, uint64_t step) { return state_is_ion_step(s, step); }
 
+// In-place mode: the electron planes are compacted by the step before every
+// N_SUB-th step (the last step of each half of a graph period) and by the
+// last step of every run, so they are compact whenever a caller sees them.
+bool is_compact_step(const cudapic_state *s, uint64_t step) { return ((step + 1) % s->params.n_sub) == 0; }
+
 // Graph period: 2 * N_SUB steps returns both species to their starting
 // side; requires N_T % N_SUB == 0 so that the ion-step pattern repeats.
 uint64_t graph_period(const cudapic_state *s) { return 2ull * s->params.n_sub; }
@@ -269,7 +297,9 @@ int build_graph(cudapic_state *s) {
     const int cur0[2] = {s->e_cur, s->i_cur};
     CUDAPIC_CHECK(check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
     int rc = CUDAPIC_OK;
-    for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k) rc = enqueue_step(s, is_ion_step(s, s->steps_done + k));
+    for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k)
+        rc = enqueue_step(s, is_ion_step(s, s->steps_done + k),
+                          is_compact_step(s, s->steps_done + k) || k + 1 == period);
     cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     // a graph of 2 N_SUB steps returns every ping-pong role to its start
     s->side[0] = side0[0];
@@ -605,6 +635,24 @@ extern "C" int cudapic_state_set_fused(cudapic_state *s, int on) {
     return CUDAPIC_OK;
 }
 
+extern "C" int cudapic_state_set_inplace(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_inplace: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_inplace sync"));
+    s->inplace = on != 0;
+    destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
+extern "C" int cudapic_state_set_spawn_collide(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_spawn_collide: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_spawn_collide sync"));
+    s->spawn_collide = on != 0;
+    destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
 extern "C" int cudapic_state_set_graphs(cudapic_state *s, int on) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_graphs: null state");
     DeviceGuard dg(s->device);
@@ -665,7 +713,8 @@ extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
             n_steps -= period;
             continue;
         }
-        CUDAPIC_CHECK(enqueue_step(s, is_ion_step(s, s->steps_done)));
+        CUDAPIC_CHECK(enqueue_step(s, is_ion_step(s, s->steps_done),
+                                   is_compact_step(s, s->steps_done) || n_steps == 1));
         s->steps_done += 1;
         if (s->measure) s->measure_steps += 1;
         n_steps -= 1;

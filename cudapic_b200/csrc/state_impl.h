@@ -20,7 +20,8 @@ struct cudapic_state {
     float *x[2][2] = {}, *vx[2][2] = {}, *vy[2][2] = {}, *vz[2][2] = {};
     int side[2] = {0, 0};
     uint32_t *rng[2][4] = {};
-    // counters block: n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work (u64 at +32)
+    // counters block: n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work (u64 at +32),
+    // [12] in-place step's collider count, [13] its scatter ticket, [14] its first spawn slot
     uint32_t *counters = nullptr;
     float *efield = nullptr, *pot = nullptr, *pot0_table = nullptr;
     // Charge densities, double-buffered for the fused step: [cur] feeds the
@@ -30,6 +31,8 @@ struct cudapic_state {
     int e_cur = 0, i_cur = 0;
     bool fused = true;        // deposit inside push / collisions (default)
     bool overlap = true;      // programmatic dependent launch between the step's kernels (default)
+    bool inplace = true;      // fused mode: in-place electron steps between compacting ones (default)
+    bool spawn_collide = false;  // in-place steps: new electrons also collide in their birth step (eduPIC)
     bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;

@@ -136,6 +136,13 @@ __device__ __forceinline__ bool may_collide(float u, float v2, float k2) {
     return !(y >= 0.0f && y * y >= k2 * v2);
 }
 
+// Adds the CTA's per-thread counts v to *work (may be null): one atomic per warp.
+__device__ __forceinline__ void add_work(unsigned long long *work, uint32_t v) {
+    if (!work) return;
+    const uint32_t s = __reduce_add_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(work, (unsigned long long)s);
+}
+
 // Initialises the stage mbarriers (thread 0) and clears the deposit
 // accumulators; the caller synchronises before the first segment.
 template <int U, bool MCC>
@@ -161,11 +168,13 @@ __device__ __forceinline__ void step_smem_init(const StepSmem<U, MCC> &sm, int s
 // scattering routine.
 // SH: dc lives in shared memory; WALL: compile the electrode counters in
 // (dc.wall may still be null at run time).
+// live: incremented by every particle of [beg, end) that is pushed (slots
+// emptied by an in-place step are skipped: not pushed, not kept, not counted).
 template <int U, bool MCC, bool SH, bool WALL>
 __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDisc &dc, const cudapic_grid &g,
                                              const cudapic_grid &gm, uint32_t off, uint32_t beg, uint32_t end,
                                              const StepSmem<U, MCC> &sm, int stages, int copies, uint32_t ef_pad,
-                                             uint32_t epoch, uint32_t &it) {
+                                             uint32_t epoch, uint32_t &it, uint32_t &live) {
     using S = StepShape<U, MCC>;
     constexpr int TILE = S::TILE;
     constexpr int PLANES = S::PLANES;
@@ -273,7 +282,8 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t j = (uint32_t)u * ES_THREADS + tid;
-            const bool valid = j < cnt;
+            const bool valid = j < cnt && !slot_dead(__uint_as_float(b[j]));
+            live += valid ? 1u : 0u;
             const float x0 = valid ? __uint_as_float(b[j]) : 0.5f * gap;
             const float v0 = valid ? __uint_as_float(b[TILE + j]) : 0.0f;
             const PushResult pr = push_one_c(x0, v0, sm.ef, factor, dt, inv_dx, n_g, gap, gm);

@@ -6,7 +6,8 @@ L2 flushed before each launch): the target of the committed ncu captures.
 Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
 check_collisions_e, check_collisions_e_deposit, check_collisions_i and
 step_electrons (the *_deposit variants also deposit the next step's density;
-step_electrons is the fused driver's electron kernel).  Prints one JSON line with the median time, the particle
+step_electrons is the fused driver's compacting electron kernel,
+step_electrons_inplace the stream pass of its in-place step).  Prints one JSON line with the median time, the particle
 count and the algorithmic bytes per launch.
 """
 import argparse
@@ -14,7 +15,8 @@ import json
 import statistics
 
 BYTES = {"get_density": 4, "move_and_compact": 32, "move_and_compact_deposit": 32, "check_collisions_e": 44,
-         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0, "step_electrons": 64}
+         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0, "step_electrons": 64,
+         "step_electrons_inplace": 56}
 
 
 def main():
@@ -48,6 +50,8 @@ def main():
     pot = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
     ef = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
     alive = u32(0)
+    clist = torch.zeros(g.capacity, dtype=torch.int32, device="cuda")
+    ccount = u32(0)
     fns = {
         "get_density": (lambda: K.get_density(b.x[0], dens, ne_c, g, stream=s), lambda: dens.zero_(), n_e),
         "solve_poisson": (lambda: K.solve_poisson_scan_f32(b.e_density, b.i_density, pot, ef, 250.0, g, stream=s),
@@ -72,6 +76,10 @@ def main():
             stream=s), lambda: (alive.zero_(), alive_i.fill_(n_i), dens.zero_()), n_e),
         "check_collisions_i": (lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                             *b.rng[1], g, stream=s), None, n_i),
+        # the in-place step's stream pass (each launch advances the live planes by one step)
+        "step_electrons_inplace": (lambda: K.step_electrons_inplace(
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.sigma_max_e, ne_c, clist, ccount,
+            dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()), n_e),
     }
     fn, pre, n = fns[a.kernel]
     from cudapic_b200.timing import L2Flusher, time_launch

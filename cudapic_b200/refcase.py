@@ -120,11 +120,12 @@ def start_states(ref, mode, seeds=(1, 2), capacity=400_000, weight=7.0e4, option
     return states
 
 
-def run(states, relax, measure):
+def run(states, relax, measure, batched=True):
     """relax cycles, then a measurement window of `measure` cycles; fused
-    states step together in one batch, others one after another."""
+    states step together in one batch (unless batched is False), others one
+    after another."""
     from cudapic_b200.sim import GpuBatch
-    if all(st.fused for st in states):
+    if batched and all(st.fused for st in states):
         with GpuBatch(states) as b:
             b.run_cycles(relax)
             b.synchronize()
@@ -179,6 +180,59 @@ def compare(got, ref):
     return errors, spread
 
 
+def load_samestart(directory, tag="ss", seeds=(1, 2, 3, 4)):
+    """eduPIC's outputs of runs from the same starts as start_states
+    (tests/golden/make_samestart.py), one dict per seed, shaped like
+    outputs(): n_e, n_i, potential, EEPF, <j E> power and the final electron
+    count."""
+    out = []
+    for s in seeds:
+        base = os.path.join(directory, "edupic_%s_s%d" % (tag, s))
+        dens = np.loadtxt(base + "_density.txt")
+        eepf = np.loadtxt(base + "_eepf.txt")
+        xt = np.loadtxt(base + "_xt_means.txt")
+        conv = np.loadtxt(base + "_conv.txt")
+        out.append({"ne": dens[:, 1], "ni": dens[:, 2], "pot": xt[:, 0], "eepf": eepf[:, 1],
+                    "power_e": float(xt[:, 4].mean()), "count_e": float(conv[-1, 1])})
+    return out
+
+
+def compare_samples(got, want):
+    """Two independent samples of runs (seeds) from the same starts: per
+    quantity, the relative L2 norm (relative difference for the scalars) of
+    the difference of the seed means, and its noise -- the same norm of the
+    standard error of that difference from the seeds' variances.  Profiles
+    are compared over all nodes, the EEPF below EEPF_BAND_EV."""
+    band = (np.arange(len(want[0]["eepf"])) + 0.5) * DE_EEPF < EEPF_BAND_EV
+    diff, noise = {}, {}
+    for key in ("ne", "ni", "pot", "eepf", "power_e", "count_e"):
+        G = np.array([g[key] for g in got], np.float64)
+        W = np.array([w[key] for w in want], np.float64)
+        d = G.mean(axis=0) - W.mean(axis=0)
+        se2 = G.var(axis=0, ddof=1) / len(G) + W.var(axis=0, ddof=1) / len(W)
+        ref = W.mean(axis=0)
+        if key in ("power_e", "count_e"):
+            diff[key] = float(abs(d) / abs(ref))
+            noise[key] = float(np.sqrt(se2) / abs(ref))
+        else:
+            sel = band if key == "eepf" else slice(None)
+            diff[key] = float(np.linalg.norm(d[sel]) / np.linalg.norm(ref[sel]))
+            noise[key] = float(np.sqrt(se2[sel].sum()) / np.linalg.norm(ref[sel]))
+    return diff, noise
+
+
+def samestart(ref, directory, mode="mixed", tag="ss", seeds=(1, 2, 3, 4), relax=300, measure=100, weight=7.0e4,
+              options=None):
+    """This library's runs against eduPIC's runs from the same starts."""
+    got = mode_outputs(ref, mode, relax, measure, seeds, weight=weight, options=options)
+    want = load_samestart(directory, tag, seeds)
+    diff, noise = compare_samples(got, want)
+    return {"mode": mode, "options": options or {}, "tag": tag, "seeds": list(seeds), "relax_cycles": relax,
+            "measured_cycles": measure, "weight": weight, "difference": diff, "noise": noise,
+            "device_errors": [g["device_error"] for g in got],
+            "gpu_count_e": [g["count_e"] for g in got], "edupic_count_e": [w["count_e"] for w in want]}
+
+
 def run_fp64(twins, relax, measure):
     """relax, then measure, cycles of all-FP64 twins (each on its state's
     stream, side by side)."""
@@ -199,10 +253,13 @@ def outputs_fp64(tw):
             "count_e": float(m["counts"][0]), "device_error": m["device_error"]}
 
 
-def mode_outputs(ref, mode, relax=300, measure=100, seeds=(1, 2)):
-    """Per seed, the outputs of one arithmetic mode (normalised as eduPIC's)."""
+def mode_outputs(ref, mode, relax=300, measure=100, seeds=(1, 2), weight=7.0e4, options=None, capacity=None):
+    """Per seed, the outputs of one arithmetic mode (normalised as eduPIC's).
+    options: driver switches (e.g. {"spawn_collide": True}); states with
+    switches the batch driver does not take run one after another."""
     from .fp64 import Fp64Discharge
-    states = start_states(ref, mode, seeds)
+    cap = capacity or int(400_000 * 7.0e4 / weight)
+    states = start_states(ref, mode, seeds, capacity=cap, weight=weight, options=options)
     twins = []
     try:
         if mode == "fp64":
@@ -210,7 +267,7 @@ def mode_outputs(ref, mode, relax=300, measure=100, seeds=(1, 2)):
             run_fp64(twins, relax, measure)
             got = [outputs_fp64(tw) for tw in twins]
         else:
-            run(states, relax, measure)
+            run(states, relax, measure, batched=not options)
             got = [outputs(st, measure) for st in states]
     finally:
         for tw in twins:
@@ -259,8 +316,21 @@ def main(argv=None):
     ap.add_argument("--relax", type=int, default=300)
     ap.add_argument("--measure", type=int, default=100)
     ap.add_argument("--cross", help="two modes a,b compared with each other instead of with eduPIC")
+    ap.add_argument("--samestart", metavar="TAG",
+                    help="compare with eduPIC's runs from the same starts (fixtures edupic_TAG_s<seed>_*)")
+    ap.add_argument("--seeds", default="1,2,3,4")
+    ap.add_argument("--weight", type=float, default=7.0e4)
+    ap.add_argument("--spawn-collide", action="store_true",
+                    help="eduPIC's same-step collisions of new electrons (in-place steps)")
     a = ap.parse_args(argv)
     ref = load_reference(a.reference)
+    if a.samestart:
+        opts = {"spawn_collide": True} if a.spawn_collide else None
+        seeds = tuple(int(v) for v in a.seeds.split(","))
+        for mode in a.modes.split(","):
+            print(json.dumps(samestart(ref, a.reference, mode, a.samestart, seeds, a.relax, a.measure, a.weight, opts)),
+                  flush=True)
+        return 0
     if a.cross:
         ma, mb = a.cross.split(",")
         print(json.dumps(cross(ref, ma, mb, a.relax, a.measure)), flush=True)

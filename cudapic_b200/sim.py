@@ -141,6 +141,18 @@ class GpuSimState:
         check(lib.cudapic_state_set_fused(self._h, 1 if on else 0))
         self.fused = bool(on)
 
+    inplace = True   # the library's default
+
+    def set_inplace(self, on=True):
+        """Fused mode: in-place electron steps between compacting ones (default on)."""
+        check(lib.cudapic_state_set_inplace(self._h, 1 if on else 0))
+        self.inplace = bool(on)
+
+    def set_spawn_collide(self, on=True):
+        """eduPIC semantics: electrons born in a step are tested for collision
+        in that step (in-place steps; default off, the GPU reference's)."""
+        check(lib.cudapic_state_set_spawn_collide(self._h, 1 if on else 0))
+
     def set_graphs(self, on=True):
         """Replay captured CUDA graphs (default) or launch every step from the host."""
         check(lib.cudapic_state_set_graphs(self._h, 1 if on else 0))
@@ -280,13 +292,19 @@ class GpuBatch:
     def run_steps(self, n_steps):
         check(lib.cudapic_batch_run_steps(self._h, int(n_steps)))
 
-    BATCH_KERNELS = ("poisson", "ion_push", "electron_step", "ion_collisions")
+    @property
+    def inplace(self):
+        """True when the batch's electron steps run in place between compacting ones."""
+        return all(st.inplace for st in self.states)
+
+    BATCH_KERNELS = ("poisson", "ion_push", "electron_step", "ion_collisions", "electron_inplace",
+                     "electron_scatter")
 
     def profile_steps(self, n_steps):
         """Runs n_steps uncaptured with CUDA events around every kernel
         (cudapic_batch_profile_steps); returns {kernel: (ms summed, launches)}."""
-        ms = (C.c_double * 4)()
-        n = (C.c_uint64 * 4)()
+        ms = (C.c_double * len(self.BATCH_KERNELS))()
+        n = (C.c_uint64 * len(self.BATCH_KERNELS))()
         check(lib.cudapic_batch_profile_steps(self._h, int(n_steps), ms, n))
         return {k: (ms[j], n[j]) for j, k in enumerate(self.BATCH_KERNELS)}
 

@@ -24,6 +24,12 @@ It writes:
       (eduPIC 1.0 built from C/eduPIC.cc by oracle/Makefile, Mersenne
       Twister seed 5489) for the init cycle plus 10 cycles from 1000 + 1000
       particles.
+  edupic_c0_conv_seeds.txt -- the same run for Mersenne-Twister seeds
+      1 .. 16 (EDUPIC_SEED): one row per seed and cycle, columns seed,
+      cycle, N_e, N_i (the spread of the growth between seeds).
+
+The same-start fixtures (edupic_ss_*, edupic_c3_*) come from
+make_samestart.py.
 """
 import filecmp
 import os
@@ -70,7 +76,28 @@ def main():
         subprocess.run([exe, "0"], cwd=d, check=True, capture_output=True)
         subprocess.run([exe, "10"], cwd=d, check=True, capture_output=True)
         shutil.copyfile(os.path.join(d, "conv.dat"), os.path.join(HERE, "edupic_c0_conv.txt"))
+    write_c0_seeds(exe, range(1, 17))
     print("fixtures written to", HERE)
+
+
+def _c0_run(exe, seed):
+    env = dict(os.environ, EDUPIC_SEED=str(seed))
+    with tempfile.TemporaryDirectory() as d:
+        subprocess.run([exe, "0"], cwd=d, check=True, capture_output=True, env=env)
+        subprocess.run([exe, "10"], cwd=d, check=True, capture_output=True, env=env)
+        with open(os.path.join(d, "conv.dat")) as f:
+            return [(seed,) + tuple(int(v) for v in ln.split()) for ln in f if ln.strip()]
+
+
+def write_c0_seeds(exe, seeds):
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        runs = list(ex.map(lambda s: _c0_run(exe, s), seeds))
+    with open(os.path.join(HERE, "edupic_c0_conv_seeds.txt"), "w") as f:
+        f.write("# eduPIC 1.0, init cycle + 10 cycles from 1000 + 1000 particles at rest; seed cycle N_e N_i\n")
+        for rows in runs:
+            for r in rows:
+                f.write("%d %d %d %d\n" % r)
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
 """GPU tests of the simulation state and the per-step driver (reference loop
 Rust-CUDA/src/main.rs:1725-1808, replayed from CUDA graphs)."""
+import math
 import os
 
 import numpy as np
@@ -48,24 +49,41 @@ def test_upload_beyond_capacity_is_rejected(cudapic, cuda_device):
 
 
 def test_c0_growth_matches_edupic(cudapic, cuda_device):
-    """Plain eduPIC case: 1000 + 1000 particles at rest, 11 RF cycles.  The
-    particle counts track the reference CPU program's (same physics, other
-    random numbers) within statistical tolerance."""
-    conv = np.loadtxt(os.path.join(GOLDEN, "edupic_c0_conv.txt"))
-    st = _c0_state(cudapic)
+    """Plain eduPIC case: 1000 + 1000 particles at rest, the initialising
+    cycle and 10 more.  16 GPU seeds (initial positions and RNG streams)
+    against 16 eduPIC seeds (its Mersenne-Twister seed,
+    tests/golden/edupic_c0_conv_seeds.txt): the mean electron and ion counts
+    after cycles 1, 6 and 11 agree within 3 standard errors of the
+    difference, and the seed-to-seed spreads are alike."""
+    from cudapic_b200.sim import GpuBatch
+    ref = np.loadtxt(os.path.join(GOLDEN, "edupic_c0_conv_seeds.txt"))
+    seeds = range(16)
+    states = []
+    for k in seeds:
+        st = _c0_state(cudapic, seed=2 * k + 100)
+        st.seed(e_master=(0x12345678 + k, 0x11112222, 0x22223333, 0x33334444),
+                i_master=(0x44445555 + k, 0x55556666, 0x66667777, 0x77778888))
+        states.append(st)
     counts = []
-    for _ in range(11):
-        st.run_cycles(1)
-        counts.append(st.counts())
-    assert st.device_error() == 0
-    ne, ni = np.array(counts).T
-    # first cycle: ions created by ionization, electrons lost to the walls
-    assert 0.6 * conv[0, 2] < ni[0] < 1.4 * conv[0, 2]
-    assert 0.6 * conv[-1, 1] < ne[-1] < 1.4 * conv[-1, 1]
-    assert 0.6 * conv[-1, 2] < ni[-1] < 1.4 * conv[-1, 2]
-    assert np.all(np.diff(ne[2:]) > 0)  # the discharge is igniting
-    assert st.steps_done() == 11 * 4000
-    st.close()
+    with GpuBatch(states) as b:
+        for _ in range(11):
+            b.run_cycles(1)
+            b.synchronize()
+            counts.append([st.counts() for st in states])
+    assert all(st.device_error() == 0 for st in states)
+    got = np.array(counts, np.float64)        # [cycle, seed, species]
+    for cyc in (1, 6, 11):
+        for sp, col in ((0, 2), (1, 3)):
+            a = got[cyc - 1, :, sp]
+            e = ref[ref[:, 1] == cyc][:, col]
+            se = math.sqrt(a.var(ddof=1) / len(a) + e.var(ddof=1) / len(e))
+            print("cycle %2d %s: GPU %.0f +- %.0f, eduPIC %.0f +- %.0f" % (cyc, "ei"[sp], a.mean(), a.std(ddof=1),
+                                                                         e.mean(), e.std(ddof=1)))
+            assert abs(a.mean() - e.mean()) <= 3.0 * se, (cyc, sp, a.mean(), e.mean(), se)
+            assert 0.33 < a.std(ddof=1) / e.std(ddof=1) < 3.0
+    for st in states:
+        assert st.steps_done() == 11 * 4000
+        st.close()
 
 
 def test_work_counter_counts_particle_steps(cudapic, cuda_device):

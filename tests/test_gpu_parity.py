@@ -565,6 +565,39 @@ def test_step_electrons_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t
         assert m < n and ne > m and ni > 1000   # absorption and ionization both exercised
 
 
+@pytest.mark.parametrize("n,n_t,temp,dead", [(1, 4000, 3.0, 0.0), (4093, 4000, 3.0, 0.05), (300_001, 100, 30.0, 0.0),
+                                             (300_001, 100, 30.0, 0.02), (1_000_003, 4000, 3.0, 0.01),
+                                             (4_194_304, 4000, 3.0, 0.0)])
+def test_step_electrons_inplace_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp, dead):
+    """In-place electron step (stream + scatter pass) against the oracle's
+    move_and_compact + check_collisions_e over the live slots, every electron
+    keeping its slot (gpu_util.check_step_inplace); slots emptied by earlier
+    in-place steps are skipped."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    from gpu_util import check_step_inplace, dead_mask
+    cap = (2 * n + 4096 + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=n_t, capacity=cap)
+    ph = oracle.phys_from_params(n_t=n_t, capacity=cap)
+    x, vx, vy, vz = steady_state(n, E_MASS, temp, dt=g.dt_e, seed=n + 13)
+    m, ne, ni, nc = check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, field_profile(400), cap,
+                                       dead_mask(n, dead))
+    if n > 100_000 and n_t <= 100:
+        assert m < n and ne > n and ni > 1000 and nc > 1000   # absorption, collisions and ionization exercised
+
+
+@pytest.mark.parametrize("n,dead", [(4093, 0.05), (300_001, 0.02)])
+def test_step_electrons_skips_emptied_slots(cudapic, K, oracle, dev_tables, tables, n, dead):
+    """The compacting fused step drops the slots an in-place step emptied."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    from gpu_util import check_step_electrons_with_dead, dead_mask
+    cap = (2 * n + 4096 + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=100, capacity=cap)
+    ph = oracle.phys_from_params(n_t=100, capacity=cap)
+    x, vx, vy, vz = steady_state(n, E_MASS, 30.0, dt=g.dt_e, seed=n + 17)
+    check_step_electrons_with_dead(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, field_profile(400), cap,
+                                   dead_mask(n, dead))
+
+
 def test_step_electrons_rejects_unaligned_planes(cudapic, K, dev_tables, tables):
     _, se, _ = tables
     dcs, dse, _ = dev_tables
