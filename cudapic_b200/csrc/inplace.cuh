@@ -45,7 +45,9 @@ constexpr int IP_RECW = 8;          // words per record: slot, vx, vy, vz, rng0.
 
 // Dynamic shared memory: E[ef_pad] f32, the 64-bit deposit accumulator
 // [ef_pad], [copies][ef_pad] fixed-point histograms, the collider records
-// [IP_RECW][IP_WARPS][IP_QREC].
+// [IP_RECW][IP_WARPS][IP_QREC].  copies == 0 selects the large-grid deposit:
+// one f32 histogram in the accumulator's place (f32 shared atomics: no
+// copies to drain, and at thousands of nodes the lanes rarely meet on one).
 __host__ __device__ constexpr size_t inplace_smem_bytes(int copies, uint32_t ef_pad) {
     return (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 + (size_t)IP_RECW * IP_WARPS * IP_QREC * 4;
 }
@@ -73,6 +75,28 @@ struct InplaceSmem {
 __device__ __forceinline__ void inplace_smem_init(const InplaceSmem &sm, int copies, uint32_t ef_pad) {
     for (uint32_t k = threadIdx.x; k < (uint32_t)copies * ef_pad; k += IP_THREADS) sm.hist[k] = 0u;
     for (uint32_t k = threadIdx.x; k < ef_pad; k += IP_THREADS) sm.acc[k] = 0ull;
+}
+
+// The large-grid deposit: CIC weights (1 - rem, rem) of the new position
+// added to an f32 histogram, and the flush of its nodes (boundary nodes
+// doubled) into dens_out, which clears them.
+__device__ __forceinline__ void dep_add_f32(float *h, float x, const cudapic_grid &g) {
+    const float pos = x * g.inv_dx;
+    const int p = cell_of(pos, g.n_g);
+    const float rem = fminf(pos - (float)p, 1.0f);
+    atomicAdd(&h[p], 1.0f - rem);
+    atomicAdd(&h[p + 1], rem);
+}
+
+__device__ __forceinline__ void dep_flush_f32(float *h, float *dens_out, const cudapic_grid &g) {
+    for (uint32_t k = threadIdx.x; k < g.n_g; k += blockDim.x) {
+        const float v = h[k];
+        if (v == 0.0f) continue;
+        h[k] = 0.0f;
+        float f = v * g.weight_factor;
+        if (k == 0 || k == g.n_g - 1) f *= 2.0f;
+        atomicAdd(&dens_out[k], f);
+    }
 }
 
 // Scatters one collider at discharge-local slot `slot` (state past the
@@ -135,13 +159,15 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
     const float inv_dx = g.inv_dx, gap = g.gap;
     const uint32_t n_g = g.n_g;
     for (uint32_t k = tid; k < n_g; k += IP_THREADS) sm.ef[k] = dcp<SH>(dc.efield)[k];
-    uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
+    const bool f32dep = copies == 0;  // the large-grid deposit
+    uint32_t *h = f32dep ? nullptr : sm.hist + (uint32_t)(warp % copies) * ef_pad;
+    float *hf = reinterpret_cast<float *>(sm.acc);
     uint32_t qn = 0;      // records queued by this warp (uniform across its lanes), < 32 between rounds
     uint32_t ncoll = 0;   // colliders met by this warp
     __syncthreads();
     const uint32_t rounds = (end - beg + IP_ROUND - 1) / IP_ROUND;
     for (uint32_t r = 0; r < rounds; ++r) {
-        if (r != 0 && r % epoch == 0) {  // drain the deposit copies before they can overflow
+        if (!f32dep && r != 0 && r % epoch == 0) {  // drain the deposit copies before they can overflow
             __syncthreads();
             dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
             __syncthreads();
@@ -206,7 +232,9 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
                 s[1][u] = rs.s1;
                 s[2][u] = rs.s2;
                 s[3][u] = rs.s3;
-                dep_add(h, x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+                // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+                if (f32dep) dep_add_f32(hf, x[u], g);
+                else dep_add(h, x[u], g);
             }
         }
         if (any) {
@@ -257,6 +285,10 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
         if (cc) atomicAdd(cc, (unsigned long long)ncoll);
     }
     __syncthreads();
+    if (f32dep) {
+        dep_flush_f32(hf, dcp<SH>(dc.dens), gm);  // each node cleared by the thread that flushed it
+        return;
+    }
     dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
     __syncthreads();
     dep_flush(sm.acc, dcp<SH>(dc.dens), gm);

@@ -554,7 +554,7 @@ int launch_batch_inplace(const InplacePlanes &pl, const BatchDisc *desc, const u
     int copies = std::max(1, std::min(t.inplace_copies, IP_WARPS));
     auto bytes = [&]() { return inplace_smem_bytes(copies, ef_pad) + plan; };
     const size_t budget = (size_t)max_smem_optin();
-    while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
+    while (bytes() > budget && copies > 0) copies = copies / 2 < 4 ? 0 : copies / 2;
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "batch in-place step: n_g too large");
     auto kern = r.measure ? batch_inplace_kernel<true> : batch_inplace_kernel<false>;
     int per_sm = 0;
@@ -565,14 +565,16 @@ int launch_batch_inplace(const InplacePlanes &pl, const BatchDisc *desc, const u
                           "occupancy(batch in-place step)");
     };
     CUDAPIC_CHECK(occupancy());
-    while (per_sm < t.inplace_ctas_per_sm && copies > 1) {
-        copies = (copies + 1) / 2;
+    // large grids: fewer copies rather than fewer CTAs; below 4 copies the
+    // drains would come every few rounds, so the f32 histogram takes over
+    while (per_sm < t.inplace_ctas_per_sm && copies > 0) {
+        copies = copies / 2 < 4 ? 0 : copies / 2;
         CUDAPIC_CHECK(occupancy());
     }
     per_sm = std::min(std::max(per_sm, 1), t.inplace_ctas_per_sm);
     const unsigned grid = persistent_grid(per_sm, (cap_sum + IP_ROUND - 1) / IP_ROUND);
-    const uint32_t per_round = (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW;
-    const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_round);
+    const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
+    const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("batch_inplace_electrons", kern, dim3(grid), dim3(IP_THREADS), bytes(), stream, pl, desc,
                          counts, D, r.dens, r.dens_i, ef_pad, copies, epoch);
 }

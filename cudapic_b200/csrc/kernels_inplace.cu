@@ -126,7 +126,7 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
     int copies = std::max(1, std::min(t.inplace_copies, IP_WARPS));
     const size_t budget = (size_t)max_smem_optin();
-    while (inplace_smem_bytes(copies, ef_pad) > budget && copies > 1) copies = (copies + 1) / 2;
+    while (inplace_smem_bytes(copies, ef_pad) > budget && copies > 0) copies = copies / 2 < 4 ? 0 : copies / 2;
     if (inplace_smem_bytes(copies, ef_pad) > budget)
         return fail(CUDAPIC_ERR_ARG, "step_electrons_inplace: n_g too large");
     const bool meas = wall || coll;
@@ -140,15 +140,17 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
                           "occupancy(step_electrons_inplace)");
     };
     CUDAPIC_CHECK(occupancy());
-    while (per_sm < t.inplace_ctas_per_sm && copies > 1) {  // large grids: fewer copies, not fewer CTAs
-        copies = (copies + 1) / 2;
+    // large grids: fewer copies rather than fewer CTAs; below 4 copies the
+    // drains would come every few rounds, so the f32 histogram takes over
+    while (per_sm < t.inplace_ctas_per_sm && copies > 0) {
+        copies = copies / 2 < 4 ? 0 : copies / 2;
         CUDAPIC_CHECK(occupancy());
     }
     per_sm = std::min(std::max(per_sm, 1), t.inplace_ctas_per_sm);
     const unsigned grid = persistent_grid(per_sm, ((uint64_t)g.capacity + IP_ROUND - 1) / IP_ROUND);
     // rounds per deposit drain: a copy receives ceil(WARPS / copies) warps x 32 lanes x IP_ROW slots per round
-    const uint32_t per_round = (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW;
-    const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_round);
+    const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
+    const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("step_electrons_inplace", kern, dim3(grid), dim3(IP_THREADS),
                          inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, cs, sigma_max, n_e, n_i,
                          scratch, scratch + 1, dens_e, dens_i, g, ef_pad, copies, epoch, wall, coll, spawn_from);

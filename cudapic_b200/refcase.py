@@ -284,12 +284,12 @@ def study(ref, mode, relax=300, measure=100, seeds=(1, 2)):
             "errors": errors, "seed_spread": spread, "device_errors": [g["device_error"] for g in got]}
 
 
-def cross(ref, a="mixed", b="fp64", relax=300, measure=100, seeds=(1, 2)):
+def cross(ref, a="mixed", b="fp64", relax=300, measure=100, seeds=(1, 2), weight=7.0e4):
     """Mode a against mode b of the same model from the same starts: the
     relative L2 (relative difference for the scalars) of the seed means, and
     each mode's seed-to-seed spread (the noise floor of the comparison)."""
-    ga = mode_outputs(ref, a, relax, measure, seeds)
-    gb = mode_outputs(ref, b, relax, measure, seeds)
+    ga = mode_outputs(ref, a, relax, measure, seeds, weight=weight)
+    gb = mode_outputs(ref, b, relax, measure, seeds, weight=weight)
     band = (np.arange(len(ref["eepf"])) + 0.5) * DE_EEPF < EEPF_BAND_EV
     diff, spread = {}, {}
     for key in ("ne", "ni", "pot", "eepf", "power_e", "count_e"):
@@ -304,7 +304,7 @@ def cross(ref, a="mixed", b="fp64", relax=300, measure=100, seeds=(1, 2)):
             spread[key] = [float(np.linalg.norm(g[0][key][sel] - g[1][key][sel]) / np.linalg.norm(g[1][key][sel]))
                            for g in (ga, gb)]
     return {"modes": [a, b], "relax_cycles": relax, "measured_cycles": measure, "seeds": list(seeds),
-            "difference": diff, "seed_spread": spread,
+            "weight": weight, "particles_e": [g["count_e"] for g in ga], "difference": diff, "seed_spread": spread,
             "device_errors": [g["device_error"] for g in ga + gb]}
 
 
@@ -333,7 +333,8 @@ def main(argv=None):
         return 0
     if a.cross:
         ma, mb = a.cross.split(",")
-        print(json.dumps(cross(ref, ma, mb, a.relax, a.measure)), flush=True)
+        seeds = tuple(int(v) for v in a.seeds.split(","))
+        print(json.dumps(cross(ref, ma, mb, a.relax, a.measure, seeds, a.weight)), flush=True)
         return 0
     for mode in a.modes.split(","):
         print(json.dumps(study(ref, mode, a.relax, a.measure)), flush=True)

@@ -585,6 +585,22 @@ def test_step_electrons_inplace_bit_exact(cudapic, K, oracle, dev_tables, tables
         assert m < n and ne > n and ni > 1000 and nc > 1000   # absorption, collisions and ionization exercised
 
 
+@pytest.mark.parametrize("n_g", [2048, 4096, 16384])
+def test_step_electrons_inplace_large_grid(cudapic, K, oracle, dev_tables, tables, n_g):
+    """Large grids: the in-place step deposits into one f32 histogram per
+    CTA (no fixed-point copies); slots, RNG states and spawns stay bit-exact,
+    the density within the f32 deposit tolerance max(2e-5, 1.5 N_G 2^-24)."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    from gpu_util import check_step_inplace, dead_mask
+    n = 600_001
+    cap = (2 * n + 4096 + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=200, n_g=n_g, capacity=cap)
+    ph = oracle.phys_from_params(n_t=200, n_g=n_g, capacity=cap)
+    x, vx, vy, vz = steady_state(n, E_MASS, 20.0, dt=g.dt_e, seed=n_g + 3)
+    check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, field_profile(n_g), cap,
+                       dead_mask(n, 0.01), dens_tol=max(2e-5, 1.5 * n_g * 2.0 ** -24))
+
+
 @pytest.mark.parametrize("n,dead", [(4093, 0.05), (300_001, 0.02)])
 def test_step_electrons_skips_emptied_slots(cudapic, K, oracle, dev_tables, tables, n, dead):
     """The compacting fused step drops the slots an in-place step emptied."""
