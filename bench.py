@@ -458,15 +458,23 @@ def kernel_breakdown(st, K, reps, flush):
         n_i_c.fill_(n_i)
         dens.zero_()
     timed("step_electrons", step_e, n_e, 64, pre=reset_step)
-    # the in-place step (on the live planes: each launch advances them by one step)
-    scratch = torch.zeros(2, dtype=torch.int32, device="cuda")
+    # the in-place step's two passes (on the live planes: each launch advances them by one step);
+    # the collider records go to the other side's planes, as in the driver
+    rec = (b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0])
+    cnt, ticket = dev_u32(0), dev_u32(0)
 
-    def step_inplace():
-        K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.cs,
-                                 b.sigma_max_e, b.x[1], b.vx[1], b.vy[1], b.vz[1], ne_c, n_i_c, scratch, dens, dens_i, g,
-                                 stream=stream.cuda_stream)
-    timed("step_electrons_inplace", step_inplace, n_e, 56,
-          pre=lambda: (ne_c.fill_(n_e), n_i_c.fill_(n_i), dens.zero_()))
+    def stream_pass():
+        K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e,
+                                 b.sigma_max_e, ne_c, *rec, cnt, dens, g, stream=stream.cuda_stream)
+
+    def scatter_pass():
+        K.scatter_colliders_e(b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.cs, *rec, cnt, ticket, b.x[1], b.vx[1],
+                              b.vy[1], b.vz[1], ne_c, n_i_c, dens, dens_i, g, stream=stream.cuda_stream)
+    timed("step_electrons_inplace", stream_pass, n_e, 56, pre=lambda: (cnt.zero_(), ne_c.fill_(n_e), dens.zero_()))
+    n_coll = int(cnt.item())
+    timed("scatter_colliders_e", scatter_pass, n_coll, 0,
+          pre=lambda: (cnt.zero_(), ne_c.fill_(n_e), n_i_c.fill_(n_i), stream_pass()))
+    res["scatter_colliders_e"]["colliders_per_step"] = n_coll
     timed("check_collisions_i", lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                              *b.rng[1], g, stream=stream.cuda_stream), n_i, 44)
     return res
@@ -512,9 +520,10 @@ def run_one_discharge(args):
     elapsed_max, work_sum = reduce_max_sum(world, elapsed, work)
     value = work_sum / elapsed_max
     ion_steps = sum(1 for k in range(STEP) if k % 20 == 0)
-    # fused driver: Poisson and the electron step (in place or compacting) every step; ion push and MCC
-    # on ion steps
-    launches = args.steps * (STEP * 2 + ion_steps * 2)
+    # fused driver: Poisson every step; the electron step (in place: stream + scatter pass, two launches;
+    # compacting: one) every step; ion push and MCC on ion steps
+    compacting = STEP // 20 if args.inplace else STEP
+    launches = args.steps * (STEP + compacting + 2 * (STEP - compacting) + ion_steps * 2)
 
     # ---------------- end to end through the C ABI with host buffers
     pinned = {}
@@ -571,7 +580,7 @@ def run_one_discharge(args):
         share_w = {"solve_poisson": STEP, "step_electrons": compacting, "move_and_compact_deposit_i": ion_steps,
                    "check_collisions_i": ion_steps}
         if args.inplace:
-            share_w["step_electrons_inplace"] = STEP - compacting
+            share_w.update({"step_electrons_inplace": STEP - compacting, "scatter_colliders_e": STEP - compacting})
         tot = sum(breakdown[k]["us"] * w for k, w in share_w.items())
         for k in breakdown:
             breakdown[k]["share"] = breakdown[k]["us"] * share_w.get(k, 0) / tot
@@ -783,7 +792,7 @@ def run_batched(args):
     if breakdown:
         dom = max((k for k in breakdown if "gbs" in breakdown[k]), key=lambda k: breakdown[k]["share"])
         d = breakdown[dom]
-        names = {"electron_inplace": ("batch_inplace_kernel (in-place electron step of all discharges)",
+        names = {"electron_inplace": ("batch_inplace_kernel (in-place electron step of all discharges, stream pass)",
                                       "batch_electron_inplace"),
                  "electron_step": ("batch_step_kernel<MCC> (compacting fused electron step of all discharges)",
                                    "batch_electron_step")}
@@ -812,7 +821,8 @@ def run_batched(args):
                 "d2h_bytes_per_step": d2h // args.steps, "wall_s": e2e_max},
         "roofline": roofline, "kernels": breakdown, "cpu_baseline": cpu,
         "stated_error": STATED_ERROR, "clocks": clk.summary(),
-        "gpu_launches": args.steps * (STEP * 2 + ion_steps * 2),
+        "gpu_launches": args.steps * (STEP + (STEP // 20) + 2 * (STEP - STEP // 20) + ion_steps * 2
+                                      if args.inplace else STEP * 2 + ion_steps * 2),
         "discharges_counted": n_clean if world == 1 else None,
         "discharges_excluded": len(flagged_all),
         "excluded_why": "device error word set in some phase (spawns beyond the capacity of %.1fx the initial "
@@ -887,7 +897,8 @@ def run_c0(args):
                        "path": "reference launch sequence, every kernel launched from the host"},
         "fused_seconds": f["seconds"], "particle_steps": f["work"], "counts_end": f["counts"],
         "e2e": res["e2e"], "cpu_baseline": cpu, "clocks": clk.summary(), "roofline": None,
-        "gpu_launches": C0_CYCLES * 4000 * 2 + C0_CYCLES * 200 * 2,
+        # per 40 steps: 40 Poisson, 38 in-place steps of two kernels, 2 compacting steps, 2 ion pushes + MCC
+        "gpu_launches": C0_CYCLES * (4000 // STEP) * (STEP + 2 * (STEP - 2) + 2 + 2 * 2),
         "device_error_bits": [f["dev_err"], p["dev_err"]],
     }
     if rank == 0:

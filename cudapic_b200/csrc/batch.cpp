@@ -39,7 +39,7 @@ struct cudapic_batch {
     std::vector<cudaEvent_t> ready;  // per state: its stream's work before a run
     cudaEvent_t done = nullptr;
     BatchDisc *desc = nullptr;
-    uint32_t *counts = nullptr;      // [2][D] written by the batched Poisson solve
+    uint32_t *counts = nullptr;      // [2][D] written by the batched Poisson solve; [2D]: scatter ticket
     bool inplace = true;             // in-place electron steps between compacting ones (all states in-place)
     float *pool = nullptr;           // POOL_PLANES x pool_len elements
     uint64_t pool_len = 0;
@@ -280,14 +280,20 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, bool compa
     }
     r.dens = b->ecur ^ 1;
     if (b->inplace && !compact) {
-        // in place: the electrons stay on their side, colliders are scattered in the pass
+        // in place: the electrons stay on their side, collider records go to
+        // the other side's planes, the scatter pass follows
         const SidePlanes es = side_planes(b, 0, b->se);
         const SidePlanes is = side_planes(b, 1, b->si);
         const InplacePlanes pl{es.x, es.vx, es.vy, es.vz, es.rng0, es.rng1, es.rng2, es.rng3,
                                is.x, is.vx, is.vy, is.vz};
+        const SidePlanes os = side_planes(b, 0, b->se ^ 1);
+        const CollList list{reinterpret_cast<uint32_t *>(os.x), os.vx, os.vy, os.vz};
         CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_INPLACE));
-        CUDAPIC_CHECK(launch_batch_inplace(pl, b->desc, b->counts, D, b->cap_sum, b->max_n_g, r, st));
+        CUDAPIC_CHECK(launch_batch_inplace(pl, list, b->desc, b->counts, D, b->cap_sum, b->max_n_g, r, st));
         CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_INPLACE));
+        CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_SCATTER));
+        CUDAPIC_CHECK(launch_batch_scatter(pl, list, b->desc, D, b->cap_sum, r, b->counts + 2 * D, st));
+        CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_SCATTER));
     } else {
         CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_STEP));
         CUDAPIC_CHECK(launch_batch_step(true, step_planes(b, 0, b->se, b->si), b->desc, b->counts, D, b->cap_sum,

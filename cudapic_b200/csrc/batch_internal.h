@@ -49,11 +49,19 @@ struct InplacePlanes {
     float *ix, *ivx, *ivy, *ivz;
 };
 
+// The collider list of an in-place step: one record (slot, vx, vy, vz) per
+// collider in four planes of capacity entries (the other side's x, vx, vy,
+// vz planes, which the in-place step does not otherwise use).
+struct CollList {
+    uint32_t *slot;
+    float *vx, *vy, *vz;
+};
+
 // Counters-block words of the in-place step (after the fused step's words:
 // n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work).
-constexpr int CTR_SPAWNED = 12;      // electrons spawned by the running in-place step
-constexpr int CTR_IP_TICKET = 13;    // its CTA completion ticket
-constexpr int CTR_SPAWN_FROM = 14;   // slot count when it started (first spawn slot)
+constexpr int CTR_COLL_COUNT = 12;   // colliders listed by the stream pass
+constexpr int CTR_COLL_TICKET = 13;  // CTA completion ticket of the scatter pass
+constexpr int CTR_SPAWN_FROM = 14;   // slot count when the stream pass ran (first spawn slot)
 
 struct BatchDisc {
     cudapic_grid g;                                        // dev_err, work: the discharge's own words
@@ -98,12 +106,16 @@ int launch_batch_poisson(const BatchDisc *desc, uint32_t *counts, uint32_t D, ui
 // launch_batch_poisson.
 int launch_batch_step(bool mcc, const StepPlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
                       uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream);
-// The in-place electron step of every discharge (inplace.cuh) over the
-// live side `pl` (counts: the electron counts written by
-// launch_batch_poisson; spawned ions go to pl.ix..ivz), colliders scattered
-// in the pass, each discharge's new slot count published by its last CTA.
-int launch_batch_inplace(const InplacePlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
-                         uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream);
+// The in-place electron step of every discharge (inplace.cuh): the stream
+// pass over the live side `pl` (counts: the electron counts written by
+// launch_batch_poisson; colliders recorded in `list`, the pooled planes of
+// the other side, at each discharge's offset), then the scatter pass
+// (spawned ions to pl.ix..ivz; ticket: a word of the batch, zero between
+// launches).
+int launch_batch_inplace(const InplacePlanes &pl, const CollList &list, const BatchDisc *desc, const uint32_t *counts,
+                         uint32_t D, uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream);
+int launch_batch_scatter(const InplacePlanes &pl, const CollList &list, const BatchDisc *desc, uint32_t D,
+                         uint64_t cap_sum, const StepRoles &r, uint32_t *ticket, cudaStream_t stream);
 // Ion collisions of every discharge (ions on the pooled side `ions`, counts
 // read from the discharges' counters).
 int launch_batch_collisions_i(const SidePlanes &ions, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,

@@ -4,28 +4,30 @@
 // The compacting fused step (step.cuh) writes every survivor into the other
 // side, so each tile needs a block-wide scan and barrier before its stores.
 // The in-place step keeps every electron in its slot instead:
-//  * one persistent pass (inplace_segment): four consecutive slots per
-//    thread and round, read with 16-byte loads from the eight SoA planes
-//    (x, vx, vy, vz, rng0..3); push (Rust-CUDA/src/main.rs:596-620),
-//    electrode absorption, collision test (:992-1012, the certain-rejection
-//    bound of step.cuh first), CIC deposit of the new position into the next
-//    density (push.cuh, 2^-20 fixed point); x, vx and the RNG state go back
-//    to the same slots (vy, vz do not change in the push: 24 B written per
-//    electron against 32 B read).  An absorbed electron leaves its slot
-//    with x = DEAD_X; later passes skip it;
-//  * a collider's whole state (slot, v, RNG past the test draw) goes to
-//    its warp's record queue in shared memory; once 32 are queued the warp
-//    scatters them together, one per lane (collision_e, :1035-1165), and
-//    writes velocity and RNG state back to their slots.  Nothing is re-read
-//    from HBM, and the other warps of the SM keep streaming meanwhile.
-//    Spawned electrons take slots n, n + 1, ... (n: the slot count at
-//    launch), spawned ions the next slots of the ion side; the last CTA
-//    publishes the new slot count.
-// No block barrier orders the stores (the only CTA barriers drain the
-// deposit histograms every few dozen rounds).  The holes are closed by the
-// compacting step, which the drivers run every N_SUB steps and as the last
-// step of every run, so the particle planes are compact whenever a caller
-// can see them.
+//  * stream pass (inplace_segment): four consecutive slots per thread and
+//    round, read with 16-byte loads from the eight SoA planes (x, vx, vy, vz,
+//    rng0..3); push (Rust-CUDA/src/main.rs:596-620), electrode absorption,
+//    collision test (:992-1012, the certain-rejection bound of step.cuh
+//    first), CIC deposit of the new position into the next density
+//    (push.cuh, 2^-20 fixed point); x, vx and the RNG state go back to the
+//    same slots (vy, vz do not change in the push: 24 B written per electron
+//    against 32 B read).  An absorbed electron leaves its slot with
+//    x = DEAD_X; later passes skip it.  A collider's record (slot, vx, vy,
+//    vz) goes to its warp's queue in shared memory and, 32 at a time, to the
+//    collider list (one atomicAdd per 32 records, coalesced stores): four
+//    planes of the other side, which the in-place step does not otherwise
+//    use, so the list holds one record for every slot;
+//  * scatter pass (inplace_scatter): one thread per listed collider reads
+//    its record (coalesced), continues the slot's RNG stream past the test
+//    draw, scatters (collision_e, :1035-1165) and writes velocity and RNG
+//    state back to the slot; spawned electrons are appended after the live
+//    slots, spawned ions to the ion side.
+// The stream pass keeps the collision code out of its registers (the
+// scattering needs ~110 per thread; the stream pass runs at 64 with four
+// CTAs per SM), and no block barrier orders its stores.  The holes are
+// closed by the compacting step, which the drivers run every N_SUB steps and
+// as the last step of every run, so the particle planes are compact
+// whenever a caller can see them.
 // Every electron draws from the RNG stream of the slot it occupies, in the
 // reference's order (test draw, then the scattering draws), as in the
 // compacting fused step.
@@ -39,9 +41,8 @@ constexpr int IP_THREADS = 256;
 constexpr int IP_WARPS = IP_THREADS / 32;
 constexpr int IP_ROW = 4;           // slots per thread and round (one 16-byte load per plane)
 constexpr int IP_ROUND = IP_THREADS * IP_ROW;
-constexpr int IP_QREC = 64;         // per-warp collider record queue (drained at 32)
-constexpr int IP_RECW = 8;          // words per record: slot, vx, vy, vz, rng0..3
-
+constexpr int IP_QREC = 32 + 32 * IP_ROW;  // per-warp collider queue: < 32 left over + one round
+constexpr int IP_RECW = 4;          // words per record: slot, vx, vy, vz
 
 // Dynamic shared memory: E[ef_pad] f32, the 64-bit deposit accumulator
 // [ef_pad], [copies][ef_pad] fixed-point histograms, the collider records
@@ -99,59 +100,53 @@ __device__ __forceinline__ void dep_flush_f32(float *h, float *dens_out, const c
     }
 }
 
-// Scatters one collider at discharge-local slot `slot` (state past the
-// test draw): collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused
-// step's algebraic sines and cosines; velocity and RNG state are written
-// back to the slot.  dc.alive counts the spawned electrons (slots n_base + k).
-template <bool SH>
-__device__ __forceinline__ void inplace_collide(const InplacePlanes &pl, const StepDisc &dc, const cudapic_grid &gm,
-                                                uint32_t off, uint32_t slot, float vxi, float vyi, float vzi,
-                                                uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t n_base) {
-    Xoshiro128p rs{r0, r1, r2, r3};
-    const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
-    const uint32_t idx = energy_index(gm.half_me_over_e * v2);
-    collide_electron_t<true>(off, slot, idx, vxi, vyi, vzi, rs, dcp<SH>(dc.cs), pl.x, pl.vx, pl.vy, pl.vz, pl.ix,
-                             pl.ivx, pl.ivy, pl.ivz, dcp<SH>(dc.alive), dcp<SH>(dc.n_i), gm, dcp<SH>(dc.dens),
-                             dcp<SH>(dc.dens_i), n_base);
-    const uint32_t k = off + slot;
-    pl.rng0[k] = rs.s0;
-    pl.rng1[k] = rs.s1;
-    pl.rng2[k] = rs.s2;
-    pl.rng3[k] = rs.s3;
-}
-
-// Lanes [0, cnt) of the calling warp each scatter record first + lane of
-// the warp's queue.  Every lane calls it.
-template <bool SH>
-__device__ __forceinline__ void drain_records(const InplaceSmem &sm, const InplacePlanes &pl, const StepDisc &dc,
-                                              const cudapic_grid &gm, uint32_t off, uint32_t first, uint32_t cnt,
-                                              uint32_t n_base) {
+// Moves whole groups of 32 queued records of the calling warp to the list
+// (one atomicAdd per call), or all of them with `all`; the rest move to the
+// front of the queue.  Every lane calls it with the same qn.
+__device__ __forceinline__ void flush_records(const InplaceSmem &sm, uint32_t &qn, bool all, const CollList &list,
+                                              uint32_t *count) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    if ((uint32_t)lane < cnt) {
-        const uint32_t j = first + (uint32_t)lane;
-        inplace_collide<SH>(pl, dc, gm, off, sm.r(0, warp, j), __uint_as_float(sm.r(1, warp, j)),
-                            __uint_as_float(sm.r(2, warp, j)), __uint_as_float(sm.r(3, warp, j)), sm.r(4, warp, j),
-                            sm.r(5, warp, j), sm.r(6, warp, j), sm.r(7, warp, j), n_base);
+    const uint32_t n = all ? qn : (qn & ~31u);
+    if (n == 0) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    // at most one record per slot: the list (capacity entries) cannot overflow
+    for (uint32_t k = lane; k < n; k += 32) {
+        list.slot[base + k] = sm.r(0, warp, k);
+        list.vx[base + k] = __uint_as_float(sm.r(1, warp, k));
+        list.vy[base + k] = __uint_as_float(sm.r(2, warp, k));
+        list.vz[base + k] = __uint_as_float(sm.r(3, warp, k));
     }
     __syncwarp();
+    const uint32_t rest = qn - n;
+    uint32_t v[IP_RECW];
+#pragma unroll
+    for (int w = 0; w < IP_RECW; ++w) v[w] = lane < (int)rest ? sm.r(w, warp, n + lane) : 0u;
+    __syncwarp();
+    if (lane < (int)rest) {
+#pragma unroll
+        for (int w = 0; w < IP_RECW; ++w) sm.r(w, warp, lane) = v[w];
+    }
+    __syncwarp();
+    qn = rest;
 }
 
-// The pass over slots [beg, end) (discharge-local, beg a multiple of 4) of
-// one discharge whose planes start at element `off`; n_base: the
-// discharge's slot count at launch (the first slot of a spawned electron).
-// Every thread of the CTA calls it with the same arguments; on entry the
-// histograms and the accumulator are zero and so they are on return (the
-// deposits flushed into dc.dens).  The live electrons processed are added
-// to `live` (per thread), the colliders to dc.coll when it is set.
-// SH: dc lives in shared memory; WALL: compile the electrode counters in.
+// The stream pass over slots [beg, end) (discharge-local, beg a multiple of
+// 4) of one discharge whose planes start at element `off`.  Every thread of
+// the CTA calls it with the same arguments; on entry the histograms and the
+// accumulator are zero and the queues empty, and so they are on return (the
+// deposits flushed into dc.dens, the colliders into `list` / `count`, both
+// relative to the discharge).  The live electrons processed are added to
+// `live` (per thread).  SH: dc lives in shared memory; WALL: compile the
+// electrode counters in.
 template <bool SH, bool WALL>
 __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const StepDisc &dc, const cudapic_grid &g,
                                                 const cudapic_grid &gm, uint32_t off, uint32_t beg, uint32_t end,
-                                                uint32_t n_base, const InplaceSmem &sm, int copies, uint32_t ef_pad,
-                                                uint32_t epoch, uint32_t &live) {
+                                                const InplaceSmem &sm, int copies, uint32_t ef_pad, uint32_t epoch,
+                                                const CollList &list, uint32_t *count, uint32_t &live) {
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
     const int warp = tid >> 5;
     const unsigned lt = lanemask_lt();
     const float factor = dc.factor, dt = dc.dt, sigma_max = dc.sigma_max;
@@ -162,8 +157,7 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
     const bool f32dep = copies == 0;  // the large-grid deposit
     uint32_t *h = f32dep ? nullptr : sm.hist + (uint32_t)(warp % copies) * ef_pad;
     float *hf = reinterpret_cast<float *>(sm.acc);
-    uint32_t qn = 0;      // records queued by this warp (uniform across its lanes), < 32 between rounds
-    uint32_t ncoll = 0;   // colliders met by this warp
+    uint32_t qn = 0;  // records queued by this warp (uniform across its lanes), < 32 between rounds
     __syncthreads();
     const uint32_t rounds = (end - beg + IP_ROUND - 1) / IP_ROUND;
     for (uint32_t r = 0; r < rounds; ++r) {
@@ -245,45 +239,26 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
             *reinterpret_cast<uint4 *>(pl.rng2 + i0) = make_uint4(s[2][0], s[2][1], s[2][2], s[2][3]);
             *reinterpret_cast<uint4 *>(pl.rng3 + i0) = make_uint4(s[3][0], s[3][1], s[3][2], s[3][3]);
         }
-        // (4) this round's colliders, after the stores they overwrite: queued as
-        //     records; a warp with more than fits scatters the rest at once
+        // (4) queue this round's colliders as records (warp-synchronous)
         if (__ballot_sync(0xffffffffu, coll != 0)) {
-            __syncwarp();  // the stores above are visible to the lanes that scatter
 #pragma unroll
             for (int u = 0; u < IP_ROW; ++u) {
                 const bool c = coll >> u & 1u;
                 const unsigned cm = __ballot_sync(0xffffffffu, c);
-                const uint32_t pos = qn + __popc(cm & lt);
                 if (c) {
-                    if (pos < IP_QREC) {
-                        sm.r(0, warp, pos) = s0 + (uint32_t)u;
-                        sm.r(1, warp, pos) = __float_as_uint(vx[u]);
-                        sm.r(2, warp, pos) = __float_as_uint(vy[u]);
-                        sm.r(3, warp, pos) = __float_as_uint(vz[u]);
-                        sm.r(4, warp, pos) = s[0][u];
-                        sm.r(5, warp, pos) = s[1][u];
-                        sm.r(6, warp, pos) = s[2][u];
-                        sm.r(7, warp, pos) = s[3][u];
-                    } else {
-                        inplace_collide<SH>(pl, dc, gm, off, s0 + (uint32_t)u, vx[u], vy[u], vz[u], s[0][u], s[1][u],
-                                            s[2][u], s[3][u], n_base);
-                    }
+                    const uint32_t pos = qn + __popc(cm & lt);
+                    sm.r(0, warp, pos) = s0 + (uint32_t)u;
+                    sm.r(1, warp, pos) = __float_as_uint(vx[u]);
+                    sm.r(2, warp, pos) = __float_as_uint(vy[u]);
+                    sm.r(3, warp, pos) = __float_as_uint(vz[u]);
                 }
-                ncoll += __popc(cm);
-                qn = min(qn + (uint32_t)__popc(cm), (uint32_t)IP_QREC);
+                qn += __popc(cm);
             }
             __syncwarp();
-            while (qn >= 32) {  // full warps of colliders, one per lane
-                qn -= 32;
-                drain_records<SH>(sm, pl, dc, gm, off, qn, 32, n_base);
-            }
+            if (qn >= 32) flush_records(sm, qn, false, list, count);
         }
     }
-    if (qn) drain_records<SH>(sm, pl, dc, gm, off, 0, qn, n_base);
-    if (lane == 0 && ncoll) {
-        unsigned long long *cc = dcp<SH>(dc.coll);
-        if (cc) atomicAdd(cc, (unsigned long long)ncoll);
-    }
+    flush_records(sm, qn, true, list, count);
     __syncthreads();
     if (f32dep) {
         dep_flush_f32(hf, dcp<SH>(dc.dens), gm);  // each node cleared by the thread that flushed it
@@ -295,23 +270,27 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
     for (uint32_t k = tid; k < n_g; k += IP_THREADS) sm.acc[k] = 0ull;
 }
 
-// End of a pass over one discharge: the last of the `expected` CTAs that met
-// it (its ticket) publishes the slot count n_e = min(n_base + spawned,
-// capacity) and clears the spawn counter and the ticket.
-__device__ __forceinline__ void publish_spawns(uint32_t *ticket, uint32_t *n_e, uint32_t *spawned, uint32_t n_base,
-                                               uint32_t capacity, uint32_t expected) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t t = atomicAdd(ticket, 1u);
-        if (t == expected - 1) {
-            __threadfence();
-            const uint32_t v = atomicExch(spawned, 0u);
-            const uint64_t n = (uint64_t)n_base + v;
-            *n_e = n < capacity ? (uint32_t)n : capacity;
-            *ticket = 0u;
-        }
-    }
+// The scatter pass for record k of a discharge's collider list (its planes
+// at element `off`): the slot's RNG stream continues past the test draw
+// (collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused step's
+// algebraic sines and cosines); velocity and RNG state go back to the slot,
+// a spawned electron takes the next slot of n_e, a spawned ion the next slot
+// of n_i.
+__device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const CollList &list, uint32_t off,
+                                                uint32_t k, const float *cs, uint32_t *n_e, uint32_t *n_i,
+                                                const cudapic_grid &g, float *dens_e, float *dens_i) {
+    const uint32_t i = list.slot[off + k];
+    const float vxi = list.vx[off + k], vyi = list.vy[off + k], vzi = list.vz[off + k];
+    const uint32_t j = off + i;
+    Xoshiro128p rs{pl.rng0[j], pl.rng1[j], pl.rng2[j], pl.rng3[j]};
+    const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
+    const uint32_t idx = energy_index(g.half_me_over_e * v2);
+    collide_electron_t<true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx, pl.ivy,
+                             pl.ivz, n_e, n_i, g, dens_e, dens_i);
+    pl.rng0[j] = rs.s0;
+    pl.rng1[j] = rs.s1;
+    pl.rng2[j] = rs.s2;
+    pl.rng3[j] = rs.s3;
 }
 
 }  // namespace cudapic

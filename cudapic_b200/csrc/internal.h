@@ -167,20 +167,23 @@ double cfl_max_energy(const cudapic_params &p);
 int rng_sidecar_write(const char *path, uint32_t capacity, const std::vector<uint32_t> planes[2][4]);
 int rng_sidecar_read(const char *path, uint32_t capacity, std::vector<uint32_t> planes[2][4]);
 
-// The in-place electron step (kernels_inplace.cu) over [0, *n_e): electrons
-// stay in their slots, absorbed ones are marked, colliders are scattered in
-// the pass; spawned electrons take slots *n_e, *n_e + 1, ... (the last CTA
-// publishes the new *n_e), spawned ions the next slots of *n_i.  scratch:
-// two words (spawn counter, CTA ticket), zero on entry and on return.
-// coll (may be null): collision events; spawn_from (may be null): receives
-// the slot count at launch.
+// The in-place electron step (kernels_inplace.cu): the stream pass over
+// [0, *n_active) -- electrons stay in their slots, absorbed ones are marked,
+// colliders are recorded in `list` / *count -- and the scatter pass over the
+// records (spawns appended at *n_e and *n_i; its last CTA adds the
+// collision count to *coll and clears *count and *ticket).  spawn_from (may
+// be null): receives the slot count the stream pass saw.
 struct InplacePlanes;
-int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, const float *cs,
-                            float sigma_max, uint32_t *n_e, uint32_t *n_i, uint32_t *scratch, float *dens_e,
-                            float *dens_i, const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
-                            unsigned long long *coll, uint32_t *spawn_from);
+struct CollList;
+int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, float sigma_max,
+                            const uint32_t *n_active, const CollList &list, uint32_t *count, float *dens_e,
+                            const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
+                            uint32_t *spawn_from);
+int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const float *cs, uint32_t *count,
+                            uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
+                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll);
 // eduPIC's same-step collisions of new electrons: one CTA tests and scatters
-// the electrons appended since *spawn_from (written by the in-place step).
+// the electrons appended since *spawn_from (written by the stream pass).
 int launch_spawn_collide(const InplacePlanes &pl, const float *sigma_tot_e, const float *cs,
                          const uint32_t *spawn_from, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
                          cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll);

@@ -204,17 +204,16 @@ __global__ void __launch_bounds__(ES_THREADS, MINB)
     }
 }
 
-// The in-place electron step of every discharge (inplace.cuh): the batch's
-// concatenated electron slots cut into equal per-CTA shares as in
-// batch_step_kernel, each segment run with that discharge's field, tables,
-// counters and densities; colliders are scattered in the pass, and each
-// discharge's new slot count is published by the last of the CTAs that met
-// it (its own ticket, expecting the CTAs whose shares meet the discharge).
+// The in-place electron step of every discharge (inplace.cuh), stream pass:
+// the batch's concatenated electron slots cut into equal per-CTA shares as
+// in batch_step_kernel, each segment run with that discharge's field,
+// tables, next density and collider list (the discharge's range of the
+// other side's planes).  No count changes: nothing is published.
 template <bool MEAS>
 __global__ void __launch_bounds__(IP_THREADS, 4)
-    batch_inplace_kernel(const __grid_constant__ InplacePlanes pl, const BatchDisc *__restrict__ desc,
-                         const uint32_t *__restrict__ counts, uint32_t D, int dens_role, int dens_i_role,
-                         uint32_t ef_pad, int copies, uint32_t epoch) {
+    batch_inplace_kernel(const __grid_constant__ InplacePlanes pl, const __grid_constant__ CollList list,
+                         const BatchDisc *__restrict__ desc, const uint32_t *__restrict__ counts, uint32_t D,
+                         int dens_role, uint32_t ef_pad, int copies, uint32_t epoch) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t wsum[ES_WARPS];
     __shared__ StepDisc s_dc;
@@ -251,31 +250,90 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
             dc.sigma_max = dd.sigma_max_e;
             dc.factor = dd.g.factor_e;
             dc.dt = dd.g.dt_e;
-            dc.alive = dd.counters + CTR_SPAWNED;
-            dc.n_i = dd.counters + 1;
+            dc.alive = dd.counters + CTR_COLL_COUNT;   // the collider count
+            dc.n_i = nullptr;
             dc.dens = dd.e_dens[dens_role];
-            dc.dens_i = dd.i_dens[dens_i_role];
+            dc.dens_i = nullptr;
             dc.wall = MEAS ? dd.wall : nullptr;
-            dc.coll = MEAS ? dd.mcount : nullptr;
+            dc.coll = nullptr;
             s_dc = dc;
         }
         __syncthreads();
         {
             const cudapic_grid g = s_g;
+            const uint32_t off = s_off;
+            const CollList mine{list.slot + off, list.vx + off, list.vy + off, list.vz + off};
             uint32_t live = 0;
-            inplace_segment<true, MEAS>(pl, s_dc, g, s_g, s_off, lo, hi, n, sm, copies, ef_pad, epoch, live);
+            inplace_segment<true, MEAS>(pl, s_dc, g, s_g, off, lo, hi, sm, copies, ef_pad, epoch, mine,
+                                        dcp<true>(s_dc.alive), live);
             add_work(s_g.work, live);
         }
         d = lds_volatile(&s_d);
-        {
-            uint32_t chunk2, beg2, end2;
-            cta_share(P[D], chunk2, beg2, end2);
-            const uint32_t n2 = counts[d];
-            const uint32_t expected = (P[d] + n2 - 1) / chunk2 - P[d] / chunk2 + 1;
-            uint32_t *ctr = desc[d].counters;
-            publish_spawns(ctr + CTR_IP_TICKET, ctr + 0, ctr + CTR_SPAWNED, n2, s_g.capacity, expected);
-        }
         __syncthreads();  // s_dc, s_g, s_d and s_off are rewritten for the next segment
+    }
+}
+
+// The in-place electron step of every discharge, scatter pass: the listed
+// colliders of all discharges (each discharge's count clamped to its
+// capacity) cut into per-CTA shares; each segment scatters with that
+// discharge's table, counters and next densities.  The last CTA of the
+// launch adds the collision counts (measurement) and empties every list.
+template <bool MEAS>
+__global__ void __launch_bounds__(IP_THREADS)
+    batch_scatter_kernel(const __grid_constant__ InplacePlanes pl, const __grid_constant__ CollList list,
+                         const BatchDisc *__restrict__ desc, uint32_t D, int dens_role, int dens_i_role,
+                         uint32_t *ticket) {
+    extern __shared__ __align__(16) uint32_t sc_smem[];
+    uint32_t *P = sc_smem;  // [D + 1]
+    __shared__ uint32_t wsum[ES_WARPS];
+    __shared__ cudapic_grid s_g;
+    __shared__ const float *s_cs;
+    __shared__ uint32_t *s_ctr;
+    __shared__ float *s_de, *s_di;
+    __shared__ uint32_t s_off;
+    grid_dep_wait();
+    auto count = [&](uint32_t d) {
+        const BatchDisc &dd = desc[d];
+        return min(*(volatile uint32_t *)(dd.counters + CTR_COLL_COUNT), dd.g.capacity);
+    };
+    plan_prefix(count, D, P, wsum);
+    uint32_t chunk, beg, end;
+    cta_share(P[D], chunk, beg, end);
+    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
+        const uint32_t n = count(d);  // unchanged until the last CTA has taken its ticket
+        const uint32_t lo = max(beg, P[d]) - P[d];
+        const uint32_t hi = min(end, P[d] + n) - P[d];
+        if (lo >= hi) continue;
+        if (threadIdx.x == 0) {
+            const BatchDisc &dd = desc[d];
+            s_g = dd.g;
+            s_cs = dd.cs;
+            s_ctr = dd.counters;
+            s_de = dd.e_dens[dens_role];
+            s_di = dd.i_dens[dens_i_role];
+            s_off = dd.off;
+        }
+        __syncthreads();
+        for (uint32_t k = lo + threadIdx.x; k < hi; k += IP_THREADS)
+            inplace_scatter(pl, list, s_off, k, s_cs, s_ctr + 0, s_ctr + 1, s_g, s_de, s_di);
+        __syncthreads();  // the segment's shared words are rewritten for the next one
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t t = atomicAdd(ticket, 1u);
+        P[0] = t == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (P[0]) {  // the last CTA: every list has been read
+        __threadfence();
+        for (uint32_t d = threadIdx.x; d < D; d += IP_THREADS) {
+            const BatchDisc &dd = desc[d];
+            uint32_t *c = dd.counters + CTR_COLL_COUNT;
+            if (MEAS) atomicAdd(dd.mcount, (unsigned long long)min(*c, dd.g.capacity));
+            *c = 0u;
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
     }
 }
 
@@ -545,8 +603,8 @@ int launch_batch_step(bool mcc, const StepPlanes &pl, const BatchDisc *desc, con
     return launch_batch_step_m<false>(mcc, pl, desc, counts, D, cap_sum, max_n_g, r, stream, t);
 }
 
-int launch_batch_inplace(const InplacePlanes &pl, const BatchDisc *desc, const uint32_t *counts, uint32_t D,
-                         uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream) {
+int launch_batch_inplace(const InplacePlanes &pl, const CollList &list, const BatchDisc *desc, const uint32_t *counts,
+                         uint32_t D, uint64_t cap_sum, uint32_t max_n_g, const StepRoles &r, cudaStream_t stream) {
     if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch in-place step: bad discharge count");
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (max_n_g + 3u) & ~3u;
@@ -575,8 +633,18 @@ int launch_batch_inplace(const InplacePlanes &pl, const BatchDisc *desc, const u
     const unsigned grid = persistent_grid(per_sm, (cap_sum + IP_ROUND - 1) / IP_ROUND);
     const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
     const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
-    return launch_kernel("batch_inplace_electrons", kern, dim3(grid), dim3(IP_THREADS), bytes(), stream, pl, desc,
-                         counts, D, r.dens, r.dens_i, ef_pad, copies, epoch);
+    return launch_kernel("batch_inplace_electrons", kern, dim3(grid), dim3(IP_THREADS), bytes(), stream, pl, list,
+                         desc, counts, D, r.dens, ef_pad, copies, epoch);
+}
+
+int launch_batch_scatter(const InplacePlanes &pl, const CollList &list, const BatchDisc *desc, uint32_t D,
+                         uint64_t cap_sum, const StepRoles &r, uint32_t *ticket, cudaStream_t stream) {
+    if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch scatter: bad discharge count");
+    const size_t plan = (size_t)(D + 1) * sizeof(uint32_t);
+    auto kern = r.measure ? batch_scatter_kernel<true> : batch_scatter_kernel<false>;
+    const unsigned grid = persistent_grid(4, (cap_sum + IP_THREADS - 1) / IP_THREADS);
+    return launch_kernel("batch_scatter_electrons", kern, dim3(grid), dim3(IP_THREADS), plan, stream, pl, list, desc,
+                         D, r.dens, r.dens_i, ticket);
 }
 
 int launch_batch_collisions_i(const SidePlanes &ions, const BatchDisc *desc, uint32_t D, uint64_t cap_sum,

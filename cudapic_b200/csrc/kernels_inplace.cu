@@ -1,15 +1,15 @@
 // kernels_inplace.cu -- the in-place electron step of one discharge
-// (inplace.cuh): one persistent kernel, its launcher (shared with the
-// driver) and the C entry point; plus eduPIC's same-step collisions of new
-// electrons (an option of the driver).
+// (inplace.cuh): the stream pass and the scatter pass as two persistent
+// kernels, their launchers (shared with the driver) and the C entry points;
+// plus eduPIC's same-step collisions of new electrons (a driver option).
 //
 // Reference: the electron half of a time step, move_and_compact
 // (Rust-CUDA/src/main.rs:566-678) + check_collisions_e / collision_e
 // (:971-1165) + the next step's get_density (:356-406), as the compacting
 // fused step (kernels_step.cu) does it, but with every electron kept in its
 // slot: no compaction, 56 B of HBM traffic per electron (x, v, RNG read;
-// x, vx, RNG written) against 64 B, plus the colliders' scattered
-// velocities and RNG states.
+// x, vx, RNG written) against 64 B, plus the colliders' records and their
+// scattered velocities and RNG states.
 #include <algorithm>
 
 #include "batch_internal.h"
@@ -21,18 +21,17 @@ namespace cudapic {
 template <bool MEAS>
 __global__ void __launch_bounds__(IP_THREADS, 4)
     electron_inplace_kernel(const InplacePlanes pl, const float *__restrict__ efield,
-                            const float *__restrict__ sigma_tot_e, const float *__restrict__ cs, float sigma_max,
-                            uint32_t *n_e, uint32_t *n_i, uint32_t *spawned, uint32_t *ticket, float *dens_e,
-                            float *dens_i, const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int copies,
-                            uint32_t epoch, cudapic_wall_counters *wall, unsigned long long *coll,
-                            uint32_t *spawn_from) {
+                            const float *__restrict__ sigma_tot_e, float sigma_max, const uint32_t *n_active,
+                            const CollList list, uint32_t *count, float *dens_e,
+                            const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int copies, uint32_t epoch,
+                            cudapic_wall_counters *wall, uint32_t *spawn_from) {
     extern __shared__ __align__(128) unsigned char smem[];
     const InplaceSmem sm(smem, copies, ef_pad);
     inplace_smem_init(sm, copies, ef_pad);
     grid_dep_wait();
-    // read by every CTA before it takes its ticket; the last one publishes the new count
-    const uint32_t n = load_count(n_e, g.capacity, g.dev_err);
-    if (spawn_from && blockIdx.x == 0 && threadIdx.x == 0) *spawn_from = n;  // first slot of a spawned electron
+    const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
+    // the first slot the scatter pass can give a spawned electron (n_e does not change in this pass)
+    if (spawn_from && blockIdx.x == 0 && threadIdx.x == 0) *spawn_from = n;
     // balanced contiguous shares, multiples of 4 (16-byte aligned loads)
     const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 3u) & ~3u;
     const uint32_t beg = min(n, blockIdx.x * chunk);
@@ -40,20 +39,42 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
     StepDisc dc;
     dc.efield = efield;
     dc.sigma_tot = sigma_tot_e;
-    dc.cs = cs;
+    dc.cs = nullptr;
     dc.sigma_max = sigma_max;
     dc.factor = g.factor_e;
     dc.dt = g.dt_e;
-    dc.alive = spawned;
-    dc.n_i = n_i;
+    dc.alive = nullptr;
+    dc.n_i = nullptr;
     dc.dens = dens_e;
-    dc.dens_i = dens_i;
+    dc.dens_i = nullptr;
     dc.wall = wall;
-    dc.coll = coll;
+    dc.coll = nullptr;
     uint32_t live = 0;
-    inplace_segment<false, MEAS>(pl, dc, g, g, 0u, beg, end, n, sm, copies, ef_pad, epoch, live);
+    inplace_segment<false, MEAS>(pl, dc, g, g, 0u, beg, end, sm, copies, ef_pad, epoch, list, count, live);
     add_work(g.work, live);
-    publish_spawns(ticket, n_e, spawned, n, g.capacity, gridDim.x);
+}
+
+__global__ void __launch_bounds__(IP_THREADS)
+    electron_scatter_kernel(const InplacePlanes pl, const CollList list, const float *__restrict__ cs,
+                            uint32_t *count, uint32_t *ticket, uint32_t *n_e, uint32_t *n_i,
+                            const __grid_constant__ cudapic_grid g, float *dens_e, float *dens_i,
+                            unsigned long long *coll) {
+    grid_dep_wait();
+    const uint32_t n = min(*count, g.capacity);  // read before this CTA takes its ticket
+    for (uint32_t k = blockIdx.x * IP_THREADS + threadIdx.x; k < n; k += gridDim.x * IP_THREADS)
+        inplace_scatter(pl, list, 0u, k, cs, n_e, n_i, g, dens_e, dens_i);
+    // the last CTA counts the collisions and empties the list for the next step
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t t = atomicAdd(ticket, 1u);
+        if (t == gridDim.x - 1) {
+            __threadfence();
+            if (coll) atomicAdd(coll, (unsigned long long)n);
+            *count = 0u;
+            *ticket = 0u;
+        }
+    }
 }
 
 // eduPIC's semantics for electrons born in a step (C/eduPIC.cc:669-703: its
@@ -118,10 +139,10 @@ bool inplace_eligible(const void *const *planes, int count, uint32_t capacity) {
     return electron_step_eligible(planes, count, capacity);
 }
 
-int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, const float *cs,
-                            float sigma_max, uint32_t *n_e, uint32_t *n_i, uint32_t *scratch, float *dens_e,
-                            float *dens_i, const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
-                            unsigned long long *coll, uint32_t *spawn_from) {
+int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, float sigma_max,
+                            const uint32_t *n_active, const CollList &list, uint32_t *count, float *dens_e,
+                            const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
+                            uint32_t *spawn_from) {
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
     int copies = std::max(1, std::min(t.inplace_copies, IP_WARPS));
@@ -129,8 +150,7 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
     while (inplace_smem_bytes(copies, ef_pad) > budget && copies > 0) copies = copies / 2 < 4 ? 0 : copies / 2;
     if (inplace_smem_bytes(copies, ef_pad) > budget)
         return fail(CUDAPIC_ERR_ARG, "step_electrons_inplace: n_g too large");
-    const bool meas = wall || coll;
-    auto kern = meas ? electron_inplace_kernel<true> : electron_inplace_kernel<false>;
+    auto kern = wall ? electron_inplace_kernel<true> : electron_inplace_kernel<false>;
     int per_sm = 0;
     auto occupancy = [&]() {
         const size_t smem = inplace_smem_bytes(copies, ef_pad);
@@ -152,29 +172,58 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
     const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
     const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("step_electrons_inplace", kern, dim3(grid), dim3(IP_THREADS),
-                         inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, cs, sigma_max, n_e, n_i,
-                         scratch, scratch + 1, dens_e, dens_i, g, ef_pad, copies, epoch, wall, coll, spawn_from);
+                         inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, sigma_max, n_active, list,
+                         count, dens_e, g, ef_pad, copies, epoch, wall, spawn_from);
+}
+
+int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const float *cs, uint32_t *count,
+                            uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
+                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll) {
+    const unsigned grid = persistent_grid(4, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
+    return launch_kernel("scatter_colliders_e", electron_scatter_kernel, dim3(grid), dim3(IP_THREADS), 0, stream, pl,
+                         list, cs, count, ticket, n_e, n_i, g, dens_e, dens_i, coll);
 }
 
 }  // namespace cudapic
 
 using namespace cudapic;
 
-extern "C" int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, float *vy, float *vz,
-                                              uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
-                                              const float *total_cs_e, const float *cs, float sigma_max_e, float *i_x,
-                                              float *i_vx, float *i_vy, float *i_vz, uint32_t *n_e, uint32_t *n_i,
-                                              uint32_t *scratch, float *e_next_density, float *i_next_density,
-                                              const cudapic_grid *grid, cudapic_stream_t stream) {
+extern "C" int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy,
+                                              const float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
+                                              uint32_t *rng3, const float *total_cs_e, float sigma_max_e,
+                                              const uint32_t *n_e, uint32_t *coll_slot, float *coll_vx,
+                                              float *coll_vy, float *coll_vz, uint32_t *n_colliders,
+                                              float *e_next_density, const cudapic_grid *grid,
+                                              cudapic_stream_t stream) {
     CUDAPIC_CHECK(validate_grid(grid));
-    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && cs && i_x && i_vx &&
-                        i_vy && i_vz && n_e && n_i && scratch && e_next_density && i_next_density,
+    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && n_e && coll_slot &&
+                        coll_vx && coll_vy && coll_vz && n_colliders && e_next_density,
                     "step_electrons_inplace: null pointer");
     CUDAPIC_REQUIRE(sigma_max_e >= 0.0f, "step_electrons_inplace: sigma_max_e must be the largest entry of total_cs_e");
     const void *planes[8] = {x, vx, vy, vz, rng0, rng1, rng2, rng3};
     CUDAPIC_REQUIRE(inplace_eligible(planes, 8, grid->capacity),
                     "step_electrons_inplace: planes must be 16-byte aligned and capacity a multiple of 4");
+    const InplacePlanes pl{x, vx, const_cast<float *>(vy), const_cast<float *>(vz), rng0, rng1, rng2, rng3,
+                           nullptr, nullptr, nullptr, nullptr};
+    const CollList list{coll_slot, coll_vx, coll_vy, coll_vz};
+    return launch_electron_inplace(pl, efield, total_cs_e, sigma_max_e, n_e, list, n_colliders, e_next_density,
+                                   *grid, (cudaStream_t)stream, nullptr, nullptr);
+}
+
+extern "C" int cudapic_scatter_colliders_e(float *x, float *vx, float *vy, float *vz, uint32_t *rng0,
+                                           uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, const float *cs,
+                                           const uint32_t *coll_slot, const float *coll_vx, const float *coll_vy,
+                                           const float *coll_vz, uint32_t *n_colliders, uint32_t *ticket,
+                                           float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *n_e,
+                                           uint32_t *n_i, float *e_next_density, float *i_next_density,
+                                           const cudapic_grid *grid, cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && cs && coll_slot && coll_vx && coll_vy &&
+                        coll_vz && n_colliders && ticket && i_x && i_vx && i_vy && i_vz && n_e && n_i,
+                    "scatter_colliders_e: null pointer");
     const InplacePlanes pl{x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz};
-    return launch_electron_inplace(pl, efield, total_cs_e, cs, sigma_max_e, n_e, n_i, scratch, e_next_density,
-                                   i_next_density, *grid, (cudaStream_t)stream, nullptr, nullptr, nullptr);
+    const CollList list{const_cast<uint32_t *>(coll_slot), const_cast<float *>(coll_vx), const_cast<float *>(coll_vy),
+                        const_cast<float *>(coll_vz)};
+    return launch_electron_scatter(pl, list, cs, n_colliders, ticket, n_e, n_i, *grid, (cudaStream_t)stream,
+                                   e_next_density, i_next_density, nullptr);
 }

@@ -193,112 +193,6 @@ __global__ void __launch_bounds__(POIS_MAX_THREADS)
                         zero_b);
 }
 
-// The same solve by ONE warp for n_g <= 32 PT: lane l owns the PT consecutive
-// nodes [l PT, l PT + PT), every sum is a register prefix plus a warp-shuffle
-// scan of the lane totals, and the field's neighbours across lane
-// boundaries come by shuffle too: no shared memory and no block barrier on
-// the step's critical path (the CTA-wide solve above waits at six barriers).
-template <typename T, int PT>
-__global__ void __launch_bounds__(32)
-    poisson_warp_kernel(const float *__restrict__ e_density, const float *__restrict__ i_density,
-                        float *__restrict__ pot_out, float *__restrict__ efield_out, float pot0_arg,
-                        const float *__restrict__ pot0_table, uint32_t *__restrict__ step_counter,
-                        const cudapic_grid g, float *__restrict__ zero_a, float *__restrict__ zero_b) {
-    grid_dep_wait();
-    const int lane = threadIdx.x;
-    const int n = (int)g.n_g;
-    float p0 = pot0_arg;
-    if (pot0_table) {
-        uint32_t t = 0;
-        if (lane == 0) {
-            t = *step_counter;
-            *step_counter = t + 1;
-        }
-        t = __shfl_sync(0xffffffffu, t, 0);
-        p0 = pot0_table[t % g.n_t];
-    }
-    const T pot0 = (T)p0;
-    const T e_charge = sizeof(T) == 8 ? (T)1.60217662e-19 : (T)g.e_charge;
-    const T alpha = sizeof(T) == 8 ? (T)(-g.dx * g.dx / 8.85418781e-12) : (T)g.alpha;
-    const int first = lane * PT;
-    T rho[PT], G[PT];
-    T local = 0;
-#pragma unroll
-    for (int j = 0; j < PT; ++j) {
-        const int i = first + j;
-        T rh = 0, gi = 0;
-        if (i < n) {
-            if (sizeof(T) == 8)
-                rh = e_charge * ((T)i_density[i] - (T)e_density[i]);
-            else
-                rh = e_charge * (T)(i_density[i] - e_density[i]);
-            if (i != 0) {
-                T fi = alpha * rh - (i == 1 ? pot0 : T(0));
-                gi = (T)i * fi;
-            }
-        }
-        rho[j] = rh;
-        local += gi;
-        G[j] = local;
-    }
-    // the next-step accumulators of the driver, cleared once the densities are read
-    __syncwarp();
-    for (int k = lane; k < n; k += 32) {
-        if (zero_a) zero_a[k] = 0.0f;
-        if (zero_b) zero_b[k] = 0.0f;
-    }
-    T off = warp_incl_scan(local, lane) - local;
-    T r[PT], R[PT];
-    local = 0;
-#pragma unroll
-    for (int j = 0; j < PT; ++j) {
-        const int i = first + j;
-        T ri = 0;
-        if (i != 0 && i < n - 1) {
-            T hi = -(G[j] + off) / ((T)i + T(1));
-            ri = hi / (T)i;
-        }
-        r[j] = ri;
-        local += ri;
-        R[j] = local;
-    }
-    off = warp_incl_scan(local, lane) - local;
-    // R_total = R[n - 2], held by lane (n - 2) / PT
-    T mine = 0;
-#pragma unroll
-    for (int j = 0; j < PT; ++j)
-        if (first + j == n - 2) mine = R[j] + off;
-    const T r_total = __shfl_sync(0xffffffffu, mine, (n - 2) / PT);
-    T pot[PT];
-#pragma unroll
-    for (int j = 0; j < PT; ++j) {
-        const int i = first + j;
-        T p = 0;
-        if (i == 0) p = pot0;
-        else if (i < n - 1) p = (T)i * (r_total - (R[j] + off) + r[j]);
-        pot[j] = p;
-    }
-    const T left = __shfl_up_sync(0xffffffffu, pot[PT - 1], 1);
-    const T right = __shfl_down_sync(0xffffffffu, pot[0], 1);
-    const T inv_dx = sizeof(T) == 8 ? (T)(1.0 / g.dx) : (T)g.inv_dx;
-    const T half_inv_dx = sizeof(T) == 8 ? (T)(0.5 / g.dx) : (T)g.half_inv_dx;
-    const T half_dx_over_eps = sizeof(T) == 8 ? (T)(g.dx / (2.0 * 8.85418781e-12)) : (T)g.half_dx_over_eps;
-#pragma unroll
-    for (int j = 0; j < PT; ++j) {
-        const int i = first + j;
-        if (i < n) {
-            const T pm = j > 0 ? pot[j > 0 ? j - 1 : 0] : left;
-            const T pp = j < PT - 1 ? pot[j < PT - 1 ? j + 1 : 0] : right;
-            T e;
-            if (i == 0) e = (pot[j] - pp) * inv_dx - rho[j] * half_dx_over_eps;
-            else if (i == n - 1) e = (pm - pot[j]) * inv_dx + rho[j] * half_dx_over_eps;
-            else e = (pm - pp) * half_inv_dx;
-            pot_out[i] = (float)pot[j];
-            efield_out[i] = (float)e;
-        }
-    }
-}
-
 // solve_poisson_dps_flexible: the same closed form with runtime n, dx and
 // both Dirichlet values (used by the reference's Hakim convergence test,
 // Rust-CUDA/src/main.rs:1895-1981).  FP64 sums.
@@ -384,28 +278,10 @@ int launch_poisson_t(const float *e_density, const float *i_density, float *pot,
                          efield, pot0, pot0_table, step_counter, g, zero_a, zero_b);
 }
 
-template <typename T, int PT>
-int launch_poisson_warp_t(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
-                          const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
-                          cudaStream_t stream, float *zero_a, float *zero_b) {
-    return launch_kernel("solve_poisson_scan", poisson_warp_kernel<T, PT>, dim3(1), dim3(32), 0, stream, e_density,
-                         i_density, pot, efield, pot0, pot0_table, step_counter, g, zero_a, zero_b);
-}
-
 template <typename T>
 int launch_poisson_pt(const float *e_density, const float *i_density, float *pot, float *efield, float pot0,
                       const float *pot0_table, uint32_t *step_counter, const cudapic_grid &g,
                       cudaStream_t stream, float *zero_a, float *zero_b) {
-    // up to 1024 nodes: one warp (no block barriers on the step's critical path)
-    if (g.n_g <= 32 * 8)
-        return launch_poisson_warp_t<T, 8>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g,
-                                           stream, zero_a, zero_b);
-    if (g.n_g <= 32 * 16)
-        return launch_poisson_warp_t<T, 16>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g,
-                                            stream, zero_a, zero_b);
-    if (g.n_g <= 32 * 32)
-        return launch_poisson_warp_t<T, 32>(e_density, i_density, pot, efield, pot0, pot0_table, step_counter, g,
-                                            stream, zero_a, zero_b);
     int threads, pt;
     poisson_shape(g.n_g, threads, pt);
     switch (pt) {

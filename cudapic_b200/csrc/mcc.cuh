@@ -165,8 +165,6 @@ __device__ __forceinline__ void deposit_global(float *dens, float xv, const cuda
 // (may be null): next-step densities that also receive the spawned
 // electron / ion.  Slots (i and the spawns' claimed slots) are relative to
 // element `off` of the planes (a discharge of a batch's pool; 0 otherwise).
-// e_base: spawned electrons take slots e_base + k, k claimed from alive_e
-// (a count of spawns when e_base > 0) below capacity - e_base.
 // ALG: the sines and cosines of the Euler angles, of the scattering angles
 // chi = acos(c) and of eta + pi from their algebraic forms (euler_angles_alg,
 // sincos_of_acos, sin(eta + pi) = -sin eta) instead of evaluating the
@@ -178,7 +176,7 @@ static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_
                                                     const float *__restrict__ cs, float *x, float *vx, float *vy,
                                                     float *vz, float *ix, float *ivx, float *ivy, float *ivz,
                                                     uint32_t *alive_e, uint32_t *alive_i, const cudapic_grid &g,
-                                                    float *dep_e, float *dep_i, uint32_t e_base = 0u) {
+                                                    float *dep_e, float *dep_i) {
     const float exc_j = 11.5f * E_CHARGE_F;
     const float ion_j = 15.8f * E_CHARGE_F;
     float gx = vxi, gy = vyi, gz = vzi;
@@ -230,8 +228,7 @@ static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_
         rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
         const float xi = x[off + i];
         uint32_t slot;
-        if (claim_slot(alive_e, g.capacity - e_base, slot)) {
-            slot += e_base;
+        if (claim_slot(alive_e, g.capacity, slot)) {
             x[off + slot] = xi;
             vx[off + slot] = wx + g.f2 * ngx;
             vy[off + slot] = wy + g.f2 * ngy;

@@ -109,9 +109,10 @@ void destroy_graphs(cudapic_state *s) {
 // [ion collisions] -> [measurement]; the kernels publish the particle counts
 // themselves (StepLink), so the step holds no copy or memset node.  The
 // electron step is the compacting fused kernel (kernels_step.cu) when
-// `compact` or when the in-place step is off, else the in-place step
-// (kernels_inplace.cu: electrons stay in their slots, absorbed ones are
-// marked dead, colliders are scattered in the same pass).  Either way an
+// `compact` or when the in-place step is off, else the in-place stream and
+// scatter passes (kernels_inplace.cu: electrons stay in their slots,
+// absorbed ones are marked dead, colliders recorded in the other side's
+// planes and scattered by the second kernel).  Either way an
 // electron draws from the RNG stream of the slot it occupies when the step
 // starts.  Returns CUDAPIC_ERR_NOT_SUPPORTED, having
 // enqueued nothing, when the electron planes are not aligned for the fused
@@ -141,10 +142,15 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
         const InplacePlanes pl{s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
                                s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3],
                                s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si]};
-        CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->cs, s->sigma_max_e, s->n_e(), s->n_i(),
-                                              s->counters + CTR_SPAWNED, e_next, i_acc, g, st,
-                                              s->measure ? s->wall : nullptr, s->measure ? s->mcount : nullptr,
-                                              s->counters + CTR_SPAWN_FROM));
+        // the collider records live in the other side's planes until the next compaction
+        const CollList list{reinterpret_cast<uint32_t *>(s->x[E][se ^ 1]), s->vx[E][se ^ 1], s->vy[E][se ^ 1],
+                            s->vz[E][se ^ 1]};
+        CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->sigma_max_e, s->n_e(), list,
+                                              s->counters + CTR_COLL_COUNT, e_next, g, st,
+                                              s->measure ? s->wall : nullptr, s->counters + CTR_SPAWN_FROM));
+        CUDAPIC_CHECK(launch_electron_scatter(pl, list, s->cs, s->counters + CTR_COLL_COUNT,
+                                              s->counters + CTR_COLL_TICKET, s->n_e(), s->n_i(), g, st, e_next, i_acc,
+                                              s->measure ? s->mcount : nullptr));
         if (s->spawn_collide)
             CUDAPIC_CHECK(launch_spawn_collide(pl, s->sigma_tot_e, s->cs, s->counters + CTR_SPAWN_FROM, s->n_e(),
                                                s->n_i(), g, st, e_next, i_acc, s->measure ? s->mcount : nullptr));

@@ -21,7 +21,7 @@ struct cudapic_state {
     int side[2] = {0, 0};
     uint32_t *rng[2][4] = {};
     // counters block: n_e, n_i, alive, step, dev_err, alive_i, ticket, pad, work (u64 at +32),
-    // [12] in-place step's spawn counter, [13] its CTA ticket, [14] its first spawn slot
+    // [12] in-place step's collider count, [13] its scatter ticket, [14] its first spawn slot
     uint32_t *counters = nullptr;
     float *efield = nullptr, *pot = nullptr, *pot0_table = nullptr;
     // Charge densities, double-buffered for the fused step: [cur] feeds the

@@ -122,15 +122,24 @@ def step_electrons_noalloc(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx,
     check(lib.cudapic_step_electrons_noalloc(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, src_x)))
 
 
-def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, cs, sigma_max_e, i_x, i_vx,
-                           i_vy, i_vz, n_e, n_i, scratch, e_next_density, i_next_density, grid, stream=None):
-    """In-place electron step: push, absorption (x set to CUDAPIC_DEAD_X),
-    collision test, scattering and next-step deposit with every electron
-    kept in its slot; spawns appended at n_e and n_i (scratch: two zero
-    words)."""
-    head = [_ptr(a) for a in (efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, cs)]
-    tail = [_ptr(a) for a in (i_x, i_vx, i_vy, i_vz, n_e, n_i, scratch, e_next_density, i_next_density)]
+def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, sigma_max_e, n_e, coll_slot,
+                           coll_vx, coll_vy, coll_vz, n_colliders, e_next_density, grid, stream=None):
+    """In-place electron step, stream pass: push, absorption (x set to
+    CUDAPIC_DEAD_X), collision test and next-step deposit with every electron
+    kept in its slot; colliders recorded (slot, vx, vy, vz) in the coll_*
+    planes."""
+    head = [_ptr(a) for a in (efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e)]
+    tail = [_ptr(a) for a in (n_e, coll_slot, coll_vx, coll_vy, coll_vz, n_colliders, e_next_density)]
     check(lib.cudapic_step_electrons_inplace(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, x)))
+
+
+def scatter_colliders_e(x, vx, vy, vz, rng0, rng1, rng2, rng3, cs, coll_slot, coll_vx, coll_vy, coll_vz, n_colliders,
+                        ticket, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density, grid, stream=None):
+    """In-place electron step, scatter pass over the recorded colliders
+    (spawns appended at n_e and n_i)."""
+    args = [_ptr(a) for a in (x, vx, vy, vz, rng0, rng1, rng2, rng3, cs, coll_slot, coll_vx, coll_vy, coll_vz,
+                              n_colliders, ticket, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density)]
+    check(lib.cudapic_scatter_colliders_e(*args, _g(grid), _stream(stream, x)))
 
 
 def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz,

@@ -7,7 +7,7 @@ Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
 check_collisions_e, check_collisions_e_deposit, check_collisions_i and
 step_electrons (the *_deposit variants also deposit the next step's density;
 step_electrons is the fused driver's compacting electron kernel,
-step_electrons_inplace its in-place step).  Prints one JSON line with the median time, the particle
+step_electrons_inplace the stream pass of its in-place step).  Prints one JSON line with the median time, the particle
 count and the algorithmic bytes per launch.
 """
 import argparse
@@ -50,7 +50,7 @@ def main():
     pot = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
     ef = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
     alive = u32(0)
-    scratch = torch.zeros(2, dtype=torch.int32, device="cuda")
+    ccount = u32(0)
     fns = {
         "get_density": (lambda: K.get_density(b.x[0], dens, ne_c, g, stream=s), lambda: dens.zero_(), n_e),
         "solve_poisson": (lambda: K.solve_poisson_scan_f32(b.e_density, b.i_density, pot, ef, 250.0, g, stream=s),
@@ -75,11 +75,11 @@ def main():
             stream=s), lambda: (alive.zero_(), alive_i.fill_(n_i), dens.zero_()), n_e),
         "check_collisions_i": (lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                             *b.rng[1], g, stream=s), None, n_i),
-        # the in-place step (each launch advances the live planes by one step)
+        # the in-place step's stream pass (each launch advances the live planes by one step)
         "step_electrons_inplace": (lambda: K.step_electrons_inplace(
-            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.cs, b.sigma_max_e, b.x[1],
-            b.vx[1], b.vy[1], b.vz[1], ne_c, alive_i, scratch, dens, pot, g, stream=s),
-            lambda: (ne_c.fill_(n_e), alive_i.fill_(n_i), dens.zero_()), n_e),
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.sigma_max_e, ne_c, b.tmp_x[0],
+            b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], ccount, dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()),
+            n_e),
     }
     fn, pre, n = fns[a.kernel]
     from cudapic_b200.timing import L2Flusher, time_launch

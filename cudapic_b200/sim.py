@@ -297,7 +297,8 @@ class GpuBatch:
         """True when the batch's electron steps run in place between compacting ones."""
         return all(st.inplace for st in self.states)
 
-    BATCH_KERNELS = ("poisson", "ion_push", "electron_step", "ion_collisions", "electron_inplace")
+    BATCH_KERNELS = ("poisson", "ion_push", "electron_step", "ion_collisions", "electron_inplace",
+                     "electron_scatter")
 
     def profile_steps(self, n_steps):
         """Runs n_steps uncaptured with CUDA events around every kernel

@@ -245,25 +245,36 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
 /* The electron step in place (no reference counterpart: the electron half
  * of the reference's step, move_and_compact + check_collisions_e + the next
  * get_density, Rust-CUDA/src/main.rs:566-678, 971-1165, 356-406, with every
- * electron kept in its slot).  Pushes electrons [0, *n_e), tests them for
- * collision (one draw of each slot's stream), scatters the colliders
- * (collision_e, the stream continuing past the test draw) and deposits the
- * survivors' new positions ADDED to e_next_density.  x, vx, the RNG state
- * and a collider's vy, vz are written back to the same slots.  An electron
- * that leaves through an electrode is marked in its slot with x = -1
- * (CUDAPIC_DEAD_X): later in-place steps skip such slots, and
- * cudapic_step_electrons drops them while compacting.  Spawned electrons
- * take slots *n_e, *n_e + 1, ... (*n_e is updated when the kernel ends),
- * spawned ions slots *n_i, ... of i_*; both are deposited into the next
- * densities.  scratch: two words, zero on entry, zero again on return.
+ * electron kept in its slot).  Two launches:
+ *  - cudapic_step_electrons_inplace pushes electrons [0, *n_e), tests them
+ *    for collision (one draw of each slot's stream) and deposits the
+ *    survivors' new positions ADDED to e_next_density; x, vx and the RNG
+ *    state are written back to the same slots (vy, vz unchanged).  An
+ *    electron that leaves through an electrode is marked in its slot with
+ *    x = -1 (CUDAPIC_DEAD_X): later in-place steps skip such slots, and
+ *    cudapic_step_electrons drops them while compacting.  Each collider is
+ *    recorded (slot, vx, vy, vz) in the four coll_* planes (capacity entries
+ *    each) and counted in *n_colliders (zero on entry).  *n_e is unchanged.
+ *  - cudapic_scatter_colliders_e scatters the recorded colliders in place,
+ *    continuing each slot's stream past the test draw (collision_e);
+ *    spawned electrons take slots *n_e, *n_e + 1, ... (updating *n_e),
+ *    spawned ions slots *n_i, ... of i_*; both are deposited into the next
+ *    densities.  Its last CTA resets *n_colliders and *ticket (zero on
+ *    entry) to zero.
  * Same plane alignment and capacity rules as cudapic_step_electrons. */
 #define CUDAPIC_DEAD_X (-1.0f)
-int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, float *vy, float *vz, uint32_t *rng0,
-                                   uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, const float *total_cs_e,
-                                   const float *cs, float sigma_max_e, float *i_x, float *i_vx, float *i_vy,
-                                   float *i_vz, uint32_t *n_e, uint32_t *n_i, uint32_t *scratch,
-                                   float *e_next_density, float *i_next_density, const cudapic_grid *grid,
+int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy, const float *vz,
+                                   uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
+                                   const float *total_cs_e, float sigma_max_e, const uint32_t *n_e,
+                                   uint32_t *coll_slot, float *coll_vx, float *coll_vy, float *coll_vz,
+                                   uint32_t *n_colliders, float *e_next_density, const cudapic_grid *grid,
                                    cudapic_stream_t stream);
+int cudapic_scatter_colliders_e(float *x, float *vx, float *vy, float *vz, uint32_t *rng0, uint32_t *rng1,
+                                uint32_t *rng2, uint32_t *rng3, const float *cs, const uint32_t *coll_slot,
+                                const float *coll_vx, const float *coll_vy, const float *coll_vz,
+                                uint32_t *n_colliders, uint32_t *ticket, float *i_x, float *i_vx, float *i_vy,
+                                float *i_vz, uint32_t *n_e, uint32_t *n_i, float *e_next_density,
+                                float *i_next_density, const cudapic_grid *grid, cudapic_stream_t stream);
 
 /* cudapic_step_electrons for callers that cannot allocate device memory
  * (a host whose device memory belongs to its own pool or framework and that
@@ -464,8 +475,9 @@ int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps);
  * cudapic_check_collisions_e_deposit.  off: the reference's launch sequence. */
 int cudapic_state_set_fused(cudapic_state *s, int on);
 /* Fused mode, on (default): between compacting steps the electrons are
- * stepped in place (cudapic_step_electrons_inplace: no compaction, absorbed
- * electrons marked in their slots, spawns appended).  The step before every N_SUB-th step and the last step
+ * stepped in place (cudapic_step_electrons_inplace + cudapic_scatter_
+ * colliders_e: no compaction, absorbed electrons marked in their slots,
+ * spawns appended).  The step before every N_SUB-th step and the last step
  * of every cudapic_state_run_steps call run the compacting fused kernel,
  * which drops the marked slots, so the planes are compact between calls.
  * off: every step compacts.  The captured graphs are rebuilt. */
@@ -614,8 +626,9 @@ int cudapic_batch_synchronize(cudapic_batch *b);
 #define CUDAPIC_BATCH_K_ION_PUSH 1          /* ion push + compaction + deposit         */
 #define CUDAPIC_BATCH_K_ELECTRON_STEP 2     /* compacting fused electron step          */
 #define CUDAPIC_BATCH_K_ION_COLLISIONS 3    /* ion MCC                                 */
-#define CUDAPIC_BATCH_K_ELECTRON_INPLACE 4  /* in-place electron step                 */
-#define CUDAPIC_BATCH_KERNELS 5
+#define CUDAPIC_BATCH_K_ELECTRON_INPLACE 4  /* in-place electron step, stream pass     */
+#define CUDAPIC_BATCH_K_ELECTRON_SCATTER 5  /* in-place electron step, scatter pass    */
+#define CUDAPIC_BATCH_KERNELS 6
 int cudapic_batch_profile_steps(cudapic_batch *b, uint64_t n_steps, double ms[CUDAPIC_BATCH_KERNELS],
                                 uint64_t launches[CUDAPIC_BATCH_KERNELS]);
 cudapic_stream_t cudapic_batch_stream(const cudapic_batch *b);

@@ -150,17 +150,17 @@ def check_step_electrons_with_dead(K, oracle, tables, dev_tables, g, ph, x, vx, 
 
 def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, cap, dead, seed=(3, 1, 4, 1),
                        n_i0=1000, dens_tol=2e-5):
-    """The in-place electron step through the C ABI against the oracle's
-    move_and_compact + check_collisions_e over the live slots, every electron
-    keeping its slot:
+    """The in-place electron step (stream pass + scatter pass) through the C
+    ABI against the oracle's move_and_compact + check_collisions_e over the
+    live slots, every electron keeping its slot:
       * every slot [0, n): x, vx, vy, vz and the four RNG words bit-exact
         (absorbed electrons marked x = -1 with vx, vy, vz and RNG untouched,
         emptied slots untouched);
-      * spawned electrons at slots n, n + 1, ... and spawned ions: bit-exact
-        as sets; the new counts published;
+      * one collider record per collision event; spawned electrons at slots
+        n, n + 1, ... and spawned ions: bit-exact as sets;
       * the next-step densities within the deposit tolerance of a fresh FP64
         deposit of the electrons (and spawned ions) present afterwards;
-      * the two scratch words back at zero.
+      * the collider count and the scatter ticket back at zero.
     Returns (survivors, electron slots after, ions after, colliders)."""
     cs, se, _ = tables
     dcs, dse, _ = dev_tables
@@ -189,12 +189,18 @@ def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, 
     e_d = [dev(pad(a)) for a in (x, vx, vy, vz)]
     r_d = [dev(p) for p in rng]
     i_d = [dev(pad(np.full(n_i0, 0.0125, np.float32))) for _ in range(4)]
-    n_e, n_i, scratch = counter(n), counter(n_i0), zeros(2, np.uint32)
+    n_e, n_i = counter(n), counter(n_i0)
+    rec = [zeros(cap, np.uint32)] + [zeros(cap) for _ in range(3)]   # collider records: slot, vx, vy, vz
+    cnt, ticket = counter(0), counter(0)
     de, di = zeros(len(ef)), zeros(len(ef))
-    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, dcs, float(se.max()), *i_d, n_e, n_i, scratch, de, di, g)
+    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, float(se.max()), n_e, *rec, cnt, de, g)
+    n_coll = int(host(cnt)[0])
+    assert n_coll == int(np.count_nonzero(events))
+    assert int(host(n_e)[0]) == n   # unchanged by the stream pass
+    K.scatter_colliders_e(*e_d, *r_d, dcs, *rec, cnt, ticket, *i_d, n_e, n_i, de, di, g)
     ne, ni = int(host(n_e)[0]), int(host(n_i)[0])
     assert (ne - n, ni) == (ne_ref - m, ni_ref)
-    assert np.array_equal(host(scratch), np.zeros(2, np.uint32))
+    assert int(host(cnt)[0]) == 0 and int(host(ticket)[0]) == 0
     got = [host(d) for d in e_d]
     for k in range(4):
         assert np.array_equal(got[k][:n].view(np.uint32), exp[k][:n].view(np.uint32)), k
