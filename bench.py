@@ -459,16 +459,16 @@ def kernel_breakdown(st, K, reps, flush):
         dens.zero_()
     timed("step_electrons", step_e, n_e, 64, pre=reset_step)
     # the in-place step's two passes (on the live planes: each launch advances them by one step);
-    # the collider records go to the other side's planes, as in the driver
-    rec = (b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0])
+    # the collider records go to the other sides' planes, as in the driver
+    rec = (b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], b.tmp_x[1], b.tmp_vx[1], b.tmp_vy[1], b.tmp_vz[1])
     cnt, ticket = dev_u32(0), dev_u32(0)
 
     def stream_pass():
         K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e,
-                                 b.sigma_max_e, ne_c, *rec, cnt, dens, g, stream=stream.cuda_stream)
+                                 b.sigma_max_e, ne_c, rec, cnt, dens, g, stream=stream.cuda_stream)
 
     def scatter_pass():
-        K.scatter_colliders_e(b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.cs, *rec, cnt, ticket, b.x[1], b.vx[1],
+        K.scatter_colliders_e(b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.cs, rec, cnt, ticket, b.x[1], b.vx[1],
                               b.vy[1], b.vz[1], ne_c, n_i_c, dens, dens_i, g, stream=stream.cuda_stream)
     timed("step_electrons_inplace", stream_pass, n_e, 56, pre=lambda: (cnt.zero_(), ne_c.fill_(n_e), dens.zero_()))
     n_coll = int(cnt.item())

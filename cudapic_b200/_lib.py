@@ -154,8 +154,8 @@ SIGNATURES = {
     "cudapic_state_load": [_VP, C.c_char_p],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],
-    "cudapic_step_electrons_inplace": [_VP] * 10 + [_F] + [_VP] * 7 + [_GP, _VP],
-    "cudapic_scatter_colliders_e": [_VP] * 23 + [_GP, _VP],
+    "cudapic_step_electrons_inplace": [_VP] * 10 + [_F] + [_VP] * 4 + [_GP, _VP],
+    "cudapic_scatter_colliders_e": [_VP] * 20 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
     "cudapic_accumulate_density": [_VP, _VP, _GP, _VP],
     "cudapic_accumulate_eepf": [_VP] * 7 + [_GP, _VP],

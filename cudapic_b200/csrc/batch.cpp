@@ -281,13 +281,16 @@ int enqueue_batch_step(cudapic_batch *b, bool ion_step, bool measure, bool compa
     r.dens = b->ecur ^ 1;
     if (b->inplace && !compact) {
         // in place: the electrons stay on their side, collider records go to
-        // the other side's planes, the scatter pass follows
+        // the other sides' planes of both species, the scatter pass follows
         const SidePlanes es = side_planes(b, 0, b->se);
         const SidePlanes is = side_planes(b, 1, b->si);
         const InplacePlanes pl{es.x, es.vx, es.vy, es.vz, es.rng0, es.rng1, es.rng2, es.rng3,
                                is.x, is.vx, is.vy, is.vz};
         const SidePlanes os = side_planes(b, 0, b->se ^ 1);
-        const CollList list{reinterpret_cast<uint32_t *>(os.x), os.vx, os.vy, os.vz};
+        const SidePlanes oi = side_planes(b, 1, b->si ^ 1);
+        const CollList list{reinterpret_cast<uint32_t *>(os.x), os.vx, os.vy, os.vz,
+                            reinterpret_cast<uint32_t *>(oi.x), reinterpret_cast<uint32_t *>(oi.vx),
+                            reinterpret_cast<uint32_t *>(oi.vy), reinterpret_cast<uint32_t *>(oi.vz)};
         CUDAPIC_CHECK(begin(CUDAPIC_BATCH_K_ELECTRON_INPLACE));
         CUDAPIC_CHECK(launch_batch_inplace(pl, list, b->desc, b->counts, D, b->cap_sum, b->max_n_g, r, st));
         CUDAPIC_CHECK(finish(CUDAPIC_BATCH_K_ELECTRON_INPLACE));

@@ -49,12 +49,14 @@ struct InplacePlanes {
     float *ix, *ivx, *ivy, *ivz;
 };
 
-// The collider list of an in-place step: one record (slot, vx, vy, vz) per
-// collider in four planes of capacity entries (the other side's x, vx, vy,
-// vz planes, which the in-place step does not otherwise use).
+// The collider list of an in-place step: one record (slot, vx, vy, vz and
+// the RNG state past the test draw) per collider in eight planes of
+// capacity entries: the other side's x, vx, vy, vz planes of the electrons
+// and of the ions, which an in-place electron step does not otherwise use.
 struct CollList {
     uint32_t *slot;
     float *vx, *vy, *vz;
+    uint32_t *r0, *r1, *r2, *r3;
 };
 
 // Counters-block words of the in-place step (after the fused step's words:

@@ -13,13 +13,14 @@
 //    same slots (vy, vz do not change in the push: 24 B written per electron
 //    against 32 B read).  An absorbed electron leaves its slot with
 //    x = DEAD_X; later passes skip it.  A collider's record (slot, vx, vy,
-//    vz) goes to its warp's queue in shared memory and, 32 at a time, to the
-//    collider list (one atomicAdd per 32 records, coalesced stores): four
-//    planes of the other side, which the in-place step does not otherwise
-//    use, so the list holds one record for every slot;
+//    vz and the RNG state past the test draw) goes to its warp's queue in
+//    shared memory and, 32 at a time, to the collider list (one atomicAdd
+//    per 32 records, coalesced stores): eight planes of the other sides of
+//    both species, which an in-place electron step does not otherwise use,
+//    so the list holds one record for every slot;
 //  * scatter pass (inplace_scatter): one thread per listed collider reads
-//    its record (coalesced), continues the slot's RNG stream past the test
-//    draw, scatters (collision_e, :1035-1165) and writes velocity and RNG
+//    its record (coalesced, no gather from the slot), continues the RNG
+//    stream, scatters (collision_e, :1035-1165) and writes velocity and RNG
 //    state back to the slot; spawned electrons are appended after the live
 //    slots, spawned ions to the ion side.
 // The stream pass keeps the collision code out of its registers (the
@@ -41,8 +42,8 @@ constexpr int IP_THREADS = 256;
 constexpr int IP_WARPS = IP_THREADS / 32;
 constexpr int IP_ROW = 4;           // slots per thread and round (one 16-byte load per plane)
 constexpr int IP_ROUND = IP_THREADS * IP_ROW;
-constexpr int IP_QREC = 32 + 32 * IP_ROW;  // per-warp collider queue: < 32 left over + one round
-constexpr int IP_RECW = 4;          // words per record: slot, vx, vy, vz
+constexpr int IP_QREC = 64;         // per-warp collider queue: < 32 left over + one row of a round
+constexpr int IP_RECW = 8;          // words per record: slot, vx, vy, vz, rng0..3
 
 // Dynamic shared memory: E[ef_pad] f32, the 64-bit deposit accumulator
 // [ef_pad], [copies][ef_pad] fixed-point histograms, the collider records
@@ -118,6 +119,10 @@ __device__ __forceinline__ void flush_records(const InplaceSmem &sm, uint32_t &q
         list.vx[base + k] = __uint_as_float(sm.r(1, warp, k));
         list.vy[base + k] = __uint_as_float(sm.r(2, warp, k));
         list.vz[base + k] = __uint_as_float(sm.r(3, warp, k));
+        list.r0[base + k] = sm.r(4, warp, k);
+        list.r1[base + k] = sm.r(5, warp, k);
+        list.r2[base + k] = sm.r(6, warp, k);
+        list.r3[base + k] = sm.r(7, warp, k);
     }
     __syncwarp();
     const uint32_t rest = qn - n;
@@ -239,7 +244,8 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
             *reinterpret_cast<uint4 *>(pl.rng2 + i0) = make_uint4(s[2][0], s[2][1], s[2][2], s[2][3]);
             *reinterpret_cast<uint4 *>(pl.rng3 + i0) = make_uint4(s[3][0], s[3][1], s[3][2], s[3][3]);
         }
-        // (4) queue this round's colliders as records (warp-synchronous)
+        // (4) queue this round's colliders as records (warp-synchronous), a
+        //     flush after every row keeps the queue below 64
         if (__ballot_sync(0xffffffffu, coll != 0)) {
 #pragma unroll
             for (int u = 0; u < IP_ROW; ++u) {
@@ -251,11 +257,15 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
                     sm.r(1, warp, pos) = __float_as_uint(vx[u]);
                     sm.r(2, warp, pos) = __float_as_uint(vy[u]);
                     sm.r(3, warp, pos) = __float_as_uint(vz[u]);
+                    sm.r(4, warp, pos) = s[0][u];
+                    sm.r(5, warp, pos) = s[1][u];
+                    sm.r(6, warp, pos) = s[2][u];
+                    sm.r(7, warp, pos) = s[3][u];
                 }
                 qn += __popc(cm);
+                __syncwarp();
+                if (qn >= 32) flush_records(sm, qn, false, list, count);
             }
-            __syncwarp();
-            if (qn >= 32) flush_records(sm, qn, false, list, count);
         }
     }
     flush_records(sm, qn, true, list, count);
@@ -271,7 +281,7 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
 }
 
 // The scatter pass for record k of a discharge's collider list (its planes
-// at element `off`): the slot's RNG stream continues past the test draw
+// at element `off`): the recorded RNG state continues past the test draw
 // (collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused step's
 // algebraic sines and cosines); velocity and RNG state go back to the slot,
 // a spawned electron takes the next slot of n_e, a spawned ion the next slot
@@ -282,7 +292,7 @@ __device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const C
     const uint32_t i = list.slot[off + k];
     const float vxi = list.vx[off + k], vyi = list.vy[off + k], vzi = list.vz[off + k];
     const uint32_t j = off + i;
-    Xoshiro128p rs{pl.rng0[j], pl.rng1[j], pl.rng2[j], pl.rng3[j]};
+    Xoshiro128p rs{list.r0[off + k], list.r1[off + k], list.r2[off + k], list.r3[off + k]};
     const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
     const uint32_t idx = energy_index(g.half_me_over_e * v2);
     collide_electron_t<true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx, pl.ivy,

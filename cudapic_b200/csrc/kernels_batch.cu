@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(ES_THREADS, MINB)
 // the batch's concatenated electron slots cut into equal per-CTA shares as
 // in batch_step_kernel, each segment run with that discharge's field,
 // tables, next density and collider list (the discharge's range of the
-// other side's planes).  No count changes: nothing is published.
+// other sides' planes).  No count changes: nothing is published.
 template <bool MEAS>
 __global__ void __launch_bounds__(IP_THREADS, 4)
     batch_inplace_kernel(const __grid_constant__ InplacePlanes pl, const __grid_constant__ CollList list,
@@ -262,7 +262,8 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
         {
             const cudapic_grid g = s_g;
             const uint32_t off = s_off;
-            const CollList mine{list.slot + off, list.vx + off, list.vy + off, list.vz + off};
+            const CollList mine{list.slot + off, list.vx + off, list.vy + off, list.vz + off,
+                                list.r0 + off,   list.r1 + off, list.r2 + off, list.r3 + off};
             uint32_t live = 0;
             inplace_segment<true, MEAS>(pl, s_dc, g, s_g, off, lo, hi, sm, copies, ef_pad, epoch, mine,
                                         dcp<true>(s_dc.alive), live);
@@ -642,7 +643,7 @@ int launch_batch_scatter(const InplacePlanes &pl, const CollList &list, const Ba
     if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch scatter: bad discharge count");
     const size_t plan = (size_t)(D + 1) * sizeof(uint32_t);
     auto kern = r.measure ? batch_scatter_kernel<true> : batch_scatter_kernel<false>;
-    const unsigned grid = persistent_grid(4, (cap_sum + IP_THREADS - 1) / IP_THREADS);
+    const unsigned grid = persistent_grid(2, (cap_sum + IP_THREADS - 1) / IP_THREADS);
     return launch_kernel("batch_scatter_electrons", kern, dim3(grid), dim3(IP_THREADS), plan, stream, pl, list, desc,
                          D, r.dens, r.dens_i, ticket);
 }

@@ -179,7 +179,9 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
 int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const float *cs, uint32_t *count,
                             uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
                             cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll) {
-    const unsigned grid = persistent_grid(4, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
+    // two CTAs per SM: every thread loops over records, and the completion
+    // ticket has fewer CTAs to count
+    const unsigned grid = persistent_grid(2, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
     return launch_kernel("scatter_colliders_e", electron_scatter_kernel, dim3(grid), dim3(IP_THREADS), 0, stream, pl,
                          list, cs, count, ticket, n_e, n_i, g, dens_e, dens_i, coll);
 }
@@ -191,39 +193,40 @@ using namespace cudapic;
 extern "C" int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy,
                                               const float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
                                               uint32_t *rng3, const float *total_cs_e, float sigma_max_e,
-                                              const uint32_t *n_e, uint32_t *coll_slot, float *coll_vx,
-                                              float *coll_vy, float *coll_vz, uint32_t *n_colliders,
+                                              const uint32_t *n_e, uint32_t *const coll[8], uint32_t *n_colliders,
                                               float *e_next_density, const cudapic_grid *grid,
                                               cudapic_stream_t stream) {
     CUDAPIC_CHECK(validate_grid(grid));
-    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && n_e && coll_slot &&
-                        coll_vx && coll_vy && coll_vz && n_colliders && e_next_density,
+    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && n_e && coll &&
+                        n_colliders && e_next_density,
                     "step_electrons_inplace: null pointer");
+    for (int k = 0; k < 8; ++k) CUDAPIC_REQUIRE(coll[k], "step_electrons_inplace: null record plane");
     CUDAPIC_REQUIRE(sigma_max_e >= 0.0f, "step_electrons_inplace: sigma_max_e must be the largest entry of total_cs_e");
     const void *planes[8] = {x, vx, vy, vz, rng0, rng1, rng2, rng3};
     CUDAPIC_REQUIRE(inplace_eligible(planes, 8, grid->capacity),
                     "step_electrons_inplace: planes must be 16-byte aligned and capacity a multiple of 4");
     const InplacePlanes pl{x, vx, const_cast<float *>(vy), const_cast<float *>(vz), rng0, rng1, rng2, rng3,
                            nullptr, nullptr, nullptr, nullptr};
-    const CollList list{coll_slot, coll_vx, coll_vy, coll_vz};
+    const CollList list{coll[0], reinterpret_cast<float *>(coll[1]), reinterpret_cast<float *>(coll[2]),
+                        reinterpret_cast<float *>(coll[3]), coll[4], coll[5], coll[6], coll[7]};
     return launch_electron_inplace(pl, efield, total_cs_e, sigma_max_e, n_e, list, n_colliders, e_next_density,
                                    *grid, (cudaStream_t)stream, nullptr, nullptr);
 }
 
 extern "C" int cudapic_scatter_colliders_e(float *x, float *vx, float *vy, float *vz, uint32_t *rng0,
                                            uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, const float *cs,
-                                           const uint32_t *coll_slot, const float *coll_vx, const float *coll_vy,
-                                           const float *coll_vz, uint32_t *n_colliders, uint32_t *ticket,
+                                           uint32_t *const coll[8], uint32_t *n_colliders, uint32_t *ticket,
                                            float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *n_e,
                                            uint32_t *n_i, float *e_next_density, float *i_next_density,
                                            const cudapic_grid *grid, cudapic_stream_t stream) {
     CUDAPIC_CHECK(validate_grid(grid));
-    CUDAPIC_REQUIRE(x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && cs && coll_slot && coll_vx && coll_vy &&
-                        coll_vz && n_colliders && ticket && i_x && i_vx && i_vy && i_vz && n_e && n_i,
+    CUDAPIC_REQUIRE(x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && cs && coll && n_colliders && ticket &&
+                        i_x && i_vx && i_vy && i_vz && n_e && n_i,
                     "scatter_colliders_e: null pointer");
+    for (int k = 0; k < 8; ++k) CUDAPIC_REQUIRE(coll[k], "scatter_colliders_e: null record plane");
     const InplacePlanes pl{x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz};
-    const CollList list{const_cast<uint32_t *>(coll_slot), const_cast<float *>(coll_vx), const_cast<float *>(coll_vy),
-                        const_cast<float *>(coll_vz)};
+    const CollList list{coll[0], reinterpret_cast<float *>(coll[1]), reinterpret_cast<float *>(coll[2]),
+                        reinterpret_cast<float *>(coll[3]), coll[4], coll[5], coll[6], coll[7]};
     return launch_electron_scatter(pl, list, cs, n_colliders, ticket, n_e, n_i, *grid, (cudaStream_t)stream,
                                    e_next_density, i_next_density, nullptr);
 }

@@ -142,9 +142,13 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
         const InplacePlanes pl{s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se],
                                s->rng[E][0], s->rng[E][1], s->rng[E][2], s->rng[E][3],
                                s->x[I][si], s->vx[I][si], s->vy[I][si], s->vz[I][si]};
-        // the collider records live in the other side's planes until the next compaction
+        // the collider records live in the other sides' planes (free until the
+        // next compaction and ion push)
         const CollList list{reinterpret_cast<uint32_t *>(s->x[E][se ^ 1]), s->vx[E][se ^ 1], s->vy[E][se ^ 1],
-                            s->vz[E][se ^ 1]};
+                            s->vz[E][se ^ 1], reinterpret_cast<uint32_t *>(s->x[I][si ^ 1]),
+                            reinterpret_cast<uint32_t *>(s->vx[I][si ^ 1]),
+                            reinterpret_cast<uint32_t *>(s->vy[I][si ^ 1]),
+                            reinterpret_cast<uint32_t *>(s->vz[I][si ^ 1])};
         CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->sigma_max_e, s->n_e(), list,
                                               s->counters + CTR_COLL_COUNT, e_next, g, st,
                                               s->measure ? s->wall : nullptr, s->counters + CTR_SPAWN_FROM));

@@ -122,24 +122,32 @@ def step_electrons_noalloc(efield, src_x, src_vx, src_vy, src_vz, dst_x, dst_vx,
     check(lib.cudapic_step_electrons_noalloc(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, src_x)))
 
 
-def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, sigma_max_e, n_e, coll_slot,
-                           coll_vx, coll_vy, coll_vz, n_colliders, e_next_density, grid, stream=None):
+def _planes8(coll):
+    """The eight collider-record planes as a C array of device pointers."""
+    import ctypes
+    if len(coll) != 8:
+        raise ValueError("eight record planes: slot, vx, vy, vz, rng0..3")
+    return (ctypes.c_void_p * 8)(*[_ptr(a) for a in coll])
+
+
+def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, sigma_max_e, n_e, coll,
+                           n_colliders, e_next_density, grid, stream=None):
     """In-place electron step, stream pass: push, absorption (x set to
     CUDAPIC_DEAD_X), collision test and next-step deposit with every electron
-    kept in its slot; colliders recorded (slot, vx, vy, vz) in the coll_*
-    planes."""
+    kept in its slot; each collider recorded in the eight `coll` planes
+    (slot, vx, vy, vz, RNG state)."""
     head = [_ptr(a) for a in (efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e)]
-    tail = [_ptr(a) for a in (n_e, coll_slot, coll_vx, coll_vy, coll_vz, n_colliders, e_next_density)]
-    check(lib.cudapic_step_electrons_inplace(*head, float(sigma_max_e), *tail, _g(grid), _stream(stream, x)))
+    check(lib.cudapic_step_electrons_inplace(*head, float(sigma_max_e), _ptr(n_e), _planes8(coll), _ptr(n_colliders),
+                                             _ptr(e_next_density), _g(grid), _stream(stream, x)))
 
 
-def scatter_colliders_e(x, vx, vy, vz, rng0, rng1, rng2, rng3, cs, coll_slot, coll_vx, coll_vy, coll_vz, n_colliders,
-                        ticket, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density, grid, stream=None):
+def scatter_colliders_e(x, vx, vy, vz, rng0, rng1, rng2, rng3, cs, coll, n_colliders, ticket, i_x, i_vx, i_vy,
+                        i_vz, n_e, n_i, e_next_density, i_next_density, grid, stream=None):
     """In-place electron step, scatter pass over the recorded colliders
     (spawns appended at n_e and n_i)."""
-    args = [_ptr(a) for a in (x, vx, vy, vz, rng0, rng1, rng2, rng3, cs, coll_slot, coll_vx, coll_vy, coll_vz,
-                              n_colliders, ticket, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density)]
-    check(lib.cudapic_scatter_colliders_e(*args, _g(grid), _stream(stream, x)))
+    head = [_ptr(a) for a in (x, vx, vy, vz, rng0, rng1, rng2, rng3, cs)]
+    tail = [_ptr(a) for a in (n_colliders, ticket, i_x, i_vx, i_vy, i_vz, n_e, n_i, e_next_density, i_next_density)]
+    check(lib.cudapic_scatter_colliders_e(*head, _planes8(coll), *tail, _g(grid), _stream(stream, x)))
 
 
 def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2, rng3, i_x, i_vx, i_vy, i_vz,

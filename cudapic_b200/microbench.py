@@ -77,9 +77,9 @@ def main():
                                                             *b.rng[1], g, stream=s), None, n_i),
         # the in-place step's stream pass (each launch advances the live planes by one step)
         "step_electrons_inplace": (lambda: K.step_electrons_inplace(
-            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.sigma_max_e, ne_c, b.tmp_x[0],
-            b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], ccount, dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()),
-            n_e),
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.sigma_max_e, ne_c,
+            (b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], b.tmp_x[1], b.tmp_vx[1], b.tmp_vy[1], b.tmp_vz[1]),
+            ccount, dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()), n_e),
     }
     fn, pre, n = fns[a.kernel]
     from cudapic_b200.timing import L2Flusher, time_launch

@@ -253,10 +253,12 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
  *    electron that leaves through an electrode is marked in its slot with
  *    x = -1 (CUDAPIC_DEAD_X): later in-place steps skip such slots, and
  *    cudapic_step_electrons drops them while compacting.  Each collider is
- *    recorded (slot, vx, vy, vz) in the four coll_* planes (capacity entries
- *    each) and counted in *n_colliders (zero on entry).  *n_e is unchanged.
+ *    recorded in the eight planes coll[0..7] (capacity entries each: slot,
+ *    vx, vy, vz, then the four words of its RNG state past the test draw)
+ *    and counted in *n_colliders (zero on entry).  *n_e is unchanged.
  *  - cudapic_scatter_colliders_e scatters the recorded colliders in place,
- *    continuing each slot's stream past the test draw (collision_e);
+ *    continuing each recorded stream (collision_e) and writing velocity and
+ *    RNG state back to the slots;
  *    spawned electrons take slots *n_e, *n_e + 1, ... (updating *n_e),
  *    spawned ions slots *n_i, ... of i_*; both are deposited into the next
  *    densities.  Its last CTA resets *n_colliders and *ticket (zero on
@@ -266,12 +268,10 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
 int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy, const float *vz,
                                    uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                                    const float *total_cs_e, float sigma_max_e, const uint32_t *n_e,
-                                   uint32_t *coll_slot, float *coll_vx, float *coll_vy, float *coll_vz,
-                                   uint32_t *n_colliders, float *e_next_density, const cudapic_grid *grid,
-                                   cudapic_stream_t stream);
+                                   uint32_t *const coll[8], uint32_t *n_colliders, float *e_next_density,
+                                   const cudapic_grid *grid, cudapic_stream_t stream);
 int cudapic_scatter_colliders_e(float *x, float *vx, float *vy, float *vz, uint32_t *rng0, uint32_t *rng1,
-                                uint32_t *rng2, uint32_t *rng3, const float *cs, const uint32_t *coll_slot,
-                                const float *coll_vx, const float *coll_vy, const float *coll_vz,
+                                uint32_t *rng2, uint32_t *rng3, const float *cs, uint32_t *const coll[8],
                                 uint32_t *n_colliders, uint32_t *ticket, float *i_x, float *i_vx, float *i_vy,
                                 float *i_vz, uint32_t *n_e, uint32_t *n_i, float *e_next_density,
                                 float *i_next_density, const cudapic_grid *grid, cudapic_stream_t stream);

@@ -190,14 +190,14 @@ def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, 
     r_d = [dev(p) for p in rng]
     i_d = [dev(pad(np.full(n_i0, 0.0125, np.float32))) for _ in range(4)]
     n_e, n_i = counter(n), counter(n_i0)
-    rec = [zeros(cap, np.uint32)] + [zeros(cap) for _ in range(3)]   # collider records: slot, vx, vy, vz
+    rec = [zeros(cap, np.uint32)] + [zeros(cap) for _ in range(3)] + [zeros(cap, np.uint32) for _ in range(4)]
     cnt, ticket = counter(0), counter(0)
     de, di = zeros(len(ef)), zeros(len(ef))
-    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, float(se.max()), n_e, *rec, cnt, de, g)
+    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, float(se.max()), n_e, rec, cnt, de, g)
     n_coll = int(host(cnt)[0])
     assert n_coll == int(np.count_nonzero(events))
     assert int(host(n_e)[0]) == n   # unchanged by the stream pass
-    K.scatter_colliders_e(*e_d, *r_d, dcs, *rec, cnt, ticket, *i_d, n_e, n_i, de, di, g)
+    K.scatter_colliders_e(*e_d, *r_d, dcs, rec, cnt, ticket, *i_d, n_e, n_i, de, di, g)
     ne, ni = int(host(n_e)[0]), int(host(n_i)[0])
     assert (ne - n, ni) == (ne_ref - m, ni_ref)
     assert int(host(cnt)[0]) == 0 and int(host(ticket)[0]) == 0
@@ -206,7 +206,8 @@ def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, 
         assert np.array_equal(got[k][:n].view(np.uint32), exp[k][:n].view(np.uint32)), k
     for d, h in zip(r_d, r_ref):
         assert np.array_equal(host(d), h)
-    assert np.array_equal(sorted_rows(*[a[n:ne] for a in got]), sorted_rows(*[h[m:ne_ref] for h in e_h]))
+    gs, es = sorted_rows(*[a[n:ne] for a in got]), sorted_rows(*[h[m:ne_ref] for h in e_h])
+    assert np.array_equal(gs, es), _row_diff(gs, es)
     gi = [host(d) for d in i_d]
     assert np.array_equal(sorted_rows(*[a[n_i0:ni] for a in gi]), sorted_rows(*[h[n_i0:ni] for h in i_h]))
     present = got[0][:ne][got[0][:ne] >= 0.0]
@@ -216,3 +217,14 @@ def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, 
         ref_i = oracle.get_density_f64(gi[0][n_i0:ni], ph)
         assert np.linalg.norm(host(di) - ref_i) / np.linalg.norm(ref_i) < dens_tol
     return m, ne, ni, int(np.count_nonzero(events))
+
+
+def _row_diff(got, exp):
+    """Which columns differ between two sorted row sets, and a few rows."""
+    if got.shape != exp.shape:
+        return "shapes %s vs %s" % (got.shape, exp.shape)
+    bad = np.nonzero(np.any(got != exp, axis=1))[0]
+    cols = np.any(got != exp, axis=0)
+    return "%d of %d rows differ, columns %s; first: got %s exp %s" % (
+        len(bad), len(got), np.nonzero(cols)[0].tolist(), got[bad[:3]].view(np.float32).tolist(),
+        exp[bad[:3]].view(np.float32).tolist())
