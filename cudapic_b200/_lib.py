@@ -69,7 +69,7 @@ class Tuning(C.Structure):
     _fields_ = [(name, C.c_int) for name in (
         "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
         "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant", "step_stages",
-        "step_ctas_per_sm", "step_rows", "inplace_ctas_per_sm", "inplace_copies")]
+        "step_ctas_per_sm", "step_rows", "inplace_ctas_per_sm", "inplace_copies", "inplace_prefetch")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -157,6 +157,7 @@ SIGNATURES = {
     "cudapic_step_electrons_inplace": [_VP] * 10 + [_F] + [_VP] * 4 + [_GP, _VP],
     "cudapic_scatter_colliders_e": [_VP] * 20 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
+    "cudapic_check_collisions_i_bounded": [_VP] * 10 + [_F, _VP, _GP, _VP],
     "cudapic_accumulate_density": [_VP, _VP, _GP, _VP],
     "cudapic_accumulate_eepf": [_VP] * 7 + [_GP, _VP],
     "cudapic_xoshiro128p_test_wrapper": [_U32, _U32, _U32, _U32, _VP, _VP],
@@ -179,6 +180,7 @@ SIGNATURES = {
     "cudapic_state_set_fused": [_VP, C.c_int],
     "cudapic_state_set_inplace": [_VP, C.c_int],
     "cudapic_state_set_spawn_collide": [_VP, C.c_int],
+    "cudapic_state_set_solve_ahead": [_VP, C.c_int],
     "cudapic_state_set_overlap": [_VP, C.c_int],
     "cudapic_state_set_graphs": [_VP, C.c_int],
     "cudapic_state_run_steps": [_VP, C.c_uint64],

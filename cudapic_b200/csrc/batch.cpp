@@ -174,6 +174,7 @@ int build(cudapic_batch *b) {
         d.sigma_tot_e = s->sigma_tot_e;
         d.sigma_tot_i = s->sigma_tot_i;
         d.sigma_max_e = s->sigma_max_e;
+        d.ion_k = s->ion_k;
         d.wall = s->wall;
         d.mcount = s->mcount;
         d.cumul_e = s->cumul_e;

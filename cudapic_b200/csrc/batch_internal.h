@@ -74,6 +74,7 @@ struct BatchDisc {
     const float *pot0_table;
     const float *cs, *sigma_tot_e, *sigma_tot_i;
     float sigma_max_e;
+    float ion_k;                                           // the ion test's certain-rejection bound
     cudapic_wall_counters *wall;                           // [2]: electrons, ions (measurement)
     unsigned long long *mcount;                            // [3]: e / i collisions, EEPF samples
     double *cumul_e, *cumul_i, *esum;

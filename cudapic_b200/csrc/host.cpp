@@ -71,7 +71,7 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1,
     /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2,
-    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8};
+    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8, /*inplace_prefetch*/ 1};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
 uint64_t g_tuning_gen = 0;  // advanced by every cudapic_set_tuning
@@ -219,6 +219,7 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
     if (!v.step_rows) v.step_rows = d.step_rows;
     if (!v.inplace_ctas_per_sm) v.inplace_ctas_per_sm = d.inplace_ctas_per_sm;
     if (!v.inplace_copies) v.inplace_copies = d.inplace_copies;
+    if (!v.inplace_prefetch) v.inplace_prefetch = d.inplace_prefetch;
     const bool ok = (v.density_threads == 256 || v.density_threads == 512 || v.density_threads == 1024) &&
                     v.density_ctas_per_sm >= 1 && v.density_ctas_per_sm <= 8 && v.density_copies >= 1 &&
                     v.density_copies <= 32 &&
@@ -229,7 +230,8 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     (v.mcc_variant == 1 || v.mcc_variant == 2) && v.step_stages >= 2 && v.step_stages <= 6 &&
                     v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 &&
                     (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4) && v.inplace_ctas_per_sm >= 1 &&
-                    v.inplace_ctas_per_sm <= 8 && v.inplace_copies >= 1 && v.inplace_copies <= 8;
+                    v.inplace_ctas_per_sm <= 8 && v.inplace_copies >= 1 && v.inplace_copies <= 8 &&
+                    (v.inplace_prefetch == -1 || (v.inplace_prefetch >= 1 && v.inplace_prefetch <= 4));
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuning = v;

@@ -48,10 +48,13 @@ constexpr int IP_RECW = 8;          // words per record: slot, vx, vy, vz, rng0.
 // Dynamic shared memory: E[ef_pad] f32, the 64-bit deposit accumulator
 // [ef_pad], [copies][ef_pad] fixed-point histograms, the collider records
 // [IP_RECW][IP_WARPS][IP_QREC].  copies == 0 selects the large-grid deposit:
-// one f32 histogram in the accumulator's place (f32 shared atomics: no
-// copies to drain, and at thousands of nodes the lanes rarely meet on one).
+// one f32 histogram [ef_pad] in the accumulator's place and no copies (f32
+// shared atomics: nothing to drain, and at thousands of nodes the lanes
+// rarely meet on one), 8 B per node in all, so that four CTAs per SM still
+// fit at N_G = 4096.
 __host__ __device__ constexpr size_t inplace_smem_bytes(int copies, uint32_t ef_pad) {
-    return (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 + (size_t)IP_RECW * IP_WARPS * IP_QREC * 4;
+    return (copies ? (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 : (size_t)ef_pad * (4 + 4)) +
+           (size_t)IP_RECW * IP_WARPS * IP_QREC * 4;
 }
 
 struct InplaceSmem {
@@ -61,8 +64,8 @@ struct InplaceSmem {
     uint32_t *rec;
     __device__ __forceinline__ InplaceSmem(unsigned char *smem, int copies, uint32_t ef_pad) {
         ef = reinterpret_cast<float *>(smem);
-        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);
-        hist = reinterpret_cast<uint32_t *>(acc + ef_pad);
+        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);  // the f32 histogram when copies == 0
+        hist = copies ? reinterpret_cast<uint32_t *>(acc + ef_pad) : reinterpret_cast<uint32_t *>(ef + 2u * ef_pad);
         rec = hist + (uint32_t)copies * ef_pad;
     }
     // word w of record j of warp `warp`
@@ -76,12 +79,17 @@ struct InplaceSmem {
 
 __device__ __forceinline__ void inplace_smem_init(const InplaceSmem &sm, int copies, uint32_t ef_pad) {
     for (uint32_t k = threadIdx.x; k < (uint32_t)copies * ef_pad; k += IP_THREADS) sm.hist[k] = 0u;
+    if (copies == 0) {
+        float *hf = reinterpret_cast<float *>(sm.acc);
+        for (uint32_t k = threadIdx.x; k < ef_pad; k += IP_THREADS) hf[k] = 0.0f;
+        return;
+    }
     for (uint32_t k = threadIdx.x; k < ef_pad; k += IP_THREADS) sm.acc[k] = 0ull;
 }
 
 // The large-grid deposit: CIC weights (1 - rem, rem) of the new position
 // added to an f32 histogram, and the flush of its nodes (boundary nodes
-// doubled) into dens_out, which clears them.
+// doubled; four nodes per vector atomic) into dens_out, which clears them.
 __device__ __forceinline__ void dep_add_f32(float *h, float x, const cudapic_grid &g) {
     const float pos = x * g.inv_dx;
     const int p = cell_of(pos, g.n_g);
@@ -91,14 +99,47 @@ __device__ __forceinline__ void dep_add_f32(float *h, float x, const cudapic_gri
 }
 
 __device__ __forceinline__ void dep_flush_f32(float *h, float *dens_out, const cudapic_grid &g) {
-    for (uint32_t k = threadIdx.x; k < g.n_g; k += blockDim.x) {
-        const float v = h[k];
-        if (v == 0.0f) continue;
-        h[k] = 0.0f;
-        float f = v * g.weight_factor;
-        if (k == 0 || k == g.n_g - 1) f *= 2.0f;
-        atomicAdd(&dens_out[k], f);
+    const uint32_t n_g = g.n_g;
+    const bool vec = (reinterpret_cast<uintptr_t>(dens_out) & 15u) == 0;
+    for (uint32_t k = 4u * threadIdx.x; k < n_g; k += 4u * blockDim.x) {
+        float v[4];
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t node = k + (uint32_t)u;
+            const float a = node < n_g ? h[node] : 0.0f;
+            if (node < n_g) h[node] = 0.0f;
+            v[u] = a * g.weight_factor;
+            if (node == 0 || node == n_g - 1) v[u] *= 2.0f;
+            any |= a != 0.0f;
+        }
+        if (any) red_add4(dens_out, k, n_g, v, vec);
     }
+}
+
+// Bulk prefetch of [p, p + bytes) into L2 (16-byte aligned, bytes a
+// multiple of 16): no registers, no completion to wait for.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Prefetches round r's slots [beg + r IP_ROUND, end) of the eight planes
+// (from element `off`) into L2; issued by one thread.
+__device__ __forceinline__ void prefetch_round(const InplacePlanes &pl, uint32_t off, uint32_t beg, uint32_t end,
+                                               uint32_t r) {
+    const uint32_t s = beg + r * IP_ROUND;
+    if (s >= end) return;
+    // slots rounded up to a multiple of 4: within the planes (capacity is one)
+    const uint32_t bytes = ((min(end - s, (uint32_t)IP_ROUND) + 3u) & ~3u) * 4u;
+    const uint32_t i = off + s;
+    prefetch_l2(pl.x + i, bytes);
+    prefetch_l2(pl.vx + i, bytes);
+    prefetch_l2(pl.vy + i, bytes);
+    prefetch_l2(pl.vz + i, bytes);
+    prefetch_l2(pl.rng0 + i, bytes);
+    prefetch_l2(pl.rng1 + i, bytes);
+    prefetch_l2(pl.rng2 + i, bytes);
+    prefetch_l2(pl.rng3 + i, bytes);
 }
 
 // Moves whole groups of 32 queued records of the calling warp to the list
@@ -144,13 +185,15 @@ __device__ __forceinline__ void flush_records(const InplaceSmem &sm, uint32_t &q
 // accumulator are zero and the queues empty, and so they are on return (the
 // deposits flushed into dc.dens, the colliders into `list` / `count`, both
 // relative to the discharge).  The live electrons processed are added to
-// `live` (per thread).  SH: dc lives in shared memory; WALL: compile the
-// electrode counters in.
+// `live` (per thread).  pf: rounds prefetched into L2 ahead of their loads
+// (0: none), so that the CTA's next loads are in flight while it computes.
+// SH: dc lives in shared memory; WALL: compile the electrode counters in.
 template <bool SH, bool WALL>
 __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const StepDisc &dc, const cudapic_grid &g,
                                                 const cudapic_grid &gm, uint32_t off, uint32_t beg, uint32_t end,
                                                 const InplaceSmem &sm, int copies, uint32_t ef_pad, uint32_t epoch,
-                                                const CollList &list, uint32_t *count, uint32_t &live) {
+                                                const CollList &list, uint32_t *count, uint32_t &live,
+                                                uint32_t pf) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const unsigned lt = lanemask_lt();
@@ -163,9 +206,12 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
     uint32_t *h = f32dep ? nullptr : sm.hist + (uint32_t)(warp % copies) * ef_pad;
     float *hf = reinterpret_cast<float *>(sm.acc);
     uint32_t qn = 0;  // records queued by this warp (uniform across its lanes), < 32 between rounds
-    __syncthreads();
     const uint32_t rounds = (end - beg + IP_ROUND - 1) / IP_ROUND;
+    if (tid == 0)
+        for (uint32_t r = 1; r < pf && r < rounds; ++r) prefetch_round(pl, off, beg, end, r);
+    __syncthreads();
     for (uint32_t r = 0; r < rounds; ++r) {
+        if (pf && tid == 0 && r + pf < rounds) prefetch_round(pl, off, beg, end, r + pf);
         if (!f32dep && r != 0 && r % epoch == 0) {  // drain the deposit copies before they can overflow
             __syncthreads();
             dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
@@ -276,12 +322,13 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
     }
     dep_drain(sm.hist, copies, ef_pad, sm.acc, n_g);
     __syncthreads();
-    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);
-    for (uint32_t k = tid; k < n_g; k += IP_THREADS) sm.acc[k] = 0ull;
+    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);  // clears the accumulator
 }
 
 // The scatter pass for record k of a discharge's collider list (its planes
-// at element `off`): the recorded RNG state continues past the test draw
+// at element `off`), the collision code inlined so that the loads of the
+// record, the table entries and the slot's position overlap: the recorded
+// RNG state continues past the test draw
 // (collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused step's
 // algebraic sines and cosines); velocity and RNG state go back to the slot,
 // a spawned electron takes the next slot of n_e, a spawned ion the next slot
@@ -293,10 +340,11 @@ __device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const C
     const float vxi = list.vx[off + k], vyi = list.vy[off + k], vzi = list.vz[off + k];
     const uint32_t j = off + i;
     Xoshiro128p rs{list.r0[off + k], list.r1[off + k], list.r2[off + k], list.r3[off + k]};
+    const float xi = pl.x[j];  // an ionization's birthplace, fetched beside the table lookups
     const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
     const uint32_t idx = energy_index(g.half_me_over_e * v2);
-    collide_electron_t<true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx, pl.ivy,
-                             pl.ivz, n_e, n_i, g, dens_e, dens_i);
+    collide_electron_body<true, true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx,
+                                      pl.ivy, pl.ivz, n_e, n_i, g, dens_e, dens_i, xi);
     pl.rng0[j] = rs.s0;
     pl.rng1[j] = rs.s1;
     pl.rng2[j] = rs.s2;

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <utility>
@@ -130,9 +131,14 @@ int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t
                         float *i_x, float *i_vx, float *i_vy, float *i_vz, uint32_t *alive_e, uint32_t *alive_i,
                         uint8_t *events, const cudapic_grid &g, cudaStream_t stream, float *dep_e = nullptr,
                         float *dep_i = nullptr, unsigned long long *coll = nullptr);
+// ion_k: max(sigma_tot_i) dt_i rounded up (the ion test's certain-rejection
+// bound, mcc.cuh ion_collides); +inf: every ion takes the full test.
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
-                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll = nullptr);
+                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll = nullptr,
+                        float ion_k = INFINITY);
+// The bound ion_k for a table whose largest entry is sigma_max_i.
+float ion_reject_k(float sigma_max_i, const cudapic_grid &g);
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
                 const uint32_t *active_e, uint32_t *eepf, const cudapic_grid &g, cudaStream_t stream,
                 double *esum = nullptr, unsigned long long *ecount = nullptr);
@@ -179,9 +185,22 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
                             const uint32_t *n_active, const CollList &list, uint32_t *count, float *dens_e,
                             const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
                             uint32_t *spawn_from);
+// The next step's Poisson solve (launch_poisson's arguments), run by the
+// last CTA of the scatter pass once every CTA has added its spawns.
+struct PoissonAhead {
+    const float *e_density, *i_density;
+    float *pot, *efield;
+    const float *pot0_table;
+    uint32_t *step_counter;
+    float *zero_a, *zero_b;
+};
+// Largest grid the scatter pass can solve (one node per thread of its
+// 1024-thread CTAs, the separate solve kernel's shape up to this size).
+constexpr uint32_t POISSON_AHEAD_MAX_NG = 1024;
 int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const float *cs, uint32_t *count,
                             uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll);
+                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll,
+                            const PoissonAhead *ahead = nullptr);
 // eduPIC's same-step collisions of new electrons: one CTA tests and scatters
 // the electrons appended since *spawn_from (written by the stream pass).
 int launch_spawn_collide(const InplacePlanes &pl, const float *sigma_tot_e, const float *cs,

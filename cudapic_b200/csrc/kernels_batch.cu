@@ -213,7 +213,7 @@ template <bool MEAS>
 __global__ void __launch_bounds__(IP_THREADS, 4)
     batch_inplace_kernel(const __grid_constant__ InplacePlanes pl, const __grid_constant__ CollList list,
                          const BatchDisc *__restrict__ desc, const uint32_t *__restrict__ counts, uint32_t D,
-                         int dens_role, uint32_t ef_pad, int copies, uint32_t epoch) {
+                         int dens_role, uint32_t ef_pad, int copies, uint32_t epoch, uint32_t pf) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t wsum[ES_WARPS];
     __shared__ StepDisc s_dc;
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
                                 list.r0 + off,   list.r1 + off, list.r2 + off, list.r3 + off};
             uint32_t live = 0;
             inplace_segment<true, MEAS>(pl, s_dc, g, s_g, off, lo, hi, sm, copies, ef_pad, epoch, mine,
-                                        dcp<true>(s_dc.alive), live);
+                                        dcp<true>(s_dc.alive), live, pf);
             add_work(s_g.work, live);
         }
         d = lds_volatile(&s_d);
@@ -319,9 +319,9 @@ __global__ void __launch_bounds__(IP_THREADS)
             inplace_scatter(pl, list, s_off, k, s_cs, s_ctr + 0, s_ctr + 1, s_g, s_de, s_di);
         __syncthreads();  // the segment's shared words are rewritten for the next one
     }
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();  // one per CTA: its spawns before its ticket
         const uint32_t t = atomicAdd(ticket, 1u);
         P[0] = t == gridDim.x - 1;
     }
@@ -351,6 +351,7 @@ struct IonCollIO {
     uint32_t *rng0, *rng1, *rng2, *rng3;
     const float *sigma_tot, *cs;
     unsigned long long *coll;
+    float ion_k;
 };
 
 __global__ void __launch_bounds__(ES_THREADS)
@@ -392,6 +393,7 @@ __global__ void __launch_bounds__(ES_THREADS)
             io.sigma_tot = dd.sigma_tot_i;
             io.cs = dd.cs;
             io.coll = measure ? dd.mcount + 1 : nullptr;
+            io.ion_k = dd.ion_k;
             s_io = io;
         }
         __syncthreads();
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(ES_THREADS)
                 bool collide = false;
                 if (i < hi) {
                     Xoshiro128p rs{s[u][0], s[u][1], s[u][2], s[u][3]};
-                    collide = test_ion(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
+                    collide = ion_collides(v[u][0], v[u][1], v[u][2], rs, table, g, io.ion_k);
                     if (!collide) {
                         io.rng0[i] = rs.s0;
                         io.rng1[i] = rs.s1;
@@ -635,7 +637,7 @@ int launch_batch_inplace(const InplacePlanes &pl, const CollList &list, const Ba
     const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
     const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("batch_inplace_electrons", kern, dim3(grid), dim3(IP_THREADS), bytes(), stream, pl, list,
-                         desc, counts, D, r.dens, ef_pad, copies, epoch);
+                         desc, counts, D, r.dens, ef_pad, copies, epoch, (uint32_t)std::max(t.inplace_prefetch, 0));
 }
 
 int launch_batch_scatter(const InplacePlanes &pl, const CollList &list, const BatchDisc *desc, uint32_t D,

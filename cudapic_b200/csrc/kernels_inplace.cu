@@ -11,10 +11,12 @@
 // x, vx, RNG written) against 64 B, plus the colliders' records and their
 // scattered velocities and RNG states.
 #include <algorithm>
+#include <type_traits>
 
 #include "batch_internal.h"
 #include "inplace.cuh"
 #include "internal.h"
+#include "poisson.cuh"
 
 namespace cudapic {
 
@@ -24,7 +26,7 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
                             const float *__restrict__ sigma_tot_e, float sigma_max, const uint32_t *n_active,
                             const CollList list, uint32_t *count, float *dens_e,
                             const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int copies, uint32_t epoch,
-                            cudapic_wall_counters *wall, uint32_t *spawn_from) {
+                            cudapic_wall_counters *wall, uint32_t *spawn_from, uint32_t pf) {
     extern __shared__ __align__(128) unsigned char smem[];
     const InplaceSmem sm(smem, copies, ef_pad);
     inplace_smem_init(sm, copies, ef_pad);
@@ -50,30 +52,49 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
     dc.wall = wall;
     dc.coll = nullptr;
     uint32_t live = 0;
-    inplace_segment<false, MEAS>(pl, dc, g, g, 0u, beg, end, sm, copies, ef_pad, epoch, list, count, live);
+    inplace_segment<false, MEAS>(pl, dc, g, g, 0u, beg, end, sm, copies, ef_pad, epoch, list, count, live, pf);
     add_work(g.work, live);
 }
 
-__global__ void __launch_bounds__(IP_THREADS)
+// SOLVE: 0, or the last CTA also solves the next step's field (1: FP64
+// scans, 2: f32 scans) with the solve kernel's own shape for N_G <= 1024
+// (one node per thread, so the sums are added in the same order and the
+// field is bit-identical to the separate kernel's): CTAs of 1024 threads,
+// dynamic shared memory n_g x the scan type.
+constexpr int SC_SOLVE_THREADS = 1024;
+
+template <int SOLVE>
+__global__ void __launch_bounds__(SOLVE ? SC_SOLVE_THREADS : IP_THREADS)
     electron_scatter_kernel(const InplacePlanes pl, const CollList list, const float *__restrict__ cs,
                             uint32_t *count, uint32_t *ticket, uint32_t *n_e, uint32_t *n_i,
                             const __grid_constant__ cudapic_grid g, float *dens_e, float *dens_i,
-                            unsigned long long *coll) {
+                            unsigned long long *coll, const PoissonAhead ahead) {
+    __shared__ uint32_t s_last;
     grid_dep_wait();
     const uint32_t n = min(*count, g.capacity);  // read before this CTA takes its ticket
-    for (uint32_t k = blockIdx.x * IP_THREADS + threadIdx.x; k < n; k += gridDim.x * IP_THREADS)
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         inplace_scatter(pl, list, 0u, k, cs, n_e, n_i, g, dens_e, dens_i);
-    // the last CTA counts the collisions and empties the list for the next step
-    __threadfence();
+    // the last CTA counts the collisions and empties the list for the next
+    // step (every CTA read the count before its ticket: no fence needed for
+    // that; one per CTA orders its spawns and deposits before the ticket)
     __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();
         const uint32_t t = atomicAdd(ticket, 1u);
-        if (t == gridDim.x - 1) {
+        s_last = t == gridDim.x - 1;
+        if (s_last) {
             __threadfence();
             if (coll) atomicAdd(coll, (unsigned long long)n);
             *count = 0u;
             *ticket = 0u;
         }
+    }
+    if (SOLVE) {
+        __syncthreads();
+        if (s_last)  // every deposit of this step is in: the next step's solve (clears its collectors)
+            poisson_body<typename std::conditional<SOLVE == 1, double, float>::type, 1>(
+                ahead.e_density, ahead.i_density, ahead.pot, ahead.efield, 0.0f, ahead.pot0_table,
+                ahead.step_counter, g, ahead.zero_a, ahead.zero_b);
     }
 }
 
@@ -173,17 +194,28 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
     const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("step_electrons_inplace", kern, dim3(grid), dim3(IP_THREADS),
                          inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, sigma_max, n_active, list,
-                         count, dens_e, g, ef_pad, copies, epoch, wall, spawn_from);
+                         count, dens_e, g, ef_pad, copies, epoch, wall, spawn_from,
+                         (uint32_t)std::max(t.inplace_prefetch, 0));
 }
 
 int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const float *cs, uint32_t *count,
                             uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
-                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll) {
+                            cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll,
+                            const PoissonAhead *ahead) {
     // two CTAs per SM: every thread loops over records, and the completion
     // ticket has fewer CTAs to count
     const unsigned grid = persistent_grid(2, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
-    return launch_kernel("scatter_colliders_e", electron_scatter_kernel, dim3(grid), dim3(IP_THREADS), 0, stream, pl,
-                         list, cs, count, ticket, n_e, n_i, g, dens_e, dens_i, coll);
+    if (!ahead)
+        return launch_kernel("scatter_colliders_e", electron_scatter_kernel<0>, dim3(grid), dim3(IP_THREADS), 0,
+                             stream, pl, list, cs, count, ticket, n_e, n_i, g, dens_e, dens_i, coll, PoissonAhead{});
+    if (g.n_g > POISSON_AHEAD_MAX_NG) return fail(CUDAPIC_ERR_ARG, "scatter_colliders_e: n_g too large for the solve");
+    const bool f32 = (g.flags & CUDAPIC_FLAG_POISSON_F32_SCAN) != 0;
+    const size_t smem = (size_t)g.n_g * (f32 ? sizeof(float) : sizeof(double));
+    const unsigned grid1 = persistent_grid(1, ((uint64_t)g.capacity + SC_SOLVE_THREADS - 1) / SC_SOLVE_THREADS);
+    return launch_kernel("scatter_colliders_e+solve_poisson", f32 ? electron_scatter_kernel<2>
+                                                                  : electron_scatter_kernel<1>,
+                         dim3(grid1), dim3(SC_SOLVE_THREADS), smem, stream, pl, list, cs, count, ticket, n_e, n_i,
+                         g, dens_e, dens_i, coll, *ahead);
 }
 
 }  // namespace cudapic

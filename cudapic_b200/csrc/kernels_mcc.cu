@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
                                 uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, float *ix,
                                 float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i,
                                 uint8_t *events, const __grid_constant__ cudapic_grid g, int stages,
-                                float *dep_e, float *dep_i, unsigned long long *coll) {
+                                float *dep_e, float *dep_i, unsigned long long *coll, float ion_k) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *in = reinterpret_cast<uint32_t *>(smem);             // [stages][7][TILE]
     uint32_t *queue = in + stages * MT_ARRAYS * MT_TILE;           // [5][QCAP]
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(MCC_THREADS, 4)
                 const float vyi = __uint_as_float(b[1 * MT_TILE + j]);
                 const float vzi = __uint_as_float(b[2 * MT_TILE + j]);
                 bool collide;
-                if (ION) collide = test_ion(vxi, vyi, vzi, rs, table, g).collide;
+                if (ION) collide = ion_collides(vxi, vyi, vzi, rs, table, g, ion_k);
                 else collide = test_electron(vxi, vyi, vzi, rs, table, g).collide;
                 if (collide) {
                     const uint32_t q = atomicAdd(&s_q, 1u);
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
                                      float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
                                      float *ix, float *ivx, float *ivy, float *ivz, uint32_t *alive_e,
                                      uint32_t *alive_i, uint8_t *events, const __grid_constant__ cudapic_grid g,
-                                     float *dep_e, float *dep_i, unsigned long long *coll) {
+                                     float *dep_e, float *dep_i, unsigned long long *coll, float ion_k) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *tab = reinterpret_cast<float *>(smem);
     const int tid = threadIdx.x;
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(MR_THREADS, 1)
             bool collide = false;
             if (i < n) {
                 Xoshiro128p rs{s[u][0], s[u][1], s[u][2], s[u][3]};
-                if (ION) collide = test_ion(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
+                if (ION) collide = ion_collides(v[u][0], v[u][1], v[u][2], rs, table, g, ion_k);
                 else collide = test_electron(v[u][0], v[u][1], v[u][2], rs, table, g).collide;
                 if (!collide) {
                     rng0[i] = rs.s0;
@@ -371,7 +371,7 @@ template <bool ION, bool EVENTS>
 int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, float *x, float *vx, float *vy,
                float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx, float *ivy,
                float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events, const cudapic_grid &g,
-               cudaStream_t stream, float *dep_e, float *dep_i, unsigned long long *coll) {
+               cudaStream_t stream, float *dep_e, float *dep_i, unsigned long long *coll, float ion_k) {
     auto kern = check_collisions_tma_kernel<ION, EVENTS>;
     const cudapic_tuning t = tuning();
     const int stages = std::min(std::max(t.mcc_stages, 2), MT_MAX_STAGES);
@@ -386,7 +386,7 @@ int launch_tma(const float *sigma_tot, const float *cs, const uint32_t *active, 
     const unsigned grid = persistent_grid(per_sm, tiles_max);
     return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(grid), dim3(MCC_THREADS), smem,
                          stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz, alive_e,
-                         alive_i, events, g, stages, dep_e, dep_i, coll);
+                         alive_i, events, g, stages, dep_e, dep_i, coll, ion_k);
 }
 
 template <bool ION, bool EVENTS>
@@ -394,7 +394,7 @@ int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *act
                     float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix, float *ivx,
                     float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
                     const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i,
-                    unsigned long long *coll) {
+                    unsigned long long *coll, float ion_k) {
     auto kern = check_collisions_resident_kernel<ION, EVENTS>;
     if (MR_SMEM > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_NOT_SUPPORTED, "check_collisions: shared memory");
     CUDAPIC_CHECK(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MR_SMEM),
@@ -402,7 +402,7 @@ int launch_resident(const float *sigma_tot, const float *cs, const uint32_t *act
     const uint64_t chunks = ((uint64_t)g.capacity + MR_THREADS * MR_U - 1) / (MR_THREADS * MR_U);
     return launch_kernel(ION ? "check_collisions_i" : "check_collisions_e", kern, dim3(persistent_grid(1, chunks)),
                          dim3(MR_THREADS), MR_SMEM, stream, sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix,
-                         ivx, ivy, ivz, alive_e, alive_i, events, g, dep_e, dep_i, coll);
+                         ivx, ivy, ivz, alive_e, alive_i, events, g, dep_e, dep_i, coll, ion_k);
 }
 
 // Variant choice: the bulk-copy kernel needs 16-byte aligned planes and a
@@ -412,20 +412,20 @@ int launch_collisions(const float *sigma_tot, const float *cs, const uint32_t *a
                       float *vy, float *vz, uint32_t *r0, uint32_t *r1, uint32_t *r2, uint32_t *r3, float *ix,
                       float *ivx, float *ivy, float *ivz, uint32_t *alive_e, uint32_t *alive_i, uint8_t *events,
                       const cudapic_grid &g, cudaStream_t stream, float *dep_e, float *dep_i,
-                      unsigned long long *coll) {
+                      unsigned long long *coll, float ion_k = INFINITY) {
     const bool bulk = tuning().mcc_variant == 2 && tma_ready(g.capacity, {vx, vy, vz, r0, r1, r2, r3});
     if (bulk) {
         if (events)
             return launch_tma<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                         alive_e, alive_i, events, g, stream, dep_e, dep_i, coll);
+                                         alive_e, alive_i, events, g, stream, dep_e, dep_i, coll, ion_k);
         return launch_tma<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                      alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll);
+                                      alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll, ion_k);
     }
     if (events)
         return launch_resident<ION, true>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                          alive_e, alive_i, events, g, stream, dep_e, dep_i, coll);
+                                          alive_e, alive_i, events, g, stream, dep_e, dep_i, coll, ion_k);
     return launch_resident<ION, false>(sigma_tot, cs, active, x, vx, vy, vz, r0, r1, r2, r3, ix, ivx, ivy, ivz,
-                                       alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll);
+                                       alive_e, alive_i, nullptr, g, stream, dep_e, dep_i, coll, ion_k);
 }
 
 }  // namespace
@@ -441,10 +441,16 @@ int launch_collisions_e(const float *total_cs_e, const float *cs, const uint32_t
 
 int launch_collisions_i(const float *total_cs_i, const float *cs, const uint32_t *active_i, float *vx, float *vy,
                         float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3, uint8_t *events,
-                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll) {
+                        const cudapic_grid &g, cudaStream_t stream, unsigned long long *coll, float ion_k) {
     return launch_collisions<true>(total_cs_i, cs, active_i, nullptr, vx, vy, vz, rng0, rng1, rng2, rng3, nullptr,
                                    nullptr, nullptr, nullptr, nullptr, nullptr, events, g, stream, nullptr, nullptr,
-                                   coll);
+                                   coll, ion_k);
+}
+
+float ion_reject_k(float sigma_max_i, const cudapic_grid &g) {
+    if (!(sigma_max_i > 0.0f) || !(g.dt_i > 0.0f) || !std::isfinite(sigma_max_i)) return INFINITY;
+    const double k = (double)sigma_max_i * (double)g.dt_i * (1.0 + 1e-5);
+    return std::nextafter((float)k, INFINITY);
 }
 
 int launch_eepf(const float *x, const float *vx, const float *vy, const float *vz, const float *efield,
@@ -523,6 +529,19 @@ extern "C" int cudapic_check_collisions_i_events(const float *total_cs_i, const 
                     "check_collisions_i_events: null pointer");
     return launch_collisions_i(total_cs_i, cs, active_i, vx, vy, vz, rng0, rng1, rng2, rng3, events, *grid,
                                (cudaStream_t)stream);
+}
+
+extern "C" int cudapic_check_collisions_i_bounded(const float *total_cs_i, const float *cs,
+                                                  const uint32_t *active_i, float *vx, float *vy, float *vz,
+                                                  uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
+                                                  float sigma_max_i, uint8_t *events, const cudapic_grid *grid,
+                                                  cudapic_stream_t stream) {
+    CUDAPIC_CHECK(validate_grid(grid));
+    CUDAPIC_REQUIRE(total_cs_i && cs && active_i && vx && vy && vz && rng0 && rng1 && rng2 && rng3,
+                    "check_collisions_i_bounded: null pointer");
+    CUDAPIC_REQUIRE(sigma_max_i >= 0.0f, "check_collisions_i_bounded: sigma_max_i must be the largest entry of total_cs_i");
+    return launch_collisions_i(total_cs_i, cs, active_i, vx, vy, vz, rng0, rng1, rng2, rng3, events, *grid,
+                               (cudaStream_t)stream, nullptr, ion_reject_k(sigma_max_i, *grid));
 }
 
 extern "C" int cudapic_accumulate_eepf(const float *x, const float *vx, const float *vy, const float *vz,

@@ -170,13 +170,16 @@ __device__ __forceinline__ void deposit_global(float *dens, float xv, const cuda
 // sincos_of_acos, sin(eta + pi) = -sin eta) instead of evaluating the
 // angles: the same draws and events, velocities equal up to the rounding of
 // the skipped transcendentals, a fraction of the arithmetic.
-template <bool ALG>
-static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_t i, uint32_t idx, float vxi,
-                                                    float vyi, float vzi, Xoshiro128p &rs,
-                                                    const float *__restrict__ cs, float *x, float *vx, float *vy,
-                                                    float *vz, float *ix, float *ivx, float *ivy, float *ivz,
-                                                    uint32_t *alive_e, uint32_t *alive_i, const cudapic_grid &g,
-                                                    float *dep_e, float *dep_i) {
+// XPRE: the caller passes the electron's position as xpre (loaded ahead,
+// alongside its other loads); else an ionization loads x[off + i] itself.
+template <bool ALG, bool XPRE>
+__device__ __forceinline__ uint32_t collide_electron_body(uint32_t off, uint32_t i, uint32_t idx, float vxi,
+                                                          float vyi, float vzi, Xoshiro128p &rs,
+                                                          const float *__restrict__ cs, float *x, float *vx,
+                                                          float *vy, float *vz, float *ix, float *ivx, float *ivy,
+                                                          float *ivz, uint32_t *alive_e, uint32_t *alive_i,
+                                                          const cudapic_grid &g, float *dep_e, float *dep_i,
+                                                          float xpre) {
     const float exc_j = 11.5f * E_CHARGE_F;
     const float ion_j = 15.8f * E_CHARGE_F;
     float gx = vxi, gy = vyi, gz = vzi;
@@ -226,7 +229,7 @@ static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_
         }
         float ngx, ngy, ngz;
         rotate(g_new, sc2, cc2, se2, ce2, eu, ngx, ngy, ngz);
-        const float xi = x[off + i];
+        const float xi = XPRE ? xpre : x[off + i];
         uint32_t slot;
         if (claim_slot(alive_e, g.capacity, slot)) {
             x[off + slot] = xi;
@@ -258,6 +261,19 @@ static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_
     vy[off + i] = wy + g.f2 * ngy;
     vz[off + i] = wz + g.f2 * ngz;
     return ev;
+}
+
+// The body as one out-of-line function: the callers that run it inside a
+// streaming loop keep its registers out of their own.
+template <bool ALG>
+static __device__ __noinline__ uint32_t collide_electron_t(uint32_t off, uint32_t i, uint32_t idx, float vxi,
+                                                    float vyi, float vzi, Xoshiro128p &rs,
+                                                    const float *__restrict__ cs, float *x, float *vx, float *vy,
+                                                    float *vz, float *ix, float *ivx, float *ivy, float *ivz,
+                                                    uint32_t *alive_e, uint32_t *alive_i, const cudapic_grid &g,
+                                                    float *dep_e, float *dep_i) {
+    return collide_electron_body<ALG, false>(off, i, idx, vxi, vyi, vzi, rs, cs, x, vx, vy, vz, ix, ivx, ivy, ivz,
+                                             alive_e, alive_i, g, dep_e, dep_i, 0.0f);
 }
 
 // The reference formulation (the drop-in collision kernels).
@@ -292,6 +308,32 @@ __device__ __forceinline__ IonTest test_ion(float vxi, float vyi, float vzi, Xos
     const float rand_val = rs.uniform();
     t.collide = collision_draw(rand_val, nu * g.dt_i);
     return t;
+}
+
+// The ion test's outcome, first without the target atom (the same decision
+// and the same five draws as test_ion, bit for bit).  Box-Muller's four draws
+// are only advanced, and the test draw is compared with a bound on nu dt
+// over every target the draws can give: with u >= 1e-9 each radius is at
+// most sqrt(-2 ln 1e-9) = 6.438, so |v_atom| <= sqrt(rad1^2 + rad2^2) sigma
+// <= 9.2 sigma, |g| <= |v| + 9.2 sigma and nu dt <= k (|v| + 9.2 sigma)
+// with k >= max(sigma_tot_i) dt_i (rounded up by 1e-5 for the f32 products).
+// A draw at or above that bound + 6e-7 cannot collide (collision_draw's
+// bound: the computed p <= a + 3.1e-7): no transcendental is evaluated, for
+// nearly every ion at the reference conditions.  Otherwise (or k = +inf,
+// no bound) the full test runs again from the saved state.
+template <typename Table>
+__device__ __forceinline__ bool ion_collides(float vxi, float vyi, float vzi, Xoshiro128p &rs,
+                                             const Table &sigma_tot_i, const cudapic_grid &g, float k) {
+    const Xoshiro128p r0 = rs;
+    rs.next();
+    rs.next();
+    rs.next();
+    rs.next();
+    const float u = rs.uniform();
+    const float vmag = sqrtf(vxi * vxi + vyi * vyi + vzi * vzi);
+    if (u >= fmaf(k, vmag + 9.2f * g.normal_range, 6e-7f)) return false;
+    rs = r0;
+    return test_ion(vxi, vyi, vzi, rs, sigma_tot_i, g).collide;
 }
 
 // collision_i, Rust-CUDA/src/main.rs:1221-1292; returns 4 isotropic, 5 backscatter.

@@ -105,14 +105,40 @@ __device__ __forceinline__ void dep_drain(uint32_t *hist, int copies, uint32_t s
     }
 }
 
-// Adds the CTA's accumulated node weights to dens_out, boundary nodes doubled.
-__device__ __forceinline__ void dep_flush(const unsigned long long *acc, float *dens_out, const cudapic_grid &g) {
+// Adds v (nodes k .. k + 3) to dens_out: one 16-byte vector atomic when
+// the four nodes exist and dens_out is 16-byte aligned (one L2 operation for
+// four nodes: the per-CTA flushes of a large grid are bound by the number of
+// global atomics), else one atomic per non-zero node.
+__device__ __forceinline__ void red_add4(float *dens_out, uint32_t k, uint32_t n_g, const float (&v)[4], bool vec) {
+    if (vec && k + 4u <= n_g) {
+        atomicAdd(reinterpret_cast<float4 *>(dens_out + k), make_float4(v[0], v[1], v[2], v[3]));
+        return;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (k + (uint32_t)u < n_g && v[u] != 0.0f) atomicAdd(&dens_out[k + u], v[u]);
+}
+
+// Adds the CTA's accumulated node weights to dens_out, boundary nodes
+// doubled, and clears the accumulator (each thread the nodes it flushed:
+// four consecutive ones per turn).
+__device__ __forceinline__ void dep_flush(unsigned long long *acc, float *dens_out, const cudapic_grid &g) {
     const double w = g.weight_factor_d * (1.0 / (double)(1u << DEP_Q));
-    for (uint32_t k = threadIdx.x; k < g.n_g; k += blockDim.x) {
-        if (acc[k] == 0ull) continue;
-        float f = (float)((double)acc[k] * w);
-        if (k == 0 || k == g.n_g - 1) f *= 2.0f;
-        atomicAdd(&dens_out[k], f);
+    const uint32_t n_g = g.n_g;
+    const bool vec = (reinterpret_cast<uintptr_t>(dens_out) & 15u) == 0;
+    for (uint32_t k = 4u * threadIdx.x; k < n_g; k += 4u * blockDim.x) {
+        float v[4];
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t node = k + (uint32_t)u;
+            const unsigned long long a = node < n_g ? acc[node] : 0ull;
+            if (node < n_g) acc[node] = 0ull;
+            v[u] = a ? (float)((double)a * w) : 0.0f;
+            if (node == 0 || node == n_g - 1) v[u] *= 2.0f;
+            any |= a != 0ull;
+        }
+        if (any) red_add4(dens_out, k, n_g, v, vec);
     }
 }
 

@@ -117,7 +117,8 @@ void destroy_graphs(cudapic_state *s) {
 // starts.  Returns CUDAPIC_ERR_NOT_SUPPORTED, having
 // enqueued nothing, when the electron planes are not aligned for the fused
 // kernels.
-int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, float *i_acc, bool compact) {
+int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, float *i_acc, bool compact,
+                            int next_ion) {
     const cudapic_grid &g = s->grid;
     cudaStream_t st = s->stream;
     const int E = 0, I = 1;
@@ -152,9 +153,29 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
         CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->sigma_max_e, s->n_e(), list,
                                               s->counters + CTR_COLL_COUNT, e_next, g, st,
                                               s->measure ? s->wall : nullptr, s->counters + CTR_SPAWN_FROM));
+        // the next step's solve in the scatter pass: only when nothing that
+        // reads this step's field or adds to the densities follows it
+        // (measurement, the spawn-collision pass) and a next step exists
+        const bool ahead = next_ion >= 0 && s->solve_ahead && !s->measure && !s->spawn_collide &&
+                           g.n_g <= POISSON_AHEAD_MAX_NG;
+        PoissonAhead pa{};
+        if (ahead) {
+            // the buffer roles enqueue_step gives the next step: e_next becomes
+            // current, the buffer read now collects; on an ion step the ion
+            // collector becomes current and the current one collects
+            pa.e_density = e_next;
+            pa.zero_a = s->e_dens[s->e_cur];
+            pa.i_density = next_ion ? s->i_dens[s->i_cur ^ 1] : s->i_dens[s->i_cur];
+            pa.zero_b = next_ion ? s->i_dens[s->i_cur] : nullptr;
+            pa.pot = s->pot;
+            pa.efield = s->efield;
+            pa.pot0_table = s->pot0_table;
+            pa.step_counter = s->step_counter();
+        }
         CUDAPIC_CHECK(launch_electron_scatter(pl, list, s->cs, s->counters + CTR_COLL_COUNT,
                                               s->counters + CTR_COLL_TICKET, s->n_e(), s->n_i(), g, st, e_next, i_acc,
-                                              s->measure ? s->mcount : nullptr));
+                                              s->measure ? s->mcount : nullptr, ahead ? &pa : nullptr));
+        s->poisson_ahead = ahead;
         if (s->spawn_collide)
             CUDAPIC_CHECK(launch_spawn_collide(pl, s->sigma_tot_e, s->cs, s->counters + CTR_SPAWN_FROM, s->n_e(),
                                                s->n_i(), g, st, e_next, i_acc, s->measure ? s->mcount : nullptr));
@@ -177,7 +198,7 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
     if (ion_step) {
         CUDAPIC_CHECK(launch_collisions_i(s->sigma_tot_i, s->cs, s->n_i(), s->vx[I][si], s->vy[I][si],
                                           s->vz[I][si], s->rng[I][0], s->rng[I][1], s->rng[I][2], s->rng[I][3],
-                                          nullptr, g, st, s->measure ? s->mcount + 1 : nullptr));
+                                          nullptr, g, st, s->measure ? s->mcount + 1 : nullptr, s->ion_k));
     }
     if (s->measure) {
         CUDAPIC_CHECK(launch_eepf(s->x[E][se], s->vx[E][se], s->vy[E][se], s->vz[E][se], s->efield, s->n_e(),
@@ -188,7 +209,9 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
 
 // One reference time step (Rust-CUDA/src/main.rs:1728-1807).  compact: a
 // fused-mode step that closes the holes of earlier in-place steps.
-int enqueue_step(cudapic_state *s, bool ion_step, bool compact) {
+// next_ion: whether the step after this one is an ion step (1 / 0), or -1
+// when this is the last step of a run or graph (no solve ahead).
+int enqueue_step(cudapic_state *s, bool ion_step, bool compact, int next_ion) {
     PdlScope pdl(s->overlap);
     const cudapic_grid &g = s->grid;
     cudaStream_t st = s->stream;
@@ -222,8 +245,10 @@ int enqueue_step(cudapic_state *s, bool ion_step, bool compact) {
         }
         i_acc = s->i_dens[s->i_cur ^ 1];
     }
-    CUDAPIC_CHECK(launch_poisson(s->e_density(), s->i_density(), s->pot, s->efield, 0.0f, s->pot0_table,
-                                 s->step_counter(), g, st, e_next, zero_b));
+    if (!s->poisson_ahead)  // else the previous step's scatter pass solved it, and cleared the collectors
+        CUDAPIC_CHECK(launch_poisson(s->e_density(), s->i_density(), s->pot, s->efield, 0.0f, s->pot0_table,
+                                     s->step_counter(), g, st, e_next, zero_b));
+    s->poisson_ahead = false;
     if (s->measure) {
         CUDAPIC_CHECK(cudapic_accumulate_density(s->e_density(), s->cumul_e, &g, (cudapic_stream_t)st));
         if (ion_step) CUDAPIC_CHECK(cudapic_accumulate_density(s->i_density(), s->cumul_i, &g, (cudapic_stream_t)st));
@@ -239,7 +264,7 @@ int enqueue_step(cudapic_state *s, bool ion_step, bool compact) {
         }
     }
     if (fused) {
-        const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc, compact);
+        const int rc = enqueue_fused_particles(s, ion_step, e_next, i_acc, compact, next_ion);
         if (rc != CUDAPIC_ERR_NOT_SUPPORTED) return rc;  // else: buffers not aligned for the fused kernel
     }
     // electrons: push + compact into the other side
@@ -306,9 +331,11 @@ int build_graph(cudapic_state *s) {
     int rc = CUDAPIC_OK;
     for (uint64_t k = 0; k < period && rc == CUDAPIC_OK; ++k)
         rc = enqueue_step(s, is_ion_step(s, s->steps_done + k),
-                          is_compact_step(s, s->steps_done + k) || k + 1 == period);
+                          is_compact_step(s, s->steps_done + k) || k + 1 == period,
+                          k + 1 == period ? -1 : (int)is_ion_step(s, s->steps_done + k + 1));
     cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     // a graph of 2 N_SUB steps returns every ping-pong role to its start
+    s->poisson_ahead = false;  // the last captured step solved nothing ahead (a failed capture may have)
     s->side[0] = side0[0];
     s->side[1] = side0[1];
     s->e_cur = cur0[0];
@@ -415,6 +442,7 @@ extern "C" int cudapic_state_create(const cudapic_params *p, int device, cudapic
     std::vector<float> cs(5ull * CUDAPIC_CS_RANGES), se(CUDAPIC_CS_RANGES), si(CUDAPIC_CS_RANGES);
     if ((rc = cudapic_cross_sections(grid.gas_density, cs.data(), se.data(), si.data()))) return cleanup(rc);
     s->sigma_max_e = *std::max_element(se.begin(), se.end());
+    s->ion_k = ion_reject_k(*std::max_element(si.begin(), si.end()), s->grid);
     table_coll_freqs(se.data(), si.data(), &s->max_e_coll_freq, &s->max_i_coll_freq);
     if ((rc = check_cuda(cudaMemcpyAsync(s->pot0_table, table.data(), table.size() * sizeof(float),
                                          cudaMemcpyHostToDevice, s->stream), "upload pot0 table")) ||
@@ -660,6 +688,15 @@ extern "C" int cudapic_state_set_spawn_collide(cudapic_state *s, int on) {
     return CUDAPIC_OK;
 }
 
+extern "C" int cudapic_state_set_solve_ahead(cudapic_state *s, int on) {
+    if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_solve_ahead: null state");
+    DeviceGuard dg(s->device);
+    CUDAPIC_CHECK(check_cuda(cudaStreamSynchronize(s->stream), "state_set_solve_ahead sync"));
+    s->solve_ahead = on != 0;
+    destroy_graphs(s);
+    return CUDAPIC_OK;
+}
+
 extern "C" int cudapic_state_set_graphs(cudapic_state *s, int on) {
     if (!s) return fail(CUDAPIC_ERR_ARG, "state_set_graphs: null state");
     DeviceGuard dg(s->device);
@@ -721,7 +758,8 @@ extern "C" int cudapic_state_run_steps(cudapic_state *s, uint64_t n_steps) {
             continue;
         }
         CUDAPIC_CHECK(enqueue_step(s, is_ion_step(s, s->steps_done),
-                                   is_compact_step(s, s->steps_done) || n_steps == 1));
+                                   is_compact_step(s, s->steps_done) || n_steps == 1,
+                                   n_steps == 1 ? -1 : (int)is_ion_step(s, s->steps_done + 1)));
         s->steps_done += 1;
         if (s->measure) s->measure_steps += 1;
         n_steps -= 1;

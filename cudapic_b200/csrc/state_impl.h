@@ -33,10 +33,16 @@ struct cudapic_state {
     bool overlap = true;      // programmatic dependent launch between the step's kernels (default)
     bool inplace = true;      // fused mode: in-place electron steps between compacting ones (default)
     bool spawn_collide = false;  // in-place steps: new electrons also collide in their birth step (eduPIC)
+    // in-place steps: the scatter pass's last CTA solves the next step's
+    // field (default); poisson_ahead: the step being enqueued finds its
+    // solve already enqueued by the step before it
+    bool solve_ahead = true;
+    bool poisson_ahead = false;
     bool dens_valid = false;  // e_dens[e_cur] and both ion buffers describe the particles
     int graph_key[2][4] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}};  // sides and buffer roles at capture
     float *cs = nullptr, *sigma_tot_e = nullptr, *sigma_tot_i = nullptr;
     float sigma_max_e = 0.0f;  // largest entry of sigma_tot_e (the fused step's certain-rejection bound)
+    float ion_k = INFINITY;    // the fused driver's ion-test bound (ion_reject_k of sigma_tot_i)
     double *cumul_e = nullptr, *cumul_i = nullptr;
     cudapic_wall_counters *wall = nullptr;  // [0] electrons, [1] ions (measurement window)
     // measurement window: [0] electron and [1] ion collision events, [2] EEPF

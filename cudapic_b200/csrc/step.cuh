@@ -457,9 +457,7 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
     __syncthreads();
     dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
     __syncthreads();
-    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);
-    // the thread that flushed a node clears it (same node ownership as dep_flush)
-    for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.acc[k] = 0ull;
+    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);  // clears the accumulator
     it = it0 + tile;
     return ok;
 }

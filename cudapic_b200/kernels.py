@@ -164,11 +164,15 @@ def check_collisions_e(total_cs_e, cs, active_e, x, vx, vy, vz, rng0, rng1, rng2
 
 
 def check_collisions_i(total_cs_i, cs, active_i, vx, vy, vz, rng0, rng1, rng2, rng3, grid, stream=None,
-                       events=None):
-    """check_collisions_i (Rust-CUDA/src/main.rs:1167-1292)."""
+                       events=None, sigma_max_i=None):
+    """check_collisions_i (Rust-CUDA/src/main.rs:1167-1292).  sigma_max_i
+    (the largest entry of total_cs_i): the bounded entry, same results."""
     args = [_ptr(a) for a in (total_cs_i, cs, active_i, vx, vy, vz, rng0, rng1, rng2, rng3)]
     s = _stream(stream, vx)
-    if events is None:
+    if sigma_max_i is not None:
+        check(lib.cudapic_check_collisions_i_bounded(*args, float(sigma_max_i), _ptr(events) if events is not None
+                                                     else None, _g(grid), s))
+    elif events is None:
         check(lib.cudapic_check_collisions_i(*args, _g(grid), s))
     else:
         check(lib.cudapic_check_collisions_i_events(*args, _ptr(events), _g(grid), s))

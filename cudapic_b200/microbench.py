@@ -1,7 +1,7 @@
 """Runs one drop-in kernel on the steady-state population (CUDA-event timed,
 L2 flushed before each launch): the target of the committed ncu captures.
 
-    python -m cudapic_b200.microbench --kernel check_collisions_e [--particles N] [--reps 3]
+    python -m cudapic_b200.microbench --kernel check_collisions_e [--particles N] [--reps 3] [--tuning k=v ...]
 
 Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
 check_collisions_e, check_collisions_e_deposit, check_collisions_i and
@@ -25,6 +25,8 @@ def main():
     ap.add_argument("--particles", type=int, default=1 << 22)
     ap.add_argument("--n-g", type=int, default=400)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--tuning", nargs="*", default=[], metavar="FIELD=VALUE",
+                    help="launch-shape overrides (cudapic_tuning fields) for the timed launches")
     a = ap.parse_args()
 
     import torch
@@ -82,6 +84,8 @@ def main():
             ccount, dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()), n_e),
     }
     fn, pre, n = fns[a.kernel]
+    if a.tuning:
+        cp.set_tuning(**{k: int(v) for k, v in (f.split("=", 1) for f in a.tuning)})
     from cudapic_b200.timing import L2Flusher, time_launch
     t = time_launch(fn, stream, a.reps, flush=L2Flusher(), pre=pre)
     out = {"kernel": a.kernel, "us": t * 1e6, "n": n, "algo_bytes": BYTES[a.kernel] * n,

@@ -153,6 +153,11 @@ class GpuSimState:
         in that step (in-place steps; default off, the GPU reference's)."""
         check(lib.cudapic_state_set_spawn_collide(self._h, 1 if on else 0))
 
+    def set_solve_ahead(self, on=True):
+        """In-place steps solve the next step's field in their scatter pass
+        (default on) instead of in a Poisson kernel of the next step."""
+        check(lib.cudapic_state_set_solve_ahead(self._h, 1 if on else 0))
+
     def set_graphs(self, on=True):
         """Replay captured CUDA graphs (default) or launch every step from the host."""
         check(lib.cudapic_state_set_graphs(self._h, 1 if on else 0))

@@ -146,6 +146,8 @@ typedef struct cudapic_tuning {
     int step_rows;            /* fused electron step particles per thread and tile: 1, 2, 4 */
     int inplace_ctas_per_sm;  /* in-place electron step: resident CTAs per SM used          */
     int inplace_copies;       /* in-place electron step: deposit histogram copies (1..8)   */
+    int inplace_prefetch;     /* in-place electron step: rounds of a CTA's slots prefetched
+                                 into L2 ahead of their loads (1..4), -1: none             */
 } cudapic_tuning;
 
 int cudapic_get_tuning(cudapic_tuning *out);
@@ -329,6 +331,19 @@ int cudapic_check_collisions_i_events(const float *total_cs_i, const float *cs,
                                       uint32_t *rng3, uint8_t *events, const cudapic_grid *grid,
                                       cudapic_stream_t stream);
 
+/* cudapic_check_collisions_i with the largest entry of total_cs_i given
+ * (sigma_max_i), as cudapic_step_electrons takes sigma_max_e: an ion whose
+ * test draw lies above a bound on its collision probability over every
+ * target atom the draws can give skips the target's Box-Muller
+ * transcendentals (its RNG state advances past the same five draws), so
+ * results are identical to cudapic_check_collisions_i's and most ions cost
+ * a few integer operations.  events may be NULL.  No reference counterpart;
+ * the state drivers use it. */
+int cudapic_check_collisions_i_bounded(const float *total_cs_i, const float *cs, const uint32_t *active_i,
+                                       float *vx, float *vy, float *vz, uint32_t *rng0, uint32_t *rng1,
+                                       uint32_t *rng2, uint32_t *rng3, float sigma_max_i, uint8_t *events,
+                                       const cudapic_grid *grid, cudapic_stream_t stream);
+
 /* accumulate_density (Rust-CUDA/src/main.rs:1294-1299): cumul[k] += density[k]. */
 int cudapic_accumulate_density(const float *density, double *cumul, const cudapic_grid *grid,
                                cudapic_stream_t stream);
@@ -489,6 +504,15 @@ int cudapic_state_set_inplace(cudapic_state *s, int on);
  * (C/eduPIC.cc:669-703).  Applies to the in-place steps (all but one step in
  * N_SUB); the compacting steps keep the reference's semantics. */
 int cudapic_state_set_spawn_collide(cudapic_state *s, int on);
+/* on (default): an in-place step whose successor is in the same run (not
+ * the last step of a cudapic_state_run_steps call or graph) solves the
+ * successor's Poisson problem in the last CTA of its scatter pass, after the
+ * step's last deposit, instead of in a kernel of its own at the start of the
+ * successor; the same solve on the same densities (N_G <= 1024; not while
+ * measuring or with spawn collisions, whose kernels read this step's field
+ * or add to the densities after the scatter pass).  off: one solve kernel
+ * per step.  The captured graphs are rebuilt. */
+int cudapic_state_set_solve_ahead(cudapic_state *s, int on);
 /* on (default): the driver launches its kernels with programmatic dependent
  * launch, so a kernel's launch and prologue overlap the previous kernel's
  * tail (every kernel waits for its predecessor before touching global data).

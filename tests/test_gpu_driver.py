@@ -53,8 +53,9 @@ def test_c0_growth_matches_edupic(cudapic, cuda_device):
     cycle and 10 more.  16 GPU seeds (initial positions and RNG streams)
     against 16 eduPIC seeds (its Mersenne-Twister seed,
     tests/golden/edupic_c0_conv_seeds.txt): the mean electron and ion counts
-    after cycles 1, 6 and 11 agree within 3 standard errors of the
-    difference, and the seed-to-seed spreads are alike."""
+    after cycles 1, 6 and 11 agree within 3.5 standard errors of the
+    difference (six comparisons of 16 + 16 runs), and the seed-to-seed
+    spreads are alike."""
     from cudapic_b200.sim import GpuBatch
     ref = np.loadtxt(os.path.join(GOLDEN, "edupic_c0_conv_seeds.txt"))
     seeds = range(16)
@@ -79,7 +80,7 @@ def test_c0_growth_matches_edupic(cudapic, cuda_device):
             se = math.sqrt(a.var(ddof=1) / len(a) + e.var(ddof=1) / len(e))
             print("cycle %2d %s: GPU %.0f +- %.0f, eduPIC %.0f +- %.0f" % (cyc, "ei"[sp], a.mean(), a.std(ddof=1),
                                                                          e.mean(), e.std(ddof=1)))
-            assert abs(a.mean() - e.mean()) <= 3.0 * se, (cyc, sp, a.mean(), e.mean(), se)
+            assert abs(a.mean() - e.mean()) <= 3.5 * se, (cyc, sp, a.mean(), e.mean(), se)
             assert 0.33 < a.std(ddof=1) / e.std(ddof=1) < 3.0
     for st in states:
         assert st.steps_done() == 11 * 4000
@@ -144,6 +145,8 @@ def _c0_counts_after(cudapic, mode, seed, cycles=4):
         st.set_fused(False)
     elif mode == "no_overlap":
         st.set_overlap(False)
+    elif mode == "no_solve_ahead":
+        st.set_solve_ahead(False)
     st.run_cycles(cycles)
     counts = st.counts()
     assert st.device_error() == 0
@@ -152,11 +155,12 @@ def _c0_counts_after(cudapic, mode, seed, cycles=4):
     return counts
 
 
-@pytest.mark.parametrize("mode", ["reference", "no_overlap"])
+@pytest.mark.parametrize("mode", ["reference", "no_overlap", "no_solve_ahead"])
 def test_fused_driver_agrees_statistically(cudapic, cuda_device, mode):
     """The fused driver (electrons drawing from their source slot's stream,
-    programmatic dependent launch) against the reference launch sequence and
-    against itself without PDL: mean electron and ion counts after 4 RF
+    programmatic dependent launch, the next step's field solved in the
+    scatter pass) against the reference launch sequence, against itself
+    without PDL and with a solve kernel per step: mean electron and ion counts after 4 RF
     cycles of the igniting C0 discharge over 6 seeds agree within 3 standard
     errors.  (Single realisations of this growth phase spread by ~5 %, so a
     pair of runs alone cannot tell a bias from noise.)"""

@@ -626,10 +626,14 @@ def test_step_electrons_rejects_unaligned_planes(cudapic, K, dev_tables, tables)
                          zeros(400), g)
 
 
+@pytest.mark.parametrize("bounded", [False, True])
 @pytest.mark.parametrize("layout", ["aligned", "unaligned"])
 @pytest.mark.parametrize("n,n_t,temp", [(1, 4000, 1.0), (65_537, 4000, 0.03), (300_001, 200, 2.0),
                                         (300_001, 20, 20.0), (4_194_304, 4000, 0.03)])
-def test_check_collisions_i_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp, layout):
+def test_check_collisions_i_bit_exact(cudapic, K, oracle, dev_tables, tables, n, n_t, temp, layout, bounded):
+    """bounded: the entry given max(sigma_tot_i), whose ions skip the
+    target's transcendentals below the certain-rejection bound -- the same
+    events, RNG states and velocities."""
     cs, se, si = tables
     dcs, _, dsi = dev_tables
     cap = (n + 3) // 4 * 4
@@ -643,7 +647,8 @@ def test_check_collisions_i_bit_exact(cudapic, K, oracle, dev_tables, tables, n,
     v_d = [_dev_layout(a, layout) for a in v_h]
     r_d = [_dev_layout(a, layout) for a in r_h]
     events = zeros(n, np.uint8)
-    K.check_collisions_i(dsi, dcs, counter(n), *v_d, *r_d, g, events=events)
+    K.check_collisions_i(dsi, dcs, counter(n), *v_d, *r_d, g, events=events,
+                         sigma_max_i=float(si.max()) if bounded else None)
     ev_ref = oracle.check_collisions_i(si, cs, n, v_h, r_h, ph)
     assert np.array_equal(host(events), ev_ref)
     if n > 60_000:
