@@ -467,7 +467,7 @@ def kernel_breakdown(st, K, reps, flush):
     cnt, ticket = dev_u32(0), dev_u32(0)
 
     def stream_pass():
-        K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e,
+        K.step_electrons_inplace(b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.cs,
                                  b.sigma_max_e, ne_c, rec, cnt, dens, g, stream=stream.cuda_stream)
 
     def scatter_pass():

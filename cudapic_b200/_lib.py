@@ -69,7 +69,8 @@ class Tuning(C.Structure):
     _fields_ = [(name, C.c_int) for name in (
         "density_threads", "density_ctas_per_sm", "density_copies", "density_cluster",
         "push_stages", "push_ctas_per_sm", "mcc_stages", "mcc_ctas_per_sm", "mcc_variant", "step_stages",
-        "step_ctas_per_sm", "step_rows", "inplace_ctas_per_sm", "inplace_copies", "inplace_prefetch")]
+        "step_ctas_per_sm", "step_rows", "inplace_ctas_per_sm", "inplace_copies", "inplace_prefetch",
+        "scatter_ctas_per_sm")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -154,7 +155,7 @@ SIGNATURES = {
     "cudapic_state_load": [_VP, C.c_char_p],
     "cudapic_step_electrons": [_VP] * 15 + [_F] + [_VP] * 9 + [_GP, _VP],
     "cudapic_step_electrons_noalloc": [_VP] * 15 + [_F] + [_VP] * 8 + [_GP, _VP],
-    "cudapic_step_electrons_inplace": [_VP] * 10 + [_F] + [_VP] * 4 + [_GP, _VP],
+    "cudapic_step_electrons_inplace": [_VP] * 11 + [_F] + [_VP] * 4 + [_GP, _VP],
     "cudapic_scatter_colliders_e": [_VP] * 20 + [_GP, _VP],
     "cudapic_check_collisions_i_events": [_VP] * 11 + [_GP, _VP],
     "cudapic_check_collisions_i_bounded": [_VP] * 10 + [_F, _VP, _GP, _VP],

@@ -203,6 +203,8 @@ def main(argv=None):
     ap.add_argument("--ctas", type=int)
     ap.add_argument("--stages", type=int)
     ap.add_argument("--copies", type=int)
+    ap.add_argument("--tuning", nargs="*", default=[], metavar="FIELD=VALUE",
+                    help="other launch-shape overrides (cudapic_tuning fields)")
     a = ap.parse_args(argv)
     import cudapic_b200 as cp
     if a.one_discharge:
@@ -216,6 +218,7 @@ def main(argv=None):
                 s.voltage = a.voltage
     shape = {k: v for k, v in (("step_rows", a.rows), ("step_ctas_per_sm", a.ctas), ("step_stages", a.stages),
                                ("density_copies", a.copies)) if v}
+    shape.update({k: int(v) for k, v in (f.split("=", 1) for f in a.tuning)})
     if shape:
         cp.set_tuning(**shape)
     with Batch(specs) as b:
@@ -229,8 +232,7 @@ def main(argv=None):
         tu = cp.get_tuning()
         print(json.dumps({"discharges": len(specs), "steps": a.steps, "particle_steps_per_s": w / t,
                           "ms_per_step": 1e3 * t / a.steps, "device_errors": sum(1 for e in b.device_errors() if e),
-                          "shape": {k: tu[k] for k in ("step_rows", "step_ctas_per_sm", "step_stages",
-                                                       "density_copies")}}))
+                          "shape": tu}))
     return 0
 
 

@@ -71,7 +71,8 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1,
     /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2,
-    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8, /*inplace_prefetch*/ 1};
+    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8, /*inplace_prefetch*/ -1,
+    /*scatter_ctas_per_sm*/ 2};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
 uint64_t g_tuning_gen = 0;  // advanced by every cudapic_set_tuning
@@ -220,6 +221,7 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
     if (!v.inplace_ctas_per_sm) v.inplace_ctas_per_sm = d.inplace_ctas_per_sm;
     if (!v.inplace_copies) v.inplace_copies = d.inplace_copies;
     if (!v.inplace_prefetch) v.inplace_prefetch = d.inplace_prefetch;
+    if (!v.scatter_ctas_per_sm) v.scatter_ctas_per_sm = d.scatter_ctas_per_sm;
     const bool ok = (v.density_threads == 256 || v.density_threads == 512 || v.density_threads == 1024) &&
                     v.density_ctas_per_sm >= 1 && v.density_ctas_per_sm <= 8 && v.density_copies >= 1 &&
                     v.density_copies <= 32 &&
@@ -231,7 +233,8 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 &&
                     (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4) && v.inplace_ctas_per_sm >= 1 &&
                     v.inplace_ctas_per_sm <= 8 && v.inplace_copies >= 1 && v.inplace_copies <= 8 &&
-                    (v.inplace_prefetch == -1 || (v.inplace_prefetch >= 1 && v.inplace_prefetch <= 4));
+                    (v.inplace_prefetch == -1 || (v.inplace_prefetch >= 1 && v.inplace_prefetch <= 4)) &&
+                    v.scatter_ctas_per_sm >= 1 && v.scatter_ctas_per_sm <= 8;
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuning = v;

@@ -17,12 +17,17 @@
 //    shared memory and, 32 at a time, to the collider list (one atomicAdd
 //    per 32 records, coalesced stores): eight planes of the other sides of
 //    both species, which an in-place electron step does not otherwise use,
-//    so the list holds one record for every slot;
+//    so the list holds one record for every slot.  The pass also makes the
+//    scattering's event draw (the process entries are fetched with the
+//    test's total) so that it knows how many draws the scattering takes (7
+//    for an ionization, else 3) and writes every slot's final RNG state in
+//    its coalesced store;
 //  * scatter pass (inplace_scatter): one thread per listed collider reads
 //    its record (coalesced, no gather from the slot), continues the RNG
-//    stream, scatters (collision_e, :1035-1165) and writes velocity and RNG
-//    state back to the slot; spawned electrons are appended after the live
-//    slots, spawned ions to the ion side.
+//    stream from the record, scatters (collision_e, :1035-1165) and writes
+//    the velocity back to the slot -- three scattered words per collider,
+//    not seven; spawned electrons are appended after the live slots,
+//    spawned ions to the ion side.
 // The stream pass keeps the collision code out of its registers (the
 // scattering needs ~110 per thread; the stream pass runs at 64 with four
 // CTAs per SM), and no block barrier orders its stores.  The holes are
@@ -85,36 +90,6 @@ __device__ __forceinline__ void inplace_smem_init(const InplaceSmem &sm, int cop
         return;
     }
     for (uint32_t k = threadIdx.x; k < ef_pad; k += IP_THREADS) sm.acc[k] = 0ull;
-}
-
-// The large-grid deposit: CIC weights (1 - rem, rem) of the new position
-// added to an f32 histogram, and the flush of its nodes (boundary nodes
-// doubled; four nodes per vector atomic) into dens_out, which clears them.
-__device__ __forceinline__ void dep_add_f32(float *h, float x, const cudapic_grid &g) {
-    const float pos = x * g.inv_dx;
-    const int p = cell_of(pos, g.n_g);
-    const float rem = fminf(pos - (float)p, 1.0f);
-    atomicAdd(&h[p], 1.0f - rem);
-    atomicAdd(&h[p + 1], rem);
-}
-
-__device__ __forceinline__ void dep_flush_f32(float *h, float *dens_out, const cudapic_grid &g) {
-    const uint32_t n_g = g.n_g;
-    const bool vec = (reinterpret_cast<uintptr_t>(dens_out) & 15u) == 0;
-    for (uint32_t k = 4u * threadIdx.x; k < n_g; k += 4u * blockDim.x) {
-        float v[4];
-        bool any = false;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const uint32_t node = k + (uint32_t)u;
-            const float a = node < n_g ? h[node] : 0.0f;
-            if (node < n_g) h[node] = 0.0f;
-            v[u] = a * g.weight_factor;
-            if (node == 0 || node == n_g - 1) v[u] *= 2.0f;
-            any |= a != 0.0f;
-        }
-        if (any) red_add4(dens_out, k, n_g, v, vec);
-    }
 }
 
 // Bulk prefetch of [p, p + bytes) into L2 (16-byte aligned, bytes a
@@ -238,7 +213,7 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
         const float vz[IP_ROW] = {VZ.x, VZ.y, VZ.z, VZ.w};
         uint32_t s[4][IP_ROW] = {{R0.x, R0.y, R0.z, R0.w}, {R1.x, R1.y, R1.z, R1.w}, {R2.x, R2.y, R2.z, R2.w},
                                  {R3.x, R3.y, R3.z, R3.w}};
-        uint32_t kept = 0, coll = 0;  // bit u: slot s0 + u survives / collides
+        uint32_t kept = 0, coll = 0, ioniz = 0;  // bit u: slot s0 + u survives / collides / ionizes
         // (1) push; dead and past-the-end slots push a harmless stand-in and are masked
 #pragma unroll
         for (int u = 0; u < IP_ROW; ++u) {
@@ -268,10 +243,22 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
                 const float v2 = vx[u] * vx[u] + vy[u] * vy[u] + vz[u] * vz[u];
                 const float rnd = rs.uniform();
                 if (may_collide(rnd, v2, rej_k2)) {
-                    // (3) the exact test where the bound cannot decide (a few per cent)
+                    // (3) the exact test where the bound cannot decide (a few per cent),
+                    //     with the scattering's three process entries fetched beside it
                     const float velocity = sqrtf(v2);
                     const uint32_t idx = energy_index(gm.half_me_over_e * v2);
-                    if (collision_draw(rnd, __ldg(dcp<SH>(dc.sigma_tot) + idx) * velocity * dt)) coll |= 1u << u;
+                    const float *cs = dcp<SH>(dc.cs);
+                    const float st = __ldg(dcp<SH>(dc.sigma_tot) + idx);
+                    const float c0 = __ldg(cs + idx), c1 = __ldg(cs + CS_RANGES + idx);
+                    const float c2 = __ldg(cs + 2 * CS_RANGES + idx);
+                    if (collision_draw(rnd, st * velocity * dt)) {
+                        coll |= 1u << u;
+                        // collision_e's event draw (its first), from a copy of the
+                        // state: an ionization takes 7 draws, the other events 3
+                        Xoshiro128p re = rs;
+                        const float t1 = c0 + c1, t2 = t1 + c2;
+                        if (!(re.uniform() < t1 / t2)) ioniz |= 1u << u;
+                    }
                 }
                 s[0][u] = rs.s0;
                 s[1][u] = rs.s1;
@@ -285,10 +272,6 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
         if (any) {
             *reinterpret_cast<float4 *>(pl.x + i0) = make_float4(x[0], x[1], x[2], x[3]);
             *reinterpret_cast<float4 *>(pl.vx + i0) = make_float4(vx[0], vx[1], vx[2], vx[3]);
-            *reinterpret_cast<uint4 *>(pl.rng0 + i0) = make_uint4(s[0][0], s[0][1], s[0][2], s[0][3]);
-            *reinterpret_cast<uint4 *>(pl.rng1 + i0) = make_uint4(s[1][0], s[1][1], s[1][2], s[1][3]);
-            *reinterpret_cast<uint4 *>(pl.rng2 + i0) = make_uint4(s[2][0], s[2][1], s[2][2], s[2][3]);
-            *reinterpret_cast<uint4 *>(pl.rng3 + i0) = make_uint4(s[3][0], s[3][1], s[3][2], s[3][3]);
         }
         // (4) queue this round's colliders as records (warp-synchronous), a
         //     flush after every row keeps the queue below 64
@@ -313,6 +296,26 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
                 if (qn >= 32) flush_records(sm, qn, false, list, count);
             }
         }
+        // (5) the RNG state of every slot; a collider's goes past all of its
+        //     scattering's draws (the record keeps the state the scattering starts from)
+#pragma unroll
+        for (int u = 0; u < IP_ROW; ++u) {
+            if (coll >> u & 1u) {
+                Xoshiro128p rs{s[0][u], s[1][u], s[2][u], s[3][u]};
+                const int draws = (ioniz >> u & 1u) ? 7 : 3;
+                for (int k = 0; k < draws; ++k) rs.next();
+                s[0][u] = rs.s0;
+                s[1][u] = rs.s1;
+                s[2][u] = rs.s2;
+                s[3][u] = rs.s3;
+            }
+        }
+        if (any) {
+            *reinterpret_cast<uint4 *>(pl.rng0 + i0) = make_uint4(s[0][0], s[0][1], s[0][2], s[0][3]);
+            *reinterpret_cast<uint4 *>(pl.rng1 + i0) = make_uint4(s[1][0], s[1][1], s[1][2], s[1][3]);
+            *reinterpret_cast<uint4 *>(pl.rng2 + i0) = make_uint4(s[2][0], s[2][1], s[2][2], s[2][3]);
+            *reinterpret_cast<uint4 *>(pl.rng3 + i0) = make_uint4(s[3][0], s[3][1], s[3][2], s[3][3]);
+        }
     }
     flush_records(sm, qn, true, list, count);
     __syncthreads();
@@ -328,7 +331,8 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
 // The scatter pass for record k of a discharge's collider list (its planes
 // at element `off`), the collision code inlined so that the loads of the
 // record, the table entries and the slot's position overlap: the recorded
-// RNG state continues past the test draw
+// RNG state (the slot's final state is already written by the stream pass)
+// continues past the test draw
 // (collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused step's
 // algebraic sines and cosines); velocity and RNG state go back to the slot,
 // a spawned electron takes the next slot of n_e, a spawned ion the next slot
@@ -345,10 +349,6 @@ __device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const C
     const uint32_t idx = energy_index(g.half_me_over_e * v2);
     collide_electron_body<true, true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx,
                                       pl.ivy, pl.ivz, n_e, n_i, g, dens_e, dens_i, xi);
-    pl.rng0[j] = rs.s0;
-    pl.rng1[j] = rs.s1;
-    pl.rng2[j] = rs.s2;
-    pl.rng3[j] = rs.s3;
 }
 
 }  // namespace cudapic

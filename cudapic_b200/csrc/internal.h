@@ -181,8 +181,9 @@ int rng_sidecar_read(const char *path, uint32_t capacity, std::vector<uint32_t> 
 // be null): receives the slot count the stream pass saw.
 struct InplacePlanes;
 struct CollList;
-int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, float sigma_max,
-                            const uint32_t *n_active, const CollList &list, uint32_t *count, float *dens_e,
+int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, const float *cs,
+                            float sigma_max, const uint32_t *n_active, const CollList &list, uint32_t *count,
+                            float *dens_e,
                             const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
                             uint32_t *spawn_from);
 // The next step's Poisson solve (launch_poisson's arguments), run by the

@@ -551,7 +551,9 @@ int launch_batch_step_t(const StepPlanes &pl, const BatchDisc *desc, const uint3
     auto bytes = [&]() { return step_smem_bytes<U, MCC>(stages, copies, ef_pad) + plan; };
     const size_t budget = (size_t)max_smem_optin();
     while (bytes() > budget && stages > 2) --stages;
-    while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
+    // below 4 copies the f32 histogram (copies = 0) takes over: 8 B per node
+    auto fewer = [&]() { copies = copies / 2 < 4 ? 0 : copies / 2; };
+    while (bytes() > budget && copies > 0) fewer();
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "batch step: n_g too large");
     auto kern = batch_step_kernel<U, MCC, MINB, MEAS>;
     int per_sm = 0;
@@ -563,15 +565,15 @@ int launch_batch_step_t(const StepPlanes &pl, const BatchDisc *desc, const uint3
     };
     CUDAPIC_CHECK(occupancy());
     // large grids: fewer histogram copies rather than fewer CTAs per SM
-    while (per_sm < t.step_ctas_per_sm && copies > 1) {
-        copies = (copies + 1) / 2;
+    while (per_sm < t.step_ctas_per_sm && copies > 0) {
+        fewer();
         CUDAPIC_CHECK(occupancy());
     }
     const size_t smem = bytes();
     per_sm = std::min(std::max(per_sm, 1), t.step_ctas_per_sm);
     const unsigned grid = persistent_grid(per_sm, (cap_sum + TILE - 1) / TILE);
-    const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
-    const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
+    const uint32_t per_tile = copies ? (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u : 1u;
+    const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_tile) : 0xffffffffu;
     return launch_kernel(MCC ? "batch_step_electrons" : "batch_push_ions", kern, dim3(grid), dim3(ES_THREADS), smem,
                          stream, pl, desc, counts, D, r, ef_pad, stages, copies, epoch);
 }
@@ -645,7 +647,7 @@ int launch_batch_scatter(const InplacePlanes &pl, const CollList &list, const Ba
     if (D == 0 || D > BATCH_MAX_DISCHARGES) return fail(CUDAPIC_ERR_ARG, "batch scatter: bad discharge count");
     const size_t plan = (size_t)(D + 1) * sizeof(uint32_t);
     auto kern = r.measure ? batch_scatter_kernel<true> : batch_scatter_kernel<false>;
-    const unsigned grid = persistent_grid(2, (cap_sum + IP_THREADS - 1) / IP_THREADS);
+    const unsigned grid = persistent_grid(tuning().scatter_ctas_per_sm, (cap_sum + IP_THREADS - 1) / IP_THREADS);
     return launch_kernel("batch_scatter_electrons", kern, dim3(grid), dim3(IP_THREADS), plan, stream, pl, list, desc,
                          D, r.dens, r.dens_i, ticket);
 }

@@ -23,7 +23,8 @@ namespace cudapic {
 template <bool MEAS>
 __global__ void __launch_bounds__(IP_THREADS, 4)
     electron_inplace_kernel(const InplacePlanes pl, const float *__restrict__ efield,
-                            const float *__restrict__ sigma_tot_e, float sigma_max, const uint32_t *n_active,
+                            const float *__restrict__ sigma_tot_e, const float *__restrict__ cs, float sigma_max,
+                            const uint32_t *n_active,
                             const CollList list, uint32_t *count, float *dens_e,
                             const __grid_constant__ cudapic_grid g, uint32_t ef_pad, int copies, uint32_t epoch,
                             cudapic_wall_counters *wall, uint32_t *spawn_from, uint32_t pf) {
@@ -41,7 +42,7 @@ __global__ void __launch_bounds__(IP_THREADS, 4)
     StepDisc dc;
     dc.efield = efield;
     dc.sigma_tot = sigma_tot_e;
-    dc.cs = nullptr;
+    dc.cs = cs;
     dc.sigma_max = sigma_max;
     dc.factor = g.factor_e;
     dc.dt = g.dt_e;
@@ -160,9 +161,9 @@ bool inplace_eligible(const void *const *planes, int count, uint32_t capacity) {
     return electron_step_eligible(planes, count, capacity);
 }
 
-int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, float sigma_max,
-                            const uint32_t *n_active, const CollList &list, uint32_t *count, float *dens_e,
-                            const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
+int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const float *sigma_tot_e, const float *cs,
+                            float sigma_max, const uint32_t *n_active, const CollList &list, uint32_t *count,
+                            float *dens_e, const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
                             uint32_t *spawn_from) {
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
@@ -193,7 +194,7 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
     const uint32_t per_round = copies ? (uint32_t)((IP_WARPS + copies - 1) / copies) * 32u * IP_ROW : 1u;
     const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_round) : 0xffffffffu;
     return launch_kernel("step_electrons_inplace", kern, dim3(grid), dim3(IP_THREADS),
-                         inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, sigma_max, n_active, list,
+                         inplace_smem_bytes(copies, ef_pad), stream, pl, efield, sigma_tot_e, cs, sigma_max, n_active, list,
                          count, dens_e, g, ef_pad, copies, epoch, wall, spawn_from,
                          (uint32_t)std::max(t.inplace_prefetch, 0));
 }
@@ -202,9 +203,10 @@ int launch_electron_scatter(const InplacePlanes &pl, const CollList &list, const
                             uint32_t *ticket, uint32_t *n_e, uint32_t *n_i, const cudapic_grid &g,
                             cudaStream_t stream, float *dens_e, float *dens_i, unsigned long long *coll,
                             const PoissonAhead *ahead) {
-    // two CTAs per SM: every thread loops over records, and the completion
-    // ticket has fewer CTAs to count
-    const unsigned grid = persistent_grid(2, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
+    // every thread loops over records; CTAs per SM from the tuning (the
+    // completion ticket counts them)
+    const unsigned grid =
+        persistent_grid(tuning().scatter_ctas_per_sm, ((uint64_t)g.capacity + IP_THREADS - 1) / IP_THREADS);
     if (!ahead)
         return launch_kernel("scatter_colliders_e", electron_scatter_kernel<0>, dim3(grid), dim3(IP_THREADS), 0,
                              stream, pl, list, cs, count, ticket, n_e, n_i, g, dens_e, dens_i, coll, PoissonAhead{});
@@ -224,12 +226,13 @@ using namespace cudapic;
 
 extern "C" int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy,
                                               const float *vz, uint32_t *rng0, uint32_t *rng1, uint32_t *rng2,
-                                              uint32_t *rng3, const float *total_cs_e, float sigma_max_e,
+                                              uint32_t *rng3, const float *total_cs_e, const float *cs,
+                                              float sigma_max_e,
                                               const uint32_t *n_e, uint32_t *const coll[8], uint32_t *n_colliders,
                                               float *e_next_density, const cudapic_grid *grid,
                                               cudapic_stream_t stream) {
     CUDAPIC_CHECK(validate_grid(grid));
-    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && n_e && coll &&
+    CUDAPIC_REQUIRE(efield && x && vx && vy && vz && rng0 && rng1 && rng2 && rng3 && total_cs_e && cs && n_e && coll &&
                         n_colliders && e_next_density,
                     "step_electrons_inplace: null pointer");
     for (int k = 0; k < 8; ++k) CUDAPIC_REQUIRE(coll[k], "step_electrons_inplace: null record plane");
@@ -241,7 +244,7 @@ extern "C" int cudapic_step_electrons_inplace(const float *efield, float *x, flo
                            nullptr, nullptr, nullptr, nullptr};
     const CollList list{coll[0], reinterpret_cast<float *>(coll[1]), reinterpret_cast<float *>(coll[2]),
                         reinterpret_cast<float *>(coll[3]), coll[4], coll[5], coll[6], coll[7]};
-    return launch_electron_inplace(pl, efield, total_cs_e, sigma_max_e, n_e, list, n_colliders, e_next_density,
+    return launch_electron_inplace(pl, efield, total_cs_e, cs, sigma_max_e, n_e, list, n_colliders, e_next_density,
                                    *grid, (cudaStream_t)stream, nullptr, nullptr);
 }
 

@@ -46,7 +46,8 @@ struct TileOut {
 
 // DEPOSIT: also deposit every survivor's new position into dens_out (the
 // charge density of the next time step), through `copies` warp-private
-// fixed-point shared histograms (see dep_add) drained every `epoch` tiles.
+// fixed-point shared histograms (see dep_add) drained every `epoch` tiles,
+// or with copies == 0 (large grids) one f32 histogram (dep_add_f32).
 template <bool DEPOSIT>
 __global__ void __launch_bounds__(MC_THREADS)
     move_and_compact_tma_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
@@ -61,7 +62,10 @@ __global__ void __launch_bounds__(MC_THREADS)
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
     float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);  // [ef_pad] (DEPOSIT)
-    uint32_t *hist = reinterpret_cast<uint32_t *>(acc + (DEPOSIT ? ef_pad : 0));     // [copies][ef_pad]
+    float *hf = reinterpret_cast<float *>(acc);  // copies == 0: the f32 histogram [ef_pad] in its place
+    uint32_t *hist = !DEPOSIT ? reinterpret_cast<uint32_t *>(acc)
+                     : copies ? reinterpret_cast<uint32_t *>(acc + ef_pad)
+                              : reinterpret_cast<uint32_t *>(ef + 2u * ef_pad);  // [copies][ef_pad]
     uint64_t *bar = reinterpret_cast<uint64_t *>(hist + (DEPOSIT ? copies * ef_pad : 0));
     __shared__ uint32_t offs[2][MC_U * MC_WARPS];        // counts, then exclusive offsets
     __shared__ uint32_t s_base[2];
@@ -77,7 +81,10 @@ __global__ void __launch_bounds__(MC_THREADS)
     }
     if (DEPOSIT) {
         for (uint32_t k = tid; k < (uint32_t)copies * ef_pad; k += MC_THREADS) hist[k] = 0u;
-        for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) acc[k] = 0ull;
+        if (copies)
+            for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) acc[k] = 0ull;
+        else
+            for (uint32_t k = tid; k < ef_pad; k += MC_THREADS) hf[k] = 0.0f;
     }
     grid_dep_wait();
     const uint32_t n = load_count(n_active, g.capacity, g.dev_err);
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(MC_THREADS)
     uint32_t pending_base = 0;  // warp 0 lane 31: atomicAdd result of the previous tile
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        if (DEPOSIT && it != 0 && it % epoch == 0) {  // drain the copies before they can overflow
+        if (DEPOSIT && copies && it != 0 && it % epoch == 0) {  // drain the copies before they can overflow
             __syncthreads();
             dep_drain(hist, copies, ef_pad, acc, g.n_g);
             __syncthreads();
@@ -146,7 +153,10 @@ __global__ void __launch_bounds__(MC_THREADS)
                 cur.vy[u] = bvy[j];
                 cur.vz[u] = bvz[j];
             }
-            if (DEPOSIT && keep) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            if (DEPOSIT && keep) {  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+                if (copies) dep_add(h, cur.x[u], g);
+                else dep_add_f32(hf, cur.x[u], g);
+            }
             if (wall) count_wall(wall, wall_ions, j < cnt && !keep, cur.x[u], cur.vx[u], cur.vy[u], cur.vz[u], g.gap);
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             cur.lane_off[u] = __popc(m & lt);
@@ -202,11 +212,15 @@ __global__ void __launch_bounds__(MC_THREADS)
             }
         }
     }
-    if (DEPOSIT) {  // sum the warp copies, one global atomic per non-empty node
+    if (DEPOSIT) {  // sum the warp copies, one global atomic per four nodes
         __syncthreads();
-        dep_drain(hist, copies, ef_pad, acc, g.n_g);
-        __syncthreads();
-        dep_flush(acc, dens_out, g);
+        if (copies) {
+            dep_drain(hist, copies, ef_pad, acc, g.n_g);
+            __syncthreads();
+            dep_flush(acc, dens_out, g);
+        } else {
+            dep_flush_f32(hf, dens_out, g);
+        }
     }
     publish_count(link.ticket, link.dst, link.src, link.clear_src, g.capacity);
 }
@@ -299,11 +313,18 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         auto bytes = [&](int st) {
             const size_t pad = (g.n_g + 3u) & ~3u;
             return tma_smem_bytes(g.n_g, st, ef_pad) +
-                   (dep ? pad * sizeof(unsigned long long) + (size_t)copies * pad * sizeof(uint32_t) : 0);
+                   (!dep ? 0
+                    : copies ? pad * sizeof(unsigned long long) + (size_t)copies * pad * sizeof(uint32_t)
+                             : pad * sizeof(float));
         };
+        // below 4 copies the f32 histogram (copies = 0) takes over
+        auto fewer = [&]() { copies = copies / 2 < 4 ? 0 : copies / 2; };
         size_t smem = bytes(stages);
         while (smem > (size_t)max_smem_optin() && stages > 2) smem = bytes(--stages);
-        while (smem > (size_t)max_smem_optin() && copies > 1) smem = bytes(copies = (copies + 1) / 2);
+        while (dep && smem > (size_t)max_smem_optin() && copies > 0) {
+            fewer();
+            smem = bytes(stages);
+        }
         if (smem > (size_t)max_smem_optin()) return fail(CUDAPIC_ERR_ARG, "move_and_compact: n_g too large");
         auto kern = dep ? move_and_compact_tma_kernel<true> : move_and_compact_tma_kernel<false>;
         int per_sm = 0;
@@ -315,8 +336,8 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         };
         CUDAPIC_CHECK(occupancy());
         // large grids: fewer histogram copies rather than fewer CTAs per SM
-        while (dep && per_sm < t.push_ctas_per_sm && copies > 1) {
-            copies = (copies + 1) / 2;
+        while (dep && per_sm < t.push_ctas_per_sm && copies > 0) {
+            fewer();
             smem = bytes(stages);
             CUDAPIC_CHECK(occupancy());
         }
@@ -325,7 +346,7 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         const unsigned grid = persistent_grid(per_sm, tiles_max);
         // tiles per drain: a copy receives the particles of ceil(MC_WARPS / copies) warps, MC_U * 32 per tile each
         const uint32_t per_tile = (uint32_t)((MC_WARPS + std::max(copies, 1) - 1) / std::max(copies, 1)) * MC_U * 32u;
-        const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
+        const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_tile) : 0xffffffffu;
         return launch_kernel("move_and_compact_tma", kern, dim3(grid), dim3(MC_THREADS), smem, stream, efield, sx, svx,
                              svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g, ef_pad, stages, dens_out,
                              copies, epoch, link, wall, (int)wall_ions);

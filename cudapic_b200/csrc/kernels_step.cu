@@ -137,7 +137,9 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     auto bytes = [&]() { return step_smem_bytes<U, true>(stages, copies, ef_pad); };
     const size_t budget = (size_t)max_smem_optin();
     while (bytes() > budget && stages > 2) --stages;
-    while (bytes() > budget && copies > 1) copies = (copies + 1) / 2;
+    // below 4 copies the f32 histogram (copies = 0) takes over: 8 B per node
+    auto fewer = [&]() { copies = copies / 2 < 4 ? 0 : copies / 2; };
+    while (bytes() > budget && copies > 0) fewer();
     if (bytes() > budget) return fail(CUDAPIC_ERR_ARG, "step_electrons: n_g too large");
     auto kern = electron_step_kernel<U>;
     int per_sm = 0;
@@ -150,8 +152,8 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     CUDAPIC_CHECK(occupancy());
     // large grids: fewer histogram copies rather than fewer CTAs per SM (the
     // copies only spread atomic conflicts, which a large grid spreads by itself)
-    while (per_sm < t.step_ctas_per_sm && copies > 1) {
-        copies = (copies + 1) / 2;
+    while (per_sm < t.step_ctas_per_sm && copies > 0) {
+        fewer();
         CUDAPIC_CHECK(occupancy());
     }
     const size_t smem = bytes();
@@ -159,8 +161,8 @@ int launch_electron_step_t(const float *efield, const float *sx, const float *sv
     const uint64_t tiles_max = ((uint64_t)g.capacity + ES_TILE - 1) / ES_TILE;
     const unsigned grid = persistent_grid(per_sm, tiles_max);
     // tiles per deposit drain: a copy receives ceil(WARPS / copies) warps x 128 particles per tile
-    const uint32_t per_tile = (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u;
-    const uint32_t epoch = std::max(1u, DEP_MAX_PER_COPY / per_tile);
+    const uint32_t per_tile = copies ? (uint32_t)((ES_WARPS + copies - 1) / copies) * U * 32u : 1u;
+    const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_tile) : 0xffffffffu;
     return launch_kernel("step_electrons", kern, dim3(grid), dim3(ES_THREADS), smem, stream, efield, sx, svx, svy, svz,
                          dx_, dvx, dvy, dvz, rng0, rng1, rng2, rng3, sigma_tot_e, cs, sigma_max_e, ix, ivx, ivy, ivz,
                          alive, n_active, n_i, dens_e, dens_i, g, ef_pad, stages, copies, epoch, link, wall, coll);

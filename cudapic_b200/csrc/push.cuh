@@ -142,4 +142,37 @@ __device__ __forceinline__ void dep_flush(unsigned long long *acc, float *dens_o
     }
 }
 
+// The large-grid deposit of the fused kernels: CIC weights (1 - rem, rem)
+// of the new position added to one f32 shared histogram per CTA (at
+// thousands of nodes the lanes rarely meet on a node, and the fixed-point
+// copies would need a drain every few tiles), and the flush of its nodes
+// (boundary nodes doubled; four nodes per vector atomic) into dens_out,
+// which clears them.
+__device__ __forceinline__ void dep_add_f32(float *h, float x, const cudapic_grid &g) {
+    const float pos = x * g.inv_dx;
+    const int p = cell_of(pos, g.n_g);
+    const float rem = fminf(pos - (float)p, 1.0f);
+    atomicAdd(&h[p], 1.0f - rem);
+    atomicAdd(&h[p + 1], rem);
+}
+
+__device__ __forceinline__ void dep_flush_f32(float *h, float *dens_out, const cudapic_grid &g) {
+    const uint32_t n_g = g.n_g;
+    const bool vec = (reinterpret_cast<uintptr_t>(dens_out) & 15u) == 0;
+    for (uint32_t k = 4u * threadIdx.x; k < n_g; k += 4u * blockDim.x) {
+        float v[4];
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t node = k + (uint32_t)u;
+            const float a = node < n_g ? h[node] : 0.0f;
+            if (node < n_g) h[node] = 0.0f;
+            v[u] = a * g.weight_factor;
+            if (node == 0 || node == n_g - 1) v[u] *= 2.0f;
+            any |= a != 0.0f;
+        }
+        if (any) red_add4(dens_out, k, n_g, v, vec);
+    }
+}
+
 }  // namespace cudapic

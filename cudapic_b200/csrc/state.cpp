@@ -150,7 +150,7 @@ int enqueue_fused_particles(cudapic_state *s, bool ion_step, float *e_next, floa
                             reinterpret_cast<uint32_t *>(s->vx[I][si ^ 1]),
                             reinterpret_cast<uint32_t *>(s->vy[I][si ^ 1]),
                             reinterpret_cast<uint32_t *>(s->vz[I][si ^ 1])};
-        CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->sigma_max_e, s->n_e(), list,
+        CUDAPIC_CHECK(launch_electron_inplace(pl, s->efield, s->sigma_tot_e, s->cs, s->sigma_max_e, s->n_e(), list,
                                               s->counters + CTR_COLL_COUNT, e_next, g, st,
                                               s->measure ? s->wall : nullptr, s->counters + CTR_SPAWN_FROM));
         // the next step's solve in the scatter pass: only when nothing that

@@ -41,11 +41,14 @@ struct StepShape {
 
 // Dynamic shared memory: [stages][PLANES][TILE] staged planes, E[ef_pad],
 // the 64-bit deposit accumulator [ef_pad], [copies][ef_pad] fixed-point
-// histograms, the warps' collider queues, the stage mbarriers.
+// histograms, the warps' collider queues, the stage mbarriers.  copies == 0
+// selects the large-grid deposit: one f32 histogram [ef_pad] in the
+// accumulator's place and no copies (push.cuh dep_add_f32).
 template <int U, bool MCC>
 __host__ __device__ constexpr size_t step_smem_bytes(int stages, int copies, uint32_t ef_pad) {
     using S = StepShape<U, MCC>;
-    return (size_t)stages * S::PLANES * S::TILE * 4 + (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 +
+    return (size_t)stages * S::PLANES * S::TILE * 4 +
+           (copies ? (size_t)ef_pad * (4 + 8) + (size_t)copies * ef_pad * 4 : (size_t)ef_pad * (4 + 4)) +
            (size_t)S::QCAP * 4 + (size_t)stages * sizeof(uint64_t);
 }
 
@@ -96,8 +99,8 @@ struct StepSmem {
         using S = StepShape<U, MCC>;
         in = reinterpret_cast<uint32_t *>(smem);
         ef = reinterpret_cast<float *>(in + stages * S::PLANES * S::TILE);
-        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);
-        hist = reinterpret_cast<uint32_t *>(acc + ef_pad);
+        acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);  // the f32 histogram when copies == 0
+        hist = copies ? reinterpret_cast<uint32_t *>(acc + ef_pad) : reinterpret_cast<uint32_t *>(ef + 2u * ef_pad);
         queue = hist + (uint32_t)copies * ef_pad;
         bar = reinterpret_cast<uint64_t *>(queue + S::QCAP);
         offs = offs_;
@@ -152,6 +155,11 @@ __device__ __forceinline__ void step_smem_init(const StepSmem<U, MCC> &sm, int s
         fence_mbar_init();
     }
     for (uint32_t k = threadIdx.x; k < (uint32_t)copies * ef_pad; k += ES_THREADS) sm.hist[k] = 0u;
+    if (copies == 0) {
+        float *hf = reinterpret_cast<float *>(sm.acc);
+        for (uint32_t k = threadIdx.x; k < ef_pad; k += ES_THREADS) hf[k] = 0.0f;
+        return;
+    }
     for (uint32_t k = threadIdx.x; k < ef_pad; k += ES_THREADS) sm.acc[k] = 0ull;
 }
 
@@ -211,7 +219,8 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
     };
 
     for (uint32_t k = tid; k < g.n_g; k += ES_THREADS) sm.ef[k] = dcp<SH>(dc.efield)[k];
-    uint32_t *h = sm.hist + (uint32_t)(warp % copies) * ef_pad;
+    uint32_t *h = copies ? sm.hist + (uint32_t)(warp % copies) * ef_pad : nullptr;
+    float *hf = reinterpret_cast<float *>(sm.acc);  // the large-grid deposit (copies == 0)
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < stages; ++s)
@@ -256,7 +265,7 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
     uint32_t tile = 0;
     for (; tile < ntiles; ++tile) {
         const uint32_t k = it0 + tile;  // position in the stage ring
-        if (tile != 0 && k % epoch == 0) {  // drain the deposit copies before they can overflow
+        if (copies && tile != 0 && k % epoch == 0) {  // drain the deposit copies before they can overflow
             __syncthreads();
             dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
             __syncthreads();
@@ -343,7 +352,10 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
             const bool kept = keep >> u & 1u;
             const bool collide = MCC && (coll >> u & 1u);
             const bool stay = kept && !collide;
-            if (kept) dep_add(h, cur.x[u], g);  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+            if (kept) {  // CIC of the new position, Rust-CUDA/src/main.rs:377-387
+                if (copies) dep_add(h, cur.x[u], g);
+                else dep_add_f32(hf, cur.x[u], g);
+            }
             if (MCC && stay) {
                 const uint32_t i = off + t0 + j;
                 pl.rng0[i] = st[u][0];
@@ -455,9 +467,13 @@ __device__ __forceinline__ bool step_segment(const StepPlanes &pl, const StepDis
         drain(qn);
     }
     __syncthreads();
-    dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
-    __syncthreads();
-    dep_flush(sm.acc, dcp<SH>(dc.dens), gm);  // clears the accumulator
+    if (copies) {
+        dep_drain(sm.hist, copies, ef_pad, sm.acc, g.n_g);
+        __syncthreads();
+        dep_flush(sm.acc, dcp<SH>(dc.dens), gm);  // clears the accumulator
+    } else {
+        dep_flush_f32(hf, dcp<SH>(dc.dens), gm);  // clears the histogram
+    }
     it = it0 + tile;
     return ok;
 }

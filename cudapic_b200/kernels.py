@@ -130,13 +130,14 @@ def _planes8(coll):
     return (ctypes.c_void_p * 8)(*[_ptr(a) for a in coll])
 
 
-def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, sigma_max_e, n_e, coll,
+def step_electrons_inplace(efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, cs, sigma_max_e, n_e, coll,
                            n_colliders, e_next_density, grid, stream=None):
     """In-place electron step, stream pass: push, absorption (x set to
     CUDAPIC_DEAD_X), collision test and next-step deposit with every electron
     kept in its slot; each collider recorded in the eight `coll` planes
-    (slot, vx, vy, vz, RNG state)."""
-    head = [_ptr(a) for a in (efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e)]
+    (slot, vx, vy, vz, RNG state), its slot's RNG state advanced past its
+    scattering's draws."""
+    head = [_ptr(a) for a in (efield, x, vx, vy, vz, rng0, rng1, rng2, rng3, total_cs_e, cs)]
     check(lib.cudapic_step_electrons_inplace(*head, float(sigma_max_e), _ptr(n_e), _planes8(coll), _ptr(n_colliders),
                                              _ptr(e_next_density), _g(grid), _stream(stream, x)))
 

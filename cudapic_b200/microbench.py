@@ -4,7 +4,8 @@ L2 flushed before each launch): the target of the committed ncu captures.
     python -m cudapic_b200.microbench --kernel check_collisions_e [--particles N] [--reps 3] [--tuning k=v ...]
 
 Kernels: get_density, solve_poisson, move_and_compact, move_and_compact_deposit,
-check_collisions_e, check_collisions_e_deposit, check_collisions_i and
+check_collisions_e, check_collisions_e_deposit, check_collisions_i (and
+check_collisions_i_bounded, the drivers' entry given max(sigma_tot_i)) and
 step_electrons (the *_deposit variants also deposit the next step's density;
 step_electrons is the fused driver's compacting electron kernel,
 step_electrons_inplace the stream pass of its in-place step).  Prints one JSON line with the median time, the particle
@@ -15,7 +16,8 @@ import json
 import statistics
 
 BYTES = {"get_density": 4, "move_and_compact": 32, "move_and_compact_deposit": 32, "check_collisions_e": 44,
-         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "solve_poisson": 0, "step_electrons": 64,
+         "check_collisions_e_deposit": 44, "check_collisions_i": 44, "check_collisions_i_bounded": 44,
+         "solve_poisson": 0, "step_electrons": 64,
          "step_electrons_inplace": 56}
 
 
@@ -53,6 +55,7 @@ def main():
     ef = torch.zeros(g.n_g, dtype=torch.float32, device="cuda")
     alive = u32(0)
     ccount = u32(0)
+    sigma_max_i = float(K.init_cross_sections(g.gas_density)[2].max())  # the ion table's largest entry
     fns = {
         "get_density": (lambda: K.get_density(b.x[0], dens, ne_c, g, stream=s), lambda: dens.zero_(), n_e),
         "solve_poisson": (lambda: K.solve_poisson_scan_f32(b.e_density, b.i_density, pot, ef, 250.0, g, stream=s),
@@ -77,9 +80,12 @@ def main():
             stream=s), lambda: (alive.zero_(), alive_i.fill_(n_i), dens.zero_()), n_e),
         "check_collisions_i": (lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                             *b.rng[1], g, stream=s), None, n_i),
+        "check_collisions_i_bounded": (lambda: K.check_collisions_i(
+            b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1], *b.rng[1], g, stream=s,
+            sigma_max_i=sigma_max_i), None, n_i),
         # the in-place step's stream pass (each launch advances the live planes by one step)
         "step_electrons_inplace": (lambda: K.step_electrons_inplace(
-            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.sigma_max_e, ne_c,
+            b.efield, b.x[0], b.vx[0], b.vy[0], b.vz[0], *b.rng[0], b.sigma_tot_e, b.cs, b.sigma_max_e, ne_c,
             (b.tmp_x[0], b.tmp_vx[0], b.tmp_vy[0], b.tmp_vz[0], b.tmp_x[1], b.tmp_vx[1], b.tmp_vy[1], b.tmp_vz[1]),
             ccount, dens, g, stream=s), lambda: (ccount.zero_(), dens.zero_()), n_e),
     }

@@ -148,6 +148,7 @@ typedef struct cudapic_tuning {
     int inplace_copies;       /* in-place electron step: deposit histogram copies (1..8)   */
     int inplace_prefetch;     /* in-place electron step: rounds of a CTA's slots prefetched
                                  into L2 ahead of their loads (1..4), -1: none             */
+    int scatter_ctas_per_sm;  /* in-place electron step, scatter pass: CTAs per SM (1..8)   */
 } cudapic_tuning;
 
 int cudapic_get_tuning(cudapic_tuning *out);
@@ -257,10 +258,13 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
  *    cudapic_step_electrons drops them while compacting.  Each collider is
  *    recorded in the eight planes coll[0..7] (capacity entries each: slot,
  *    vx, vy, vz, then the four words of its RNG state past the test draw)
- *    and counted in *n_colliders (zero on entry).  *n_e is unchanged.
+ *    and counted in *n_colliders (zero on entry); the RNG state written to
+ *    a collider's slot is already the one past all of its scattering's
+ *    draws (the event draw, made here from cs, tells how many).  *n_e is
+ *    unchanged.
  *  - cudapic_scatter_colliders_e scatters the recorded colliders in place,
- *    continuing each recorded stream (collision_e) and writing velocity and
- *    RNG state back to the slots;
+ *    continuing each recorded stream (collision_e) and writing the velocity
+ *    back to the slots (not the RNG state: the stream pass wrote it);
  *    spawned electrons take slots *n_e, *n_e + 1, ... (updating *n_e),
  *    spawned ions slots *n_i, ... of i_*; both are deposited into the next
  *    densities.  Its last CTA resets *n_colliders and *ticket (zero on
@@ -269,7 +273,7 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
 #define CUDAPIC_DEAD_X (-1.0f)
 int cudapic_step_electrons_inplace(const float *efield, float *x, float *vx, const float *vy, const float *vz,
                                    uint32_t *rng0, uint32_t *rng1, uint32_t *rng2, uint32_t *rng3,
-                                   const float *total_cs_e, float sigma_max_e, const uint32_t *n_e,
+                                   const float *total_cs_e, const float *cs, float sigma_max_e, const uint32_t *n_e,
                                    uint32_t *const coll[8], uint32_t *n_colliders, float *e_next_density,
                                    const cudapic_grid *grid, cudapic_stream_t stream);
 int cudapic_scatter_colliders_e(float *x, float *vx, float *vy, float *vz, uint32_t *rng0, uint32_t *rng1,

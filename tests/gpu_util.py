@@ -193,7 +193,7 @@ def check_step_inplace(K, oracle, tables, dev_tables, g, ph, x, vx, vy, vz, ef, 
     rec = [zeros(cap, np.uint32)] + [zeros(cap) for _ in range(3)] + [zeros(cap, np.uint32) for _ in range(4)]
     cnt, ticket = counter(0), counter(0)
     de, di = zeros(len(ef)), zeros(len(ef))
-    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, float(se.max()), n_e, rec, cnt, de, g)
+    K.step_electrons_inplace(dev(ef), *e_d, *r_d, dse, dcs, float(se.max()), n_e, rec, cnt, de, g)
     n_coll = int(host(cnt)[0])
     assert n_coll == int(np.count_nonzero(events))
     assert int(host(n_e)[0]) == n   # unchanged by the stream pass
