@@ -377,6 +377,7 @@ ALGO_BYTES = {  # algorithmic bytes per particle per launch
     "move_and_compact": 32,      # read x, vx, vy, vz; write them for survivors
     "check_collisions_e": 44,    # read v (12) + RNG (16), write RNG (16); colliders' v writes not counted
     "check_collisions_i": 44,
+    "check_collisions_i_bounded": 44,
     "step_electrons": 64,        # read x, v, RNG (32); write x, v, RNG of survivors (32)
     "step_electrons_inplace": 56,  # read x, v, RNG (32); write x, vx, RNG in place (24)
 }
@@ -480,6 +481,11 @@ def kernel_breakdown(st, K, reps, flush):
     res["scatter_colliders_e"]["colliders_per_step"] = n_coll
     timed("check_collisions_i", lambda: K.check_collisions_i(b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1],
                                                              *b.rng[1], g, stream=stream.cuda_stream), n_i, 44)
+    # the drivers' ion MCC: the same entry given max(sigma_tot_i), same results
+    sigma_max_i = float(K.init_cross_sections(g.gas_density)[2].max())
+    timed("check_collisions_i_bounded", lambda: K.check_collisions_i(
+        b.sigma_tot_i, b.cs, ni_c, b.vx[1], b.vy[1], b.vz[1], *b.rng[1], g, stream=stream.cuda_stream,
+        sigma_max_i=sigma_max_i), n_i, 44)
     return res
 
 
@@ -585,7 +591,7 @@ def run_one_discharge(args):
         compacting = STEP // 20 if args.inplace else STEP
         # (the solve counts every step: in the scatter pass or in a kernel of its own)
         share_w = {"solve_poisson": STEP, "step_electrons": compacting, "move_and_compact_deposit_i": ion_steps,
-                   "check_collisions_i": ion_steps}
+                   "check_collisions_i_bounded": ion_steps}
         if args.inplace:
             share_w.update({"step_electrons_inplace": STEP - compacting, "scatter_colliders_e": STEP - compacting})
         tot = sum(breakdown[k]["us"] * w for k, w in share_w.items())

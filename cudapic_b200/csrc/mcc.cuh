@@ -324,15 +324,17 @@ __device__ __forceinline__ IonTest test_ion(float vxi, float vyi, float vzi, Xos
 template <typename Table>
 __device__ __forceinline__ bool ion_collides(float vxi, float vyi, float vzi, Xoshiro128p &rs,
                                              const Table &sigma_tot_i, const cudapic_grid &g, float k) {
-    const Xoshiro128p r0 = rs;
-    rs.next();
-    rs.next();
-    rs.next();
-    rs.next();
-    const float u = rs.uniform();
-    const float vmag = sqrtf(vxi * vxi + vyi * vyi + vzi * vzi);
-    if (u >= fmaf(k, vmag + 9.2f * g.normal_range, 6e-7f)) return false;
-    rs = r0;
+    if (k < INFINITY) {  // uniform across the launch: the drop-in entry passes +inf
+        const Xoshiro128p r0 = rs;
+        rs.next();
+        rs.next();
+        rs.next();
+        rs.next();
+        const float u = rs.uniform();
+        const float vmag = sqrtf(vxi * vxi + vyi * vyi + vzi * vzi);
+        if (u >= fmaf(k, vmag + 9.2f * g.normal_range, 6e-7f)) return false;
+        rs = r0;
+    }
     return test_ion(vxi, vyi, vzi, rs, sigma_tot_i, g).collide;
 }
 
