@@ -48,9 +48,6 @@ struct TileOut {
 // charge density of the next time step), through `copies` warp-private
 // fixed-point shared histograms (see dep_add) drained every `epoch` tiles,
 // or with copies == 0 (large grids) one f32 histogram (dep_add_f32).
-// ef_glob: the push reads the field from global memory (through L1)
-// instead of a shared copy, so that a large grid's histogram leaves room
-// for the tuned CTAs per SM (the same values: results are unchanged).
 template <bool DEPOSIT>
 __global__ void __launch_bounds__(MC_THREADS)
     move_and_compact_tma_kernel(const float *__restrict__ efield, const float *__restrict__ sx,
@@ -60,17 +57,15 @@ __global__ void __launch_bounds__(MC_THREADS)
                                 uint32_t *__restrict__ alive, const uint32_t *__restrict__ n_active,
                                 float factor, float dt, const cudapic_grid g, uint32_t ef_pad, int stages,
                                 float *__restrict__ dens_out, int copies, uint32_t epoch, const StepLink link,
-                                cudapic_wall_counters *wall, int wall_ions, int ef_glob) {
+                                cudapic_wall_counters *wall, int wall_ions) {
     extern __shared__ __align__(128) unsigned char smem[];
     float *in = reinterpret_cast<float *>(smem);        // [stages][4][TILE]
-    float *ef = in + stages * 4 * MC_TILE;               // [ef_pad], or nothing with ef_glob
-    const bool eg = DEPOSIT && ef_glob;  // only a large grid's deposit ever needs it
-    const uint32_t ef_len = eg ? 0u : ef_pad;
-    unsigned long long *acc = reinterpret_cast<unsigned long long *>(ef + ef_len);  // [ef_pad] (DEPOSIT)
+    float *ef = in + stages * 4 * MC_TILE;               // [ef_pad]
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(ef + ef_pad);  // [ef_pad] (DEPOSIT)
     float *hf = reinterpret_cast<float *>(acc);  // copies == 0: the f32 histogram [ef_pad] in its place
     uint32_t *hist = !DEPOSIT ? reinterpret_cast<uint32_t *>(acc)
                      : copies ? reinterpret_cast<uint32_t *>(acc + ef_pad)
-                              : reinterpret_cast<uint32_t *>(ef + ef_len + ef_pad);  // [copies][ef_pad]
+                              : reinterpret_cast<uint32_t *>(ef + 2u * ef_pad);  // [copies][ef_pad]
     uint64_t *bar = reinterpret_cast<uint64_t *>(hist + (DEPOSIT ? copies * ef_pad : 0));
     __shared__ uint32_t offs[2][MC_U * MC_WARPS];        // counts, then exclusive offsets
     __shared__ uint32_t s_base[2];
@@ -106,9 +101,7 @@ __global__ void __launch_bounds__(MC_THREADS)
         for (int a = 0; a < 4; ++a) bulk_load(in + (stage * 4 + a) * MC_TILE, src[a] + t0, bytes, &bar[stage]);
     };
 
-    if (!eg)
-        for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
-    const float *efp = eg ? efield : ef;
+    for (uint32_t k = tid; k < g.n_g; k += MC_THREADS) ef[k] = efield[k];
     uint32_t *h = hist + (uint32_t)(warp % max(copies, 1)) * ef_pad;
     __syncthreads();
     if (tid == 0) {
@@ -153,7 +146,7 @@ __global__ void __launch_bounds__(MC_THREADS)
             bool keep = false;
             cur.x[u] = cur.vx[u] = cur.vy[u] = cur.vz[u] = 0.0f;
             if (j < cnt) {
-                const PushResult pr = push_one(bx[j], bvx[j], efp, factor, dt, g);
+                const PushResult pr = push_one(bx[j], bvx[j], ef, factor, dt, g);
                 keep = pr.keep;
                 cur.x[u] = pr.x;
                 cur.vx[u] = pr.vx;
@@ -317,10 +310,9 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         int copies = dep ? std::max(1, std::min(t.density_copies, MC_WARPS)) : 0;
         int stages = std::min(std::max(t.push_stages, 2), MC_MAX_STAGES);
         uint32_t ef_pad;
-        int ef_glob = 0;  // the field read from global memory (no shared copy)
         auto bytes = [&](int st) {
             const size_t pad = (g.n_g + 3u) & ~3u;
-            return tma_smem_bytes(g.n_g, st, ef_pad) - (ef_glob ? pad * sizeof(float) : 0) +
+            return tma_smem_bytes(g.n_g, st, ef_pad) +
                    (!dep ? 0
                     : copies ? pad * sizeof(unsigned long long) + (size_t)copies * pad * sizeof(uint32_t)
                              : pad * sizeof(float));
@@ -349,11 +341,6 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
             smem = bytes(stages);
             CUDAPIC_CHECK(occupancy());
         }
-        if (dep && copies == 0 && per_sm < t.push_ctas_per_sm) {  // still short: drop the shared field copy
-            ef_glob = 1;
-            smem = bytes(stages);
-            CUDAPIC_CHECK(occupancy());
-        }
         per_sm = std::min(std::max(per_sm, 1), t.push_ctas_per_sm);
         const uint64_t tiles_max = ((uint64_t)g.capacity + MC_TILE - 1) / MC_TILE;
         const unsigned grid = persistent_grid(per_sm, tiles_max);
@@ -362,7 +349,7 @@ int launch_move_and_compact(const float *efield, const float *sx, const float *s
         const uint32_t epoch = copies ? std::max(1u, DEP_MAX_PER_COPY / per_tile) : 0xffffffffu;
         return launch_kernel("move_and_compact_tma", kern, dim3(grid), dim3(MC_THREADS), smem, stream, efield, sx, svx,
                              svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor, dt, g, ef_pad, stages, dens_out,
-                             copies, epoch, link, wall, (int)wall_ions, ef_glob);
+                             copies, epoch, link, wall, (int)wall_ions);
     }
     if (dens_out || link.ticket) {  // unaligned buffers: separate deposit and count copy
         CUDAPIC_CHECK(launch_move_and_compact(efield, sx, svx, svy, svz, dx_, dvx, dvy, dvz, alive, n_active, factor,
