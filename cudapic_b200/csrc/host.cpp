@@ -232,7 +232,7 @@ extern "C" int cudapic_set_tuning(const cudapic_tuning *t) {
                     (v.mcc_variant == 1 || v.mcc_variant == 2) && v.step_stages >= 2 && v.step_stages <= 6 &&
                     v.step_ctas_per_sm >= 1 && v.step_ctas_per_sm <= 8 &&
                     (v.step_rows == 1 || v.step_rows == 2 || v.step_rows == 4) && v.inplace_ctas_per_sm >= 1 &&
-                    v.inplace_ctas_per_sm <= 8 && v.inplace_copies >= 1 && v.inplace_copies <= 8 &&
+                    v.inplace_ctas_per_sm <= 8 && (v.inplace_copies == -1 || (v.inplace_copies >= 1 && v.inplace_copies <= 8)) &&
                     (v.inplace_prefetch == -1 || (v.inplace_prefetch >= 1 && v.inplace_prefetch <= 4)) &&
                     v.scatter_ctas_per_sm >= 1 && v.scatter_ctas_per_sm <= 8;
     if (!ok) return fail(CUDAPIC_ERR_ARG, "set_tuning: value out of range");

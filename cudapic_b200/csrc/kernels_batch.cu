@@ -614,7 +614,7 @@ int launch_batch_inplace(const InplacePlanes &pl, const CollList &list, const Ba
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (max_n_g + 3u) & ~3u;
     const size_t plan = (size_t)(D + 1) * sizeof(uint32_t);
-    int copies = std::max(1, std::min(t.inplace_copies, IP_WARPS));
+    int copies = t.inplace_copies < 0 ? 0 : std::max(1, std::min(t.inplace_copies, IP_WARPS));  // 0: f32
     auto bytes = [&]() { return inplace_smem_bytes(copies, ef_pad) + plan; };
     const size_t budget = (size_t)max_smem_optin();
     while (bytes() > budget && copies > 0) copies = copies / 2 < 4 ? 0 : copies / 2;

@@ -167,7 +167,7 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
                             uint32_t *spawn_from) {
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
-    int copies = std::max(1, std::min(t.inplace_copies, IP_WARPS));
+    int copies = t.inplace_copies < 0 ? 0 : std::max(1, std::min(t.inplace_copies, IP_WARPS));  // 0: f32
     const size_t budget = (size_t)max_smem_optin();
     while (inplace_smem_bytes(copies, ef_pad) > budget && copies > 0) copies = copies / 2 < 4 ? 0 : copies / 2;
     if (inplace_smem_bytes(copies, ef_pad) > budget)

@@ -145,7 +145,8 @@ typedef struct cudapic_tuning {
     int step_ctas_per_sm;
     int step_rows;            /* fused electron step particles per thread and tile: 1, 2, 4 */
     int inplace_ctas_per_sm;  /* in-place electron step: resident CTAs per SM used          */
-    int inplace_copies;       /* in-place electron step: deposit histogram copies (1..8)   */
+    int inplace_copies;       /* in-place electron step: fixed-point deposit histogram copies
+                                 (1..8), -1: one f32 shared histogram                     */
     int inplace_prefetch;     /* in-place electron step: rounds of a CTA's slots prefetched
                                  into L2 ahead of their loads (1..4), -1: none             */
     int scatter_ctas_per_sm;  /* in-place electron step, scatter pass: CTAs per SM (1..8)   */

@@ -77,3 +77,33 @@ def test_kernels_exact_under_every_shape(cudapic, oracle, tables, cuda_device, r
     g2 = cudapic.grid_from_params(capacity=cap2, n_t=100)
     ph2 = oracle.phys_from_params(capacity=cap2, n_t=100)
     check_step_electrons(K, oracle, tables, dev_tables, g2, ph2, x, vx, vy, vz, ef, cap2)
+
+
+INPLACE_SHAPES = [
+    dict(inplace_copies=-1, inplace_ctas_per_sm=4, inplace_prefetch=1, scatter_ctas_per_sm=4),
+    dict(inplace_copies=1, inplace_ctas_per_sm=2, inplace_prefetch=-1, scatter_ctas_per_sm=1),
+    dict(inplace_copies=4, inplace_ctas_per_sm=3, inplace_prefetch=3, scatter_ctas_per_sm=8),
+]
+
+
+@pytest.mark.parametrize("shape", range(len(INPLACE_SHAPES)))
+def test_inplace_step_exact_under_every_shape(cudapic, oracle, tables, cuda_device, restore_tuning, shape):
+    """The in-place electron step (stream + scatter pass) under the
+    in-place launch shapes the tuner may pick: f32 or fixed-point
+    histograms, CTAs per SM, L2 prefetch distance, scatter CTAs per SM --
+    slots, RNG states and spawns bit-exact, density within the deposit
+    tolerance of the f32 histogram."""
+    from cudapic_b200.workloads import field_profile, steady_state
+    from gpu_util import check_step_inplace, dead_mask
+    cudapic.set_tuning(**INPLACE_SHAPES[shape])
+    cs, se, si = tables
+    dev_tables = (dev(cs), dev(se), dev(si))
+    n = 300_001
+    cap = (2 * n + 4096 + 3) // 4 * 4
+    g = cudapic.grid_from_params(n_t=100, capacity=cap)
+    ph = oracle.phys_from_params(n_t=100, capacity=cap)
+    x, vx, vy, vz = steady_state(n, E_MASS, 30.0, dt=g.dt_e, seed=40 + shape)
+    m, ne, ni, nc = check_step_inplace(K=cudapic.kernels, oracle=oracle, tables=tables, dev_tables=dev_tables,
+                                       g=g, ph=ph, x=x, vx=vx, vy=vy, vz=vz, ef=field_profile(400), cap=cap,
+                                       dead=dead_mask(n, 0.02), dens_tol=max(2e-5, 1.5 * 400 * 2.0 ** -24))
+    assert nc > 1000 and ne > n
