@@ -73,8 +73,15 @@ __global__ void __launch_bounds__(SOLVE ? SC_SOLVE_THREADS : IP_THREADS)
     __shared__ uint32_t s_last;
     grid_dep_wait();
     const uint32_t n = min(*count, g.capacity);  // read before this CTA takes its ticket
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        inplace_scatter(pl, list, 0u, k, cs, n_e, n_i, g, dens_e, dens_i);
+    // chunks of 32 consecutive records, chunk c to CTA c % gridDim (a warp
+    // reads its records coalesced, and a few thousand colliders still reach
+    // every SM instead of the first few CTAs)
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t chunks = (n + 31u) / 32u, per_pass = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t c = blockIdx.x + warp * gridDim.x; c < chunks; c += per_pass) {
+        const uint32_t k = c * 32u + lane;
+        if (k < n) inplace_scatter(pl, list, 0u, k, cs, n_e, n_i, g, dens_e, dens_i);
+    }
     // the last CTA counts the collisions and empties the list for the next
     // step (every CTA read the count before its ticket: no fence needed for
     // that; one per CTA orders its spawns and deposits before the ticket)
