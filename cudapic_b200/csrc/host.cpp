@@ -71,7 +71,7 @@ constexpr cudapic_tuning kDefaultTuning = {
     /*push_stages*/ 2, /*push_ctas_per_sm*/ 4,
     /*mcc_stages*/ 2, /*mcc_ctas_per_sm*/ 4, /*mcc_variant*/ 1,
     /*step_stages*/ 2, /*step_ctas_per_sm*/ 3, /*step_rows*/ 2,
-    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 8, /*inplace_prefetch*/ 1,
+    /*inplace_ctas_per_sm*/ 4, /*inplace_copies*/ 4, /*inplace_prefetch*/ 1,
     /*scatter_ctas_per_sm*/ 4};
 std::mutex g_tune_mu;
 cudapic_tuning g_tuning = kDefaultTuning;
