@@ -17,7 +17,8 @@
 //    shared memory and, 32 at a time, to the collider list (one atomicAdd
 //    per 32 records, coalesced stores): eight planes of the other sides of
 //    both species, which an in-place electron step does not otherwise use,
-//    so the list holds one record for every slot.  The pass also makes the
+//    so the list holds one record for every slot (slots < 2^31: bit 31 of
+//    the slot word marks an ionization).  The pass also makes the
 //    scattering's event draw (the process entries are fetched with the
 //    test's total) so that it knows how many draws the scattering takes (7
 //    for an ionization, else 3) and writes every slot's final RNG state in
@@ -282,7 +283,7 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
                 const unsigned cm = __ballot_sync(0xffffffffu, c);
                 if (c) {
                     const uint32_t pos = qn + __popc(cm & lt);
-                    sm.r(0, warp, pos) = s0 + (uint32_t)u;
+                    sm.r(0, warp, pos) = (s0 + (uint32_t)u) | (ioniz >> u & 1u) << 31;  // bit 31: ionization
                     sm.r(1, warp, pos) = __float_as_uint(vx[u]);
                     sm.r(2, warp, pos) = __float_as_uint(vy[u]);
                     sm.r(3, warp, pos) = __float_as_uint(vz[u]);
@@ -340,11 +341,12 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
 __device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const CollList &list, uint32_t off,
                                                 uint32_t k, const float *cs, uint32_t *n_e, uint32_t *n_i,
                                                 const cudapic_grid &g, float *dens_e, float *dens_i) {
-    const uint32_t i = list.slot[off + k];
+    const uint32_t w = list.slot[off + k];
+    const uint32_t i = w & 0x7fffffffu;  // bit 31: the stream pass's event draw said ionization
     const float vxi = list.vx[off + k], vyi = list.vy[off + k], vzi = list.vz[off + k];
     const uint32_t j = off + i;
     Xoshiro128p rs{list.r0[off + k], list.r1[off + k], list.r2[off + k], list.r3[off + k]};
-    const float xi = pl.x[j];  // an ionization's birthplace, fetched beside the table lookups
+    const float xi = (w >> 31) ? pl.x[j] : 0.0f;  // an ionization's birthplace, fetched beside the table lookups
     const float v2 = vxi * vxi + vyi * vyi + vzi * vzi;
     const uint32_t idx = energy_index(g.half_me_over_e * v2);
     collide_electron_body<true, true>(off, i, idx, vxi, vyi, vzi, rs, cs, pl.x, pl.vx, pl.vy, pl.vz, pl.ix, pl.ivx,

@@ -172,6 +172,8 @@ int launch_electron_inplace(const InplacePlanes &pl, const float *efield, const 
                             float sigma_max, const uint32_t *n_active, const CollList &list, uint32_t *count,
                             float *dens_e, const cudapic_grid &g, cudaStream_t stream, cudapic_wall_counters *wall,
                             uint32_t *spawn_from) {
+    if (g.capacity > 0x80000000u)  // a record's slot word keeps bit 31 for the event
+        return fail(CUDAPIC_ERR_ARG, "step_electrons_inplace: capacity above 2^31");
     const cudapic_tuning t = tuning();
     const uint32_t ef_pad = (g.n_g + 3u) & ~3u;
     int copies = t.inplace_copies < 0 ? 0 : std::max(1, std::min(t.inplace_copies, IP_WARPS));  // 0: f32

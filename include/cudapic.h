@@ -258,8 +258,9 @@ int cudapic_step_electrons(const float *efield, const float *src_x, const float 
  *    x = -1 (CUDAPIC_DEAD_X): later in-place steps skip such slots, and
  *    cudapic_step_electrons drops them while compacting.  Each collider is
  *    recorded in the eight planes coll[0..7] (capacity entries each: slot,
- *    vx, vy, vz, then the four words of its RNG state past the test draw)
- *    and counted in *n_colliders (zero on entry); the RNG state written to
+ *    with bit 31 set for an ionization, vx, vy, vz, then the four words of
+ *    its RNG state past the test draw; capacity at most 2^31) and counted
+ *    in *n_colliders (zero on entry); the RNG state written to
  *    a collider's slot is already the one past all of its scattering's
  *    draws (the event draw, made here from cs, tells how many).  *n_e is
  *    unchanged.
