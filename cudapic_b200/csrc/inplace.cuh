@@ -303,8 +303,15 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
         for (int u = 0; u < IP_ROW; ++u) {
             if (coll >> u & 1u) {
                 Xoshiro128p rs{s[0][u], s[1][u], s[2][u], s[3][u]};
-                const int draws = (ioniz >> u & 1u) ? 7 : 3;
-                for (int k = 0; k < draws; ++k) rs.next();
+                rs.next();  // the event draw
+                rs.next();
+                rs.next();
+                if (ioniz >> u & 1u) {  // an ionization's four more
+                    rs.next();
+                    rs.next();
+                    rs.next();
+                    rs.next();
+                }
                 s[0][u] = rs.s0;
                 s[1][u] = rs.s1;
                 s[2][u] = rs.s2;
