@@ -9,7 +9,7 @@
 // fused step (kernels_step.cu) does it, but with every electron kept in its
 // slot: no compaction, 56 B of HBM traffic per electron (x, v, RNG read;
 // x, vx, RNG written) against 64 B, plus the colliders' records and their
-// scattered velocities and RNG states.
+// scattered velocities.
 #include <algorithm>
 #include <type_traits>
 
