@@ -342,7 +342,7 @@ __device__ __forceinline__ void inplace_segment(const InplacePlanes &pl, const S
 // RNG state (the slot's final state is already written by the stream pass)
 // continues past the test draw
 // (collision_e, Rust-CUDA/src/main.rs:1035-1165, with the fused step's
-// algebraic sines and cosines); velocity and RNG state go back to the slot,
+// algebraic sines and cosines); the velocity goes back to the slot,
 // a spawned electron takes the next slot of n_e, a spawned ion the next slot
 // of n_i.
 __device__ __forceinline__ void inplace_scatter(const InplacePlanes &pl, const CollList &list, uint32_t off,
