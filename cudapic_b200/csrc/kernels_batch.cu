@@ -294,10 +294,7 @@ __global__ void __launch_bounds__(IP_THREADS)
     };
     plan_prefix(count, D, P, wsum);  // the counts do not change until the last CTA has its ticket
     // the batch's records in chunks of 32, chunk c to CTA c mod gridDim (no
-    // block barrier per discharge); each lane finds its discharge in the plan.
-    // The plan rounds every count up to a multiple of 4: an index past the
-    // discharge's own count (at most 3 per discharge) is skipped, its record
-    // slot holds nothing of this step.
+    // block barrier per discharge); each lane finds its discharge in the plan
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t total = P[D];
     const uint32_t chunks = (total + 31u) / 32u, per_pass = gridDim.x * (blockDim.x >> 5);
@@ -310,12 +307,9 @@ __global__ void __launch_bounds__(IP_THREADS)
                 if (P[mid] <= k) lo = mid;
                 else hi = mid;
             }
-            const uint32_t kd = k - P[lo];
-            if (kd < count(lo)) {
-                const BatchDisc &dd = desc[lo];
-                inplace_scatter(pl, list, dd.off, kd, dd.cs, dd.counters + 0, dd.counters + 1, dd.g,
-                                dd.e_dens[dens_role], dd.i_dens[dens_i_role]);
-            }
+            const BatchDisc &dd = desc[lo];
+            inplace_scatter(pl, list, dd.off, k - P[lo], dd.cs, dd.counters + 0, dd.counters + 1, dd.g,
+                            dd.e_dens[dens_role], dd.i_dens[dens_i_role]);
         }
     }
     __syncthreads();
