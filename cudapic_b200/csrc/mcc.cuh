@@ -79,7 +79,10 @@ __device__ __forceinline__ void rotate(float g, float sc, float cc, float se, fl
 }
 
 // Claims one slot of `counter` for every lane of the calling coalesced
-// group with a single atomicAdd; never hands out a slot >= capacity.
+// group with a single atomicAdd; never hands out a slot >= capacity.  The
+// group's leader claims for every lane: all lanes that reach it together
+// must pass the same counter (the kernels keep a warp within one
+// discharge while it scatters).
 __device__ __forceinline__ bool claim_slot(uint32_t *counter, uint32_t capacity, uint32_t &slot) {
     cg::coalesced_group grp = cg::coalesced_threads();
     uint32_t base = 0, granted = 0;
