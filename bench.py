@@ -650,7 +650,8 @@ STATED_ERROR = {"kernels": "RNG, push/compaction, collisions bit-exact with the 
                               "quantity within 1 standard error; FP64 twin and reference f32 launch sequence the same",
                 "precision": "1000 RF cycles at ~2e5 particles per species: every cycle-averaged profile of the "
                              "mixed path within 0.3 % relative L2 of the all-FP64 GPU twin (seed spread "
-                             "0.3-0.9 %); <j E> power 0.29 %"}
+                             "0.3-0.9 %); <j E> power 0.29 %; from the same starts at that size, mixed, FP64 twin and "
+                             "reference arithmetic within 0.1-0.6 % of eduPIC after 300 + 100 cycles"}
 
 
 # ---------------------------------------------------------------- GPU arm: the batched sweep (c2)
