@@ -107,25 +107,30 @@ def test_adjoint_against_central_difference(cudapic, cuda_device):
     """The reference-case discharge with 2e5 electrons, relaxed one RF cycle
     (by the fused driver, whose compaction order varies from run to run, so
     the start differs between runs); a 200-step window: the pathwise adjoint
-    against central differences at dV0 = 0.5 V with common random numbers.
+    against central differences with common random numbers.
     Measured over four starts: ion flux 0.4 - 4.5 % apart; electron power
     adjoint / difference 0.58 - 0.78, because the pathwise derivative omits
     what the difference also contains, the electrons whose collision
     decision or absorption at an electrode flips between V0 - dV and
-    V0 + dV (the frozen events).  Asserted: the flux within 10 %, the power's
-    sign and a factor 2.5.  The exact checks of the adjoint are the oracle's
-    (central differences at 1 mV, 1e-4) and the GPU against the oracle."""
+    V0 + dV (the frozen events).  Such a flip can throw a single difference
+    far off on an unlucky start (one start gave -3.1e15 for the flux at
+    dV0 = 0.5 V against an adjoint of 1.9e14), and it depends on dV0: the
+    difference taken is the median of those at dV0 = 0.5, 0.25 and 0.1 V.
+    Asserted: the flux within 10 %, the power's sign and a factor 2.5.  The
+    exact checks of the adjoint are the oracle's (central differences at
+    1 mV, 1e-4) and the GPU against the oracle."""
     from cudapic_b200.sensitivity import VoltageSensitivity, steady_state
     st = steady_state(200_000, relax_cycles=1)
     try:
         with VoltageSensitivity(st, 200, 200) as s:
             s.forward(V0)
             g = s.backward()
-            fd = s.central_difference(V0, 0.5)
+            fds = [s.central_difference(V0, dv) for dv in (0.5, 0.25, 0.1)]
             assert s.info()["device_error"] == 0
     finally:
         st.close()
-    print("\nadjoint %s\ncentral difference %s" % (g, fd))
+    fd = {k: float(np.median([f[k] for f in fds])) for k in g}
+    print("\nadjoint %s\ncentral differences %s\nmedian %s" % (g, fds, fd))
     assert g["ion_flux_gnd"] == pytest.approx(fd["ion_flux_gnd"], rel=0.10)
     ratio = g["power_e"] / fd["power_e"]
     assert 0.4 < ratio < 2.5, ratio
