@@ -287,37 +287,36 @@ __global__ void __launch_bounds__(IP_THREADS)
     extern __shared__ __align__(16) uint32_t sc_smem[];
     uint32_t *P = sc_smem;  // [D + 1]
     __shared__ uint32_t wsum[ES_WARPS];
-    __shared__ cudapic_grid s_g;
-    __shared__ const float *s_cs;
-    __shared__ uint32_t *s_ctr;
-    __shared__ float *s_de, *s_di;
-    __shared__ uint32_t s_off;
     grid_dep_wait();
     auto count = [&](uint32_t d) {
         const BatchDisc &dd = desc[d];
         return min(*(volatile uint32_t *)(dd.counters + CTR_COLL_COUNT), dd.g.capacity);
     };
-    plan_prefix(count, D, P, wsum);
-    uint32_t chunk, beg, end;
-    cta_share(P[D], chunk, beg, end);
-    for (uint32_t d = first_discharge(P, D, beg); d < D && P[d] < end; ++d) {
-        const uint32_t n = count(d);  // unchanged until the last CTA has taken its ticket
-        const uint32_t lo = max(beg, P[d]) - P[d];
-        const uint32_t hi = min(end, P[d] + n) - P[d];
-        if (lo >= hi) continue;
-        if (threadIdx.x == 0) {
-            const BatchDisc &dd = desc[d];
-            s_g = dd.g;
-            s_cs = dd.cs;
-            s_ctr = dd.counters;
-            s_de = dd.e_dens[dens_role];
-            s_di = dd.i_dens[dens_i_role];
-            s_off = dd.off;
+    plan_prefix(count, D, P, wsum);  // the counts do not change until the last CTA has its ticket
+    // the batch's records in chunks of 32, chunk c to CTA c mod gridDim (no
+    // block barrier per discharge); each lane finds its discharge in the plan.
+    // The plan rounds every count up to a multiple of 4: an index past the
+    // discharge's own count (at most 3 per discharge) is skipped, its record
+    // slot holds nothing of this step.
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t total = P[D];
+    const uint32_t chunks = (total + 31u) / 32u, per_pass = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t c = blockIdx.x + warp * gridDim.x; c < chunks; c += per_pass) {
+        const uint32_t k = c * 32u + lane;
+        if (k < total) {
+            uint32_t lo = 0, hi = D;  // the last d with P[d] <= k: P[d] <= k < P[d + 1]
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (P[mid] <= k) lo = mid;
+                else hi = mid;
+            }
+            const uint32_t kd = k - P[lo];
+            if (kd < count(lo)) {
+                const BatchDisc &dd = desc[lo];
+                inplace_scatter(pl, list, dd.off, kd, dd.cs, dd.counters + 0, dd.counters + 1, dd.g,
+                                dd.e_dens[dens_role], dd.i_dens[dens_i_role]);
+            }
         }
-        __syncthreads();
-        for (uint32_t k = lo + threadIdx.x; k < hi; k += IP_THREADS)
-            inplace_scatter(pl, list, s_off, k, s_cs, s_ctr + 0, s_ctr + 1, s_g, s_de, s_di);
-        __syncthreads();  // the segment's shared words are rewritten for the next one
     }
     __syncthreads();
     if (threadIdx.x == 0) {

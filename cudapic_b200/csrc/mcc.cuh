@@ -78,25 +78,28 @@ __device__ __forceinline__ void rotate(float g, float sc, float cc, float se, fl
     gz = g * (a.st * a.sp * cc + a.ct * a.sp * sc * ce + a.cp * sc * se);
 }
 
-// Claims one slot of `counter` for every lane of the calling coalesced
-// group with a single atomicAdd; never hands out a slot >= capacity.  The
-// group's leader claims for every lane: all lanes that reach it together
-// must pass the same counter (the kernels keep a warp within one
-// discharge while it scatters).
+// Claims one slot of `counter` for every lane that reaches it together
+// with the same counter, one atomicAdd per such group (lanes of a warp that
+// scatter for different discharges of a batch form separate groups; within
+// a group, lanes take consecutive slots in lane order); never hands out a
+// slot >= capacity (the same capacity for every lane of a group).
 __device__ __forceinline__ bool claim_slot(uint32_t *counter, uint32_t capacity, uint32_t &slot) {
-    cg::coalesced_group grp = cg::coalesced_threads();
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(counter));
+    const int leader = __ffs(peers) - 1;
+    const uint32_t rank = __popc(peers & lanemask_lt());
     uint32_t base = 0, granted = 0;
-    if (grp.thread_rank() == 0) {
-        const uint32_t cnt = grp.size();
+    if ((int)(threadIdx.x & 31u) == leader) {
+        const uint32_t cnt = __popc(peers);
         const uint32_t old = atomicAdd(counter, cnt);
         granted = old >= capacity ? 0u : min(cnt, capacity - old);
         if (granted < cnt) atomicSub(counter, cnt - granted);
         base = old;
     }
-    base = grp.shfl(base, 0);
-    granted = grp.shfl(granted, 0);
-    slot = base + grp.thread_rank();
-    return grp.thread_rank() < granted;
+    base = __shfl_sync(peers, base, leader);
+    granted = __shfl_sync(peers, granted, leader);
+    slot = base + rank;
+    return rank < granted;
 }
 
 // Collision decision u < p with p = 1 - exp(-a), a = nu dt (the reference
