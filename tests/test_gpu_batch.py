@@ -247,3 +247,47 @@ def test_batch_class_steps_every_discharge(cudapic, cuda_device):
             assert 0 < e1 < 2 * s.particles and 0 < i1 < 2 * s.particles
         assert 120 * min(e for e, _ in n1) <= w
         assert [st.steps_done() for st in b.states] == [120] * len(specs)
+
+
+def test_batch_spawns_stay_with_their_discharge(cudapic, cuda_device):
+    """Strongly ionizing discharges of ragged sizes in one batch, so that
+    warps of the batched scatter pass straddle two discharges while both
+    ionize: over 38 in-place steps (two compacting ones) every discharge's
+    electron and ion counts stay with the same discharge run alone (each
+    spawn claims a slot of its own discharge's counter), and no capacity
+    is exceeded."""
+    import cudapic_b200 as cp
+    from cudapic_b200.sim import GpuBatch, GpuSimState, ParticlesSoA
+    from cudapic_b200.workloads import steady_state
+    sizes = [1203, 2999, 517, 4001, 1777, 3333, 901, 2500]
+
+    def make(k, n):
+        params = cp.default_params(voltage=480.0, pressure=40.0, gap=0.025, n_g=400, capacity=16384,
+                                   weight=7.0e4)
+        st = GpuSimState(params)
+        g = st.grid
+        st.upload_electrons(ParticlesSoA(*steady_state(n, E_MASS, 20.0, gap=0.025, dt=g.dt_e, seed=300 + k)))
+        st.upload_ions(ParticlesSoA(*steady_state(n, AR_MASS, 0.03, gap=0.025, dt=g.dt_i, seed=400 + k)))
+        st.seed(e_master=(0x5151 + k, 0x11112222, 0x22223333, 0x33334444),
+                i_master=(0x6161 + k, 0x55556666, 0x66667777, 0x77778888))
+        return st
+
+    together = [make(k, n) for k, n in enumerate(sizes)]
+    alone = [make(k, n) for k, n in enumerate(sizes)]
+    try:
+        with GpuBatch(together) as b:
+            b.run_steps(40)
+            b.synchronize()
+        for st in alone:
+            st.run_steps(40)
+        grew = 0
+        for k, (x, y) in enumerate(zip(together, alone)):
+            assert x.device_error() == 0 and y.device_error() == 0, k
+            (ex, ix), (ey, iy) = x.counts(), y.counts()
+            grew += ix > sizes[k] + 20  # ions: spawned by ionizations, barely absorbed in two ion steps
+            assert abs(ex - ey) <= 0.05 * ey + 20, (k, ex, ey)
+            assert abs(ix - iy) <= 0.05 * iy + 20, (k, ix, iy)
+        assert grew == len(sizes)  # every discharge ionizes
+    finally:
+        for st in together + alone:
+            st.close()
