@@ -306,8 +306,9 @@ def cpu_reference(args):
 
 
 def edupic_c0():
-    """configs[0] on the reference CPU program: the initialising cycle
-    (eduPIC 0), then C0_CYCLES RF cycles (eduPIC 10) timed from its marks (set-up excluded)."""
+    """The plain eduPIC case (1000 + 1000 particles at rest) on the reference
+    CPU program: the initialising cycle (eduPIC 0), then C0_CYCLES RF cycles
+    (eduPIC 10) timed from its marks (set-up excluded)."""
     import shutil
     import tempfile
     from oracle import edupic_runner as R
